@@ -1,0 +1,269 @@
+/*
+ * nektar_b200.h -- C ABI of the B200 (sm_100a) matrix-free spectral/hp
+ * element path: sum-factorised BwdTrans / IProductWRTBase / PhysDeriv /
+ * Helmholtz operators for Hex, Prism and Tet collections, the C0 local <->
+ * global assembly map, and the Jacobi-preconditioned conjugate-gradient solve
+ * of GlobalLinSysIterativeFull.
+ *
+ * Plain C: pointers, sizes and int status codes; no exceptions and no torch
+ * types cross this boundary. Every call returns NKB_OK (0) or a negative
+ * status; nkb_last_error() gives a message for the calling thread.
+ *
+ * Numbering of shapes, operators, points and basis types is that of the
+ * reference (LibUtilities::ShapeType, Collections::OperatorType,
+ * LibUtilities::PointsType, LibUtilities::BasisType) so that an adaptor can
+ * pass the reference's enums through unchanged.
+ *
+ * Array layouts are those of the reference's Collections layer:
+ *   - per-element data contiguous and element-major: coefficients
+ *     in[e*ncoeffs + m], physical values phys[e*nqtot + q], q = (k*nq1+j)*nq0+i;
+ *   - coefficient order: Hex p fastest then q then r; Prism / Tet r fastest
+ *     inside (p, q) with the triangular truncation of the Modified_B/C bases;
+ *   - jac: CoalescedGeomData::GetJac (nelmt*nqtot deformed, nelmt regular);
+ *   - df : CoalescedGeomData::GetDerivFactors, 9 rows of ncol (= nelmt*nqtot
+ *          deformed, nelmt regular) values; row k*3+j holds d xi_j / d x_k;
+ *   - bdata/dbdata: Basis::GetBdata / GetDbdata; w: Points weights (raw, the
+ *     Radau factors of MatrixFree SetUpZW are applied inside); D: column-major
+ *     collocation derivative D[k*nq+i] = d l_k/dz(z_i) (Points::GetD()).
+ */
+#ifndef NEKTAR_B200_H
+#define NEKTAR_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define NKB_OK 0
+#define NKB_ERR_INVALID -1     /* bad argument (NULL, size, unsupported combo) */
+#define NKB_ERR_UNSUPPORTED -2 /* valid request this build does not implement */
+#define NKB_ERR_CUDA -3        /* a CUDA runtime call failed */
+#define NKB_ERR_NOMEM -4       /* device or host allocation failed */
+#define NKB_ERR_NOT_CONVERGED -5 /* CG reached maxit (reference: warning + return) */
+#define NKB_ERR_NONFINITE -6   /* NaN/Inf detected in a CG scalar */
+#define NKB_ERR_NO_DEVICE -7   /* no CUDA device visible */
+
+/* ---- enums (reference numbering) ---------------------------------------- */
+#define NKB_TET 5   /* LibUtilities::eTetrahedron */
+#define NKB_PRISM 7 /* LibUtilities::ePrism */
+#define NKB_HEX 8   /* LibUtilities::eHexahedron */
+
+#define NKB_BWDTRANS 0  /* Collections::eBwdTrans */
+#define NKB_HELMHOLTZ 1 /* Collections::eHelmholtz */
+#define NKB_IPRODUCT 3  /* Collections::eIProductWRTBase */
+#define NKB_PHYSDERIV 5 /* Collections::ePhysDeriv */
+
+#define NKB_GLL 4       /* LibUtilities::eGaussLobattoLegendre */
+#define NKB_RADAU_A1 11 /* LibUtilities::eGaussRadauMAlpha1Beta0 */
+#define NKB_RADAU_A2 12 /* LibUtilities::eGaussRadauMAlpha2Beta0 */
+
+#define NKB_MODIFIED_A 4 /* LibUtilities::eModified_A */
+#define NKB_MODIFIED_B 5 /* LibUtilities::eModified_B */
+#define NKB_MODIFIED_C 6 /* LibUtilities::eModified_C */
+
+/* arithmetic of an operator */
+#define NKB_FP64 0
+#define NKB_FP32 1
+
+/* nkb_op_apply / nkb_cg_solve flags */
+#define NKB_DEVICE_PTRS 0 /* arrays are device pointers; call is stream-ordered */
+#define NKB_HOST_PTRS 1   /* arrays are host pointers; copies in/out, synchronous */
+
+/* Helmholtz diffusion modes (Collections::Helmholtz_MatrixFree::UpdateFactors) */
+#define NKB_DIFF_NONE 0  /* identity diffusion */
+#define NKB_DIFF_CONST 1 /* eFactorCoeffD00..D22: constant anisotropic tensor */
+#define NKB_DIFF_VAR 2   /* eFactorTau: per-point tensor (SetVarDiffusion) */
+
+/* ---- library ------------------------------------------------------------ */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *nkb_last_error(void);
+
+/* Build string (version, sm arch, CUDA runtime). */
+const char *nkb_version(void);
+
+/* ---- 1-D setup tables (FP64, host) ---------------------------------------
+ * Replace what the reference gets from LibUtilities::PointsManager and
+ * BasisManager (GaussPoints.cpp:79-240, Basis.cpp:466-644). Provided for
+ * callers that do not run the reference's Foundations library. */
+
+/* z, w (raw weights) and D (column-major, D[k*np+i] = l_k'(z_i)) of a points
+ * type: NKB_GLL, NKB_RADAU_A1, NKB_RADAU_A2. */
+int nkb_points(int ptype, int np, double *z, double *w, double *D);
+
+/* bdata / dbdata of a modified basis (NKB_MODIFIED_A/B/C) with nm modes at
+ * the np points z with derivative matrix D. Returns the number of tabulated
+ * modes (nm, nm(nm+1)/2, nm(nm+1)(nm+2)/6) or a negative status. */
+int nkb_basis(int btype, int nm, int np, const double *z, const double *D, double *bdata,
+              double *dbdata);
+
+/* ---- element operators ---------------------------------------------------
+ * One operator = one reference Collection of nelmt elements of the same
+ * shape, basis and geometry type, i.e. one Collections::Operator instance:
+ *   Collections::Operator (Collections/Operator.h:137-245), constructed
+ *   through OPERATOR_CREATE / GetOperatorFactory (Operator.h:43-54,118-129),
+ *   implemented by Helmholtz_MatrixFree (Collections/Helmholtz.cpp:586-761),
+ *   BwdTrans_MatrixFree (BwdTrans.cpp:160-243), IProductWRTBase_MatrixFree
+ *   (IProductWRTBase.cpp:182-268), PhysDeriv_MatrixFree (PhysDeriv.cpp:272-).
+ */
+typedef struct nkb_op nkb_op;
+
+typedef struct nkb_op_desc
+{
+    int shape;    /* NKB_HEX / NKB_PRISM / NKB_TET */
+    int optype;   /* NKB_BWDTRANS / NKB_HELMHOLTZ / NKB_IPRODUCT / NKB_PHYSDERIV */
+    int nm;       /* modes per direction (equal in all directions) */
+    int nq[3];    /* points per direction (Tet: nq0, nq0-1, nq0-1; Prism: nq0, nq0, nq0-1) */
+    int ptype[3]; /* points type per direction */
+    int nelmt;    /* elements in the collection */
+    int deformed; /* 1: geometry per quadrature point (eDeformed), 0: per element */
+    /* host arrays, reference layouts (see top of file); NULL where the
+     * operator does not need them: BwdTrans needs bdata; IProduct bdata, w, jac;
+     * PhysDeriv z, D, df; Helmholtz bdata, w, z, D, jac, df. */
+    const double *bdata[3];
+    const double *w[3];
+    const double *z[3];
+    const double *D[3];
+    const double *jac;
+    const double *df;
+    int precision; /* NKB_FP64 or NKB_FP32 (FP32 storage and arithmetic) */
+    int device;    /* CUDA device ordinal */
+} nkb_op_desc;
+
+/* Replaces OPERATOR_CREATE(...)::create + the MatrixFree constructors
+ * (Helmholtz.cpp:713-760 etc.): uploads tables, packs the geometry. */
+int nkb_op_create(const nkb_op_desc *desc, nkb_op **op);
+
+/* Replaces Helmholtz_MatrixFree::UpdateFactors (Helmholtz.cpp:615-691):
+ * lambda (eFactorLambda); diff_mode NKB_DIFF_CONST with diff =
+ * (d00 d01 d11 d02 d12 d22) from eFactorCoeffD00..D22; NKB_DIFF_VAR fills the
+ * per-point tensor with diff as SetVarDiffusion does under eFactorTau. */
+int nkb_op_set_factors(nkb_op *op, double lambda, int diff_mode, const double *diff);
+
+/* Replaces Collections::Operator::operator()(in, out0, out1, out2, wsp)
+ * (Operator.h:148-152): out0 is overwritten (no accumulate); PhysDeriv
+ * writes d/dx, d/dy, d/dz to out0, out1, out2. flags: NKB_HOST_PTRS or
+ * NKB_DEVICE_PTRS; stream: a cudaStream_t (NULL = legacy default). With
+ * host pointers the result is in out0.. on return, as the reference's is. */
+int nkb_op_apply(nkb_op *op, const double *in, double *out0, double *out1, double *out2,
+                 int flags, void *stream);
+
+/* FP32 variant of nkb_op_apply for NKB_FP32 operators (device pointers). */
+int nkb_op_apply_f32(nkb_op *op, const float *in, float *out0, float *out1, float *out2,
+                     void *stream);
+
+/* GetInputSize / GetOutputSize (Operator.h:178-226), per output array. */
+int nkb_op_sizes(const nkb_op *op, long *in_size, long *out_size);
+
+/* Diagonal of every element's Helmholtz matrix (nelmt*ncoeffs values, host
+ * or device per flags), computed matrix-free on the device. The reference
+ * builds it from dense element matrices (PreconditionerDiagonal.cpp:93-125). */
+int nkb_op_helmholtz_diag(nkb_op *op, double *diag, int flags, void *stream);
+
+/* Time in ms of the last nkb_op_apply's kernel on the device (CUDA events). */
+int nkb_op_last_kernel_ms(const nkb_op *op, float *ms);
+
+void nkb_op_destroy(nkb_op *op);
+
+/* ---- global system + CG --------------------------------------------------
+ * One nkb_sys = GlobalLinSysIterativeFull with PreconditionerDiagonal over
+ * an AssemblyMapCG (MultiRegions/GlobalLinSysIterativeFull.cpp:96-384,
+ * PreconditionerDiagonal.cpp:93-189, AssemblyMap/AssemblyMapCG.cpp:2772-2906)
+ * driving NekLinSysIterCG (LinearAlgebra/NekLinSysIterCG.cpp:118-372). */
+typedef struct nkb_sys nkb_sys;
+
+typedef struct nkb_sys_desc
+{
+    int nops;             /* Helmholtz operators (collections), in local-space order */
+    nkb_op *const *ops;   /* FP64 Helmholtz operators */
+    nkb_op *const *ops32; /* optional FP32 twins for mixed precision (or NULL) */
+    long nloc;            /* local coefficients = sum of nelmt*ncoeffs */
+    int nglob;            /* global coefficients, Dirichlet ones first */
+    int ndir;             /* Dirichlet global coefficients */
+    const int *map;       /* host, nloc: local -> global (GetLocalToGlobalMap) */
+    const double *sign;   /* host, nloc, or NULL when no sign change */
+    int device;
+} nkb_sys_desc;
+
+typedef struct nkb_cg_opts
+{
+    double tol;         /* IterativeSolverTolerance (relative, default 1e-9) */
+    int maxit;          /* NekLinSysMaxIterations (default 5000) */
+    int check_interval; /* host convergence poll every k iterations (device
+                           kernels stop updating once converged) */
+    int use_graph;      /* capture the k-iteration block in a CUDA graph */
+    int mixed;          /* 0: FP64 CG; 1: FP64 iterative refinement around
+                           an FP32 CG (needs ops32) */
+    double inner_tol;   /* mixed: relative residual reduction per inner solve */
+    int max_outer;      /* mixed: maximum refinement steps */
+} nkb_cg_opts;
+
+typedef struct nkb_cg_report
+{
+    int iterations;       /* CG iterations (total inner for mixed) */
+    int outer_iterations; /* mixed: refinement steps */
+    double rel_residual;  /* sqrt(eps / rhs_magnitude) as NekLinSysIterCG reports */
+    int converged;
+    double device_ms;     /* device time of the solve (CUDA events) */
+} nkb_cg_report;
+
+int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **sys);
+
+/* GlobalLinSysIterativeFull::v_Solve with Dirichlet lifting: b_loc is the
+ * local right-hand side (pLocInput), x_loc on input holds the Dirichlet
+ * values in local layout (ContField::v_ImposeDirichletConditions) and zeros
+ * elsewhere, on output the solution (pLocOutput). flags as nkb_op_apply. */
+int nkb_cg_solve(nkb_sys *sys, const double *b_loc, double *x_loc, const nkb_cg_opts *opts,
+                 nkb_cg_report *report, int flags, void *stream);
+
+/* AssemblyMapCG::Assemble / GlobalToLocal on device arrays. */
+int nkb_sys_assemble(nkb_sys *sys, const double *loc, double *glob, void *stream);
+int nkb_sys_global_to_local(nkb_sys *sys, const double *glob, double *loc, void *stream);
+
+/* Local-space matvec y = A x (GeneralMatrixOp over all collections). */
+int nkb_sys_matvec_local(nkb_sys *sys, const double *x_loc, double *y_loc, void *stream);
+
+/* Inverse assembled diagonal (nglob - ndir entries) the preconditioner uses. */
+int nkb_sys_diag_inv(nkb_sys *sys, double *diag_inv, int flags, void *stream);
+
+void nkb_sys_destroy(nkb_sys *sys);
+
+/* ---- structured test meshes (FP64 setup, host) ---------------------------
+ * Unit-cube box of n^3 cells, optionally curved by
+ *   x' = x + amp * sin(pi x) sin(pi y) sin(pi z) in every coordinate,
+ * with geometric factors from the analytic Jacobian at the quadrature points
+ * of the given tables (no isoparametric interpolation). Cells are hexes, or
+ * split into 2 prisms or 6 tets. Used by tests and benchmarks; a Nektar++
+ * caller passes its own GeomFactors through nkb_op_desc instead. */
+typedef struct nkb_geom_request
+{
+    int shape;        /* NKB_HEX / NKB_PRISM / NKB_TET */
+    int n;            /* cells per direction */
+    double amp;       /* curvature amplitude (0 = affine) */
+    int ncells;       /* number of cells to use (<= n^3), or 0 for all */
+    const int *cells; /* optional list of cell ids (x fastest) of length ncells */
+    int nq[3];
+    const double *z[3]; /* quadrature points per direction (collapsed for Tet/Prism) */
+    int deformed;       /* 1: per-point factors, 0: one value per element */
+} nkb_geom_request;
+
+/* Number of elements the request produces. */
+long nkb_geom_nelmt(const nkb_geom_request *req);
+
+/* Fill jac (nelmt*nqtot or nelmt) and df (9 rows of ncol) and, if xyz is not
+ * NULL, the physical coordinates of every quadrature point (3 rows of
+ * nelmt*nqtot). */
+int nkb_geom_fill(const nkb_geom_request *req, double *jac, double *df, double *xyz);
+
+/* C0 assembly map for a hex box of n^3 elements with nm modes per direction
+ * (Modified_A): boundary (Dirichlet) coefficients numbered first, as
+ * AssemblyMapCG orders them. map has n^3*nm^3 entries; all signs are +1 for
+ * this consistently oriented mesh. Returns nglob via *nglob and ndir. */
+int nkb_hex_box_assembly(int n, int nm, int *map, int *nglob, int *ndir);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NEKTAR_B200_H */

@@ -1,0 +1,285 @@
+"""nektar_b200: B200 (sm_100a) matrix-free spectral/hp element operators,
+C0 assembly and Jacobi-preconditioned CG, behind the C ABI of
+include/nektar_b200.h.
+
+Python mirror of the reference's Collections operator interface
+(Collections/Operator.h:137-245): an `Operator` is one collection of
+same-shape elements; `GlobalLinSys` is GlobalLinSysIterativeFull with the
+diagonal preconditioner. Arrays are numpy (host; copied in and out, the call
+is synchronous like the reference's) or device pointers (torch tensors'
+data_ptr(), stream ordered).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi as C
+from ._capi import (BWDTRANS, DEVICE_PTRS, DIFF_CONST, DIFF_NONE, DIFF_VAR, FP32, FP64, GLL,
+                    HELMHOLTZ, HEX, HOST_PTRS, IPRODUCT, MODIFIED_A, MODIFIED_B, MODIFIED_C,
+                    PHYSDERIV, PRISM, RADAU_A1, RADAU_A2, TET, NektarB200Error, check)
+
+SHAPES = {"hex": HEX, "prism": PRISM, "tet": TET}
+OPTYPES = {"bwdtrans": BWDTRANS, "helmholtz": HELMHOLTZ, "iproduct": IPRODUCT,
+           "physderiv": PHYSDERIV}
+WEIGHT_FACTOR = {GLL: 1.0, RADAU_A1: 0.5, RADAU_A2: 0.25}
+
+__all__ = ["Operator", "GlobalLinSys", "BoxMesh", "points", "basis", "shape_tables", "lib",
+           "NektarB200Error", "SHAPES", "OPTYPES"]
+
+
+def lib():
+    return C.lib()
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(C.dp)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def points(ptype, n):
+    """z, raw weights w and column-major D of a points type (GaussPoints)."""
+    z, w, D = np.zeros(n), np.zeros(n), np.zeros(n * n)
+    check(lib().nkb_points(ptype, n, _dp(z), _dp(w), _dp(D)))
+    return z, w, D
+
+
+def basis(btype, nm, z, D):
+    """bdata, dbdata of a modified basis (Basis::GenBasis layout)."""
+    n = len(z)
+    nb = {MODIFIED_A: nm, MODIFIED_B: nm * (nm + 1) // 2,
+          MODIFIED_C: nm * (nm + 1) * (nm + 2) // 6}[btype]
+    b, db = np.zeros(nb * n), np.zeros(nb * n)
+    rc = lib().nkb_basis(btype, nm, n, _dp(_f64(z)), _dp(_f64(D)), _dp(b), _dp(db))
+    if rc < 0:
+        check(rc)
+    return b, db
+
+
+def shape_spec(shape, nq0):
+    """(basis type, points type, npoints) per direction for a 3-D shape, as
+    Nektar sets them up (SpatialDomains/MeshGraph.cpp:1709-1750): GLL in the
+    Cartesian directions, Gauss-Radau alpha=1 / alpha=2 in collapsed ones."""
+    if shape == "hex":
+        return [(MODIFIED_A, GLL, nq0)] * 3
+    if shape == "prism":
+        return [(MODIFIED_A, GLL, nq0), (MODIFIED_A, GLL, nq0), (MODIFIED_B, RADAU_A1, nq0 - 1)]
+    if shape == "tet":
+        return [(MODIFIED_A, GLL, nq0), (MODIFIED_B, RADAU_A1, nq0 - 1),
+                (MODIFIED_C, RADAU_A2, nq0 - 1)]
+    raise ValueError(shape)
+
+
+def ncoeffs(shape, nm):
+    if shape == "hex":
+        return nm ** 3
+    if shape == "prism":
+        return nm * nm * (nm + 1) // 2
+    return nm * (nm + 1) * (nm + 2) // 6
+
+
+def shape_tables(shape, nm, nq0):
+    """1-D tables of a shape: dict with per-direction lists b, db, w (raw),
+    ws (Radau-scaled, as MatrixFree SetUpZW), z, D, ptype; and nq."""
+    T = {"b": [], "db": [], "w": [], "ws": [], "z": [], "D": [], "ptype": []}
+    nq = []
+    for bt, pt, n in shape_spec(shape, nq0):
+        z, w, D = points(pt, n)
+        b, db = basis(bt, nm, z, D)
+        for k, v in (("b", b), ("db", db), ("w", w), ("ws", w * WEIGHT_FACTOR[pt]), ("z", z),
+                     ("D", D), ("ptype", pt)):
+            T[k].append(v)
+        nq.append(n)
+    return T, tuple(nq)
+
+
+class BoxMesh:
+    """Unit-cube box of n^3 cells (hexes, or 2 prisms / 6 tets per cell),
+    optionally curved by x' = x + amp sin(pi x) sin(pi y) sin(pi z), with
+    analytic geometric factors at the quadrature points (Collections layout)."""
+
+    def __init__(self, shape, n, nm, nq0, amp=0.0, deformed=None, cells=None, coords=False):
+        self.shape, self.n, self.nm, self.amp = shape, n, nm, amp
+        self.deformed = bool(amp != 0.0) if deformed is None else bool(deformed)
+        self.T, self.nq = shape_tables(shape, nm, nq0)
+        self.nt = self.nq[0] * self.nq[1] * self.nq[2]
+        self.nc = ncoeffs(shape, nm)
+        self.cells = None if cells is None else np.ascontiguousarray(cells, dtype=np.int32)
+        req = C.GeomRequest()
+        req.shape, req.n, req.amp = SHAPES[shape], n, amp
+        req.ncells = 0 if self.cells is None else len(self.cells)
+        req.cells = None if self.cells is None else self.cells.ctypes.data_as(C.ip)
+        req.nq = (ctypes.c_int * 3)(*self.nq)
+        self._z = [_f64(z) for z in self.T["z"]]
+        req.z = (C.dp * 3)(*[_dp(z) for z in self._z])
+        req.deformed = int(self.deformed)
+        self.nelmt = int(lib().nkb_geom_nelmt(ctypes.byref(req)))
+        ncol = self.nelmt * self.nt if self.deformed else self.nelmt
+        self.jac = np.zeros(ncol)
+        self.df = np.zeros((9, ncol))
+        self.xyz = np.zeros((3, self.nelmt * self.nt)) if coords else None
+        check(lib().nkb_geom_fill(ctypes.byref(req), _dp(self.jac), _dp(self.df),
+                                  _dp(self.xyz)))
+
+    def assembly(self):
+        """(map, nglob, ndir) of the hex box's C0 numbering, Dirichlet first."""
+        if self.shape != "hex" or self.cells is not None:
+            raise ValueError("assembly maps are built for full hex boxes")
+        gmap = np.zeros(self.nelmt * self.nc, dtype=np.int32)
+        nglob, ndir = ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().nkb_hex_box_assembly(self.n, self.nm, gmap.ctypes.data_as(C.ip),
+                                         ctypes.byref(nglob), ctypes.byref(ndir)))
+        return gmap, nglob.value, ndir.value
+
+
+class Operator:
+    """One collection operator (Collections::Operator) on the device."""
+
+    def __init__(self, optype, mesh=None, *, shape=None, nm=None, nq=None, nelmt=None, T=None,
+                 jac=None, df=None, deformed=None, precision="fp64", device=0):
+        if mesh is not None:
+            shape, nm, nq, nelmt, T = mesh.shape, mesh.nm, mesh.nq, mesh.nelmt, mesh.T
+            jac, df, deformed = mesh.jac, mesh.df, mesh.deformed
+        self.optype = OPTYPES[optype] if isinstance(optype, str) else optype
+        self.shape, self.nm, self.nq, self.nelmt = shape, nm, tuple(nq), nelmt
+        self.precision = FP64 if precision in ("fp64", FP64) else FP32
+        self._keep = []
+        d = C.OpDesc()
+        d.shape, d.optype, d.nm = SHAPES[shape], self.optype, nm
+        d.nq = (ctypes.c_int * 3)(*nq)
+        d.ptype = (ctypes.c_int * 3)(*T["ptype"])
+        d.nelmt, d.deformed = nelmt, int(bool(deformed))
+
+        def arr3(key):
+            arrs = [_f64(a) for a in T[key]]
+            self._keep.extend(arrs)
+            return (C.dp * 3)(*[_dp(a) for a in arrs])
+
+        d.bdata, d.w, d.z, d.D = arr3("b"), arr3("w"), arr3("z"), arr3("D")
+        if jac is not None:
+            jac = _f64(jac)
+            self._keep.append(jac)
+            d.jac = _dp(jac)
+        if df is not None:
+            df = _f64(df)
+            self._keep.append(df)
+            d.df = _dp(df)
+        d.precision, d.device = self.precision, device
+        h = ctypes.c_void_p()
+        check(lib().nkb_op_create(ctypes.byref(d), ctypes.byref(h)))
+        self.h = h
+        self._keep = []
+        nin, nout = ctypes.c_long(), ctypes.c_long()
+        check(lib().nkb_op_sizes(self.h, ctypes.byref(nin), ctypes.byref(nout)))
+        self.in_size, self.out_size = nin.value, nout.value
+
+    def set_factors(self, lam=1.0, diff_mode=DIFF_NONE, diff=None):
+        """Helmholtz_MatrixFree::UpdateFactors: lambda and diffusion tensor."""
+        d = None if diff is None else _f64(diff)
+        check(lib().nkb_op_set_factors(self.h, float(lam), diff_mode, _dp(d)))
+
+    def __call__(self, x):
+        """Host arrays in, host arrays out (synchronous)."""
+        x = _f64(x)
+        if x.size != self.in_size:
+            raise ValueError("input size %d != %d" % (x.size, self.in_size))
+        nout = 3 if self.optype == PHYSDERIV else 1
+        outs = [np.zeros(self.out_size) for _ in range(nout)] + [None] * (3 - nout)
+        check(lib().nkb_op_apply(self.h, x.ctypes.data, *[None if o is None else o.ctypes.data
+                                                           for o in outs], HOST_PTRS, None))
+        return tuple(outs[:nout]) if nout > 1 else outs[0]
+
+    def apply_device(self, x_ptr, out0, out1=None, out2=None, stream=None):
+        """Device pointers (ints); stream-ordered on `stream` (cudaStream_t int)."""
+        fn = lib().nkb_op_apply if self.precision == FP64 else lib().nkb_op_apply_f32
+        if self.precision == FP64:
+            check(fn(self.h, x_ptr, out0, out1, out2, DEVICE_PTRS, stream))
+        else:
+            check(fn(self.h, x_ptr, out0, out1, out2, stream))
+
+    def last_kernel_ms(self):
+        ms = ctypes.c_float()
+        check(lib().nkb_op_last_kernel_ms(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def helmholtz_diag(self):
+        out = np.zeros(self.nelmt * ncoeffs(self.shape, self.nm))
+        check(lib().nkb_op_helmholtz_diag(self.h, out.ctypes.data, HOST_PTRS, None))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().nkb_op_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GlobalLinSys:
+    """GlobalLinSysIterativeFull + PreconditionerDiagonal + NekLinSysIterCG."""
+
+    def __init__(self, ops, gmap, nglob, ndir, sign=None, device=0):
+        self.ops = list(ops)
+        self.nloc = int(sum(o.nelmt * ncoeffs(o.shape, o.nm) for o in self.ops))
+        self.nglob, self.ndir = int(nglob), int(ndir)
+        gmap = np.ascontiguousarray(gmap, dtype=np.int32)
+        sign = None if sign is None else _f64(sign)
+        handles = (ctypes.c_void_p * len(self.ops))(*[o.h.value for o in self.ops])
+        d = C.SysDesc()
+        d.nops, d.ops, d.ops32 = len(self.ops), handles, None
+        d.nloc, d.nglob, d.ndir = self.nloc, self.nglob, self.ndir
+        d.map = gmap.ctypes.data_as(C.ip)
+        d.sign = _dp(sign)
+        d.device = device
+        h = ctypes.c_void_p()
+        check(lib().nkb_sys_create(ctypes.byref(d), ctypes.byref(h)))
+        self.h = h
+
+    @staticmethod
+    def _opts(tol, maxit, check_interval, use_graph):
+        o = C.CGOpts()
+        o.tol, o.maxit, o.check_interval, o.use_graph = tol, maxit, check_interval, int(use_graph)
+        return o
+
+    def solve(self, b_loc, x_loc=None, tol=1e-9, maxit=5000, check_interval=16, use_graph=True,
+              raise_on_maxit=True):
+        """Host arrays: local rhs and local Dirichlet values -> local solution."""
+        b = _f64(b_loc)
+        x = np.zeros(self.nloc) if x_loc is None else _f64(x_loc).copy()
+        rep = C.CGReport()
+        rc = lib().nkb_cg_solve(self.h, b.ctypes.data, x.ctypes.data,
+                                ctypes.byref(self._opts(tol, maxit, check_interval, use_graph)),
+                                ctypes.byref(rep), HOST_PTRS, None)
+        if rc != C.NKB_OK and (raise_on_maxit or rc != C.NKB_ERR_NOT_CONVERGED):
+            check(rc)
+        return x, rep
+
+    def solve_device(self, b_ptr, x_ptr, tol=1e-9, maxit=5000, check_interval=16,
+                     use_graph=True, stream=None):
+        rep = C.CGReport()
+        check(lib().nkb_cg_solve(self.h, b_ptr, x_ptr,
+                                 ctypes.byref(self._opts(tol, maxit, check_interval, use_graph)),
+                                 ctypes.byref(rep), DEVICE_PTRS, stream))
+        return rep
+
+    def diag_inv(self):
+        out = np.zeros(self.nglob - self.ndir)
+        check(lib().nkb_sys_diag_inv(self.h, out.ctypes.data, HOST_PTRS, None))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().nkb_sys_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

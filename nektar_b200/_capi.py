@@ -1,0 +1,118 @@
+"""ctypes declarations of the C ABI in include/nektar_b200.h.
+
+The product path has no CPU fallback: importing this module raises if
+libnekb200.so has not been built (python -m nektar_b200.build).
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnekb200.so")
+
+c_int, c_long, c_double, c_float = ctypes.c_int, ctypes.c_long, ctypes.c_double, ctypes.c_float
+c_void_p, c_char_p = ctypes.c_void_p, ctypes.c_char_p
+P = ctypes.POINTER
+dp, fp, ip = P(c_double), P(c_float), P(c_int)
+
+# status codes
+NKB_OK = 0
+NKB_ERR_INVALID = -1
+NKB_ERR_UNSUPPORTED = -2
+NKB_ERR_CUDA = -3
+NKB_ERR_NOMEM = -4
+NKB_ERR_NOT_CONVERGED = -5
+NKB_ERR_NONFINITE = -6
+NKB_ERR_NO_DEVICE = -7
+
+TET, PRISM, HEX = 5, 7, 8
+BWDTRANS, HELMHOLTZ, IPRODUCT, PHYSDERIV = 0, 1, 3, 5
+GLL, RADAU_A1, RADAU_A2 = 4, 11, 12
+MODIFIED_A, MODIFIED_B, MODIFIED_C = 4, 5, 6
+FP64, FP32 = 0, 1
+DEVICE_PTRS, HOST_PTRS = 0, 1
+DIFF_NONE, DIFF_CONST, DIFF_VAR = 0, 1, 2
+
+
+class OpDesc(ctypes.Structure):
+    _fields_ = [("shape", c_int), ("optype", c_int), ("nm", c_int), ("nq", c_int * 3),
+                ("ptype", c_int * 3), ("nelmt", c_int), ("deformed", c_int),
+                ("bdata", dp * 3), ("w", dp * 3), ("z", dp * 3), ("D", dp * 3),
+                ("jac", dp), ("df", dp), ("precision", c_int), ("device", c_int)]
+
+
+class SysDesc(ctypes.Structure):
+    _fields_ = [("nops", c_int), ("ops", P(c_void_p)), ("ops32", P(c_void_p)), ("nloc", c_long),
+                ("nglob", c_int), ("ndir", c_int), ("map", ip), ("sign", dp), ("device", c_int)]
+
+
+class CGOpts(ctypes.Structure):
+    _fields_ = [("tol", c_double), ("maxit", c_int), ("check_interval", c_int),
+                ("use_graph", c_int), ("mixed", c_int), ("inner_tol", c_double),
+                ("max_outer", c_int)]
+
+
+class CGReport(ctypes.Structure):
+    _fields_ = [("iterations", c_int), ("outer_iterations", c_int), ("rel_residual", c_double),
+                ("converged", c_int), ("device_ms", c_double)]
+
+
+class GeomRequest(ctypes.Structure):
+    _fields_ = [("shape", c_int), ("n", c_int), ("amp", c_double), ("ncells", c_int),
+                ("cells", ip), ("nq", c_int * 3), ("z", dp * 3), ("deformed", c_int)]
+
+
+# every symbol the header declares, with its signature
+SIGNATURES = {
+    "nkb_last_error": (c_char_p, []),
+    "nkb_version": (c_char_p, []),
+    "nkb_points": (c_int, [c_int, c_int, dp, dp, dp]),
+    "nkb_basis": (c_int, [c_int, c_int, c_int, dp, dp, dp, dp]),
+    "nkb_op_create": (c_int, [P(OpDesc), P(c_void_p)]),
+    "nkb_op_set_factors": (c_int, [c_void_p, c_double, c_int, dp]),
+    "nkb_op_apply": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "nkb_op_apply_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "nkb_op_sizes": (c_int, [c_void_p, P(c_long), P(c_long)]),
+    "nkb_op_helmholtz_diag": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    "nkb_op_last_kernel_ms": (c_int, [c_void_p, P(c_float)]),
+    "nkb_op_destroy": (None, [c_void_p]),
+    "nkb_sys_create": (c_int, [P(SysDesc), P(c_void_p)]),
+    "nkb_cg_solve": (c_int, [c_void_p, c_void_p, c_void_p, P(CGOpts), P(CGReport), c_int,
+                             c_void_p]),
+    "nkb_sys_assemble": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "nkb_sys_global_to_local": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "nkb_sys_matvec_local": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "nkb_sys_diag_inv": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    "nkb_sys_destroy": (None, [c_void_p]),
+    "nkb_geom_nelmt": (c_long, [P(GeomRequest)]),
+    "nkb_geom_fill": (c_int, [P(GeomRequest), dp, dp, dp]),
+    "nkb_hex_box_assembly": (c_int, [c_int, c_int, ip, ip, ip]),
+}
+
+_lib = None
+
+
+class NektarB200Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("nektar_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libnekb200.so is not built (%s); run python -m nektar_b200.build"
+                              % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != NKB_OK:
+        raise NektarB200Error(rc, lib().nkb_last_error().decode(errors="replace"))
+    return rc

@@ -1,0 +1,59 @@
+// Internal definition of the operator object behind the C ABI handle.
+#pragma once
+
+#include "nkb_generic.cuh"
+#include "nkb_internal.h"
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+struct nkb_op
+{
+    int shape = 0, optype = 0, nm = 0, nq[3] = {0, 0, 0}, ptype[3] = {0, 0, 0};
+    int nelmt = 0, deformed = 0, precision = 0, device = 0;
+    int nc = 0, nt = 0, ncomp = 0;
+
+    // 1-D tables on the device (FP64 and FP32 copies)
+    double *dB[3] = {nullptr, nullptr, nullptr};
+    float *fB[3]  = {nullptr, nullptr, nullptr};
+    double *dD[3] = {nullptr, nullptr, nullptr};
+    float *fD[3]  = {nullptr, nullptr, nullptr};
+    double *dz[3] = {nullptr, nullptr, nullptr};
+    double *dw[3] = {nullptr, nullptr, nullptr}; // Radau-scaled weights
+    std::vector<double> hB[3], hD[3], hz[3], hw[3];
+
+    // geometry: raw (Collections layout) and packed per point
+    double *djac = nullptr, *ddf = nullptr;
+    double *geo  = nullptr; // [e][ncomp][nt]
+    float *geo32 = nullptr;
+
+    double lambda    = 1.0;
+    int diff_mode    = NKB_DIFF_NONE;
+    double diff[6]   = {1, 0, 1, 0, 0, 1};
+
+    // kernel selection (nkb_hex.cu): 0 generic, >0 tuned variant
+    int variant = 0;
+    void *kdata = nullptr;
+
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    void *scratch        = nullptr;
+    size_t scratch_bytes = 0;
+};
+
+namespace nkb
+{
+// generic kernels (nkb_ops.cu)
+template <typename T>
+int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
+                  const double *gsign, cudaStream_t s);
+// dispatch: tuned kernel if selected, else generic (nkb_hex.cu)
+template <typename T>
+int LaunchOp(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
+             const double *gsign, cudaStream_t s);
+int ChooseKernel(nkb_op *op);
+size_t GenericSmemBytes(const nkb_op *op, int elem_bytes);
+void FreeKernelData(nkb_op *op);
+int HelmholtzDiag(const nkb_op *op, double *d_out, cudaStream_t s);
+} // namespace nkb

@@ -1,0 +1,909 @@
+// Element operators of the B200 matrix-free path: nkb_op create / apply /
+// destroy (the Collections::Operator boundary), geometry packing and the
+// shape-generic CUDA kernels. The tuned Hex kernels live in nkb_hex.cu.
+//
+// Formulation. For every element the reference's fused Helmholtz kernel
+// (MatrixFreeOps/Helmholtz.h:549-599) computes
+//   y = IP(lambda J w u; B) + sum_a IP(J w (G grad u)_a; B with dB in dir a)
+// with u = BwdTrans(x) and G the DiffusionCoeff metric
+// (HelmholtzKernels.hpp:390-1114). Because dB = D B (Basis.cpp:493-495), the
+// three derivative inner products equal one inner product of
+//   f = lambda W u + sum_a D_a^T (G' grad u)_a ,  W = J w0 w1 w2, G' = W G,
+// so one BwdTrans, one raw inner product and two collocation derivative
+// passes do the work of the reference's one BwdTrans + four inner products.
+// W and the six unique entries of G' are packed per quadrature point at
+// create time in FP64 (the geometric-factor setup stays FP64).
+#include "nkb_internal.h"
+#include "nkb_op.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace nkb
+{
+
+static thread_local std::string g_err;
+
+int SetError(int code, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+void ClearError()
+{
+    g_err.clear();
+}
+
+// ---------------------------------------------------------------------------
+// geometry packing (FP64 on the device)
+// ---------------------------------------------------------------------------
+
+// Rows a_a of d eta_a / d x_k for the shape at point (i, j, k): the chain rule
+// of PhysDerivKernels.hpp:184-344 folded with the derivative factors, the
+// same combination HelmholtzKernels.hpp uses for its metric (h0..h3 of
+// GetHelmholtz3DHalfSpace, HelmholtzKernels.hpp:1357-1425).
+__device__ void ShapeRows(int shape, const double *f, double z0, double z1, double z2, double a[9])
+{
+    if (shape == NKB_HEX)
+    {
+        for (int k = 0; k < 3; ++k)
+        {
+            a[0 + k] = f[k * 3 + 0];
+            a[3 + k] = f[k * 3 + 1];
+            a[6 + k] = f[k * 3 + 2];
+        }
+    }
+    else if (shape == NKB_TET)
+    {
+        const double h0 = 0.5 * (1.0 + z0), h1 = 0.5 * (1.0 + z1);
+        const double h2 = 2.0 / (1.0 - z1), h3 = 2.0 / (1.0 - z2);
+        const double h2h3 = h2 * h3, h1h3 = h1 * h3, h0h2h3 = h0 * h2h3;
+        for (int k = 0; k < 3; ++k)
+        {
+            a[0 + k] = fma(f[k * 3 + 0], h2h3, h0h2h3 * (f[k * 3 + 1] + f[k * 3 + 2]));
+            a[3 + k] = fma(f[k * 3 + 2], h1h3, f[k * 3 + 1] * h3);
+            a[6 + k] = f[k * 3 + 2];
+        }
+    }
+    else
+    {
+        const double h0 = 0.5 * (1.0 + z0), h1 = 2.0 / (1.0 - z2);
+        for (int k = 0; k < 3; ++k)
+        {
+            a[0 + k] = h1 * (h0 * f[k * 3 + 2] + f[k * 3 + 0]);
+            a[3 + k] = f[k * 3 + 1];
+            a[6 + k] = f[k * 3 + 2];
+        }
+    }
+}
+
+struct PackArgs
+{
+    int shape, optype, deformed, nelmt, nq0, nq1, nq2, nt;
+    const double *jac, *df;       // Collections layout
+    const double *z0, *z1, *z2;   // points
+    const double *w0, *w1, *w2;   // scaled weights
+    int diff_mode;                // NKB_DIFF_*
+    double K[6];                  // d00 d01 d11 d02 d12 d22
+    double *geo;                  // packed FP64
+    float *geo32;                 // optional FP32 copy
+    int ncomp;                    // 7 Helmholtz, 9 PhysDeriv, 1 IProduct
+};
+
+__global__ void k_pack(PackArgs a)
+{
+    const long nt  = a.nt;
+    const long tot = long(a.nelmt) * nt;
+    for (long g = blockIdx.x * long(blockDim.x) + threadIdx.x; g < tot;
+         g += long(gridDim.x) * blockDim.x)
+    {
+        const long e = g / nt, q = g % nt;
+        const int i = int(q % a.nq0), j = int((q / a.nq0) % a.nq1), k = int(q / (long(a.nq0) * a.nq1));
+        const long ncol = a.deformed ? tot : long(a.nelmt);
+        const long col  = a.deformed ? g : e;
+        const double J  = a.jac ? a.jac[col] : 1.0;
+        double *out     = a.geo + e * a.ncomp * nt + q;
+        float *out32    = a.geo32 ? a.geo32 + e * a.ncomp * nt + q : nullptr;
+        if (a.optype == NKB_IPRODUCT)
+        {
+            double W = J * a.w0[i] * a.w1[j] * a.w2[k];
+            out[0]   = W;
+            if (out32)
+                out32[0] = float(W);
+            continue;
+        }
+        double f[9];
+        for (int d = 0; d < 9; ++d)
+            f[d] = a.df[d * ncol + col];
+        double A[9];
+        ShapeRows(a.shape, f, a.z0[i], a.z1[j], a.z2[k], A);
+        if (a.optype == NKB_PHYSDERIV)
+        {
+            for (int c = 0; c < 9; ++c)
+            {
+                out[c * nt] = A[c];
+                if (out32)
+                    out32[c * nt] = float(A[c]);
+            }
+            continue;
+        }
+        // Helmholtz: W and W * A K A^T (six unique entries)
+        double K[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+        if (a.diff_mode != NKB_DIFF_NONE)
+        {
+            K[0][0] = a.K[0];
+            K[0][1] = K[1][0] = a.K[1];
+            K[1][1]           = a.K[2];
+            K[0][2] = K[2][0] = a.K[3];
+            K[1][2] = K[2][1] = a.K[4];
+            K[2][2]           = a.K[5];
+            // the reference Tet kernel keeps d11 = 1 under variable diffusion
+            // (HelmholtzKernels.hpp:453-460 never loads varD11)
+            if (a.shape == NKB_TET && a.diff_mode == NKB_DIFF_VAR)
+                K[1][1] = 1.0;
+        }
+        double t[3][3];
+        for (int x = 0; x < 3; ++x)
+            for (int l = 0; l < 3; ++l)
+                t[x][l] = A[x * 3 + 0] * K[0][l] + A[x * 3 + 1] * K[1][l] + A[x * 3 + 2] * K[2][l];
+        double G[3][3];
+        for (int x = 0; x < 3; ++x)
+            for (int y = 0; y < 3; ++y)
+                G[x][y] = t[x][0] * A[y * 3 + 0] + t[x][1] * A[y * 3 + 1] + t[x][2] * A[y * 3 + 2];
+        const double W = J * a.w0[i] * a.w1[j] * a.w2[k];
+        const double v[7] = {W,           W * G[0][0], W * G[1][1], W * G[2][2],
+                             W * G[0][1], W * G[0][2], W * G[1][2]};
+        for (int c = 0; c < 7; ++c)
+        {
+            out[c * nt] = v[c];
+            if (out32)
+                out32[c * nt] = float(v[c]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// generic kernels
+// ---------------------------------------------------------------------------
+static Dims MakeDims(const nkb_op *op);
+
+enum
+{
+    GK_BWD  = 0,
+    GK_HELM = 1,
+    GK_IP   = 3,
+    GK_PD   = 5,
+    GK_DIAG = 9
+};
+
+// per-element shared memory: x[nc] u[nt] g0 g1 g2 [nt] wa[wsz] wb[wsz]
+__host__ __device__ inline int ElemSmem(const Dims &d)
+{
+    int s = d.nc + 4 * d.nt + 2 * d.wsz;
+    return (s + 1) & ~1;
+}
+
+template <typename T> struct GenArgs
+{
+    Dims d;
+    Tabs<T> t;
+    const T *geo;
+    T lambda;
+    const T *in;
+    T *out0, *out1, *out2;
+    // optional gather of the input from a global vector: in[e*nc+m] = sign * gvec[map]
+    const int *gmap;
+    const double *gsign;
+    int nelmt, epb;
+};
+
+#define NKB_STAGE(SIZE, ...)                                                                     \
+    for (int idx = threadIdx.x; idx < ne * (SIZE); idx += blockDim.x)                             \
+    {                                                                                             \
+        const int le = idx / (SIZE);                                                              \
+        const int l  = idx - le * (SIZE);                                                         \
+        T *sm        = smem + le * es;                                                            \
+        T *x = sm, *u = sm + d.nc, *g0 = u + d.nt, *g1 = g0 + d.nt, *g2 = g1 + d.nt;              \
+        T *wa = g2 + d.nt, *wb = wa + d.wsz;                                                      \
+        (void)x;                                                                                  \
+        (void)u;                                                                                  \
+        (void)g0;                                                                                 \
+        (void)g1;                                                                                 \
+        (void)g2;                                                                                 \
+        (void)wa;                                                                                 \
+        (void)wb;                                                                                 \
+        const long e = e0 + le;                                                                   \
+        (void)e;                                                                                  \
+        __VA_ARGS__                                                                               \
+    }                                                                                             \
+    __syncthreads();
+
+template <int SHAPE, int OP, typename T> __global__ void k_generic(GenArgs<T> a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *smem       = reinterpret_cast<T *>(smem_raw);
+    const Dims &d = a.d;
+    const int es  = ElemSmem(d);
+    const long e0 = long(blockIdx.x) * a.epb;
+    const int ne  = int(min(long(a.epb), long(a.nelmt) - e0));
+    if (ne <= 0)
+        return;
+    using BW = Bwd<SHAPE>;
+    using IP = Ipr<SHAPE>;
+
+    if (OP == GK_BWD || OP == GK_HELM || OP == GK_DIAG)
+    {
+        if (OP != GK_DIAG)
+        {
+            NKB_STAGE(d.nc, {
+                if (a.gmap)
+                {
+                    const long gi = e * d.nc + l;
+                    const T v = a.in[a.gmap[gi]];
+                    x[l]      = a.gsign ? T(a.gsign[gi]) * v : v;
+                }
+                else
+                {
+                    x[l] = a.in[e * d.nc + l];
+                }
+            })
+        }
+    }
+    else
+    {
+        NKB_STAGE(d.nt, { u[l] = a.in[e * d.nt + l]; })
+    }
+
+    if (OP == GK_BWD || OP == GK_HELM)
+    {
+        NKB_STAGE(BW::SizeA(d), { BW::A(d, a.t, x, wa, l); })
+        NKB_STAGE(BW::SizeB(d), { BW::B(d, a.t, x, wa, wb, l); })
+        NKB_STAGE(d.nt, { BW::C(d, a.t, x, wb, u, l); })
+        if (OP == GK_BWD)
+        {
+            NKB_STAGE(d.nt, { a.out0[e * d.nt + l] = u[l]; })
+            return;
+        }
+    }
+
+    if (OP == GK_PD)
+    {
+        NKB_STAGE(d.nt, {
+            T q0, q1, q2;
+            Grad(d, a.t, u, l, q0, q1, q2);
+            const T *A = a.geo + e * 9 * d.nt + l;
+            const long o = e * d.nt + l;
+            a.out0[o] = fma(A[6 * d.nt], q2, fma(A[3 * d.nt], q1, A[0] * q0));
+            a.out1[o] = fma(A[7 * d.nt], q2, fma(A[4 * d.nt], q1, A[1 * d.nt] * q0));
+            a.out2[o] = fma(A[8 * d.nt], q2, fma(A[5 * d.nt], q1, A[2 * d.nt] * q0));
+        })
+        return;
+    }
+
+    if (OP == GK_IP)
+    {
+        // f = W * in
+        NKB_STAGE(d.nt, { u[l] = u[l] * a.geo[e * d.nt + l]; })
+    }
+
+    if (OP == GK_HELM)
+    {
+        // v = G' grad u, f = lambda W u
+        NKB_STAGE(d.nt, {
+            T q0, q1, q2;
+            Grad(d, a.t, u, l, q0, q1, q2);
+            const T *G = a.geo + e * 7 * d.nt + l;
+            const T W = G[0], G00 = G[d.nt], G11 = G[2 * d.nt], G22 = G[3 * d.nt];
+            const T G01 = G[4 * d.nt], G02 = G[5 * d.nt], G12 = G[6 * d.nt];
+            g0[l] = fma(G02, q2, fma(G01, q1, G00 * q0));
+            g1[l] = fma(G12, q2, fma(G11, q1, G01 * q0));
+            g2[l] = fma(G22, q2, fma(G12, q1, G02 * q0));
+            wa[l] = a.lambda * W * u[l];
+        })
+        NKB_STAGE(d.nt, { u[l] = wa[l] + GradT(d, a.t, g0, g1, g2, l); })
+    }
+
+    if (OP == GK_HELM || OP == GK_IP)
+    {
+        NKB_STAGE(IP::SizeA(d), { IprStageA(d, a.t, u, wa, l); })
+        NKB_STAGE(IP::SizeB(d), { IP::B(d, a.t, wa, wb, l); })
+        NKB_STAGE(d.nc, { a.out0[e * d.nc + l] = IP::C(d, a.t, wb, l); })
+    }
+}
+
+// Diagonal of the element Helmholtz matrix: for every mode m,
+// diag_m = sum_q lambda W phi_m^2 + grad phi_m . G' grad phi_m,
+// phi_m = BwdTrans(e_m). One CTA per element.
+template <int SHAPE, typename T> __global__ void k_diag(GenArgs<T> a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *smem       = reinterpret_cast<T *>(smem_raw);
+    const Dims &d = a.d;
+    const long e  = blockIdx.x;
+    if (e >= a.nelmt)
+        return;
+    using BW = Bwd<SHAPE>;
+    T *x = smem, *u = x + d.nc, *wa = u + d.nt, *wb = wa + d.wsz, *red = wb + d.wsz;
+    const T *G = a.geo + e * 7 * d.nt;
+    for (int m = 0; m < d.nc; ++m)
+    {
+        for (int l = threadIdx.x; l < d.nc; l += blockDim.x)
+            x[l] = (l == m) ? T(1) : T(0);
+        __syncthreads();
+        for (int l = threadIdx.x; l < BW::SizeA(d); l += blockDim.x)
+            BW::A(d, a.t, x, wa, l);
+        __syncthreads();
+        for (int l = threadIdx.x; l < BW::SizeB(d); l += blockDim.x)
+            BW::B(d, a.t, x, wa, wb, l);
+        __syncthreads();
+        for (int l = threadIdx.x; l < d.nt; l += blockDim.x)
+            BW::C(d, a.t, x, wb, u, l);
+        __syncthreads();
+        T acc = 0;
+        for (int l = threadIdx.x; l < d.nt; l += blockDim.x)
+        {
+            T q0, q1, q2;
+            Grad(d, a.t, u, l, q0, q1, q2);
+            const T W = G[l], G00 = G[d.nt + l], G11 = G[2 * d.nt + l], G22 = G[3 * d.nt + l];
+            const T G01 = G[4 * d.nt + l], G02 = G[5 * d.nt + l], G12 = G[6 * d.nt + l];
+            T v = a.lambda * W * u[l] * u[l];
+            v   = fma(q0, fma(G00, q0, 2 * (G01 * q1 + G02 * q2)), v);
+            v   = fma(q1, fma(G11, q1, 2 * G12 * q2), v);
+            v   = fma(q2, G22 * q2, v);
+            acc += v;
+        }
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1)
+        {
+            if (threadIdx.x < s)
+                red[threadIdx.x] += red[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            a.out0[e * d.nc + m] = red[0];
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+static Dims MakeDims(const nkb_op *op)
+{
+    Dims d;
+    d.nm    = op->nm;
+    d.nq0   = op->nq[0];
+    d.nq1   = op->nq[1];
+    d.nq2   = op->nq[2];
+    d.nc    = op->nc;
+    d.nt    = op->nt;
+    d.npair = op->nm * (op->nm + 1) / 2;
+    int M   = std::max(op->nm, op->nq[0]);
+    d.wsz   = M * M * M + 2 * op->nq[2] + M * M;
+    return d;
+}
+
+template <typename T> static Tabs<T> MakeTabs(const nkb_op *op)
+{
+    Tabs<T> t;
+    const T *const *B = reinterpret_cast<const T *const *>(
+        std::is_same<T, double>::value ? (const void *)op->dB : (const void *)op->fB);
+    const T *const *D = reinterpret_cast<const T *const *>(
+        std::is_same<T, double>::value ? (const void *)op->dD : (const void *)op->fD);
+    t.B0 = B[0];
+    t.B1 = B[1];
+    t.B2 = B[2];
+    t.D0 = D[0];
+    t.D1 = D[1];
+    t.D2 = D[2];
+    return t;
+}
+
+size_t GenericSmemBytes(const nkb_op *op, int elem_bytes)
+{
+    return size_t(ElemSmem(MakeDims(op))) * elem_bytes;
+}
+
+template <int SHAPE, int OP, typename T>
+static int LaunchGenericT(const nkb_op *op, GenArgs<T> a, cudaStream_t s)
+{
+    const int es      = ElemSmem(a.d);
+    const size_t ebyt = size_t(es) * sizeof(T);
+    int epb           = int(std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / ebyt)));
+    a.epb             = epb;
+    const size_t smem = ebyt * epb;
+    auto kern         = k_generic<SHAPE, OP, T>;
+    // raise the dynamic shared-memory limit once per instantiation, before any
+    // stream capture can contain this launch
+    static size_t s_smem_set = 48 * 1024;
+    if (smem > s_smem_set)
+    {
+        NKB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        s_smem_set = smem;
+    }
+    const long nb = (long(a.nelmt) + epb - 1) / epb;
+    if (nb > 0)
+        kern<<<unsigned(nb), 128, smem, s>>>(a);
+    NKB_CUDA_TRY(cudaGetLastError());
+    return NKB_OK;
+}
+
+template <int OP, typename T> static int LaunchGenericShape(const nkb_op *op, GenArgs<T> a, cudaStream_t s)
+{
+    switch (op->shape)
+    {
+        case NKB_HEX:
+            return LaunchGenericT<NKB_HEX, OP, T>(op, a, s);
+        case NKB_PRISM:
+            return LaunchGenericT<NKB_PRISM, OP, T>(op, a, s);
+        default:
+            return LaunchGenericT<NKB_TET, OP, T>(op, a, s);
+    }
+}
+
+template <typename T>
+int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
+                  const double *gsign, cudaStream_t s)
+{
+    GenArgs<T> a;
+    a.d      = MakeDims(op);
+    a.t      = MakeTabs<T>(op);
+    a.geo    = std::is_same<T, double>::value ? (const T *)op->geo : (const T *)op->geo32;
+    a.lambda = T(op->lambda);
+    a.in     = in;
+    a.out0   = o0;
+    a.out1   = o1;
+    a.out2   = o2;
+    a.gmap   = gmap;
+    a.gsign  = gsign;
+    a.nelmt  = op->nelmt;
+    a.epb    = 1;
+    switch (op->optype)
+    {
+        case NKB_BWDTRANS:
+            return LaunchGenericShape<GK_BWD, T>(op, a, s);
+        case NKB_IPRODUCT:
+            return LaunchGenericShape<GK_IP, T>(op, a, s);
+        case NKB_PHYSDERIV:
+            return LaunchGenericShape<GK_PD, T>(op, a, s);
+        default:
+            return LaunchGenericShape<GK_HELM, T>(op, a, s);
+    }
+}
+
+template int LaunchGeneric<double>(const nkb_op *, const double *, double *, double *, double *,
+                                   const int *, const double *, cudaStream_t);
+template int LaunchGeneric<float>(const nkb_op *, const float *, float *, float *, float *,
+                                  const int *, const double *, cudaStream_t);
+
+static int Repack(nkb_op *op)
+{
+    PackArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.shape     = op->shape;
+    a.optype    = op->optype;
+    a.deformed  = op->deformed;
+    a.nelmt     = op->nelmt;
+    a.nq0       = op->nq[0];
+    a.nq1       = op->nq[1];
+    a.nq2       = op->nq[2];
+    a.nt        = op->nt;
+    a.jac       = op->djac;
+    a.df        = op->ddf;
+    a.z0        = op->dz[0];
+    a.z1        = op->dz[1];
+    a.z2        = op->dz[2];
+    a.w0        = op->dw[0];
+    a.w1        = op->dw[1];
+    a.w2        = op->dw[2];
+    a.diff_mode = op->diff_mode;
+    for (int c = 0; c < 6; ++c)
+        a.K[c] = op->diff[c];
+    a.geo   = op->geo;
+    a.geo32 = op->geo32;
+    a.ncomp = op->ncomp;
+    if (op->ncomp == 0)
+        return NKB_OK;
+    long tot = long(op->nelmt) * op->nt;
+    int nb   = int(std::min<long>((tot + 255) / 256, 148L * 16));
+    k_pack<<<std::max(nb, 1), 256, 0, op->stream>>>(a);
+    NKB_CUDA_TRY(cudaGetLastError());
+    NKB_CUDA_TRY(cudaStreamSynchronize(op->stream));
+    return NKB_OK;
+}
+
+template <typename T> static int Upload(T **dst, const double *src, size_t n)
+{
+    std::vector<T> tmp(n);
+    for (size_t i = 0; i < n; ++i)
+        tmp[i] = T(src[i]);
+    NKB_CUDA_TRY(cudaMalloc(dst, n * sizeof(T)));
+    NKB_CUDA_TRY(cudaMemcpy(*dst, tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+    return NKB_OK;
+}
+
+} // namespace nkb
+
+using namespace nkb;
+
+extern "C" const char *nkb_last_error(void)
+{
+    return g_err.c_str();
+}
+
+extern "C" const char *nkb_version(void)
+{
+    static std::string v;
+    if (v.empty())
+    {
+        int rt = 0;
+        cudaRuntimeGetVersion(&rt);
+        v = "nektar_b200 0.1 (sm_100a, CUDA runtime " + std::to_string(rt) + ")";
+    }
+    return v.c_str();
+}
+
+extern "C" int nkb_op_create(const nkb_op_desc *desc, nkb_op **out)
+{
+    ClearError();
+    if (!desc || !out)
+        return SetError(NKB_ERR_INVALID, "nkb_op_create: NULL argument");
+    *out = nullptr;
+    const int shape = desc->shape, nm = desc->nm;
+    if (shape != NKB_HEX && shape != NKB_PRISM && shape != NKB_TET)
+        return SetError(NKB_ERR_INVALID, "nkb_op_create: unsupported shape %d", shape);
+    if (desc->optype != NKB_BWDTRANS && desc->optype != NKB_HELMHOLTZ &&
+        desc->optype != NKB_IPRODUCT && desc->optype != NKB_PHYSDERIV)
+        return SetError(NKB_ERR_INVALID, "nkb_op_create: unsupported operator %d", desc->optype);
+    if (nm < 2 || nm > 16 || desc->nelmt < 0)
+        return SetError(NKB_ERR_INVALID, "nkb_op_create: nm=%d nelmt=%d out of range", nm,
+                        desc->nelmt);
+    for (int d = 0; d < 3; ++d)
+        if (desc->nq[d] < 2 || desc->nq[d] > 24)
+            return SetError(NKB_ERR_INVALID, "nkb_op_create: nq[%d]=%d out of range", d,
+                            desc->nq[d]);
+    // MatrixFree preconditions (BwdTransKernels.hpp:537-545)
+    const int *nq = desc->nq;
+    bool ok = (shape == NKB_HEX && nq[0] == nq[1] && nq[0] == nq[2]) ||
+              (shape == NKB_PRISM && nq[0] == nq[1] && nq[0] == nq[2] + 1) ||
+              (shape == NKB_TET && nq[0] == nq[1] + 1 && nq[0] == nq[2] + 1);
+    if (!ok)
+        return SetError(NKB_ERR_INVALID, "nkb_op_create: point counts (%d,%d,%d) not homogeneous "
+                        "for shape %d", nq[0], nq[1], nq[2], shape);
+    if (desc->precision != NKB_FP64 && desc->precision != NKB_FP32)
+        return SetError(NKB_ERR_INVALID, "nkb_op_create: bad precision %d", desc->precision);
+    const int opt = desc->optype;
+    auto need = [&](const void *p, const char *what) -> int {
+        if (!p)
+            return SetError(NKB_ERR_INVALID, "nkb_op_create: %s is required for operator %d", what,
+                            opt);
+        return NKB_OK;
+    };
+    for (int d = 0; d < 3; ++d)
+    {
+        if (opt != NKB_PHYSDERIV && need(desc->bdata[d], "bdata"))
+            return NKB_ERR_INVALID;
+        if ((opt == NKB_IPRODUCT || opt == NKB_HELMHOLTZ) && need(desc->w[d], "w"))
+            return NKB_ERR_INVALID;
+        if ((opt == NKB_PHYSDERIV || opt == NKB_HELMHOLTZ) &&
+            (need(desc->D[d], "D") || need(desc->z[d], "z")))
+            return NKB_ERR_INVALID;
+    }
+    if ((opt == NKB_IPRODUCT || opt == NKB_HELMHOLTZ) && need(desc->jac, "jac"))
+        return NKB_ERR_INVALID;
+    if ((opt == NKB_PHYSDERIV || opt == NKB_HELMHOLTZ) && need(desc->df, "df"))
+        return NKB_ERR_INVALID;
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return SetError(NKB_ERR_NO_DEVICE, "nkb_op_create: no CUDA device");
+    if (desc->device < 0 || desc->device >= ndev)
+        return SetError(NKB_ERR_INVALID, "nkb_op_create: device %d of %d", desc->device, ndev);
+    NKB_CUDA_TRY(cudaSetDevice(desc->device));
+
+    nkb_op *op    = new nkb_op();
+    op->shape     = shape;
+    op->optype    = opt;
+    op->nm        = nm;
+    op->nelmt     = desc->nelmt;
+    op->deformed  = desc->deformed ? 1 : 0;
+    op->precision = desc->precision;
+    op->device    = desc->device;
+    for (int d = 0; d < 3; ++d)
+    {
+        op->nq[d]    = nq[d];
+        op->ptype[d] = desc->ptype[d];
+    }
+    op->nc = NumCoeffs(shape, nm);
+    op->nt = nq[0] * nq[1] * nq[2];
+    op->ncomp = (opt == NKB_HELMHOLTZ) ? 7 : (opt == NKB_PHYSDERIV ? 9 : (opt == NKB_IPRODUCT ? 1 : 0));
+    int rc = NKB_OK;
+    auto fail = [&](int code) {
+        nkb_op_destroy(op);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&op->ev0) != cudaSuccess || cudaEventCreate(&op->ev1) != cudaSuccess)
+        return fail(SetError(NKB_ERR_CUDA, "nkb_op_create: stream/event creation failed"));
+
+    // 1-D tables
+    for (int d = 0; d < 3; ++d)
+    {
+        const size_t nb = size_t(TableModes(shape, d, nm)) * nq[d];
+        std::vector<double> zero(std::max<size_t>(nb, size_t(nq[d]) * nq[d]), 0.0);
+        const double *B = desc->bdata[d] ? desc->bdata[d] : zero.data();
+        const double *D = desc->D[d] ? desc->D[d] : zero.data();
+        if ((rc = Upload(&op->dB[d], B, nb)) || (rc = Upload(&op->fB[d], B, nb)) ||
+            (rc = Upload(&op->dD[d], D, size_t(nq[d]) * nq[d])) ||
+            (rc = Upload(&op->fD[d], D, size_t(nq[d]) * nq[d])))
+            return fail(rc);
+        std::vector<double> z(nq[d], 0.0), w(nq[d], 0.0);
+        if (desc->z[d])
+            std::copy(desc->z[d], desc->z[d] + nq[d], z.begin());
+        if (desc->w[d])
+            for (int i = 0; i < nq[d]; ++i)
+                w[i] = WeightFactor(desc->ptype[d]) * desc->w[d][i];
+        if ((rc = Upload(&op->dz[d], z.data(), nq[d])) || (rc = Upload(&op->dw[d], w.data(), nq[d])))
+            return fail(rc);
+        op->hz[d].assign(z.begin(), z.end());
+        op->hw[d].assign(w.begin(), w.end());
+        op->hB[d].assign(B, B + nb);
+        op->hD[d].assign(D, D + size_t(nq[d]) * nq[d]);
+    }
+    // raw geometry (kept on the device so factor updates can repack)
+    const long ncol = op->deformed ? long(op->nelmt) * op->nt : long(op->nelmt);
+    if (desc->jac && op->ncomp && op->nelmt)
+        if ((rc = Upload(&op->djac, desc->jac, size_t(ncol))))
+            return fail(rc);
+    if (desc->df && op->ncomp > 1 && op->nelmt)
+        if ((rc = Upload(&op->ddf, desc->df, size_t(9) * ncol)))
+            return fail(rc);
+    if (op->ncomp && op->nelmt)
+    {
+        const size_t n = size_t(op->nelmt) * op->ncomp * op->nt;
+        if (cudaMalloc(&op->geo, n * sizeof(double)) != cudaSuccess)
+            return fail(SetError(NKB_ERR_NOMEM, "nkb_op_create: geometry (%zu doubles)", n));
+        if (op->precision == NKB_FP32 && cudaMalloc(&op->geo32, n * sizeof(float)) != cudaSuccess)
+            return fail(SetError(NKB_ERR_NOMEM, "nkb_op_create: FP32 geometry"));
+        if ((rc = Repack(op)))
+            return fail(rc);
+    }
+    if ((rc = ChooseKernel(op)))
+        return fail(rc);
+    *out = op;
+    return NKB_OK;
+}
+
+extern "C" int nkb_op_set_factors(nkb_op *op, double lambda, int diff_mode, const double *diff)
+{
+    ClearError();
+    if (!op)
+        return SetError(NKB_ERR_INVALID, "nkb_op_set_factors: NULL op");
+    if (diff_mode < NKB_DIFF_NONE || diff_mode > NKB_DIFF_VAR || (diff_mode && !diff))
+        return SetError(NKB_ERR_INVALID, "nkb_op_set_factors: bad diffusion mode %d", diff_mode);
+    op->lambda = lambda;
+    bool repack = (diff_mode != op->diff_mode);
+    if (diff_mode)
+        for (int c = 0; c < 6; ++c)
+            if (diff[c] != op->diff[c])
+            {
+                repack     = true;
+                op->diff[c] = diff[c];
+            }
+    op->diff_mode = diff_mode;
+    if (!diff_mode)
+    {
+        const double id[6] = {1, 0, 1, 0, 0, 1};
+        for (int c = 0; c < 6; ++c)
+            op->diff[c] = id[c];
+    }
+    if (repack && op->optype == NKB_HELMHOLTZ)
+    {
+        NKB_CUDA_TRY(cudaSetDevice(op->device));
+        return Repack(op);
+    }
+    return NKB_OK;
+}
+
+extern "C" int nkb_op_sizes(const nkb_op *op, long *in_size, long *out_size)
+{
+    if (!op)
+        return SetError(NKB_ERR_INVALID, "nkb_op_sizes: NULL op");
+    const long nc = long(op->nelmt) * op->nc, nt = long(op->nelmt) * op->nt;
+    long in = nc, out = nc;
+    if (op->optype == NKB_BWDTRANS)
+        out = nt;
+    else if (op->optype == NKB_IPRODUCT)
+        in = nt;
+    else if (op->optype == NKB_PHYSDERIV)
+        in = out = nt;
+    if (in_size)
+        *in_size = in;
+    if (out_size)
+        *out_size = out;
+    return NKB_OK;
+}
+
+static int EnsureScratch(nkb_op *op, size_t bytes)
+{
+    if (op->scratch_bytes >= bytes)
+        return NKB_OK;
+    if (op->scratch)
+        cudaFree(op->scratch);
+    op->scratch       = nullptr;
+    op->scratch_bytes = 0;
+    if (cudaMalloc(&op->scratch, bytes) != cudaSuccess)
+        return SetError(NKB_ERR_NOMEM, "nkb_op_apply: staging buffer of %zu bytes", bytes);
+    op->scratch_bytes = bytes;
+    return NKB_OK;
+}
+
+extern "C" int nkb_op_apply(nkb_op *op, const double *in, double *out0, double *out1,
+                            double *out2, int flags, void *stream)
+{
+    ClearError();
+    if (!op || !in || !out0)
+        return SetError(NKB_ERR_INVALID, "nkb_op_apply: NULL argument");
+    if (op->precision != NKB_FP64)
+        return SetError(NKB_ERR_INVALID, "nkb_op_apply: FP32 operator; use nkb_op_apply_f32");
+    if (op->optype == NKB_PHYSDERIV && (!out1 || !out2))
+        return SetError(NKB_ERR_INVALID, "nkb_op_apply: PhysDeriv needs three outputs");
+    NKB_CUDA_TRY(cudaSetDevice(op->device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : op->stream;
+    long nin, nout;
+    nkb_op_sizes(op, &nin, &nout);
+    const int nouts = op->optype == NKB_PHYSDERIV ? 3 : 1;
+    if (flags & NKB_HOST_PTRS)
+    {
+        const size_t bytes = size_t(nin + nouts * nout) * sizeof(double);
+        int rc             = EnsureScratch(op, bytes);
+        if (rc)
+            return rc;
+        double *din = static_cast<double *>(op->scratch);
+        double *dout = din + nin;
+        NKB_CUDA_TRY(cudaMemcpyAsync(din, in, nin * sizeof(double), cudaMemcpyHostToDevice, s));
+        NKB_CUDA_TRY(cudaEventRecord(op->ev0, s));
+        rc = LaunchOp<double>(op, din, dout, nouts > 1 ? dout + nout : nullptr,
+                              nouts > 2 ? dout + 2 * nout : nullptr, nullptr, nullptr, s);
+        if (rc)
+            return rc;
+        NKB_CUDA_TRY(cudaEventRecord(op->ev1, s));
+        double *outs[3] = {out0, out1, out2};
+        for (int o = 0; o < nouts; ++o)
+            NKB_CUDA_TRY(cudaMemcpyAsync(outs[o], dout + o * nout, nout * sizeof(double),
+                                         cudaMemcpyDeviceToHost, s));
+        NKB_CUDA_TRY(cudaStreamSynchronize(s));
+        return NKB_OK;
+    }
+    NKB_CUDA_TRY(cudaEventRecord(op->ev0, s));
+    int rc = LaunchOp<double>(op, in, out0, out1, out2, nullptr, nullptr, s);
+    if (rc)
+        return rc;
+    NKB_CUDA_TRY(cudaEventRecord(op->ev1, s));
+    return NKB_OK;
+}
+
+extern "C" int nkb_op_apply_f32(nkb_op *op, const float *in, float *out0, float *out1,
+                                float *out2, void *stream)
+{
+    ClearError();
+    if (!op || !in || !out0)
+        return SetError(NKB_ERR_INVALID, "nkb_op_apply_f32: NULL argument");
+    if (op->precision != NKB_FP32)
+        return SetError(NKB_ERR_INVALID, "nkb_op_apply_f32: operator is not FP32");
+    NKB_CUDA_TRY(cudaSetDevice(op->device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : op->stream;
+    NKB_CUDA_TRY(cudaEventRecord(op->ev0, s));
+    int rc = LaunchOp<float>(op, in, out0, out1, out2, nullptr, nullptr, s);
+    if (rc)
+        return rc;
+    NKB_CUDA_TRY(cudaEventRecord(op->ev1, s));
+    return NKB_OK;
+}
+
+extern "C" int nkb_op_last_kernel_ms(const nkb_op *op, float *ms)
+{
+    if (!op || !ms)
+        return SetError(NKB_ERR_INVALID, "nkb_op_last_kernel_ms: NULL argument");
+    NKB_CUDA_TRY(cudaEventSynchronize(op->ev1));
+    NKB_CUDA_TRY(cudaEventElapsedTime(ms, op->ev0, op->ev1));
+    return NKB_OK;
+}
+
+namespace nkb
+{
+int HelmholtzDiag(const nkb_op *op, double *d_out, cudaStream_t s)
+{
+    if (op->optype != NKB_HELMHOLTZ)
+        return SetError(NKB_ERR_INVALID, "Helmholtz diagonal needs a Helmholtz operator");
+    GenArgs<double> a;
+    a.d      = MakeDims(op);
+    a.t      = MakeTabs<double>(op);
+    a.geo    = op->geo;
+    a.lambda = op->lambda;
+    a.in     = nullptr;
+    a.out0   = d_out;
+    a.out1 = a.out2 = nullptr;
+    a.gmap          = nullptr;
+    a.gsign         = nullptr;
+    a.nelmt         = op->nelmt;
+    a.epb           = 1;
+    const int threads = 128;
+    size_t smem = size_t(a.d.nc + a.d.nt + 2 * a.d.wsz + threads) * sizeof(double);
+    void (*kern)(GenArgs<double>) = op->shape == NKB_HEX     ? k_diag<NKB_HEX, double>
+                                    : op->shape == NKB_PRISM ? k_diag<NKB_PRISM, double>
+                                                             : k_diag<NKB_TET, double>;
+    NKB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    if (op->nelmt > 0)
+        kern<<<op->nelmt, threads, smem, s>>>(a);
+    NKB_CUDA_TRY(cudaGetLastError());
+    return NKB_OK;
+}
+} // namespace nkb
+
+extern "C" int nkb_op_helmholtz_diag(nkb_op *op, double *diag, int flags, void *stream)
+{
+    ClearError();
+    if (!op || !diag)
+        return SetError(NKB_ERR_INVALID, "nkb_op_helmholtz_diag: NULL argument");
+    if (op->precision != NKB_FP64)
+        return SetError(NKB_ERR_INVALID, "nkb_op_helmholtz_diag: needs an FP64 operator");
+    NKB_CUDA_TRY(cudaSetDevice(op->device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : op->stream;
+    const size_t n = size_t(op->nelmt) * op->nc;
+    if (flags & NKB_HOST_PTRS)
+    {
+        int rc = EnsureScratch(op, n * sizeof(double));
+        if (rc)
+            return rc;
+        double *d = static_cast<double *>(op->scratch);
+        if ((rc = HelmholtzDiag(op, d, s)))
+            return rc;
+        NKB_CUDA_TRY(cudaMemcpyAsync(diag, d, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        NKB_CUDA_TRY(cudaStreamSynchronize(s));
+        return NKB_OK;
+    }
+    return HelmholtzDiag(op, diag, s);
+}
+
+extern "C" void nkb_op_destroy(nkb_op *op)
+{
+    if (!op)
+        return;
+    cudaSetDevice(op->device);
+    for (int d = 0; d < 3; ++d)
+    {
+        cudaFree(op->dB[d]);
+        cudaFree(op->fB[d]);
+        cudaFree(op->dD[d]);
+        cudaFree(op->fD[d]);
+        cudaFree(op->dz[d]);
+        cudaFree(op->dw[d]);
+    }
+    cudaFree(op->djac);
+    cudaFree(op->ddf);
+    cudaFree(op->geo);
+    cudaFree(op->geo32);
+    cudaFree(op->scratch);
+    FreeKernelData(op);
+    if (op->ev0)
+        cudaEventDestroy(op->ev0);
+    if (op->ev1)
+        cudaEventDestroy(op->ev1);
+    if (op->stream)
+        cudaStreamDestroy(op->stream);
+    delete op;
+}

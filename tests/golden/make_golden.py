@@ -1,0 +1,127 @@
+"""Generate the golden fixtures of tests/golden/*.npz from the reference's own
+MatrixFreeOps kernels and Polylib, compiled in place into oracle/_ref by
+`make -C oracle ref` (this needs the reference source tree, so it runs where
+the reference is mounted; the fixtures are committed and travel instead).
+
+    python tests/golden/make_golden.py
+
+Every case stores its seeded inputs, the reference-generated 1-D tables and
+the reference kernels' outputs. Inputs follow the pattern of the reference's
+Collections unit tests (TestHexCollection.cpp:4334-4605 and the Tet/Prism
+analogues): a few elements, coefficients i+1 or seeded uniform[-1,1] values,
+lambda = 1.5, regular and deformed geometry.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import ref  # noqa: E402
+
+SPEC = {
+    "hex": [(ref.MOD_A, ref.GLL, 0)] * 3,
+    "prism": [(ref.MOD_A, ref.GLL, 0), (ref.MOD_A, ref.GLL, 0), (ref.MOD_B, ref.RADAU_A1, -1)],
+    "tet": [(ref.MOD_A, ref.GLL, 0), (ref.MOD_B, ref.RADAU_A1, -1), (ref.MOD_C, ref.RADAU_A2, -1)],
+}
+
+
+def ref_tables(shape, nm, nq0):
+    T = {"b": [], "db": [], "w": [], "ws": [], "z": [], "D": [], "ptype": []}
+    nq = []
+    for bt, pt, dq in SPEC[shape]:
+        n = nq0 + dq
+        z, w, D = ref.points(pt, n)
+        b, db = ref.basis(bt, nm, pt, n)
+        for k, v in (("b", b), ("db", db), ("w", w), ("ws", w * ref.weight_factor(pt)),
+                     ("z", z), ("D", D), ("ptype", pt)):
+            T[k].append(v)
+        nq.append(n)
+    return T, tuple(nq)
+
+
+def ncoeffs(shape, nm):
+    return {"hex": nm ** 3, "prism": nm * nm * (nm + 1) // 2,
+            "tet": nm * (nm + 1) * (nm + 2) // 6}[shape]
+
+
+def make_case(shape, nm, nq0, deformed, seed, ne=3):
+    rng = np.random.default_rng(seed)
+    T, nq = ref_tables(shape, nm, nq0)
+    nt = nq[0] * nq[1] * nq[2]
+    nc = ncoeffs(shape, nm)
+    ncol = ne * nt if deformed else ne
+    jac = rng.uniform(0.5, 1.5, ncol)
+    df = rng.uniform(-1.0, 1.0, (9, ncol))
+    x = np.arange(1, ne * nc + 1, dtype=np.float64)
+    x_rand = rng.uniform(-1.0, 1.0, ne * nc)
+    f = rng.uniform(-1.0, 1.0, ne * nt)
+    # the harness takes weights already scaled as MatrixFree SetUpZW scales them
+    T = dict(T)
+    T["w_raw"], T["w"] = T["w"], T["ws"]
+    out = {}
+    op = ref.RefOp(shape, "bwdtrans", nm, nq, ne, T)
+    y = np.zeros(ne * nt)
+    op.apply(x_rand, y)
+    out["bwdtrans"] = y
+    op = ref.RefOp(shape, "iproduct", nm, nq, ne, T, jac=jac, deformed=deformed)
+    y = np.zeros(ne * nc)
+    op.apply(f, y)
+    out["iproduct"] = y
+    op = ref.RefOp(shape, "physderiv", nm, nq, ne, T, df=df, deformed=deformed)
+    d = [np.zeros(ne * nt) for _ in range(3)]
+    op.apply(f, *d)
+    out["physderiv"] = np.stack(d)
+    diff = np.array([1.3, 0.2, 0.9, 0.1, -0.3, 1.1])
+    for mode, tag in ((0, "helmholtz"), (1, "helmholtz_constdiff"), (2, "helmholtz_vardiff")):
+        op = ref.RefOp(shape, "helmholtz", nm, nq, ne, T, jac=jac, df=df, deformed=deformed)
+        op.set_factors(1.5, const_diff=diff if mode == 1 else None,
+                       var_diff=diff if mode == 2 else None)
+        y = np.zeros(ne * nc)
+        op.apply(x, y)
+        out[tag] = y
+    arrays = {"nq": np.array(nq), "nm": np.array(nm), "ne": np.array(ne),
+              "deformed": np.array(int(deformed)), "jac": jac, "df": df, "x": x,
+              "x_rand": x_rand, "f": f, "lam": np.array(1.5), "diff": diff,
+              "ptype": np.array(T["ptype"])}
+    for k, src in (("b", "b"), ("db", "db"), ("w", "w_raw"), ("ws", "ws"), ("z", "z"),
+                   ("D", "D")):
+        for dd in range(3):
+            arrays["%s%d" % (k, dd)] = T[src][dd]
+    for k, v in out.items():
+        arrays["out_" + k] = v
+    return arrays
+
+
+CASES = [(s, nm, nm + 1, dfm) for s in ("hex", "prism", "tet") for nm in (2, 3, 5)
+         for dfm in (False, True)]
+
+
+def main():
+    for shape, nm, nq0, deformed in CASES:
+        name = "%s_nm%d_nq%d_%s.npz" % (shape, nm, nq0, "deformed" if deformed else "regular")
+        arrays = make_case(shape, nm, nq0, deformed, seed=1000 * nm + nq0 + int(deformed))
+        np.savez_compressed(os.path.join(HERE, name), **arrays)
+        print("wrote", name)
+    # quadrature / basis known answers from the reference Polylib
+    pts = {}
+    for pt in (ref.GLL, ref.RADAU_A1, ref.RADAU_A2):
+        for n in range(2, 14):
+            z, w, D = ref.points(pt, n)
+            pts["z_%d_%d" % (pt, n)] = z
+            pts["w_%d_%d" % (pt, n)] = w
+            pts["D_%d_%d" % (pt, n)] = D
+    for bt, pt in ((ref.MOD_A, ref.GLL), (ref.MOD_B, ref.RADAU_A1), (ref.MOD_C, ref.RADAU_A2)):
+        for nm in range(2, 12):
+            n = nm + 1
+            b, db = ref.basis(bt, nm, pt, n)
+            pts["b_%d_%d" % (bt, nm)] = b
+            pts["db_%d_%d" % (bt, nm)] = db
+    np.savez_compressed(os.path.join(HERE, "polylib_basis.npz"), **pts)
+    print("wrote polylib_basis.npz")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,86 @@
+"""Global Helmholtz solve on the device (GlobalLinSysIterativeFull + diagonal
+preconditioner + NekLinSysIterCG) against the oracle's CG, and against a
+manufactured solution."""
+import numpy as np
+import pytest
+
+import nektar_b200 as nb
+from oracle import oracle as O
+from tests.helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(n, nm, amp, lam=1.0):
+    m = nb.BoxMesh("hex", n, nm, nm + 1, amp=amp, coords=True)
+    gmap, nglob, ndir = m.assembly()
+    op = nb.Operator("helmholtz", m)
+    op.set_factors(lam)
+    return m, op, nb.GlobalLinSys([op], gmap, nglob, ndir), gmap, nglob, ndir
+
+
+def test_diagonal_preconditioner_matches_oracle():
+    m, op, S, gmap, nglob, ndir = _system(3, 4, 0.05, 1.0)
+    T = dict(m.T)
+    T["w"] = m.T["ws"]
+    dloc = O.helmholtz_diag("hex", m.nm, m.nq, m.nelmt, T, m.jac, m.df, 1.0, True)
+    dinv = 1.0 / O.assemble(gmap, None, dloc, nglob)[ndir:]
+    assert rel_l2(S.diag_inv(), dinv) < 1e-12
+
+
+@pytest.mark.parametrize("n,nm", [(3, 4), (4, 5)])
+def test_cg_matches_oracle_cg(n, nm):
+    lam = 1.0
+    m, op, S, gmap, nglob, ndir = _system(n, nm, 0.05, lam)
+    rng = np.random.default_rng(n)
+    b_loc = rng.uniform(-1, 1, m.nelmt * m.nc)
+    x_loc, rep = S.solve(b_loc, tol=1e-10, check_interval=4)
+    assert rep.converged and rep.rel_residual < 1e-10
+    T = dict(m.T)
+    T["w"] = m.T["ws"]
+    b_glob = O.assemble(gmap, None, b_loc, nglob)
+    dinv = S.diag_inv()
+    x_o, it_o, err_o = O.pcg("hex", nm, m.nq, m.nelmt, T, m.jac, m.df, lam, True, nglob, ndir,
+                             gmap, None, dinv, b_glob, tol=1e-10)
+    assert abs(rep.iterations - it_o) <= max(3, int(0.03 * it_o)), (rep.iterations, it_o)
+    assert rel_l2(x_loc, O.global_to_local(gmap, None, x_o)) < 1e-9
+    x_loc2, _ = S.solve(b_loc, tol=1e-13, check_interval=8)
+    x_o2, _, _ = O.pcg("hex", nm, m.nq, m.nelmt, T, m.jac, m.df, lam, True, nglob, ndir, gmap,
+                       None, dinv, b_glob, tol=1e-13)
+    assert rel_l2(x_loc2, O.global_to_local(gmap, None, x_o2)) < 1e-11
+
+
+def test_cg_graph_and_direct_launch_agree_bitwise():
+    m, op, S, gmap, nglob, ndir = _system(3, 4, 0.05)
+    b = np.random.default_rng(7).uniform(-1, 1, m.nelmt * m.nc)
+    x1, r1 = S.solve(b, tol=1e-10, use_graph=True, check_interval=5)
+    x2, r2 = S.solve(b, tol=1e-10, use_graph=False, check_interval=3)
+    assert r1.iterations == r2.iterations
+    assert np.array_equal(x1, x2)  # deterministic reductions, no atomics
+
+
+def test_manufactured_solution():
+    """-lap u + lambda u = f, u = sin(pi x) sin(pi y) sin(pi z) on the curved
+    unit cube (the map fixes the boundary, so the Dirichlet data are zero).
+    Nektar solves L + lambda M with RHS -(g, phi) for forcing g = -f
+    (ContField.cpp:813-816), i.e. the local RHS is IProductWRTBase(f)."""
+    lam = 1.0
+    errs = []
+    for nm in (4, 6):
+        m, op, S, gmap, nglob, ndir = _system(3, nm, 0.05, lam)
+        x, y, z = m.xyz
+        u = np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z)
+        f = (3 * np.pi ** 2 + lam) * u
+        b_loc = nb.Operator("iproduct", m)(f)
+        c_loc, rep = S.solve(b_loc, tol=1e-12)
+        uh = nb.Operator("bwdtrans", m)(c_loc)
+        errs.append(np.sqrt(np.mean((uh - u) ** 2)))
+    assert errs[0] < 2e-3 and errs[1] < errs[0] / 20, errs
+
+
+def test_maxit_is_reported():
+    m, op, S, gmap, nglob, ndir = _system(3, 4, 0.05)
+    b = np.random.default_rng(2).uniform(-1, 1, m.nelmt * m.nc)
+    with pytest.raises(nb.NektarB200Error) as e:
+        S.solve(b, tol=1e-14, maxit=5)
+    assert e.value.code == nb.C.NKB_ERR_NOT_CONVERGED
