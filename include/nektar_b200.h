@@ -145,7 +145,8 @@ int nkb_op_set_factors(nkb_op *op, double lambda, int diff_mode, const double *d
 /* Replaces Collections::Operator::operator()(in, out0, out1, out2, wsp)
  * (Operator.h:148-152): out0 is overwritten (no accumulate); PhysDeriv
  * writes d/dx, d/dy, d/dz to out0, out1, out2. flags: NKB_HOST_PTRS or
- * NKB_DEVICE_PTRS; stream: a cudaStream_t (NULL = legacy default). With
+ * NKB_DEVICE_PTRS; stream: a cudaStream_t (NULL = the legacy default
+ * stream), on which the kernel is enqueued. With
  * host pointers the result is in out0.. on return, as the reference's is. */
 int nkb_op_apply(nkb_op *op, const double *in, double *out0, double *out1, double *out2,
                  int flags, void *stream);
@@ -207,6 +208,7 @@ typedef struct nkb_cg_report
     double rel_residual;  /* sqrt(eps / rhs_magnitude) as NekLinSysIterCG reports */
     int converged;
     double device_ms;     /* device time of the solve (CUDA events) */
+    long kernel_launches; /* kernels of this library launched by the solve */
 } nkb_cg_report;
 
 int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **sys);
@@ -214,7 +216,9 @@ int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **sys);
 /* GlobalLinSysIterativeFull::v_Solve with Dirichlet lifting: b_loc is the
  * local right-hand side (pLocInput), x_loc on input holds the Dirichlet
  * values in local layout (ContField::v_ImposeDirichletConditions) and zeros
- * elsewhere, on output the solution (pLocOutput). flags as nkb_op_apply. */
+ * elsewhere, on output the solution (pLocOutput). flags as nkb_op_apply.
+ * The solve runs on `stream`, or on the system's own stream when it is NULL,
+ * and returns once it has finished (the host polls convergence). */
 int nkb_cg_solve(nkb_sys *sys, const double *b_loc, double *x_loc, const nkb_cg_opts *opts,
                  nkb_cg_report *report, int flags, void *stream);
 
@@ -227,6 +231,21 @@ int nkb_sys_matvec_local(nkb_sys *sys, const double *x_loc, double *y_loc, void 
 
 /* Inverse assembled diagonal (nglob - ndir entries) the preconditioner uses. */
 int nkb_sys_diag_inv(nkb_sys *sys, double *diag_inv, int flags, void *stream);
+
+/* Per-kernel device time of one CG iteration, averaged over `iters`
+ * back-to-back launches of each kernel on the system's stream with the
+ * current vectors (CUDA events): element operators with the fused gather,
+ * assemble + (s,w) dot, update + preconditioner + (r,w),(r,r) dots, scalars.
+ * No counterpart in the reference (its LIKWID regions time the same phases,
+ * NekLinSysIterCG.cpp:207-276). */
+typedef struct nkb_sys_profile
+{
+    double op_ms, assemble_ms, update_ms, scalars_ms;
+    double op_bytes;    /* algorithmic bytes of one operator pass */
+    double op_flops;    /* algorithmic flops of one operator pass */
+} nkb_sys_profile;
+
+int nkb_sys_profile_iteration(nkb_sys *sys, int iters, nkb_sys_profile *prof);
 
 void nkb_sys_destroy(nkb_sys *sys);
 

@@ -268,6 +268,22 @@ class GlobalLinSys:
                                  ctypes.byref(rep), DEVICE_PTRS, stream))
         return rep
 
+    def solve_host_ptrs(self, b_ptr, x_ptr, tol=1e-9, maxit=5000, check_interval=16,
+                        use_graph=True, stream=None):
+        """Host (ideally pinned) buffers by address: copies in and out inside
+        the call, on `stream`."""
+        rep = C.CGReport()
+        check(lib().nkb_cg_solve(self.h, b_ptr, x_ptr,
+                                 ctypes.byref(self._opts(tol, maxit, check_interval, use_graph)),
+                                 ctypes.byref(rep), HOST_PTRS, stream))
+        return rep
+
+    def profile(self, iters=20):
+        """Per-kernel device time of one CG iteration (CUDA events)."""
+        p = C.SysProfile()
+        check(lib().nkb_sys_profile_iteration(self.h, iters, ctypes.byref(p)))
+        return {k: getattr(p, k) for k, _ in C.SysProfile._fields_}
+
     def diag_inv(self):
         out = np.zeros(self.nglob - self.ndir)
         check(lib().nkb_sys_diag_inv(self.h, out.ctypes.data, HOST_PTRS, None))

@@ -53,7 +53,12 @@ class CGOpts(ctypes.Structure):
 
 class CGReport(ctypes.Structure):
     _fields_ = [("iterations", c_int), ("outer_iterations", c_int), ("rel_residual", c_double),
-                ("converged", c_int), ("device_ms", c_double)]
+                ("converged", c_int), ("device_ms", c_double), ("kernel_launches", c_long)]
+
+
+class SysProfile(ctypes.Structure):
+    _fields_ = [("op_ms", c_double), ("assemble_ms", c_double), ("update_ms", c_double),
+                ("scalars_ms", c_double), ("op_bytes", c_double), ("op_flops", c_double)]
 
 
 class GeomRequest(ctypes.Structure):
@@ -82,6 +87,7 @@ SIGNATURES = {
     "nkb_sys_global_to_local": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "nkb_sys_matvec_local": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "nkb_sys_diag_inv": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
+    "nkb_sys_profile_iteration": (c_int, [c_void_p, c_int, P(SysProfile)]),
     "nkb_sys_destroy": (None, [c_void_p]),
     "nkb_geom_nelmt": (c_long, [P(GeomRequest)]),
     "nkb_geom_fill": (c_int, [P(GeomRequest), dp, dp, dp]),

@@ -313,6 +313,7 @@ struct nkb_sys
     int graph_k = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double *stage = nullptr; // host-pointer staging (2*nloc)
+    long launches = 0;       // kernels launched by the current solve
 };
 
 namespace nkb
@@ -320,7 +321,8 @@ namespace nkb
 
 // y_loc = A x_loc over all collections; x given either as a local vector or
 // as a global vector gathered through the map (gather = true).
-static int Matvec(nkb_sys *S, const double *xin, double *yl, bool gather, cudaStream_t s)
+static int Matvec(nkb_sys *S, const double *xin, double *yl, bool gather, cudaStream_t s,
+                  const int *skip = nullptr)
 {
     for (size_t c = 0; c < S->ops.size(); ++c)
     {
@@ -329,9 +331,9 @@ static int Matvec(nkb_sys *S, const double *xin, double *yl, bool gather, cudaSt
         int rc;
         if (gather)
             rc = LaunchOp<double>(op, xin, yl + o, nullptr, nullptr, S->d_map + o,
-                                  S->d_sign ? S->d_sign + o : nullptr, s);
+                                  S->d_sign ? S->d_sign + o : nullptr, s, skip);
         else
-            rc = LaunchOp<double>(op, xin + o, yl + o, nullptr, nullptr, nullptr, nullptr, s);
+            rc = LaunchOp<double>(op, xin + o, yl + o, nullptr, nullptr, nullptr, nullptr, s, skip);
         if (rc)
             return rc;
     }
@@ -341,9 +343,10 @@ static int Matvec(nkb_sys *S, const double *xin, double *yl, bool gather, cudaSt
 static int Iteration(nkb_sys *S, cudaStream_t s)
 {
     const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
+    S->launches += 3 + long(S->ops.size());
     k_update<double><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st, S->p, S->q, S->x, S->r,
                                                  S->w, S->s, S->d_dinv, S->partA);
-    int rc = Matvec(S, S->w, S->yl, true, s);
+    int rc = Matvec(S, S->w, S->yl, true, s, &S->st->done);
     if (rc)
         return rc;
     k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
@@ -530,6 +533,7 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
     if (o.mixed)
         return SetError(NKB_ERR_UNSUPPORTED, "nkb_cg_solve: mixed precision not built in");
     NKB_CUDA_TRY(cudaSetDevice(S->device));
+    // NULL (or the legacy default stream) -> the system's own stream
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : S->stream;
     const long nloc = S->nloc;
 
@@ -545,6 +549,7 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
         dx = S->stage + nloc;
     }
     NKB_CUDA_TRY(cudaEventRecord(S->ev0, s));
+    S->launches = 0;
 
     // Dirichlet lifting (GlobalLinSysIterativeFull.cpp:104-164):
     // rhs = b - A x_D (local), gloIn = Assemble(rhs)
@@ -574,17 +579,19 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
                                                    S->d_sign, S->yl, S->s, S->w, S->st, S->partB);
     k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbU, S->partB, nbA, 1);
     NKB_CUDA_TRY(cudaGetLastError());
+    // lift (ops + sub + assemble), init, scalars, precon, ops, assemble, scalars
+    S->launches += 2 * long(S->ops.size()) + 7;
 
     const int K = o.check_interval;
     bool use_graph = o.use_graph != 0;
-    if (use_graph && (S->graph == nullptr || S->graph_k != K || s != S->stream))
+    if (use_graph && (S->graph == nullptr || S->graph_k != K))
     {
         if (S->graph)
         {
             cudaGraphExecDestroy(S->graph);
             S->graph = nullptr;
         }
-        if (s == S->stream)
+        if (s != cudaStreamLegacy && s != cudaStreamPerThread)
         {
             cudaGraph_t g;
             NKB_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -601,6 +608,7 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
             if (ce != cudaSuccess)
                 return SetError(NKB_ERR_CUDA, "nkb_cg_solve: graph instantiate: %s", cudaGetErrorString(ce));
             S->graph_k = K;
+            S->launches -= long(K) * (3 + long(S->ops.size())); // captured, not launched
         }
         else
         {
@@ -619,6 +627,7 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
         if (use_graph)
         {
             NKB_CUDA_TRY(cudaGraphLaunch(S->graph, s));
+            S->launches += long(K) * (3 + long(S->ops.size()));
         }
         else
         {
@@ -631,6 +640,7 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
     // x_loc += GlobalToLocal(x) (the Dirichlet part of x is zero)
     k_global_to_local<<<Blocks(nloc), kRedThreads, 0, s>>>(nloc, S->d_map, S->d_sign, S->x, S->tl);
     k_axpy_loc<<<Blocks(nloc), kRedThreads, 0, s>>>(nloc, 1.0, S->tl, dx);
+    S->launches += 2;
     NKB_CUDA_TRY(cudaEventRecord(S->ev1, s));
     if (flags & NKB_HOST_PTRS)
         NKB_CUDA_TRY(cudaMemcpyAsync(x_loc, dx, nloc * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -644,7 +654,8 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
         rep->converged        = (h.done && h.status == NKB_OK) ? 1 : 0;
         float ms              = 0.f;
         cudaEventElapsedTime(&ms, S->ev0, S->ev1);
-        rep->device_ms = ms;
+        rep->device_ms       = ms;
+        rep->kernel_launches = S->launches;
     }
     if (h.status == NKB_ERR_NONFINITE)
         return SetError(NKB_ERR_NONFINITE, "nkb_cg_solve: non-finite CG scalar at iteration %d", h.iter);
@@ -652,6 +663,88 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
         return SetError(NKB_ERR_NOT_CONVERGED,
                         "nkb_cg_solve: CG iterations made = %d exceeded maxit (error = %g)", h.iter,
                         std::sqrt(h.eps / h.rhs_mag));
+    return NKB_OK;
+}
+
+extern "C" int nkb_sys_profile_iteration(nkb_sys *S, int iters, nkb_sys_profile *prof)
+{
+    ClearError();
+    if (!S || !prof || iters < 1)
+        return SetError(NKB_ERR_INVALID, "nkb_sys_profile_iteration: bad arguments");
+    NKB_CUDA_TRY(cudaSetDevice(S->device));
+    cudaStream_t s = S->stream;
+    const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
+    cudaEvent_t e[5];
+    for (auto &ev : e)
+        NKB_CUDA_TRY(cudaEventCreate(&ev));
+    // the kernels read the live state; make sure they run (done = 0) on a copy
+    CGState h;
+    NKB_CUDA_TRY(cudaMemcpy(&h, S->st, sizeof(h), cudaMemcpyDeviceToHost));
+    CGState run = h;
+    run.done    = 0;
+    run.maxit   = 1 << 30;
+    NKB_CUDA_TRY(cudaMemcpy(S->st, &run, sizeof(run), cudaMemcpyHostToDevice));
+    int rc = NKB_OK;
+    NKB_CUDA_TRY(cudaEventRecord(e[0], s));
+    for (int it = 0; it < iters && !rc; ++it)
+        rc = Matvec(S, S->w, S->yl, true, s);
+    NKB_CUDA_TRY(cudaEventRecord(e[1], s));
+    for (int it = 0; it < iters; ++it)
+        k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
+                                                       S->d_sign, S->yl, S->s, S->w, S->st,
+                                                       S->partB);
+    NKB_CUDA_TRY(cudaEventRecord(e[2], s));
+    // the update kernel with alpha = beta = 0 leaves x unchanged and w = dinv r
+    CGState zero = run;
+    zero.alpha = zero.beta = 0.0;
+    NKB_CUDA_TRY(cudaStreamSynchronize(s));
+    NKB_CUDA_TRY(cudaMemcpy(S->st, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+    NKB_CUDA_TRY(cudaEventRecord(e[2], s));
+    for (int it = 0; it < iters; ++it)
+        k_update<double><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st, S->p, S->q, S->x,
+                                                     S->r, S->w, S->s, S->d_dinv, S->partA);
+    NKB_CUDA_TRY(cudaEventRecord(e[3], s));
+    NKB_CUDA_TRY(cudaStreamSynchronize(s));
+    cudaEvent_t e4, e5;
+    NKB_CUDA_TRY(cudaEventCreate(&e4));
+    NKB_CUDA_TRY(cudaEventCreate(&e5));
+    NKB_CUDA_TRY(cudaEventRecord(e4, s));
+    for (int it = 0; it < iters; ++it)
+        k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbU, S->partB, nbA, 2);
+    NKB_CUDA_TRY(cudaEventRecord(e5, s));
+    NKB_CUDA_TRY(cudaStreamSynchronize(s));
+    NKB_CUDA_TRY(cudaGetLastError());
+    float t01 = 0, t12 = 0, t23 = 0, t45 = 0;
+    cudaEventElapsedTime(&t01, e[0], e[1]);
+    cudaEventElapsedTime(&t12, e[1], e[2]);
+    cudaEventElapsedTime(&t23, e[2], e[3]);
+    cudaEventElapsedTime(&t45, e4, e5);
+    for (auto &ev : e)
+        cudaEventDestroy(ev);
+    cudaEventDestroy(e4);
+    cudaEventDestroy(e5);
+    // restore the state of the last solve
+    NKB_CUDA_TRY(cudaMemcpy(S->st, &h, sizeof(h), cudaMemcpyHostToDevice));
+    if (rc)
+        return rc;
+    prof->op_ms       = t01 / iters;
+    prof->assemble_ms = t12 / iters;
+    prof->update_ms   = t23 / iters;
+    prof->scalars_ms  = t45 / iters;
+    double bytes = 0.0, flops = 0.0;
+    for (const nkb_op *op : S->ops)
+    {
+        const double nq = op->nq[0], nm = op->nm;
+        // geometry (7 values per point), coefficients in through the int32
+        // map, coefficients out
+        bytes += double(op->nelmt) * (8.0 * 7.0 * op->nt + 20.0 * op->nc);
+        if (op->shape == NKB_HEX)
+            flops += double(op->nelmt) *
+                     (4.0 * (nq * nm * nm * nm + nq * nq * nm * nm + nq * nq * nq * nm) +
+                      12.0 * nq * nq * nq * nq + 18.0 * nq * nq * nq);
+    }
+    prof->op_bytes = bytes;
+    prof->op_flops = flops;
     return NKB_OK;
 }
 

@@ -13,6 +13,7 @@ struct nkb_op
     int shape = 0, optype = 0, nm = 0, nq[3] = {0, 0, 0}, ptype[3] = {0, 0, 0};
     int nelmt = 0, deformed = 0, precision = 0, device = 0;
     int nc = 0, nt = 0, ncomp = 0;
+    long gstride = 0; // packed geometry stride per element (multiple of 4 values)
 
     // 1-D tables on the device (FP64 and FP32 copies)
     double *dB[3] = {nullptr, nullptr, nullptr};
@@ -25,7 +26,7 @@ struct nkb_op
 
     // geometry: raw (Collections layout) and packed per point
     double *djac = nullptr, *ddf = nullptr;
-    double *geo  = nullptr; // [e][ncomp][nt]
+    double *geo  = nullptr; // [e][ncomp][nt], element stride gstride
     float *geo32 = nullptr;
 
     double lambda    = 1.0;
@@ -35,6 +36,7 @@ struct nkb_op
     // kernel selection (nkb_hex.cu): 0 generic, >0 tuned variant
     int variant = 0;
     void *kdata = nullptr;
+    int *d_err  = nullptr; // device error word (bounded waits that gave up)
 
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -47,11 +49,13 @@ namespace nkb
 // generic kernels (nkb_ops.cu)
 template <typename T>
 int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
-                  const double *gsign, cudaStream_t s);
+                  const double *gsign, cudaStream_t s, const int *skip = nullptr);
 // dispatch: tuned kernel if selected, else generic (nkb_hex.cu)
+// skip: optional device flag; when it reads nonzero the kernels return at once
+// (a converged CG keeps its captured graph but stops doing work)
 template <typename T>
 int LaunchOp(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
-             const double *gsign, cudaStream_t s);
+             const double *gsign, cudaStream_t s, const int *skip = nullptr);
 int ChooseKernel(nkb_op *op);
 size_t GenericSmemBytes(const nkb_op *op, int elem_bytes);
 void FreeKernelData(nkb_op *op);

@@ -99,6 +99,7 @@ struct PackArgs
     double *geo;                  // packed FP64
     float *geo32;                 // optional FP32 copy
     int ncomp;                    // 7 Helmholtz, 9 PhysDeriv, 1 IProduct
+    long gstride;                 // element stride of the packed arrays
 };
 
 __global__ void k_pack(PackArgs a)
@@ -113,8 +114,8 @@ __global__ void k_pack(PackArgs a)
         const long ncol = a.deformed ? tot : long(a.nelmt);
         const long col  = a.deformed ? g : e;
         const double J  = a.jac ? a.jac[col] : 1.0;
-        double *out     = a.geo + e * a.ncomp * nt + q;
-        float *out32    = a.geo32 ? a.geo32 + e * a.ncomp * nt + q : nullptr;
+        double *out     = a.geo + e * a.gstride + q;
+        float *out32    = a.geo32 ? a.geo32 + e * a.gstride + q : nullptr;
         if (a.optype == NKB_IPRODUCT)
         {
             double W = J * a.w0[i] * a.w1[j] * a.w2[k];
@@ -205,7 +206,9 @@ template <typename T> struct GenArgs
     // optional gather of the input from a global vector: in[e*nc+m] = sign * gvec[map]
     const int *gmap;
     const double *gsign;
+    long gstride;
     int nelmt, epb;
+    const int *skip;
 };
 
 #define NKB_STAGE(SIZE, ...)                                                                     \
@@ -237,7 +240,7 @@ template <int SHAPE, int OP, typename T> __global__ void k_generic(GenArgs<T> a)
     const int es  = ElemSmem(d);
     const long e0 = long(blockIdx.x) * a.epb;
     const int ne  = int(min(long(a.epb), long(a.nelmt) - e0));
-    if (ne <= 0)
+    if (ne <= 0 || (a.skip && *a.skip))
         return;
     using BW = Bwd<SHAPE>;
     using IP = Ipr<SHAPE>;
@@ -282,7 +285,7 @@ template <int SHAPE, int OP, typename T> __global__ void k_generic(GenArgs<T> a)
         NKB_STAGE(d.nt, {
             T q0, q1, q2;
             Grad(d, a.t, u, l, q0, q1, q2);
-            const T *A = a.geo + e * 9 * d.nt + l;
+            const T *A = a.geo + e * a.gstride + l;
             const long o = e * d.nt + l;
             a.out0[o] = fma(A[6 * d.nt], q2, fma(A[3 * d.nt], q1, A[0] * q0));
             a.out1[o] = fma(A[7 * d.nt], q2, fma(A[4 * d.nt], q1, A[1 * d.nt] * q0));
@@ -294,7 +297,7 @@ template <int SHAPE, int OP, typename T> __global__ void k_generic(GenArgs<T> a)
     if (OP == GK_IP)
     {
         // f = W * in
-        NKB_STAGE(d.nt, { u[l] = u[l] * a.geo[e * d.nt + l]; })
+        NKB_STAGE(d.nt, { u[l] = u[l] * a.geo[e * a.gstride + l]; })
     }
 
     if (OP == GK_HELM)
@@ -303,7 +306,7 @@ template <int SHAPE, int OP, typename T> __global__ void k_generic(GenArgs<T> a)
         NKB_STAGE(d.nt, {
             T q0, q1, q2;
             Grad(d, a.t, u, l, q0, q1, q2);
-            const T *G = a.geo + e * 7 * d.nt + l;
+            const T *G = a.geo + e * a.gstride + l;
             const T W = G[0], G00 = G[d.nt], G11 = G[2 * d.nt], G22 = G[3 * d.nt];
             const T G01 = G[4 * d.nt], G02 = G[5 * d.nt], G12 = G[6 * d.nt];
             g0[l] = fma(G02, q2, fma(G01, q1, G00 * q0));
@@ -335,7 +338,7 @@ template <int SHAPE, typename T> __global__ void k_diag(GenArgs<T> a)
         return;
     using BW = Bwd<SHAPE>;
     T *x = smem, *u = x + d.nc, *wa = u + d.nt, *wb = wa + d.wsz, *red = wb + d.wsz;
-    const T *G = a.geo + e * 7 * d.nt;
+    const T *G = a.geo + e * a.gstride;
     for (int m = 0; m < d.nc; ++m)
     {
         for (int l = threadIdx.x; l < d.nc; l += blockDim.x)
@@ -456,7 +459,7 @@ template <int OP, typename T> static int LaunchGenericShape(const nkb_op *op, Ge
 
 template <typename T>
 int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
-                  const double *gsign, cudaStream_t s)
+                  const double *gsign, cudaStream_t s, const int *skip)
 {
     GenArgs<T> a;
     a.d      = MakeDims(op);
@@ -469,8 +472,10 @@ int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int 
     a.out2   = o2;
     a.gmap   = gmap;
     a.gsign  = gsign;
+    a.gstride = op->gstride;
     a.nelmt  = op->nelmt;
     a.epb    = 1;
+    a.skip   = skip;
     switch (op->optype)
     {
         case NKB_BWDTRANS:
@@ -485,9 +490,9 @@ int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int 
 }
 
 template int LaunchGeneric<double>(const nkb_op *, const double *, double *, double *, double *,
-                                   const int *, const double *, cudaStream_t);
+                                   const int *, const double *, cudaStream_t, const int *);
 template int LaunchGeneric<float>(const nkb_op *, const float *, float *, float *, float *,
-                                  const int *, const double *, cudaStream_t);
+                                  const int *, const double *, cudaStream_t, const int *);
 
 static int Repack(nkb_op *op)
 {
@@ -512,9 +517,10 @@ static int Repack(nkb_op *op)
     a.diff_mode = op->diff_mode;
     for (int c = 0; c < 6; ++c)
         a.K[c] = op->diff[c];
-    a.geo   = op->geo;
-    a.geo32 = op->geo32;
-    a.ncomp = op->ncomp;
+    a.geo     = op->geo;
+    a.geo32   = op->geo32;
+    a.ncomp   = op->ncomp;
+    a.gstride = op->gstride;
     if (op->ncomp == 0)
         return NKB_OK;
     long tot = long(op->nelmt) * op->nt;
@@ -630,6 +636,9 @@ extern "C" int nkb_op_create(const nkb_op_desc *desc, nkb_op **out)
     op->nc = NumCoeffs(shape, nm);
     op->nt = nq[0] * nq[1] * nq[2];
     op->ncomp = (opt == NKB_HELMHOLTZ) ? 7 : (opt == NKB_PHYSDERIV ? 9 : (opt == NKB_IPRODUCT ? 1 : 0));
+    // element blocks of the packed geometry start on 32-byte boundaries so a
+    // bulk (TMA) copy of one element is legal in FP64 and FP32
+    op->gstride = (long(op->ncomp) * op->nt + 3) & ~3L;
     int rc = NKB_OK;
     auto fail = [&](int code) {
         nkb_op_destroy(op);
@@ -638,6 +647,9 @@ extern "C" int nkb_op_create(const nkb_op_desc *desc, nkb_op **out)
     if (cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&op->ev0) != cudaSuccess || cudaEventCreate(&op->ev1) != cudaSuccess)
         return fail(SetError(NKB_ERR_CUDA, "nkb_op_create: stream/event creation failed"));
+    if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess ||
+        cudaMemset(op->d_err, 0, sizeof(int)) != cudaSuccess)
+        return fail(SetError(NKB_ERR_CUDA, "nkb_op_create: error word"));
 
     // 1-D tables
     for (int d = 0; d < 3; ++d)
@@ -673,7 +685,7 @@ extern "C" int nkb_op_create(const nkb_op_desc *desc, nkb_op **out)
             return fail(rc);
     if (op->ncomp && op->nelmt)
     {
-        const size_t n = size_t(op->nelmt) * op->ncomp * op->nt;
+        const size_t n = size_t(op->nelmt) * op->gstride;
         if (cudaMalloc(&op->geo, n * sizeof(double)) != cudaSuccess)
             return fail(SetError(NKB_ERR_NOMEM, "nkb_op_create: geometry (%zu doubles)", n));
         if (op->precision == NKB_FP32 && cudaMalloc(&op->geo32, n * sizeof(float)) != cudaSuccess)
@@ -762,7 +774,7 @@ extern "C" int nkb_op_apply(nkb_op *op, const double *in, double *out0, double *
     if (op->optype == NKB_PHYSDERIV && (!out1 || !out2))
         return SetError(NKB_ERR_INVALID, "nkb_op_apply: PhysDeriv needs three outputs");
     NKB_CUDA_TRY(cudaSetDevice(op->device));
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : op->stream;
+    cudaStream_t s = static_cast<cudaStream_t>(stream); // NULL: legacy default stream
     long nin, nout;
     nkb_op_sizes(op, &nin, &nout);
     const int nouts = op->optype == NKB_PHYSDERIV ? 3 : 1;
@@ -805,7 +817,7 @@ extern "C" int nkb_op_apply_f32(nkb_op *op, const float *in, float *out0, float 
     if (op->precision != NKB_FP32)
         return SetError(NKB_ERR_INVALID, "nkb_op_apply_f32: operator is not FP32");
     NKB_CUDA_TRY(cudaSetDevice(op->device));
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : op->stream;
+    cudaStream_t s = static_cast<cudaStream_t>(stream); // NULL: legacy default stream
     NKB_CUDA_TRY(cudaEventRecord(op->ev0, s));
     int rc = LaunchOp<float>(op, in, out0, out1, out2, nullptr, nullptr, s);
     if (rc)
@@ -839,8 +851,10 @@ int HelmholtzDiag(const nkb_op *op, double *d_out, cudaStream_t s)
     a.out1 = a.out2 = nullptr;
     a.gmap          = nullptr;
     a.gsign         = nullptr;
+    a.gstride       = op->gstride;
     a.nelmt         = op->nelmt;
     a.epb           = 1;
+    a.skip          = nullptr;
     const int threads = 128;
     size_t smem = size_t(a.d.nc + a.d.nt + 2 * a.d.wsz + threads) * sizeof(double);
     void (*kern)(GenArgs<double>) = op->shape == NKB_HEX     ? k_diag<NKB_HEX, double>
@@ -862,7 +876,7 @@ extern "C" int nkb_op_helmholtz_diag(nkb_op *op, double *diag, int flags, void *
     if (op->precision != NKB_FP64)
         return SetError(NKB_ERR_INVALID, "nkb_op_helmholtz_diag: needs an FP64 operator");
     NKB_CUDA_TRY(cudaSetDevice(op->device));
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : op->stream;
+    cudaStream_t s = static_cast<cudaStream_t>(stream); // NULL: legacy default stream
     const size_t n = size_t(op->nelmt) * op->nc;
     if (flags & NKB_HOST_PTRS)
     {
@@ -898,6 +912,7 @@ extern "C" void nkb_op_destroy(nkb_op *op)
     cudaFree(op->geo);
     cudaFree(op->geo32);
     cudaFree(op->scratch);
+    cudaFree(op->d_err);
     FreeKernelData(op);
     if (op->ev0)
         cudaEventDestroy(op->ev0);

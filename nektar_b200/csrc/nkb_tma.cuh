@@ -1,0 +1,80 @@
+// Bulk (TMA) copies into shared memory completed through an mbarrier, for
+// sm_100a. Untiled cp.async.bulk from this GPU's own global memory into the
+// issuing CTA's shared memory; no cluster multicast anywhere.
+//
+// Rules kept by the callers: source and destination 16-byte aligned, size a
+// multiple of 16 bytes. Every wait is bounded: after kMaxPolls failed polls
+// the waiter records an error word, keeps waiting for at most the same
+// bound again so no copy is left writing into shared memory of a CTA that
+// has exited, and then returns false.
+#pragma once
+
+#include <cstdint>
+
+namespace nkb
+{
+
+constexpr unsigned kMaxPolls = 1u << 24; // try_wait polls (each may suspend briefly)
+
+__device__ __forceinline__ uint32_t SmemAddr(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void MbarInit(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(bar)), "r"(count)
+                 : "memory");
+    // make the initialised barrier visible to the async (TMA) proxy
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void MbarInval(uint64_t *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(SmemAddr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void MbarArriveExpectTx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(SmemAddr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// global -> shared bulk copy, completion counted on bar (bytes % 16 == 0)
+__device__ __forceinline__ void BulkG2S(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], "
+                 "%2, [%3];" ::"r"(SmemAddr(dst)),
+                 "l"(src), "r"(bytes), "r"(SmemAddr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool MbarTryWait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(SmemAddr(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for phase `parity` of bar. Returns true when the phase
+// completed; false (with *err set) when it did not within two bounds.
+__device__ __forceinline__ bool MbarWaitBounded(uint64_t *bar, uint32_t parity, int *err, int code)
+{
+    for (unsigned n = 0; n < kMaxPolls; ++n)
+        if (MbarTryWait(bar, parity))
+            return true;
+    if (err)
+        atomicExch(err, code);
+    for (unsigned n = 0; n < kMaxPolls; ++n)
+        if (MbarTryWait(bar, parity))
+            return false;
+    return false;
+}
+
+} // namespace nkb

@@ -1,0 +1,53 @@
+"""Micro-benchmark of one element operator on a curved box (device-resident
+input, CUDA-event timing), used for profiling captures:
+
+    python -m nektar_b200.opbench --op helmholtz --shape hex --n 24 --p 6 --iters 20
+"""
+import argparse
+import json
+
+import numpy as np
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--op", default="helmholtz")
+    ap.add_argument("--shape", default="hex")
+    ap.add_argument("--n", type=int, default=24)
+    ap.add_argument("--p", type=int, default=6)
+    ap.add_argument("--amp", type=float, default=0.05)
+    ap.add_argument("--precision", default="fp64")
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--iters", type=int, default=20)
+    a = ap.parse_args()
+    import torch
+
+    import nektar_b200 as nb
+    nm = a.p + 1
+    m = nb.BoxMesh(a.shape, a.n, nm, nm + 1, amp=a.amp)
+    op = nb.Operator(a.op, m, precision=a.precision)
+    dt = torch.float64 if a.precision == "fp64" else torch.float32
+    x = torch.rand(op.in_size, dtype=dt, device="cuda")
+    outs = [torch.empty(op.out_size, dtype=dt, device="cuda")
+            for _ in range(3 if a.op == "physderiv" else 1)]
+    ptrs = [o.data_ptr() for o in outs] + [None] * (3 - len(outs))
+    s = torch.cuda.Stream()
+    for _ in range(a.warmup):
+        op.apply_device(x.data_ptr(), *ptrs, stream=s.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(a.iters):
+        op.apply_device(x.data_ptr(), *ptrs, stream=s.cuda_stream)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.iters
+    ncomp = {"helmholtz": 7, "physderiv": 9, "iproduct": 1, "bwdtrans": 0}[a.op]
+    esz = 8 if a.precision == "fp64" else 4
+    byts = m.nelmt * esz * (ncomp * m.nt + (op.in_size + len(outs) * op.out_size) / m.nelmt)
+    print(json.dumps({"op": a.op, "shape": a.shape, "n": a.n, "P": a.p, "nelmt": m.nelmt,
+                      "precision": a.precision, "ms": ms, "GB_s": byts / ms / 1e6,
+                      "GDOF_s": m.nelmt * m.nc / ms / 1e6}))
+
+
+if __name__ == "__main__":
+    main()

@@ -189,3 +189,38 @@ def pcg_solve(nglob, ndir, gmap, sign, asm_ptr, asm_idx, op, diag_inv, b_glob, t
         asm_idx.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), op._apply_ptr, op.h,
         _dp(diag_inv), _dp(b_glob), _dp(x), tol, maxit, nthreads, max_iters_to_run, _dp(err))
     return x, its, float(err[0])
+
+
+def tables(shape, nm, nq0):
+    """Reference tables (reference Polylib + restated GenBasis) with weights
+    scaled as MatrixFree SetUpZW scales them, and the point counts."""
+    spec = {"hex": [(MOD_A, GLL, 0)] * 3,
+            "prism": [(MOD_A, GLL, 0), (MOD_A, GLL, 0), (MOD_B, RADAU_A1, -1)],
+            "tet": [(MOD_A, GLL, 0), (MOD_B, RADAU_A1, -1), (MOD_C, RADAU_A2, -1)]}[shape]
+    T = {"b": [], "db": [], "w": [], "z": [], "D": []}
+    nq = []
+    for bt, pt, dq in spec:
+        n = nq0 + dq
+        z, w, D = points(pt, n)
+        b, db = basis(bt, nm, pt, n)
+        for k, v in (("b", b), ("db", db), ("w", w * weight_factor(pt)), ("z", z), ("D", D)):
+            T[k].append(v)
+        nq.append(n)
+    return T, tuple(nq)
+
+
+def helmholtz_diag(op, ncoef):
+    """Diagonal of every element's Helmholtz matrix with the reference
+    kernels: apply the operator to the m-th unit vector of all elements at
+    once, for every m (the reference assembles it from dense element
+    matrices, PreconditionerDiagonal.cpp:93-125)."""
+    ne = op.nelmt
+    x = np.zeros(ne * ncoef)
+    y = np.zeros(ne * ncoef)
+    out = np.zeros(ne * ncoef)
+    for m in range(ncoef):
+        x[m::ncoef] = 1.0
+        op.apply(x, y)
+        out[m::ncoef] = y[m::ncoef]
+        x[m::ncoef] = 0.0
+    return out

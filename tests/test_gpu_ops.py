@@ -112,3 +112,17 @@ def test_device_pointer_path_matches_host_path():
     op.apply_device(xd.data_ptr(), yd.data_ptr(), stream=s.cuda_stream)
     s.synchronize()
     assert np.array_equal(yd.cpu().numpy(), yh)  # same kernel, same order: bitwise
+
+
+@pytest.mark.parametrize("n,nm", [(1, 5), (3, 7), (2, 9), (1, 11), (5, 2)])
+def test_tuned_and_generic_hex_helmholtz_agree(monkeypatch, n, nm):
+    """The tuned Hex kernel (nkb_hex.cu) against the shape-generic one, odd
+    element counts included (partially filled last CTA)."""
+    m = nb.BoxMesh("hex", n, nm, nm + 1, amp=0.05)
+    x = np.random.default_rng(nm).uniform(-1, 1, m.nelmt * m.nc)
+    tuned = nb.Operator("helmholtz", m)
+    tuned.set_factors(0.3)
+    monkeypatch.setenv("NKB_KERNEL", "generic")
+    generic = nb.Operator("helmholtz", m)
+    generic.set_factors(0.3)
+    assert rel_l2(tuned(x), generic(x)) < 1e-13

@@ -95,3 +95,17 @@ def test_hex_box_assembly_sizes_and_multiplicity():
     assert np.array_equal(e[0][1, :, :], e[9][0, :, :])
     # Dirichlet coefficients first: every boundary-face coefficient is < ndir
     assert e[0][:, :, 0].max() < nd2
+
+
+def test_product_geometry_and_assembly_match_oracle_restatement():
+    """The product's C++ setup against the oracle's numpy restatement."""
+    from oracle import mesh as OM
+    m = nb.BoxMesh("hex", 4, 5, 6, amp=0.05, coords=True)
+    jac, df, xyz = OM.hex_box_geometry(4, m.T["z"][0], 0.05)
+    assert rel_l2(m.jac, jac) < 1e-14
+    assert rel_l2(m.df, df) < 1e-13
+    assert rel_l2(m.xyz, xyz) < 1e-15
+    g, ng, nd = m.assembly()
+    go, ngo, ndo = OM.hex_box_assembly(4, 5)
+    assert (ng, nd) == (ngo, ndo)
+    assert np.array_equal(g, go)
