@@ -24,7 +24,8 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-r
               "-Xptxas", "-warn-spills"] + ARCH
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC"]
 
-SOURCES = ["nkb_setup.cpp", "nkb_ops.cu", "nkb_hex.cu", "nkb_cg.cu"]
+SOURCES = ["nkb_setup.cpp", "nkb_ops.cu", "nkb_hex.cu", "nkb_hex_f64.cu", "nkb_hex_f32.cu",
+           "nkb_cg.cu"]
 
 
 def _nvcc():

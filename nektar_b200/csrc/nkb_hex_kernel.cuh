@@ -1,0 +1,453 @@
+// The tuned Hex Helmholtz kernel template (see nkb_hex.cu for the design) and
+// its variant launcher. Included by nkb_hex_f64.cu / nkb_hex_f32.cu, which
+// instantiate it per precision, and declared for nkb_hex.cu.
+#pragma once
+
+#include "nkb_op.h"
+#include "nkb_tma.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace nkb
+{
+
+template <typename T> struct HexArgs
+{
+    const T *in;
+    T *out;
+    const int *gmap;    // optional gather (CG): in is the global vector
+    const double *gsign;
+    const T *geo;       // packed [e][7][nt], element stride gstride
+    long gstride;
+    const T *B0, *B1, *B2, *D;
+    T lambda;
+    int nelmt;
+    int *err;
+    const int *skip;    // optional: nonzero -> nothing to do (converged CG)
+};
+
+// geometry staging
+enum
+{
+    kGeoTma    = 0, // the element's whole geometry by one bulk TMA copy into shared memory
+    kGeoStream = 1  // coalesced loads into registers, one k-plane ahead
+};
+
+__host__ __device__ constexpr int RoundUp(int a, int b)
+{
+    return (a + b - 1) / b * b;
+}
+
+template <int NQ, int EPB> __host__ __device__ constexpr int HexThreads()
+{
+    return RoundUp(EPB * NQ * NQ, 32);
+}
+
+template <typename T, int NM, int NQ> constexpr int HexTabBytes()
+{
+    return RoundUp(16 + (3 * NM * NQ + NQ * (NQ + 1)) * int(sizeof(T)), 128);
+}
+
+// shared memory of one CTA (the TMA variant adds EPB element geometry blocks)
+template <typename T, int NM, int NQ, int GEO, int EPB> size_t HexSmem(long gstride)
+{
+    return size_t(HexTabBytes<T, NM, NQ>()) +
+           size_t(EPB) * ((GEO == kGeoTma ? size_t(gstride) : 0) + 3 * NQ * NQ * NQ) * sizeof(T);
+}
+
+template <typename T, int NQ, int GEO, int EPB> __host__ __device__ constexpr int HexMinBlocks()
+{
+    // resident CTAs per SM the register allocation must allow: a register
+    // budget per thread of 128 (nq <= 8), 168 (nq <= 10) or 255
+    constexpr int regs = NQ <= 8 ? 128 : (NQ <= 10 ? 168 : 255);
+    constexpr int b    = 65536 / (HexThreads<NQ, EPB>() * regs);
+    return b < 1 ? 1 : b;
+}
+
+template <typename T, int NM, int NQ, int GEO, int EPB, bool GATHER>
+__global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GEO, EPB>()))
+    k_hex_helm(HexArgs<T> a)
+{
+    constexpr int NQ2 = NQ * NQ, NQ3 = NQ2 * NQ, NC = NM * NM * NM, NQP = NQ + 1;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
+    T *sB0        = reinterpret_cast<T *>(smem + 16);
+    T *sB1        = sB0 + NM * NQ;
+    T *sB2        = sB1 + NM * NQ;
+    T *sD         = sB2 + NM * NQ; // sD[i*NQP + m] = D(i, m) = l_m'(z_i)
+    const long GS = a.gstride;
+    T *geo        = reinterpret_cast<T *>(smem + HexTabBytes<T, NM, NQ>());
+    T *us         = geo + (GEO == kGeoTma ? EPB * GS : 0);
+    T *v0s        = us + EPB * NQ3;
+    T *v1s        = v0s + EPB * NQ3;
+
+    const int tid = threadIdx.x;
+    const long e0 = long(blockIdx.x) * EPB;
+    const int ne  = int(min(long(EPB), long(a.nelmt) - e0));
+    if (ne <= 0 || (a.skip && *a.skip))
+        return;
+
+    if (GEO == kGeoTma && tid == 0)
+    {
+        MbarInit(bar, 1);
+        const uint32_t bytes = uint32_t(ne * GS * long(sizeof(T)));
+        MbarArriveExpectTx(bar, bytes);
+        BulkG2S(geo, a.geo + e0 * GS, bytes, bar);
+    }
+
+    const int le   = tid / NQ2;
+    const int ij   = tid - le * NQ2;
+    const int i    = ij % NQ, j = ij / NQ;
+    bool act       = le < ne;
+    const int lec  = le < EPB ? le : 0;
+    const int eoff = lec * NQ3;
+    T *xs = v0s + eoff, *As = v1s + eoff, *u_ = us + eoff, *v0 = v0s + eoff, *v1 = v1s + eoff;
+
+    // streamed geometry: plane 0 requested before any arithmetic
+    const T *Gg = a.geo + (e0 + lec) * GS;
+    T gc[7];
+    if (GEO == kGeoStream && act)
+    {
+        const int q0 = j * NQ + i;
+#pragma unroll
+        for (int c = 0; c < 7; ++c)
+            gc[c] = __ldg(Gg + c * NQ3 + q0);
+    }
+
+    for (int t = tid; t < NM * NQ; t += blockDim.x)
+    {
+        sB0[t] = a.B0[t];
+        sB1[t] = a.B1[t];
+        sB2[t] = a.B2[t];
+    }
+    for (int t = tid; t < NQ2; t += blockDim.x)
+    {
+        const int r = t / NQ, c = t - r * NQ;
+        sD[r * NQP + c] = a.D[c * NQ + r];
+    }
+    // coefficients into the v0 region (element stride NQ3 >= NC)
+    for (int t = tid; t < ne * NC; t += blockDim.x)
+    {
+        const int lt  = t / NC;
+        const int m   = t - lt * NC;
+        const long gi = (e0 + lt) * NC + m;
+        T v;
+        if (GATHER)
+        {
+            v = a.in[a.gmap[gi]];
+            if (a.gsign)
+                v *= T(a.gsign[gi]);
+        }
+        else
+        {
+            v = a.in[gi];
+        }
+        v0s[lt * NQ3 + m] = v;
+    }
+    __syncthreads();
+
+    // BwdTrans, contraction over p: A[r][q][i], thread (i, q = j)
+    if (act && j < NM)
+    {
+        T b0[NM];
+#pragma unroll
+        for (int p = 0; p < NM; ++p)
+            b0[p] = sB0[p * NQ + i];
+#pragma unroll
+        for (int r = 0; r < NM; ++r)
+        {
+            const T *xr = xs + (r * NM + j) * NM;
+            T s         = 0;
+#pragma unroll
+            for (int p = 0; p < NM; ++p)
+                s = fma(xr[p], b0[p], s);
+            As[(r * NM + j) * NQ + i] = s;
+        }
+    }
+    __syncthreads();
+
+    // contraction over q (shared memory) then over r (registers): u[k] at (i, j)
+    T ur[NQ];
+    if (act)
+    {
+        T b1[NM], bv[NM];
+#pragma unroll
+        for (int q = 0; q < NM; ++q)
+            b1[q] = sB1[q * NQ + j];
+#pragma unroll
+        for (int r = 0; r < NM; ++r)
+        {
+            T s = 0;
+#pragma unroll
+            for (int q = 0; q < NM; ++q)
+                s = fma(As[(r * NM + q) * NQ + i], b1[q], s);
+            bv[r] = s;
+        }
+#pragma unroll
+        for (int k = 0; k < NQ; ++k)
+        {
+            T s = 0;
+#pragma unroll
+            for (int r = 0; r < NM; ++r)
+                s = fma(sB2[r * NQ + k], bv[r], s);
+            ur[k]                     = s;
+            u_[(k * NQ + j) * NQ + i] = s;
+        }
+    }
+    __syncthreads();
+
+    // TMA geometry must have landed: bounded wait by every thread
+    if (GEO == kGeoTma && !MbarWaitBounded(bar, 0, a.err, 1))
+        act = false;
+
+    // gradient (i, j from shared memory, k from registers) and metric:
+    // v = G' grad u (v0, v1 to shared memory, v2 kept), f = lambda W u
+    T v2r[NQ], fr[NQ];
+    if (act)
+    {
+        T d0[NQ], d1[NQ];
+#pragma unroll
+        for (int m = 0; m < NQ; ++m)
+        {
+            d0[m] = sD[i * NQP + m];
+            d1[m] = sD[j * NQP + m];
+        }
+        const T *G = geo + lec * GS;
+#pragma unroll
+        for (int k = 0; k < NQ; ++k)
+        {
+            const int q = (k * NQ + j) * NQ + i;
+            T gn[7];
+            if (GEO == kGeoStream && k + 1 < NQ)
+            {
+#pragma unroll
+                for (int c = 0; c < 7; ++c)
+                    gn[c] = __ldg(Gg + c * NQ3 + q + NQ2);
+            }
+            T g0 = 0, g1 = 0, g2 = 0;
+            const T *row = u_ + (k * NQ + j) * NQ;
+#pragma unroll
+            for (int m = 0; m < NQ; ++m)
+                g0 = fma(d0[m], row[m], g0);
+            const T *col = u_ + k * NQ2 + i;
+#pragma unroll
+            for (int m = 0; m < NQ; ++m)
+                g1 = fma(d1[m], col[m * NQ], g1);
+#pragma unroll
+            for (int m = 0; m < NQ; ++m)
+                g2 = fma(sD[k * NQP + m], ur[m], g2);
+            T W, G00, G11, G22, G01, G02, G12;
+            if (GEO == kGeoTma)
+            {
+                W   = G[q];
+                G00 = G[NQ3 + q];
+                G11 = G[2 * NQ3 + q];
+                G22 = G[3 * NQ3 + q];
+                G01 = G[4 * NQ3 + q];
+                G02 = G[5 * NQ3 + q];
+                G12 = G[6 * NQ3 + q];
+            }
+            else
+            {
+                W   = gc[0];
+                G00 = gc[1];
+                G11 = gc[2];
+                G22 = gc[3];
+                G01 = gc[4];
+                G02 = gc[5];
+                G12 = gc[6];
+            }
+            v0[q]  = fma(G02, g2, fma(G01, g1, G00 * g0));
+            v1[q]  = fma(G12, g2, fma(G11, g1, G01 * g0));
+            v2r[k] = fma(G22, g2, fma(G12, g1, G02 * g0));
+            fr[k]  = a.lambda * W * ur[k];
+            if (GEO == kGeoStream && k + 1 < NQ)
+            {
+#pragma unroll
+                for (int c = 0; c < 7; ++c)
+                    gc[c] = gn[c];
+            }
+        }
+    }
+    __syncthreads();
+
+    // f += sum_a D_a^T v_a
+    if (act)
+    {
+        T dt0[NQ], dt1[NQ];
+#pragma unroll
+        for (int m = 0; m < NQ; ++m)
+        {
+            dt0[m] = sD[m * NQP + i];
+            dt1[m] = sD[m * NQP + j];
+        }
+#pragma unroll
+        for (int k = 0; k < NQ; ++k)
+        {
+            T s          = fr[k];
+            const T *row = v0 + (k * NQ + j) * NQ;
+#pragma unroll
+            for (int m = 0; m < NQ; ++m)
+                s = fma(dt0[m], row[m], s);
+            const T *col = v1 + k * NQ2 + i;
+#pragma unroll
+            for (int m = 0; m < NQ; ++m)
+                s = fma(dt1[m], col[m * NQ], s);
+#pragma unroll
+            for (int m = 0; m < NQ; ++m)
+                s = fma(sD[m * NQP + k], v2r[m], s);
+            fr[k] = s;
+        }
+    }
+    __syncthreads();
+
+    // raw inner product, contraction over k (registers): T1[r][j][i] in the u region
+    if (act)
+    {
+#pragma unroll
+        for (int r = 0; r < NM; ++r)
+        {
+            T s = 0;
+#pragma unroll
+            for (int k = 0; k < NQ; ++k)
+                s = fma(sB2[r * NQ + k], fr[k], s);
+            u_[(r * NQ + j) * NQ + i] = s;
+        }
+    }
+    __syncthreads();
+
+    // contraction over j: T2[r][q][i], thread (i, q = j), into the v0 region
+    if (act && j < NM)
+    {
+        T b1c[NQ];
+#pragma unroll
+        for (int jj = 0; jj < NQ; ++jj)
+            b1c[jj] = sB1[j * NQ + jj];
+#pragma unroll
+        for (int r = 0; r < NM; ++r)
+        {
+            T s = 0;
+#pragma unroll
+            for (int jj = 0; jj < NQ; ++jj)
+                s = fma(b1c[jj], u_[(r * NQ + jj) * NQ + i], s);
+            v0[(r * NM + j) * NQ + i] = s;
+        }
+    }
+    __syncthreads();
+
+    // contraction over i: y[r][q][p], thread (p = i, q = j); coalesced stores
+    if (act && i < NM && j < NM)
+    {
+        T b0c[NQ];
+#pragma unroll
+        for (int ii = 0; ii < NQ; ++ii)
+            b0c[ii] = sB0[i * NQ + ii];
+        T *o = a.out + (e0 + le) * NC;
+#pragma unroll
+        for (int r = 0; r < NM; ++r)
+        {
+            const T *t2 = v0 + (r * NM + j) * NQ;
+            T s         = 0;
+#pragma unroll
+            for (int ii = 0; ii < NQ; ++ii)
+                s = fma(b0c[ii], t2[ii], s);
+            o[(r * NM + j) * NM + i] = s;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// variants, autotuning and dispatch
+// ---------------------------------------------------------------------------
+
+enum
+{
+    kVariantGeneric = 0,
+    kVariantHexHelm = 1
+};
+
+// candidate (geometry staging, elements per CTA) of the tuned Hex kernel
+constexpr int kNumHexVariants = 3;
+
+template <typename T, int NQ> constexpr int TmaEpb()
+{
+    constexpr int per = (10 * NQ * NQ * NQ + 4) * int(sizeof(T));
+    constexpr int e   = (90 * 1024) / per;
+    constexpr int lim = 512 / (NQ * NQ);
+    constexpr int v   = e < lim ? e : lim;
+    return v < 1 ? 1 : (v > 8 ? 8 : v);
+}
+
+template <typename T, int NM, int GEO, int EPB>
+static int HexVariantLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStream_t s,
+                            bool set_attr)
+{
+    constexpr int NQ   = NM + 1;
+    const size_t bytes = HexSmem<T, NM, NQ, GEO, EPB>(op->gstride);
+    if (bytes > 227 * 1024 || HexThreads<NQ, EPB>() > 1024)
+        return SetError(NKB_ERR_UNSUPPORTED, "Hex variant needs %zu bytes of shared memory", bytes);
+    if (set_attr)
+    {
+        NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm<T, NM, NQ, GEO, EPB, false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+        NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm<T, NM, NQ, GEO, EPB, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+        return NKB_OK;
+    }
+    const long nb = (long(op->nelmt) + EPB - 1) / EPB;
+    if (nb == 0)
+        return NKB_OK;
+    if (gather)
+        k_hex_helm<T, NM, NQ, GEO, EPB, true><<<unsigned(nb), HexThreads<NQ, EPB>(), bytes, s>>>(a);
+    else
+        k_hex_helm<T, NM, NQ, GEO, EPB, false><<<unsigned(nb), HexThreads<NQ, EPB>(), bytes, s>>>(a);
+    NKB_CUDA_TRY(cudaGetLastError());
+    return NKB_OK;
+}
+
+template <typename T, int NM>
+static int HexLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStream_t s, int variant,
+                     bool set_attr)
+{
+    constexpr int NQ = NM + 1;
+    switch (variant)
+    {
+        case 0:
+            return HexVariantLaunch<T, NM, kGeoTma, TmaEpb<T, NQ>()>(op, a, gather, s, set_attr);
+        case 1:
+            return HexVariantLaunch<T, NM, kGeoStream, 1>(op, a, gather, s, set_attr);
+        default:
+            return HexVariantLaunch<T, NM, kGeoStream, 2>(op, a, gather, s, set_attr);
+    }
+}
+
+#define NKB_HEX_SWITCH(NMV, CALL)                                                                  \
+    switch (NMV)                                                                                   \
+    {                                                                                              \
+        case 2: return CALL(2);                                                                    \
+        case 3: return CALL(3);                                                                    \
+        case 4: return CALL(4);                                                                    \
+        case 5: return CALL(5);                                                                    \
+        case 6: return CALL(6);                                                                    \
+        case 7: return CALL(7);                                                                    \
+        case 8: return CALL(8);                                                                    \
+        case 9: return CALL(9);                                                                    \
+        case 10: return CALL(10);                                                                  \
+        case 11: return CALL(11);                                                                  \
+        default: return SetError(NKB_ERR_UNSUPPORTED, "no tuned Hex kernel for nm=%d", NMV);        \
+    }
+
+template <typename T>
+int HexLaunchT(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStream_t s, int variant,
+               bool set_attr)
+{
+#define NKB_CALL(N) HexLaunch<T, N>(op, a, gather, s, variant, set_attr)
+    NKB_HEX_SWITCH(op->nm, NKB_CALL)
+#undef NKB_CALL
+}
+
+
+} // namespace nkb

@@ -34,7 +34,8 @@ struct nkb_op
     double diff[6]   = {1, 0, 1, 0, 0, 1};
 
     // kernel selection (nkb_hex.cu): 0 generic, >0 tuned variant
-    int variant = 0;
+    int variant     = 0;
+    int hex_variant = 0; // tuned Hex kernel variant chosen by the autotuner
     void *kdata = nullptr;
     int *d_err  = nullptr; // device error word (bounded waits that gave up)
 

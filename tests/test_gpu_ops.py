@@ -115,11 +115,14 @@ def test_device_pointer_path_matches_host_path():
 
 
 @pytest.mark.parametrize("n,nm", [(1, 5), (3, 7), (2, 9), (1, 11), (5, 2)])
-def test_tuned_and_generic_hex_helmholtz_agree(monkeypatch, n, nm):
-    """The tuned Hex kernel (nkb_hex.cu) against the shape-generic one, odd
-    element counts included (partially filled last CTA)."""
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_tuned_and_generic_hex_helmholtz_agree(monkeypatch, n, nm, variant):
+    """Every variant of the tuned Hex kernel (nkb_hex.cu: TMA-staged or
+    streamed geometry, 1-2 elements per CTA) against the shape-generic
+    kernel, odd element counts included (partially filled last CTA)."""
     m = nb.BoxMesh("hex", n, nm, nm + 1, amp=0.05)
     x = np.random.default_rng(nm).uniform(-1, 1, m.nelmt * m.nc)
+    monkeypatch.setenv("NKB_HEX_VARIANT", str(variant))
     tuned = nb.Operator("helmholtz", m)
     tuned.set_factors(0.3)
     monkeypatch.setenv("NKB_KERNEL", "generic")
