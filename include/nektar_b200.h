@@ -151,6 +151,21 @@ int nkb_op_set_factors(nkb_op *op, double lambda, int diff_mode, const double *d
 int nkb_op_apply(nkb_op *op, const double *in, double *out0, double *out1, double *out2,
                  int flags, void *stream);
 
+/* Host-pointer apply that allocates no device memory. No counterpart in the
+ * reference. nkb_op_apply with NKB_HOST_PTRS stages the arrays in device
+ * memory it obtains with cudaMalloc; callers that may not allocate at this
+ * point (a fixed device-memory budget reserved at start-up, or a time loop
+ * that must not take the synchronisation cudaMalloc/cudaFree can cause) use
+ * this instead: staging goes through one file-scope 32 MiB device array, so
+ * the operator's input plus outputs must fit in 4 Mi doubles (larger ones
+ * get NKB_ERR_INVALID). The first call on a device looks the array up
+ * (cudaGetSymbolAddress); make it before capturing any stream. All calls
+ * share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. FP64 operators; synchronous, like the
+ * NKB_HOST_PTRS path it mirrors. */
+int nkb_op_apply_host_static(nkb_op *op, const double *in, double *out0, double *out1,
+                             double *out2, void *stream);
+
 /* FP32 variant of nkb_op_apply for NKB_FP32 operators (device pointers). */
 int nkb_op_apply_f32(nkb_op *op, const float *in, float *out0, float *out1, float *out2,
                      void *stream);

@@ -76,6 +76,8 @@ SIGNATURES = {
     "nkb_op_set_factors": (c_int, [c_void_p, c_double, c_int, dp]),
     "nkb_op_apply": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "nkb_op_apply_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "nkb_op_apply_host_static": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                         c_void_p]),
     "nkb_op_sizes": (c_int, [c_void_p, P(c_long), P(c_long)]),
     "nkb_op_helmholtz_diag": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "nkb_op_last_kernel_ms": (c_int, [c_void_p, P(c_float)]),
