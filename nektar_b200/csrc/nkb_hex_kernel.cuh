@@ -52,26 +52,82 @@ template <typename T, int NM, int NQ> constexpr int HexTabBytes()
 }
 
 // shared memory of one CTA (the TMA variant adds EPB element geometry blocks)
+// element stride of the work regions: nq^3 rounded up to an even count, so every
+// element's region (and every even-length row in it) starts 16-byte aligned
+template <int NQ> __host__ __device__ constexpr int HexRegion()
+{
+    return NQ * NQ * NQ + ((NQ * NQ * NQ) & 1);
+}
+
 template <typename T, int NM, int NQ, int GEO, int EPB> size_t HexSmem(long gstride)
 {
     return size_t(HexTabBytes<T, NM, NQ>()) +
-           size_t(EPB) * ((GEO == kGeoTma ? size_t(gstride) : 0) + 3 * NQ * NQ * NQ) * sizeof(T);
+           size_t(EPB) * ((GEO == kGeoTma ? size_t(gstride) : 0) + 3 * HexRegion<NQ>()) * sizeof(T);
+}
+
+// 1-D tables passed by value as a kernel parameter: entries read with
+// compile-time indices (the uniform, register-direction contractions) become
+// constant-bank operands of the FMAs instead of shared-memory loads.
+template <typename T, int NM, int NQ> struct HexConst
+{
+    T B0[NM * NQ], B1[NM * NQ], B2[NM * NQ]; // B[p*NQ + i] = phi_p(z_i)
+    T D[NQ * NQ];                            // D[i*NQ + m] = l_m'(z_i)
+};
+
+template <typename T> struct Vec2;
+template <> struct Vec2<double>
+{
+    using type = double2;
+};
+template <> struct Vec2<float>
+{
+    using type = float2;
+};
+
+// sum_m c[m] v[m] over a shared-memory row, 16-byte (FP64) loads when the row
+// length is even (rows are then aligned)
+template <typename T, int N>
+__device__ __forceinline__ T DotRow(const T *__restrict__ row, const T (&c)[N], T s)
+{
+    if constexpr (N % 2 == 0)
+    {
+        using V = typename Vec2<T>::type;
+#pragma unroll
+        for (int m = 0; m < N; m += 2)
+        {
+            const V v = *reinterpret_cast<const V *>(row + m);
+            s         = fma(c[m], v.x, s);
+            s         = fma(c[m + 1], v.y, s);
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int m = 0; m < N; ++m)
+            s = fma(c[m], row[m], s);
+    }
+    return s;
 }
 
 template <typename T, int NQ, int GEO, int EPB> __host__ __device__ constexpr int HexMinBlocks()
 {
     // resident CTAs per SM the register allocation must allow: a register
-    // budget per thread of 128 (nq <= 8), 168 (nq <= 10) or 255
-    constexpr int regs = NQ <= 8 ? 128 : (NQ <= 10 ? 168 : 255);
+    // budget per thread of 160 (nq <= 8), 168 (nq <= 10) or 255
+    constexpr int regs = NQ <= 8 ? 160 : (NQ <= 10 ? 168 : 255);
     constexpr int b    = 65536 / (HexThreads<NQ, EPB>() * regs);
     return b < 1 ? 1 : b;
 }
 
 template <typename T, int NM, int NQ, int GEO, int EPB, bool GATHER>
 __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GEO, EPB>()))
-    k_hex_helm(HexArgs<T> a)
+    k_hex_helm(HexArgs<T> a, const __grid_constant__ HexConst<T, NM, NQ> c)
 {
     constexpr int NQ2 = NQ * NQ, NQ3 = NQ2 * NQ, NC = NM * NM * NM, NQP = NQ + 1;
+    constexpr int NMP = NM + (NM & 1); // coefficient rows padded to an even length
+    constexpr int RS  = HexRegion<NQ>(); // element stride of the work regions (even)
+    static_assert(RS % 2 == 0 && NMP % 2 == 0, "vector loads need even strides");
+    static_assert(HexTabBytes<T, NM, NQ>() % 16 == 0, "work regions must start 16-byte aligned");
+    static_assert(NM * NM * NMP <= RS && NM * NQ * NQ <= RS, "regions too small");
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
     T *sB0        = reinterpret_cast<T *>(smem + 16);
@@ -80,9 +136,9 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
     T *sD         = sB2 + NM * NQ; // sD[i*NQP + m] = D(i, m) = l_m'(z_i)
     const long GS = a.gstride;
     T *geo        = reinterpret_cast<T *>(smem + HexTabBytes<T, NM, NQ>());
-    T *us         = geo + (GEO == kGeoTma ? EPB * GS : 0);
-    T *v0s        = us + EPB * NQ3;
-    T *v1s        = v0s + EPB * NQ3;
+    T *us         = geo + (GEO == kGeoTma ? EPB * GS : 0); // GS is a multiple of 4
+    T *v0s        = us + EPB * RS;
+    T *v1s        = v0s + EPB * RS;
 
     const int tid = threadIdx.x;
     const long e0 = long(blockIdx.x) * EPB;
@@ -97,13 +153,19 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
         MbarArriveExpectTx(bar, bytes);
         BulkG2S(geo, a.geo + e0 * GS, bytes, bar);
     }
+    if (GEO == kGeoStream && tid == 0)
+    {
+        // the CTA's whole geometry requested from DRAM at once (into L2); the
+        // per-plane loads below then hit L2
+        BulkPrefetchL2(a.geo + e0 * GS, uint32_t(ne * GS * long(sizeof(T))));
+    }
 
     const int le   = tid / NQ2;
     const int ij   = tid - le * NQ2;
     const int i    = ij % NQ, j = ij / NQ;
     bool act       = le < ne;
     const int lec  = le < EPB ? le : 0;
-    const int eoff = lec * NQ3;
+    const int eoff = lec * RS;
     T *xs = v0s + eoff, *As = v1s + eoff, *u_ = us + eoff, *v0 = v0s + eoff, *v1 = v1s + eoff;
 
     // streamed geometry: plane 0 requested before any arithmetic
@@ -113,22 +175,22 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
     {
         const int q0 = j * NQ + i;
 #pragma unroll
-        for (int c = 0; c < 7; ++c)
-            gc[c] = __ldg(Gg + c * NQ3 + q0);
+        for (int cc = 0; cc < 7; ++cc)
+            gc[cc] = __ldg(Gg + cc * NQ3 + q0);
     }
 
     for (int t = tid; t < NM * NQ; t += blockDim.x)
     {
-        sB0[t] = a.B0[t];
-        sB1[t] = a.B1[t];
-        sB2[t] = a.B2[t];
+        sB0[t] = c.B0[t];
+        sB1[t] = c.B1[t];
+        sB2[t] = c.B2[t];
     }
     for (int t = tid; t < NQ2; t += blockDim.x)
     {
-        const int r = t / NQ, c = t - r * NQ;
-        sD[r * NQP + c] = a.D[c * NQ + r];
+        const int r = t / NQ, cc = t - r * NQ;
+        sD[r * NQP + cc] = c.D[r * NQ + cc];
     }
-    // coefficients into the v0 region (element stride NQ3 >= NC)
+    // coefficients into the v0 region, rows (r, q) padded to NMP (NM^2 NMP <= NQ3)
     for (int t = tid; t < ne * NC; t += blockDim.x)
     {
         const int lt  = t / NC;
@@ -145,7 +207,8 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
         {
             v = a.in[gi];
         }
-        v0s[lt * NQ3 + m] = v;
+        const int rq = m / NM;
+        v0s[lt * RS + rq * NMP + (m - rq * NM)] = v;
     }
     __syncthreads();
 
@@ -159,11 +222,17 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
 #pragma unroll
         for (int r = 0; r < NM; ++r)
         {
-            const T *xr = xs + (r * NM + j) * NM;
+            const T *xr = xs + (r * NM + j) * NMP;
             T s         = 0;
+            using V     = typename Vec2<T>::type;
 #pragma unroll
-            for (int p = 0; p < NM; ++p)
-                s = fma(xr[p], b0[p], s);
+            for (int p = 0; p < NMP; p += 2)
+            {
+                const V v = *reinterpret_cast<const V *>(xr + p);
+                s         = fma(v.x, b0[p], s);
+                if (p + 1 < NM)
+                    s = fma(v.y, b0[p + 1], s);
+            }
             As[(r * NM + j) * NQ + i] = s;
         }
     }
@@ -192,7 +261,7 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
             T s = 0;
 #pragma unroll
             for (int r = 0; r < NM; ++r)
-                s = fma(sB2[r * NQ + k], bv[r], s);
+                s = fma(c.B2[r * NQ + k], bv[r], s);
             ur[k]                     = s;
             u_[(k * NQ + j) * NQ + i] = s;
         }
@@ -224,21 +293,18 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
             if (GEO == kGeoStream && k + 1 < NQ)
             {
 #pragma unroll
-                for (int c = 0; c < 7; ++c)
-                    gn[c] = __ldg(Gg + c * NQ3 + q + NQ2);
+                for (int cc = 0; cc < 7; ++cc)
+                    gn[cc] = __ldg(Gg + cc * NQ3 + q + NQ2);
             }
-            T g0 = 0, g1 = 0, g2 = 0;
-            const T *row = u_ + (k * NQ + j) * NQ;
-#pragma unroll
-            for (int m = 0; m < NQ; ++m)
-                g0 = fma(d0[m], row[m], g0);
+            T g1 = 0, g2 = 0;
+            const T g0   = DotRow<T, NQ>(u_ + (k * NQ + j) * NQ, d0, T(0));
             const T *col = u_ + k * NQ2 + i;
 #pragma unroll
             for (int m = 0; m < NQ; ++m)
                 g1 = fma(d1[m], col[m * NQ], g1);
 #pragma unroll
             for (int m = 0; m < NQ; ++m)
-                g2 = fma(sD[k * NQP + m], ur[m], g2);
+                g2 = fma(c.D[k * NQ + m], ur[m], g2);
             T W, G00, G11, G22, G01, G02, G12;
             if (GEO == kGeoTma)
             {
@@ -267,8 +333,8 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
             if (GEO == kGeoStream && k + 1 < NQ)
             {
 #pragma unroll
-                for (int c = 0; c < 7; ++c)
-                    gc[c] = gn[c];
+                for (int cc = 0; cc < 7; ++cc)
+                    gc[cc] = gn[cc];
             }
         }
     }
@@ -287,18 +353,14 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
 #pragma unroll
         for (int k = 0; k < NQ; ++k)
         {
-            T s          = fr[k];
-            const T *row = v0 + (k * NQ + j) * NQ;
-#pragma unroll
-            for (int m = 0; m < NQ; ++m)
-                s = fma(dt0[m], row[m], s);
+            T s          = DotRow<T, NQ>(v0 + (k * NQ + j) * NQ, dt0, fr[k]);
             const T *col = v1 + k * NQ2 + i;
 #pragma unroll
             for (int m = 0; m < NQ; ++m)
                 s = fma(dt1[m], col[m * NQ], s);
 #pragma unroll
             for (int m = 0; m < NQ; ++m)
-                s = fma(sD[m * NQP + k], v2r[m], s);
+                s = fma(c.D[m * NQ + k], v2r[m], s);
             fr[k] = s;
         }
     }
@@ -313,7 +375,7 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
             T s = 0;
 #pragma unroll
             for (int k = 0; k < NQ; ++k)
-                s = fma(sB2[r * NQ + k], fr[k], s);
+                s = fma(c.B2[r * NQ + k], fr[k], s);
             u_[(r * NQ + j) * NQ + i] = s;
         }
     }
@@ -349,12 +411,7 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
 #pragma unroll
         for (int r = 0; r < NM; ++r)
         {
-            const T *t2 = v0 + (r * NM + j) * NQ;
-            T s         = 0;
-#pragma unroll
-            for (int ii = 0; ii < NQ; ++ii)
-                s = fma(b0c[ii], t2[ii], s);
-            o[(r * NM + j) * NM + i] = s;
+            o[(r * NM + j) * NM + i] = DotRow<T, NQ>(v0 + (r * NM + j) * NQ, b0c, T(0));
         }
     }
 }
@@ -381,6 +438,22 @@ template <typename T, int NQ> constexpr int TmaEpb()
     return v < 1 ? 1 : (v > 8 ? 8 : v);
 }
 
+template <typename T, int NM, int NQ> static HexConst<T, NM, NQ> MakeHexConst(const nkb_op *op)
+{
+    HexConst<T, NM, NQ> c;
+    for (int t = 0; t < NM * NQ; ++t)
+    {
+        c.B0[t] = T(op->hB[0][t]);
+        c.B1[t] = T(op->hB[1][t]);
+        c.B2[t] = T(op->hB[2][t]);
+    }
+    // host D is column-major (D[m*NQ + i] = l_m'(z_i)); the table is row-major
+    for (int i = 0; i < NQ; ++i)
+        for (int m = 0; m < NQ; ++m)
+            c.D[i * NQ + m] = T(op->hD[0][size_t(m) * NQ + i]);
+    return c;
+}
+
 template <typename T, int NM, int GEO, int EPB>
 static int HexVariantLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStream_t s,
                             bool set_attr)
@@ -400,10 +473,11 @@ static int HexVariantLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, 
     const long nb = (long(op->nelmt) + EPB - 1) / EPB;
     if (nb == 0)
         return NKB_OK;
+    const HexConst<T, NM, NQ> c = MakeHexConst<T, NM, NQ>(op);
     if (gather)
-        k_hex_helm<T, NM, NQ, GEO, EPB, true><<<unsigned(nb), HexThreads<NQ, EPB>(), bytes, s>>>(a);
+        k_hex_helm<T, NM, NQ, GEO, EPB, true><<<unsigned(nb), HexThreads<NQ, EPB>(), bytes, s>>>(a, c);
     else
-        k_hex_helm<T, NM, NQ, GEO, EPB, false><<<unsigned(nb), HexThreads<NQ, EPB>(), bytes, s>>>(a);
+        k_hex_helm<T, NM, NQ, GEO, EPB, false><<<unsigned(nb), HexThreads<NQ, EPB>(), bytes, s>>>(a, c);
     NKB_CUDA_TRY(cudaGetLastError());
     return NKB_OK;
 }

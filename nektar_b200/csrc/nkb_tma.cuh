@@ -50,6 +50,13 @@ __device__ __forceinline__ void BulkG2S(void *dst, const void *src, uint32_t byt
                  : "memory");
 }
 
+// bulk prefetch of [src, src+bytes) into L2 (bytes % 16 == 0, src 16-byte
+// aligned); no shared memory, no completion to wait for
+__device__ __forceinline__ void BulkPrefetchL2(const void *src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ bool MbarTryWait(uint64_t *bar, uint32_t parity)
 {
     uint32_t ok;
