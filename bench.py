@@ -34,6 +34,7 @@ sys.path.insert(0, ROOT)
 WORKLOAD = "fp64 Helmholtz solve, 32^3 curved hex, P=6 Q=8, PCG+Jacobi to 1e-10"
 METRIC = "Helmholtz CG solves/s (FP64, PCG+Jacobi, rel. residual 1e-10)"
 N_CELLS, NM, AMP, LAM, TOL = 32, 7, 0.05, 1.0, 1e-10
+MIXED_INNER_TOL = 1e-4
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -244,7 +245,9 @@ def run_b200(args, rank, world, local):
     gmap, nglob, ndir = mesh.assembly()
     op = nb.Operator("helmholtz", mesh, device=dev)
     op.set_factors(LAM)
-    S = nb.GlobalLinSys([op], gmap, nglob, ndir, device=dev)
+    op32 = nb.Operator("helmholtz", mesh, device=dev, precision="fp32")
+    op32.set_factors(LAM)
+    S = nb.GlobalLinSys([op], gmap, nglob, ndir, device=dev, ops32=[op32])
     x, y, z = mesh.xyz
     u = np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z)
     ipo = nb.Operator("iproduct", mesh, device=dev)
@@ -297,8 +300,9 @@ def run_b200(args, rank, world, local):
     value = world * args.steps / (ms_max / 1e3)
 
     # accuracy of the last solve against the manufactured solution
+    x_fp64 = x_dev.cpu().numpy()
     bwd = nb.Operator("bwdtrans", mesh, device=dev)
-    uh = bwd(x_dev.cpu().numpy())
+    uh = bwd(x_fp64)
     rms = float(np.sqrt(np.mean((uh - u) ** 2)))
     del bwd
 
@@ -318,6 +322,38 @@ def run_b200(args, rank, world, local):
     if pg:
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
     e2e = world * args.steps / (float(t.item()) / 1e3)
+
+    # ---- mixed precision: FP64 refinement around the FP32 CG, same criterion --
+    def solve_mixed():
+        with torch.cuda.stream(stream):
+            x_dev.zero_()
+        return S.solve_device(b_dev.data_ptr(), x_dev.data_ptr(), tol=TOL, check_interval=K_CHECK,
+                              stream=sp, mixed=True, inner_tol=MIXED_INNER_TOL)
+
+    solve_mixed()
+    mreps = []
+    barrier()
+    torch.cuda.synchronize()
+    m0 = torch.cuda.Event(enable_timing=True)
+    m1 = torch.cuda.Event(enable_timing=True)
+    m0.record(stream)
+    for _ in range(args.steps):
+        mreps.append(solve_mixed())
+    m1.record(stream)
+    torch.cuda.synchronize()
+    t = torch.tensor([m0.elapsed_time(m1)], dtype=torch.float64, device=f"cuda:{dev}")
+    if pg:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    mixed_value = world * args.steps / (float(t.item()) / 1e3)
+    xm = x_dev.cpu().numpy()
+    mixed = {"value": mixed_value, "unit": "solves/s", "speedup_vs_fp64": mixed_value / value,
+             "rel_l2_vs_fp64_solution": float(np.linalg.norm(xm - x_fp64) / np.linalg.norm(x_fp64)),
+             "rel_residual": mreps[-1].rel_residual, "inner_iterations": mreps[-1].iterations,
+             "outer_iterations": mreps[-1].outer_iterations, "inner_tol": MIXED_INNER_TOL,
+             "latency_ms": {"p50": float(np.percentile([r.device_ms for r in mreps], 50)),
+                            "p99": float(np.percentile([r.device_ms for r in mreps], 99))},
+             "scheme": "FP64 residual, norms, solution and geometry setup; FP32 operator, "
+                       "vectors and preconditioner inside the inner CG (FP64 dot sums)"}
 
     # ---- roofline of the dominant kernel (element Helmholtz, gather fused) ------
     prof = S.profile(iters=20)
@@ -374,11 +410,12 @@ def run_b200(args, rank, world, local):
         "helmholtz_gdof_s": nloc / (prof["op_ms"] * 1e-3) / 1e9,
         "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": 2 * nloc * 8,
                 "d2h_bytes_per_step": nloc * 8},
-        "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clocks.summary(),
-        "gpu_launches": int(sum(r.kernel_launches for r in reps)),
+        "mixed": mixed, "roofline": roofline, "cpu_baseline": cpu_base,
+        "clocks": clocks.summary(), "gpu_launches": int(sum(r.kernel_launches for r in reps)),
     }
     S.close()
     op.close()
+    op32.close()
     if pg:
         pg.barrier()
         pg.destroy_process_group()

@@ -224,15 +224,21 @@ class Operator:
 class GlobalLinSys:
     """GlobalLinSysIterativeFull + PreconditionerDiagonal + NekLinSysIterCG."""
 
-    def __init__(self, ops, gmap, nglob, ndir, sign=None, device=0):
+    def __init__(self, ops, gmap, nglob, ndir, sign=None, device=0, ops32=None):
+        """ops: FP64 Helmholtz operators in local-space order; ops32: optional
+        FP32 twins (same meshes) enabling the mixed-precision solve."""
         self.ops = list(ops)
+        self.ops32 = None if ops32 is None else list(ops32)
         self.nloc = int(sum(o.nelmt * ncoeffs(o.shape, o.nm) for o in self.ops))
         self.nglob, self.ndir = int(nglob), int(ndir)
         gmap = np.ascontiguousarray(gmap, dtype=np.int32)
         sign = None if sign is None else _f64(sign)
         handles = (ctypes.c_void_p * len(self.ops))(*[o.h.value for o in self.ops])
         d = C.SysDesc()
-        d.nops, d.ops, d.ops32 = len(self.ops), handles, None
+        h32 = None
+        if self.ops32 is not None:
+            h32 = (ctypes.c_void_p * len(self.ops32))(*[o.h.value for o in self.ops32])
+        d.nops, d.ops, d.ops32 = len(self.ops), handles, h32
         d.nloc, d.nglob, d.ndir = self.nloc, self.nglob, self.ndir
         d.map = gmap.ctypes.data_as(C.ip)
         d.sign = _dp(sign)
@@ -242,40 +248,42 @@ class GlobalLinSys:
         self.h = h
 
     @staticmethod
-    def _opts(tol, maxit, check_interval, use_graph):
+    def _opts(tol, maxit, check_interval, use_graph, mixed=False, inner_tol=0.0, max_outer=0):
         o = C.CGOpts()
         o.tol, o.maxit, o.check_interval, o.use_graph = tol, maxit, check_interval, int(use_graph)
+        o.mixed, o.inner_tol, o.max_outer = int(bool(mixed)), inner_tol, max_outer
         return o
 
     def solve(self, b_loc, x_loc=None, tol=1e-9, maxit=5000, check_interval=16, use_graph=True,
-              raise_on_maxit=True):
-        """Host arrays: local rhs and local Dirichlet values -> local solution."""
+              raise_on_maxit=True, mixed=False, inner_tol=0.0, max_outer=0):
+        """Host arrays: local rhs and local Dirichlet values -> local solution.
+        mixed=True: FP64 iterative refinement around the FP32 CG."""
         b = _f64(b_loc)
         x = np.zeros(self.nloc) if x_loc is None else _f64(x_loc).copy()
         rep = C.CGReport()
-        rc = lib().nkb_cg_solve(self.h, b.ctypes.data, x.ctypes.data,
-                                ctypes.byref(self._opts(tol, maxit, check_interval, use_graph)),
+        opts = self._opts(tol, maxit, check_interval, use_graph, mixed, inner_tol, max_outer)
+        rc = lib().nkb_cg_solve(self.h, b.ctypes.data, x.ctypes.data, ctypes.byref(opts),
                                 ctypes.byref(rep), HOST_PTRS, None)
         if rc != C.NKB_OK and (raise_on_maxit or rc != C.NKB_ERR_NOT_CONVERGED):
             check(rc)
         return x, rep
 
     def solve_device(self, b_ptr, x_ptr, tol=1e-9, maxit=5000, check_interval=16,
-                     use_graph=True, stream=None):
+                     use_graph=True, stream=None, mixed=False, inner_tol=0.0, max_outer=0):
         rep = C.CGReport()
-        check(lib().nkb_cg_solve(self.h, b_ptr, x_ptr,
-                                 ctypes.byref(self._opts(tol, maxit, check_interval, use_graph)),
-                                 ctypes.byref(rep), DEVICE_PTRS, stream))
+        opts = self._opts(tol, maxit, check_interval, use_graph, mixed, inner_tol, max_outer)
+        check(lib().nkb_cg_solve(self.h, b_ptr, x_ptr, ctypes.byref(opts), ctypes.byref(rep),
+                                 DEVICE_PTRS, stream))
         return rep
 
     def solve_host_ptrs(self, b_ptr, x_ptr, tol=1e-9, maxit=5000, check_interval=16,
-                        use_graph=True, stream=None):
+                        use_graph=True, stream=None, mixed=False, inner_tol=0.0, max_outer=0):
         """Host (ideally pinned) buffers by address: copies in and out inside
         the call, on `stream`."""
         rep = C.CGReport()
-        check(lib().nkb_cg_solve(self.h, b_ptr, x_ptr,
-                                 ctypes.byref(self._opts(tol, maxit, check_interval, use_graph)),
-                                 ctypes.byref(rep), HOST_PTRS, stream))
+        opts = self._opts(tol, maxit, check_interval, use_graph, mixed, inner_tol, max_outer)
+        check(lib().nkb_cg_solve(self.h, b_ptr, x_ptr, ctypes.byref(opts), ctypes.byref(rep),
+                                 HOST_PTRS, stream))
         return rep
 
     def profile(self, iters=20):

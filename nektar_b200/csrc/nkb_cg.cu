@@ -283,6 +283,84 @@ __global__ void k_invert(int nn, int ndir, const double *__restrict__ dglob, dou
         dinv[i] = 1.0 / dglob[ndir + i];
 }
 
+// ---- mixed precision (FP64 iterative refinement around an FP32 PCG) --------
+
+// inner solve start: r32 = (float) r64, x32 = w32 = s32 = p32 = q32 = 0, partial (r,r)
+__global__ void k_init_inner(int nglob, int ndir, const double *__restrict__ r64,
+                             float *__restrict__ r32, float *__restrict__ x32,
+                             float *__restrict__ w32, float *__restrict__ s32,
+                             float *__restrict__ p32, float *__restrict__ q32, double *part)
+{
+    double rr = 0.0;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nglob; g += gridDim.x * blockDim.x)
+    {
+        x32[g] = 0.f;
+        w32[g] = 0.f;
+        s32[g] = 0.f;
+        if (g >= ndir)
+        {
+            const float r   = float(r64[g - ndir]);
+            r32[g - ndir] = r;
+            p32[g - ndir] = 0.f;
+            q32[g - ndir] = 0.f;
+            rr += double(r) * double(r);
+        }
+    }
+    BlockSum2(0.0, rr, part);
+}
+
+// x64 += x32 on the non-Dirichlet part
+__global__ void k_add_correction(int nn, int ndir, double *__restrict__ x64,
+                                 const float *__restrict__ x32)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x)
+        x64[ndir + i] += double(x32[ndir + i]);
+}
+
+// r = b - s on the non-Dirichlet part (s = A x assembled), partial (r,r)
+__global__ void k_residual(int nn, int ndir, const double *__restrict__ b, const double *__restrict__ s,
+                           double *__restrict__ r, double *part)
+{
+    double rr = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x)
+    {
+        const double v = b[ndir + i] - s[ndir + i];
+        r[i]           = v;
+        rr += v * v;
+    }
+    BlockSum2(0.0, rr, part);
+}
+
+// start of an inner solve: eps = (r,r) = rhs_mag (relative criterion), iter = 0
+__global__ void k_scalars_inner_init(CGState *st, const double *part, int nb, double tol2,
+                                     int maxit)
+{
+    const double rr = ReducePart(part, nb, 1);
+    if (threadIdx.x != 0)
+        return;
+    st->eps     = rr;
+    st->rhs_mag = rr > 0.0 ? rr : 1.0;
+    st->tol2    = tol2;
+    st->maxit   = maxit;
+    st->iter    = 0;
+    st->status  = NKB_OK;
+    st->done    = (rr > 0.0) ? 0 : 1;
+}
+
+// outer residual norm into st->eps
+__global__ void k_scalars_outer(CGState *st, const double *part, int nb)
+{
+    const double rr = ReducePart(part, nb, 1);
+    if (threadIdx.x == 0)
+        st->eps = rr;
+}
+
+__global__ void k_float_copy(long n, const double *__restrict__ a, float *__restrict__ b)
+{
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+        b[i] = float(a[i]);
+}
+
 static int Blocks(long n, int threads = kRedThreads)
 {
     return int(std::max<long>(1, std::min<long>((n + threads - 1) / threads, kRedBlocks)));
@@ -314,6 +392,13 @@ struct nkb_sys
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double *stage = nullptr; // host-pointer staging (2*nloc)
     long launches = 0;       // kernels launched by the current solve
+    // mixed precision: FP32 twins of the operators and the inner-CG state
+    std::vector<nkb_op *> ops32;
+    float *w32 = nullptr, *s32 = nullptr, *x32 = nullptr, *p32 = nullptr, *r32 = nullptr,
+          *q32 = nullptr, *yl32 = nullptr, *dinv32 = nullptr;
+    CGState *st32 = nullptr;
+    cudaGraphExec_t graph32 = nullptr;
+    int graph32_k = 0;
 };
 
 namespace nkb
@@ -337,6 +422,37 @@ static int Matvec(nkb_sys *S, const double *xin, double *yl, bool gather, cudaSt
         if (rc)
             return rc;
     }
+    return NKB_OK;
+}
+
+static int Matvec32(nkb_sys *S, const float *xin, float *yl, cudaStream_t s, const int *skip)
+{
+    for (size_t c = 0; c < S->ops32.size(); ++c)
+    {
+        const long o = S->off[c];
+        int rc = LaunchOp<float>(S->ops32[c], xin, yl + o, nullptr, nullptr, S->d_map + o,
+                                 S->d_sign ? S->d_sign + o : nullptr, s, skip);
+        if (rc)
+            return rc;
+    }
+    return NKB_OK;
+}
+
+// one FP32 inner-CG iteration (same recurrence as Iteration, FP64 dot sums)
+static int Iteration32(nkb_sys *S, cudaStream_t s)
+{
+    const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
+    S->launches += 3 + long(S->ops32.size());
+    k_update<float><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st32, S->p32, S->q32, S->x32,
+                                                S->r32, S->w32, S->s32, S->dinv32, S->partA);
+    int rc = Matvec32(S, S->w32, S->yl32, s, &S->st32->done);
+    if (rc)
+        return rc;
+    k_assemble<float><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
+                                                  S->d_sign, S->yl32, S->s32, S->w32, S->st32,
+                                                  S->partB);
+    k_scalars<<<1, 1024, 0, s>>>(S->st32, S->partA, nbU, S->partB, nbA, 2);
+    NKB_CUDA_TRY(cudaGetLastError());
     return NKB_OK;
 }
 
@@ -437,6 +553,30 @@ extern "C" int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **out)
         return fail(SetError(NKB_ERR_NOMEM, "nkb_sys_create: device allocation failed"));
     if (cudaMallocHost(&S->h_st, sizeof(CGState)) != cudaSuccess)
         return fail(SetError(NKB_ERR_NOMEM, "nkb_sys_create: pinned state"));
+    if (desc->ops32)
+    {
+        for (int c = 0; c < desc->nops; ++c)
+        {
+            const nkb_op *a = desc->ops[c], *b = desc->ops32[c];
+            if (!b || b->optype != NKB_HELMHOLTZ || b->precision != NKB_FP32 ||
+                b->nelmt != a->nelmt || b->nc != a->nc)
+                return fail(SetError(NKB_ERR_INVALID,
+                                     "nkb_sys_create: ops32[%d] is not an FP32 twin of ops[%d]", c,
+                                     c));
+            S->ops32.push_back(desc->ops32[c]);
+        }
+        bool ok32 = dalloc((void **)&S->w32, S->nglob * sizeof(float)) &&
+                    dalloc((void **)&S->s32, S->nglob * sizeof(float)) &&
+                    dalloc((void **)&S->x32, S->nglob * sizeof(float)) &&
+                    dalloc((void **)&S->p32, S->nn * sizeof(float)) &&
+                    dalloc((void **)&S->r32, S->nn * sizeof(float)) &&
+                    dalloc((void **)&S->q32, S->nn * sizeof(float)) &&
+                    dalloc((void **)&S->dinv32, S->nn * sizeof(float)) &&
+                    dalloc((void **)&S->yl32, nloc * sizeof(float)) &&
+                    dalloc((void **)&S->st32, sizeof(CGState));
+        if (!ok32)
+            return fail(SetError(NKB_ERR_NOMEM, "nkb_sys_create: FP32 vectors"));
+    }
     NKB_CUDA_TRY(cudaMemcpy(S->d_map, desc->map, nloc * sizeof(int), cudaMemcpyHostToDevice));
     NKB_CUDA_TRY(cudaMemcpy(S->d_aptr, aptr.data(), (S->nglob + 1) * sizeof(int), cudaMemcpyHostToDevice));
     NKB_CUDA_TRY(cudaMemcpy(S->d_aidx, aidx.data(), nloc * sizeof(int), cudaMemcpyHostToDevice));
@@ -458,6 +598,8 @@ extern "C" int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **out)
     k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, S->stream>>>(
         S->nglob, S->ndir, S->d_aptr, S->d_aidx, nullptr, S->tl, S->bglob, nullptr, nullptr, nullptr);
     k_invert<<<Blocks(S->nn), kRedThreads, 0, S->stream>>>(S->nn, S->ndir, S->bglob, S->d_dinv);
+    if (S->dinv32)
+        k_float_copy<<<Blocks(S->nn), kRedThreads, 0, S->stream>>>(S->nn, S->d_dinv, S->dinv32);
     NKB_CUDA_TRY(cudaGetLastError());
     NKB_CUDA_TRY(cudaStreamSynchronize(S->stream));
     *out = S;
@@ -510,6 +652,123 @@ extern "C" int nkb_sys_matvec_local(nkb_sys *S, const double *x_loc, double *y_l
     return Matvec(S, x_loc, y_loc, false, s);
 }
 
+namespace nkb
+{
+// FP64 iterative refinement around an FP32 PCG, on the lifted system (bglob
+// already assembled): r = b - A x in FP64, an FP32 PCG solves A d = r to a
+// relative reduction inner_tol (FP64 sums of the dot products), x += d in
+// FP64, until ||r||^2 < tol^2 ||b||^2 (NekLinSysIterCG's criterion). The
+// geometry, the residual, the norms and the solution stay FP64; S->st ends
+// with the FP64 residual and the total inner iteration count.
+static int MixedSolve(nkb_sys *S, const nkb_cg_opts &o, cudaStream_t s, int *outer_out)
+{
+    const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
+    const int K   = o.check_interval;
+    const double tol       = std::fmax(o.tol, 1.0e-16);
+    const double inner_tol = o.inner_tol > 0 ? o.inner_tol : 1.0e-5;
+    const int max_outer    = o.max_outer > 0 ? o.max_outer : 40;
+    CGState h0;
+    std::memset(&h0, 0, sizeof(h0));
+    h0.tol2  = tol * tol;
+    h0.maxit = o.maxit;
+    NKB_CUDA_TRY(cudaMemcpyAsync(S->st, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
+    k_init<<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->bglob, S->r, S->x, S->w, S->s, S->p,
+                                       S->q, S->partA);
+    k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbA, S->partA, nbA, 0);
+    S->launches += 2;
+    if (S->graph32 == nullptr || S->graph32_k != K)
+    {
+        if (S->graph32)
+            cudaGraphExecDestroy(S->graph32);
+        S->graph32 = nullptr;
+        cudaGraph_t g;
+        NKB_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        int crc = NKB_OK;
+        for (int k = 0; k < K && !crc; ++k)
+            crc = Iteration32(S, s);
+        cudaError_t ce = cudaStreamEndCapture(s, &g);
+        S->launches -= long(K) * (3 + long(S->ops32.size()));
+        if (crc)
+            return crc;
+        if (ce != cudaSuccess)
+            return SetError(NKB_ERR_CUDA, "mixed CG graph capture: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&S->graph32, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess)
+            return SetError(NKB_ERR_CUDA, "mixed CG graph instantiate: %s", cudaGetErrorString(ce));
+        S->graph32_k = K;
+    }
+    int total = 0, outer = 0, rc = NKB_OK;
+    CGState h, h32;
+    for (; outer <= max_outer; ++outer)
+    {
+        NKB_CUDA_TRY(cudaMemcpyAsync(&h, S->st, sizeof(h), cudaMemcpyDeviceToHost, s));
+        NKB_CUDA_TRY(cudaStreamSynchronize(s));
+        if (!std::isfinite(h.eps))
+        {
+            h.done   = 1;
+            h.status = NKB_ERR_NONFINITE;
+            break;
+        }
+        if (h.done || h.eps < h.tol2 * h.rhs_mag)
+        {
+            h.done   = 1;
+            h.status = NKB_OK;
+            break;
+        }
+        if (outer == max_outer || total >= o.maxit)
+        {
+            h.done   = 1;
+            h.status = NKB_ERR_NOT_CONVERGED;
+            break;
+        }
+        // inner FP32 PCG on A d = r
+        k_init_inner<<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->r, S->r32, S->x32, S->w32,
+                                                 S->s32, S->p32, S->q32, S->partA);
+        k_scalars_inner_init<<<1, 1024, 0, s>>>(S->st32, S->partA, nbA, inner_tol * inner_tol,
+                                                o.maxit - total);
+        k_precon<float><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st32, S->r32, S->w32,
+                                                    S->dinv32, S->partA);
+        if ((rc = Matvec32(S, S->w32, S->yl32, s, &S->st32->done)))
+            return rc;
+        k_assemble<float><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
+                                                      S->d_sign, S->yl32, S->s32, S->w32, S->st32,
+                                                      S->partB);
+        k_scalars<<<1, 1024, 0, s>>>(S->st32, S->partA, nbU, S->partB, nbA, 1);
+        S->launches += 6 + long(S->ops32.size());
+        const int max_passes = (o.maxit - total) / K + 2;
+        for (int pass = 0; pass < max_passes; ++pass)
+        {
+            NKB_CUDA_TRY(cudaMemcpyAsync(&h32, S->st32, sizeof(h32), cudaMemcpyDeviceToHost, s));
+            NKB_CUDA_TRY(cudaStreamSynchronize(s));
+            if (h32.done)
+                break;
+            NKB_CUDA_TRY(cudaGraphLaunch(S->graph32, s));
+            S->launches += long(K) * (3 + long(S->ops32.size()));
+        }
+        NKB_CUDA_TRY(cudaMemcpyAsync(&h32, S->st32, sizeof(h32), cudaMemcpyDeviceToHost, s));
+        NKB_CUDA_TRY(cudaStreamSynchronize(s));
+        total += std::max(h32.iter, 1);
+        // x += d; r = b - A x and its norm, all FP64
+        k_add_correction<<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->x, S->x32);
+        if ((rc = Matvec(S, S->x, S->yl, true, s)))
+            return rc;
+        k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
+                                                       S->d_sign, S->yl, S->s, nullptr, nullptr,
+                                                       nullptr);
+        k_residual<<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->bglob, S->s, S->r, S->partA);
+        k_scalars_outer<<<1, 1024, 0, s>>>(S->st, S->partA, nbU);
+        S->launches += 4 + long(S->ops.size());
+        NKB_CUDA_TRY(cudaGetLastError());
+    }
+    h.iter = total;
+    NKB_CUDA_TRY(cudaMemcpyAsync(S->st, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+    NKB_CUDA_TRY(cudaStreamSynchronize(s));
+    *outer_out = outer;
+    return NKB_OK;
+}
+} // namespace nkb
+
 extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
                             const nkb_cg_opts *opts, nkb_cg_report *rep, int flags, void *stream)
 {
@@ -530,8 +789,9 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
         o.maxit = 5000;
     if (o.check_interval <= 0)
         o.check_interval = 16;
-    if (o.mixed)
-        return SetError(NKB_ERR_UNSUPPORTED, "nkb_cg_solve: mixed precision not built in");
+    if (o.mixed && S->ops32.empty())
+        return SetError(NKB_ERR_INVALID, "nkb_cg_solve: mixed precision needs FP32 operators "
+                                         "(nkb_sys_desc.ops32)");
     NKB_CUDA_TRY(cudaSetDevice(S->device));
     // NULL (or the legacy default stream) -> the system's own stream
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : S->stream;
@@ -560,6 +820,14 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
     k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, s>>>(
         S->nglob, S->ndir, S->d_aptr, S->d_aidx, S->d_sign, S->tl, S->bglob, nullptr, nullptr, nullptr);
 
+    int outer_done = 0;
+    if (o.mixed)
+    {
+        if ((rc = MixedSolve(S, o, s, &outer_done)))
+            return rc;
+        goto finish;
+    }
+    {
     CGState h0;
     std::memset(&h0, 0, sizeof(h0));
     const double tol = std::fmax(o.tol, 1.0e-16); // NekLinSysIter.cpp:57
@@ -636,6 +904,8 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
                     return rc;
         }
     }
+    }
+finish:
     NKB_CUDA_TRY(cudaMemcpyAsync(S->h_st, S->st, sizeof(CGState), cudaMemcpyDeviceToHost, s));
     // x_loc += GlobalToLocal(x) (the Dirichlet part of x is zero)
     k_global_to_local<<<Blocks(nloc), kRedThreads, 0, s>>>(nloc, S->d_map, S->d_sign, S->x, S->tl);
@@ -649,7 +919,7 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
     if (rep)
     {
         rep->iterations       = h.iter;
-        rep->outer_iterations = 0;
+        rep->outer_iterations = outer_done;
         rep->rel_residual     = std::sqrt(h.eps / h.rhs_mag);
         rep->converged        = (h.done && h.status == NKB_OK) ? 1 : 0;
         float ms              = 0.f;
@@ -755,6 +1025,12 @@ extern "C" void nkb_sys_destroy(nkb_sys *S)
     cudaSetDevice(S->device);
     if (S->graph)
         cudaGraphExecDestroy(S->graph);
+    if (S->graph32)
+        cudaGraphExecDestroy(S->graph32);
+    for (void *ptr : {(void *)S->w32, (void *)S->s32, (void *)S->x32, (void *)S->p32,
+                      (void *)S->r32, (void *)S->q32, (void *)S->dinv32, (void *)S->yl32,
+                      (void *)S->st32})
+        cudaFree(ptr);
     cudaFree(S->d_map);
     cudaFree(S->d_sign);
     cudaFree(S->d_aptr);

@@ -84,3 +84,34 @@ def test_maxit_is_reported():
     with pytest.raises(nb.NektarB200Error) as e:
         S.solve(b, tol=1e-14, maxit=5)
     assert e.value.code == nb.C.NKB_ERR_NOT_CONVERGED
+
+
+def _mixed_system(n, nm, amp, lam=1.0):
+    m = nb.BoxMesh("hex", n, nm, nm + 1, amp=amp, coords=True)
+    gmap, nglob, ndir = m.assembly()
+    op = nb.Operator("helmholtz", m)
+    op.set_factors(lam)
+    op32 = nb.Operator("helmholtz", m, precision="fp32")
+    op32.set_factors(lam)
+    S = nb.GlobalLinSys([op], gmap, nglob, ndir, ops32=[op32])
+    return m, S, (op, op32)
+
+
+@pytest.mark.parametrize("n,nm", [(3, 5), (4, 9)])
+def test_mixed_precision_refinement_matches_fp64(n, nm):
+    """FP64 iterative refinement around the FP32 CG reaches the FP64 residual
+    criterion, and its solution matches the FP64 solve to the stated error."""
+    m, S, keep = _mixed_system(n, nm, 0.05)
+    b = np.random.default_rng(n).uniform(-1, 1, m.nelmt * m.nc)
+    x64, r64 = S.solve(b, tol=1e-12)
+    xm, rm = S.solve(b, tol=1e-12, mixed=True, inner_tol=1e-4)
+    assert rm.converged and rm.rel_residual < 1e-12 and rm.outer_iterations >= 2
+    assert rel_l2(xm, x64) < 1e-10, rel_l2(xm, x64)
+
+
+def test_mixed_requires_fp32_operators():
+    m, op, S, gmap, nglob, ndir = _system(2, 4, 0.05)
+    b = np.ones(m.nelmt * m.nc)
+    with pytest.raises(nb.NektarB200Error) as e:
+        S.solve(b, mixed=True)
+    assert e.value.code == nb.C.NKB_ERR_INVALID
