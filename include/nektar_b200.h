@@ -183,6 +183,22 @@ int nkb_op_last_kernel_ms(const nkb_op *op, float *ms);
 
 void nkb_op_destroy(nkb_op *op);
 
+/* ---- batched application over many collections --------------------------
+ * ExpList::GeneralMatrixOp (MultiRegions/ExpList.cpp:2666-2757) applies one
+ * operator type collection by collection (one collection per shape and basis
+ * key). nkb_batch does the same for a set of operators of one type in one
+ * call: in/out are the concatenated per-collection local vectors in the
+ * order given (PhysDeriv: each collection's three derivatives consecutively).
+ * The collections run concurrently on nstreams streams (0: 4), largest first,
+ * captured once as a CUDA graph per (in, out) pair. */
+typedef struct nkb_batch nkb_batch;
+int nkb_batch_create(nkb_op *const *ops, int nops, int nstreams, nkb_batch **batch);
+int nkb_batch_sizes(const nkb_batch *batch, long *in_size, long *out_size);
+int nkb_batch_apply(nkb_batch *batch, const double *in, double *out, int flags, void *stream);
+/* device time of the last nkb_batch_apply (waits for it) */
+int nkb_batch_last_ms(nkb_batch *batch, float *ms);
+void nkb_batch_destroy(nkb_batch *batch);
+
 /* ---- global system + CG --------------------------------------------------
  * One nkb_sys = GlobalLinSysIterativeFull with PreconditionerDiagonal over
  * an AssemblyMapCG (MultiRegions/GlobalLinSysIterativeFull.cpp:96-384,
@@ -210,20 +226,24 @@ typedef struct nkb_cg_opts
     int check_interval; /* host convergence poll every k iterations (device
                            kernels stop updating once converged) */
     int use_graph;      /* capture the k-iteration block in a CUDA graph */
-    int mixed;          /* 0: FP64 CG; 1: FP64 iterative refinement around
-                           an FP32 CG (needs ops32) */
-    double inner_tol;   /* mixed: relative residual reduction per inner solve */
-    int max_outer;      /* mixed: maximum refinement steps */
+    int mixed;          /* 0: FP64 CG; 1: FP32 CG with FP64 reliable updates
+                           (true residual b - Ax recomputed with the FP64
+                           operators; needs ops32). Stops on the FP64
+                           residual with the FP64 criterion. */
+    double inner_tol;   /* mixed: FP32-residual reduction between reliable
+                           updates (default 0.1, at most 0.5) */
+    int max_outer;      /* mixed: maximum reliable updates (default 1000) */
 } nkb_cg_opts;
 
 typedef struct nkb_cg_report
 {
-    int iterations;       /* CG iterations (total inner for mixed) */
-    int outer_iterations; /* mixed: refinement steps */
+    int iterations;       /* CG iterations (FP32 iterations for mixed) */
+    int outer_iterations; /* mixed: reliable updates (FP64 residuals) */
     double rel_residual;  /* sqrt(eps / rhs_magnitude) as NekLinSysIterCG reports */
     int converged;
     double device_ms;     /* device time of the solve (CUDA events) */
     long kernel_launches; /* kernels of this library launched by the solve */
+    int restarts;         /* mixed: FP32 recurrence restarts after drift */
 } nkb_cg_report;
 
 int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **sys);
@@ -236,6 +256,32 @@ int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **sys);
  * and returns once it has finished (the host polls convergence). */
 int nkb_cg_solve(nkb_sys *sys, const double *b_loc, double *x_loc, const nkb_cg_opts *opts,
                  nkb_cg_report *report, int flags, void *stream);
+
+/* The same solve without blocking (no reference counterpart: the serving
+ * layer keeps many systems' solves in flight from one host thread).
+ * nkb_cg_begin issues the lifting and the first direction and returns;
+ * nkb_cg_poll advances the solve by at most one block of device work and
+ * sets *done once the result is in x_loc (wait = 1: block until the pending
+ * block has finished first); nkb_cg_end returns what nkb_cg_solve would
+ * return and fills the report. b_loc/x_loc must stay valid until done.
+ * Host pointers make the final poll synchronous. */
+int nkb_cg_begin(nkb_sys *sys, const double *b_loc, double *x_loc, const nkb_cg_opts *opts,
+                 int flags, void *stream);
+int nkb_cg_poll(nkb_sys *sys, int wait, int *done);
+int nkb_cg_end(nkb_sys *sys, nkb_cg_report *report);
+
+/* A second system over the same operators, map and diagonal with its own
+ * vectors and stream (concurrent solves of one mesh). */
+int nkb_sys_clone(const nkb_sys *sys, nkb_sys **clone);
+
+/* Helmholtz lambda of this system (overrides the operators' eFactorLambda for
+ * its solves, Jacobi diagonal rebuilt from the split mass / Laplacian
+ * diagonal, computed once per shared system). */
+int nkb_sys_set_lambda(nkb_sys *sys, double lambda);
+
+/* Device bytes: shared by all clones (map, CSR, sign, split diagonal) and
+ * owned by this instance (vectors, state, staging). Operators not included. */
+int nkb_sys_footprint(const nkb_sys *sys, size_t *shared_bytes, size_t *instance_bytes);
 
 /* AssemblyMapCG::Assemble / GlobalToLocal on device arrays. */
 int nkb_sys_assemble(nkb_sys *sys, const double *loc, double *glob, void *stream);

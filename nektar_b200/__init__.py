@@ -221,6 +221,50 @@ class Operator:
             pass
 
 
+class Batch:
+    """Many collections' operators of one type applied in one call
+    (ExpList::GeneralMatrixOp over the collections), concurrently on the
+    device. in/out: concatenated per-collection local vectors."""
+
+    def __init__(self, ops, nstreams=4):
+        self.ops = list(ops)
+        handles = (ctypes.c_void_p * len(self.ops))(*[o.h.value for o in self.ops])
+        h = ctypes.c_void_p()
+        check(lib().nkb_batch_create(handles, len(self.ops), int(nstreams), ctypes.byref(h)))
+        self.h = h
+        nin, nout = ctypes.c_long(), ctypes.c_long()
+        check(lib().nkb_batch_sizes(self.h, ctypes.byref(nin), ctypes.byref(nout)))
+        self.in_size, self.out_size = nin.value, nout.value
+
+    def __call__(self, x):
+        """Host arrays in and out (copies inside the call)."""
+        x = _f64(x)
+        if x.size != self.in_size:
+            raise ValueError("batch input has %d values, expected %d" % (x.size, self.in_size))
+        y = np.zeros(self.out_size)
+        check(lib().nkb_batch_apply(self.h, x.ctypes.data, y.ctypes.data, HOST_PTRS, None))
+        return y
+
+    def apply_device(self, x_ptr, y_ptr, stream=None):
+        check(lib().nkb_batch_apply(self.h, x_ptr, y_ptr, DEVICE_PTRS, stream))
+
+    def last_ms(self):
+        ms = ctypes.c_float(0.0)
+        check(lib().nkb_batch_last_ms(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().nkb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class GlobalLinSys:
     """GlobalLinSysIterativeFull + PreconditionerDiagonal + NekLinSysIterCG."""
 
@@ -257,7 +301,8 @@ class GlobalLinSys:
     def solve(self, b_loc, x_loc=None, tol=1e-9, maxit=5000, check_interval=16, use_graph=True,
               raise_on_maxit=True, mixed=False, inner_tol=0.0, max_outer=0):
         """Host arrays: local rhs and local Dirichlet values -> local solution.
-        mixed=True: FP64 iterative refinement around the FP32 CG."""
+        mixed=True: FP32 CG with FP64 reliable updates (inner_tol = FP32
+        residual reduction between updates, max_outer = maximum updates)."""
         b = _f64(b_loc)
         x = np.zeros(self.nloc) if x_loc is None else _f64(x_loc).copy()
         rep = C.CGReport()
@@ -285,6 +330,50 @@ class GlobalLinSys:
         check(lib().nkb_cg_solve(self.h, b_ptr, x_ptr, ctypes.byref(opts), ctypes.byref(rep),
                                  HOST_PTRS, stream))
         return rep
+
+    # ---- non-blocking solve, clones, per-system lambda (serving layer) ----
+    def begin(self, b_ptr, x_ptr, tol=1e-9, maxit=5000, check_interval=16, use_graph=True,
+              stream=None, mixed=False, inner_tol=0.0, max_outer=0):
+        """Start a solve on device buffers and return at once; drive it with
+        poll() until it reports done, then end()."""
+        self._opts_keep = self._opts(tol, maxit, check_interval, use_graph, mixed, inner_tol,
+                                     max_outer)
+        check(lib().nkb_cg_begin(self.h, b_ptr, x_ptr, ctypes.byref(self._opts_keep),
+                                 DEVICE_PTRS, stream))
+
+    def poll(self, wait=False):
+        """Advance the solve by at most one block of device work; True once done."""
+        done = ctypes.c_int(0)
+        check(lib().nkb_cg_poll(self.h, int(bool(wait)), ctypes.byref(done)))
+        return bool(done.value)
+
+    def end(self, raise_on_maxit=True):
+        rep = C.CGReport()
+        rc = lib().nkb_cg_end(self.h, ctypes.byref(rep))
+        if rc != C.NKB_OK and (raise_on_maxit or rc != C.NKB_ERR_NOT_CONVERGED):
+            check(rc)
+        return rep
+
+    def clone(self):
+        """Another system over the same operators, map and diagonal, with its
+        own vectors and stream."""
+        c = object.__new__(GlobalLinSys)
+        c.ops, c.ops32 = self.ops, self.ops32
+        c.nloc, c.nglob, c.ndir = self.nloc, self.nglob, self.ndir
+        h = ctypes.c_void_p()
+        check(lib().nkb_sys_clone(self.h, ctypes.byref(h)))
+        c.h = h
+        return c
+
+    def set_lambda(self, lam):
+        """Helmholtz lambda of this system's solves (overrides the operators')."""
+        check(lib().nkb_sys_set_lambda(self.h, float(lam)))
+
+    def footprint(self):
+        """(shared bytes, instance bytes) of device memory held by the system."""
+        a, b = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        check(lib().nkb_sys_footprint(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return int(a.value), int(b.value)
 
     def profile(self, iters=20):
         """Per-kernel device time of one CG iteration (CUDA events)."""

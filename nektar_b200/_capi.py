@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libnekb200.so")
 
 c_int, c_long, c_double, c_float = ctypes.c_int, ctypes.c_long, ctypes.c_double, ctypes.c_float
-c_void_p, c_char_p = ctypes.c_void_p, ctypes.c_char_p
+c_void_p, c_char_p, c_size_t = ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t
 P = ctypes.POINTER
 dp, fp, ip = P(c_double), P(c_float), P(c_int)
 
@@ -53,7 +53,8 @@ class CGOpts(ctypes.Structure):
 
 class CGReport(ctypes.Structure):
     _fields_ = [("iterations", c_int), ("outer_iterations", c_int), ("rel_residual", c_double),
-                ("converged", c_int), ("device_ms", c_double), ("kernel_launches", c_long)]
+                ("converged", c_int), ("device_ms", c_double), ("kernel_launches", c_long),
+                ("restarts", c_int)]
 
 
 class SysProfile(ctypes.Structure):
@@ -91,6 +92,17 @@ SIGNATURES = {
     "nkb_sys_diag_inv": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "nkb_sys_profile_iteration": (c_int, [c_void_p, c_int, P(SysProfile)]),
     "nkb_sys_destroy": (None, [c_void_p]),
+    "nkb_batch_create": (c_int, [P(c_void_p), c_int, c_int, P(c_void_p)]),
+    "nkb_batch_sizes": (c_int, [c_void_p, P(c_long), P(c_long)]),
+    "nkb_batch_apply": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "nkb_batch_last_ms": (c_int, [c_void_p, P(c_float)]),
+    "nkb_batch_destroy": (None, [c_void_p]),
+    "nkb_cg_begin": (c_int, [c_void_p, c_void_p, c_void_p, P(CGOpts), c_int, c_void_p]),
+    "nkb_cg_poll": (c_int, [c_void_p, c_int, P(c_int)]),
+    "nkb_cg_end": (c_int, [c_void_p, P(CGReport)]),
+    "nkb_sys_clone": (c_int, [c_void_p, P(c_void_p)]),
+    "nkb_sys_set_lambda": (c_int, [c_void_p, c_double]),
+    "nkb_sys_footprint": (c_int, [c_void_p, P(c_size_t), P(c_size_t)]),
     "nkb_geom_nelmt": (c_long, [P(GeomRequest)]),
     "nkb_geom_fill": (c_int, [P(GeomRequest), dp, dp, dp]),
     "nkb_hex_box_assembly": (c_int, [c_int, c_int, ip, ip, ip]),

@@ -15,7 +15,11 @@
 //   k_scalars   fixed-order reduction of the partials, convergence test
 //               eps < tol^2 |b|^2, new alpha / beta; sets done
 // Scalars stay on the device; the host polls "done" once per block of
-// check_interval iterations, which can be captured as a CUDA graph.
+// check_interval iterations, which can be captured as a CUDA graph. The solve
+// is a non-blocking state machine (nkb_cg_begin / nkb_cg_poll / nkb_cg_end), so
+// one host thread can keep many systems' solves in flight on their own streams;
+// nkb_cg_solve polls it with waits. Clones (nkb_sys_clone) share operators, map
+// and diagonal and own their vectors, and may each carry their own lambda.
 #include "nkb_internal.h"
 #include "nkb_op.h"
 
@@ -24,6 +28,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <vector>
 
 namespace nkb
@@ -176,6 +182,7 @@ __device__ double ReducePart(const double *part, int nb, int which)
 // mode 0: initial residual: eps = (r,r) from partA[1], rhs_mag = (b,b) from partB[0]
 // mode 1: first direction:  rho = (r,w) partA[0], mu = (s,w) partB[0]; alpha = rho/mu
 // mode 2: iteration:        rho_new, eps from partA, mu from partB
+// mode 3: restart of the recurrence after a reliable update (mixed precision)
 __global__ void k_scalars(CGState *st, const double *partA, int nbA, const double *partB, int nbB,
                           int mode)
 {
@@ -206,6 +213,25 @@ __global__ void k_scalars(CGState *st, const double *partA, int nbA, const doubl
         st->alpha = a0 / b0;
         st->iter  = 1;
         if (!isfinite(st->alpha))
+        {
+            st->done   = 1;
+            st->status = NKB_ERR_NONFINITE;
+        }
+        return;
+    }
+    if (mode == 3)
+    {
+        // the residual was replaced by the true one (reliable update): new
+        // rho, mu from it; beta, alpha against the last accepted rho, alpha
+        // (a paused iteration did not overwrite them); iteration count kept
+        const double beta  = a0 / st->rho;
+        const double alpha = a0 / (b0 - a0 * beta / st->alpha);
+        st->mu    = b0;
+        st->eps   = a1;
+        st->beta  = beta;
+        st->alpha = alpha;
+        st->rho   = a0;
+        if (!isfinite(alpha) || !isfinite(a1))
         {
             st->done   = 1;
             st->status = NKB_ERR_NONFINITE;
@@ -283,7 +309,7 @@ __global__ void k_invert(int nn, int ndir, const double *__restrict__ dglob, dou
         dinv[i] = 1.0 / dglob[ndir + i];
 }
 
-// ---- mixed precision (FP64 iterative refinement around an FP32 PCG) --------
+// ---- mixed precision (FP32 PCG with FP64 reliable updates) -----------------
 
 // inner solve start: r32 = (float) r64, x32 = w32 = s32 = p32 = q32 = 0, partial (r,r)
 __global__ void k_init_inner(int nglob, int ndir, const double *__restrict__ r64,
@@ -309,42 +335,44 @@ __global__ void k_init_inner(int nglob, int ndir, const double *__restrict__ r64
     BlockSum2(0.0, rr, part);
 }
 
-// x64 += x32 on the non-Dirichlet part
-__global__ void k_add_correction(int nn, int ndir, double *__restrict__ x64,
-                                 const float *__restrict__ x32)
+// x64 += x32 and x32 = 0 on the non-Dirichlet part (a reliable update folds
+// the FP32 correction into the FP64 solution)
+__global__ void k_add_correction(int nn, int ndir, double *__restrict__ x64, float *__restrict__ x32)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x)
+    {
         x64[ndir + i] += double(x32[ndir + i]);
+        x32[ndir + i] = 0.f;
+    }
 }
 
-// r = b - s on the non-Dirichlet part (s = A x assembled), partial (r,r)
+// r = b - s on the non-Dirichlet part (s = A x assembled), r32 = (float) r,
+// partial (r,r)
 __global__ void k_residual(int nn, int ndir, const double *__restrict__ b, const double *__restrict__ s,
-                           double *__restrict__ r, double *part)
+                           double *__restrict__ r, float *__restrict__ r32, double *part)
 {
     double rr = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x)
     {
         const double v = b[ndir + i] - s[ndir + i];
         r[i]           = v;
+        r32[i]         = float(v);
         rr += v * v;
     }
     BlockSum2(0.0, rr, part);
 }
 
-// start of an inner solve: eps = (r,r) = rhs_mag (relative criterion), iter = 0
-__global__ void k_scalars_inner_init(CGState *st, const double *part, int nb, double tol2,
-                                     int maxit)
+// FP32 CG (re)start after a reliable update: the iterated residual pauses
+// the CG once (r,r) < thr; reset = 1 also zeroes the iteration count
+__global__ void k_resume(CGState *st, double thr, int maxit, int reset)
 {
-    const double rr = ReducePart(part, nb, 1);
-    if (threadIdx.x != 0)
-        return;
-    st->eps     = rr;
-    st->rhs_mag = rr > 0.0 ? rr : 1.0;
-    st->tol2    = tol2;
+    st->tol2    = thr;
+    st->rhs_mag = 1.0;
     st->maxit   = maxit;
-    st->iter    = 0;
     st->status  = NKB_OK;
-    st->done    = (rr > 0.0) ? 0 : 1;
+    st->done    = 0;
+    if (reset)
+        st->iter = 0;
 }
 
 // outer residual norm into st->eps
@@ -361,6 +389,21 @@ __global__ void k_float_copy(long n, const double *__restrict__ a, float *__rest
         b[i] = float(a[i]);
 }
 
+// Jacobi inverse for a system lambda from the split assembled diagonal:
+// dinv = 1 / (lambda dM + dL) on the non-Dirichlet part (and its FP32 copy)
+__global__ void k_combine_dinv(int nn, int ndir, double lambda, const double *__restrict__ dM,
+                               const double *__restrict__ dL, double *__restrict__ dinv,
+                               float *__restrict__ dinv32)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x)
+    {
+        const double v = 1.0 / fma(lambda, dM[ndir + i], dL[ndir + i]);
+        dinv[i]        = v;
+        if (dinv32)
+            dinv32[i] = float(v);
+    }
+}
+
 static int Blocks(long n, int threads = kRedThreads)
 {
     return int(std::max<long>(1, std::min<long>((n + threads - 1) / threads, kRedBlocks)));
@@ -368,41 +411,108 @@ static int Blocks(long n, int threads = kRedThreads)
 
 } // namespace nkb
 
+namespace nkb
+{
+// What a system and its clones share: the operators, the local->global map
+// with its global->local CSR and optional sign, and the split assembled
+// Jacobi diagonal (mass and Laplacian parts, built on first use).
+struct SysShared
+{
+    int device = 0;
+    std::vector<nkb_op *> ops, ops32;
+    std::vector<long> off;
+    long nloc = 0;
+    int nglob = 0, ndir = 0, nn = 0;
+    int *d_map = nullptr, *d_aptr = nullptr, *d_aidx = nullptr;
+    double *d_sign = nullptr;
+    double *d_dM = nullptr, *d_dL = nullptr; // nglob each
+    size_t bytes = 0;
+    std::mutex mu; // guards the lazy split diagonal
+
+    ~SysShared()
+    {
+        cudaSetDevice(device);
+        for (void *p : {(void *)d_map, (void *)d_aptr, (void *)d_aidx, (void *)d_sign,
+                        (void *)d_dM, (void *)d_dL})
+            cudaFree(p);
+    }
+};
+
+// the non-blocking solve (nkb_cg_begin / nkb_cg_poll / nkb_cg_end)
+enum SolvePhase
+{
+    kIdle = 0,  // no solve
+    kRun64,     // FP64 CG: blocks of check_interval iterations
+    kMixStart,  // mixed: waiting for |b|^2 before the FP32 recurrence starts
+    kRun32,     // mixed: FP32 iterations until the recurrence pauses
+    kUpdate,    // mixed: waiting for the FP64 residual of a reliable update
+    kFinishing, // solution written back, waiting for the last copies
+    kFinished   // result ready for nkb_cg_end
+};
+
+struct SolveCtx
+{
+    int phase = kIdle;
+    nkb_cg_opts o{};
+    cudaStream_t s = nullptr;
+    int flags       = 0;
+    double *x_user  = nullptr; // caller's x_loc
+    double *dx      = nullptr; // device local x (caller's or staging)
+    bool use_graph  = false;
+    int passes = 0, max_passes = 0, updates = 0, max_upd = 0;
+    int restarts = 0, iter_base = 0; // FP32 restarts and the iterations before the last one
+    double cycle_min = 0.0;          // smallest iterated FP32 residual of this cycle
+    int stall = 0;                   // polls without a new minimum
+    bool force_restart = false;
+    double thr_final = 0.0, delta = 0.0;
+    CGState last32{};
+};
+} // namespace nkb
+
 using namespace nkb;
 
 struct nkb_sys
 {
+    std::shared_ptr<SysShared> sh;
     int device = 0;
     cudaStream_t stream = nullptr;
-    std::vector<nkb_op *> ops;
+    // read-only views of the shared data
+    std::vector<nkb_op *> ops, ops32;
     std::vector<long> off;
     long nloc = 0;
     int nglob = 0, ndir = 0, nn = 0;
-    int *d_map = nullptr;
+    int *d_map = nullptr, *d_aptr = nullptr, *d_aidx = nullptr;
     double *d_sign = nullptr;
-    int *d_aptr = nullptr, *d_aidx = nullptr;
-    double *d_dinv = nullptr;
+    // per instance
+    bool has_lambda = false; // lambda overrides the operators' own
+    double lambda   = 1.0;
+    double *d_dinv  = nullptr;
     double *w = nullptr, *s = nullptr, *x = nullptr, *p = nullptr, *r = nullptr, *q = nullptr;
     double *bglob = nullptr, *yl = nullptr, *tl = nullptr;
     double *partA = nullptr, *partB = nullptr;
     CGState *st = nullptr;
-    CGState *h_st = nullptr; // pinned
+    CGState *h_st = nullptr; // pinned [3]: FP64 state, FP32 state, state to write
     cudaGraphExec_t graph = nullptr;
     int graph_k = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evq = nullptr;
     double *stage = nullptr; // host-pointer staging (2*nloc)
     long launches = 0;       // kernels launched by the current solve
-    // mixed precision: FP32 twins of the operators and the inner-CG state
-    std::vector<nkb_op *> ops32;
     float *w32 = nullptr, *s32 = nullptr, *x32 = nullptr, *p32 = nullptr, *r32 = nullptr,
           *q32 = nullptr, *yl32 = nullptr, *dinv32 = nullptr;
     CGState *st32 = nullptr;
     cudaGraphExec_t graph32 = nullptr;
     int graph32_k = 0;
+    size_t bytes = 0; // device bytes of this instance
+    SolveCtx sv;
 };
 
 namespace nkb
 {
+
+static const double *LambdaOf(const nkb_sys *S)
+{
+    return S->has_lambda ? &S->lambda : nullptr;
+}
 
 // y_loc = A x_loc over all collections; x given either as a local vector or
 // as a global vector gathered through the map (gather = true).
@@ -416,9 +526,10 @@ static int Matvec(nkb_sys *S, const double *xin, double *yl, bool gather, cudaSt
         int rc;
         if (gather)
             rc = LaunchOp<double>(op, xin, yl + o, nullptr, nullptr, S->d_map + o,
-                                  S->d_sign ? S->d_sign + o : nullptr, s, skip);
+                                  S->d_sign ? S->d_sign + o : nullptr, s, skip, LambdaOf(S));
         else
-            rc = LaunchOp<double>(op, xin + o, yl + o, nullptr, nullptr, nullptr, nullptr, s, skip);
+            rc = LaunchOp<double>(op, xin + o, yl + o, nullptr, nullptr, nullptr, nullptr, s, skip,
+                                  LambdaOf(S));
         if (rc)
             return rc;
     }
@@ -431,14 +542,14 @@ static int Matvec32(nkb_sys *S, const float *xin, float *yl, cudaStream_t s, con
     {
         const long o = S->off[c];
         int rc = LaunchOp<float>(S->ops32[c], xin, yl + o, nullptr, nullptr, S->d_map + o,
-                                 S->d_sign ? S->d_sign + o : nullptr, s, skip);
+                                 S->d_sign ? S->d_sign + o : nullptr, s, skip, LambdaOf(S));
         if (rc)
             return rc;
     }
     return NKB_OK;
 }
 
-// one FP32 inner-CG iteration (same recurrence as Iteration, FP64 dot sums)
+// one FP32 CG iteration (same recurrence as Iteration, FP64 dot sums)
 static int Iteration32(nkb_sys *S, cudaStream_t s)
 {
     const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
@@ -472,6 +583,159 @@ static int Iteration(nkb_sys *S, cudaStream_t s)
     return NKB_OK;
 }
 
+// (re)capture K iterations of the FP64 or the FP32 recurrence as a CUDA graph
+static int EnsureGraph(nkb_sys *S, bool fp32, cudaStream_t s, int K)
+{
+    cudaGraphExec_t &ge = fp32 ? S->graph32 : S->graph;
+    int &gk             = fp32 ? S->graph32_k : S->graph_k;
+    if (ge && gk == K)
+        return NKB_OK;
+    if (ge)
+        cudaGraphExecDestroy(ge);
+    ge = nullptr;
+    cudaGraph_t g;
+    NKB_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int crc = NKB_OK;
+    for (int k = 0; k < K && !crc; ++k)
+        crc = fp32 ? Iteration32(S, s) : Iteration(S, s);
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    S->launches -= long(K) * (3 + long(fp32 ? S->ops32.size() : S->ops.size())); // captured
+    if (crc)
+        return crc;
+    if (ce != cudaSuccess)
+        return SetError(NKB_ERR_CUDA, "CG graph capture: %s", cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess)
+        return SetError(NKB_ERR_CUDA, "CG graph instantiate: %s", cudaGetErrorString(ce));
+    gk = K;
+    return NKB_OK;
+}
+
+static void DropGraphs(nkb_sys *S)
+{
+    if (S->graph)
+        cudaGraphExecDestroy(S->graph);
+    if (S->graph32)
+        cudaGraphExecDestroy(S->graph32);
+    S->graph = S->graph32 = nullptr;
+    S->graph_k = S->graph32_k = 0;
+}
+
+} // namespace nkb
+
+namespace nkb
+{
+static void ViewShared(nkb_sys *S)
+{
+    const SysShared &h = *S->sh;
+    S->device = h.device;
+    S->ops    = h.ops;
+    S->ops32  = h.ops32;
+    S->off    = h.off;
+    S->nloc   = h.nloc;
+    S->nglob  = h.nglob;
+    S->ndir   = h.ndir;
+    S->nn     = h.nn;
+    S->d_map  = h.d_map;
+    S->d_aptr = h.d_aptr;
+    S->d_aidx = h.d_aidx;
+    S->d_sign = h.d_sign;
+}
+
+// per-instance vectors, state, stream and events
+static int AllocInstance(nkb_sys *S)
+{
+    auto dalloc = [&](void **ptr, size_t bytes) -> bool {
+        bytes = std::max<size_t>(bytes, 8);
+        if (cudaMalloc(ptr, bytes) != cudaSuccess)
+            return false;
+        S->bytes += bytes;
+        return true;
+    };
+    if (cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&S->ev0) != cudaSuccess || cudaEventCreate(&S->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->evq, cudaEventDisableTiming) != cudaSuccess)
+        return SetError(NKB_ERR_CUDA, "nkb_sys: stream/event creation failed");
+    const long nloc = S->nloc;
+    bool ok = dalloc((void **)&S->d_dinv, S->nn * sizeof(double)) &&
+              dalloc((void **)&S->w, S->nglob * sizeof(double)) &&
+              dalloc((void **)&S->s, S->nglob * sizeof(double)) &&
+              dalloc((void **)&S->x, S->nglob * sizeof(double)) &&
+              dalloc((void **)&S->bglob, S->nglob * sizeof(double)) &&
+              dalloc((void **)&S->p, S->nn * sizeof(double)) &&
+              dalloc((void **)&S->r, S->nn * sizeof(double)) &&
+              dalloc((void **)&S->q, S->nn * sizeof(double)) &&
+              dalloc((void **)&S->yl, nloc * sizeof(double)) &&
+              dalloc((void **)&S->tl, nloc * sizeof(double)) &&
+              dalloc((void **)&S->partA, 2 * kRedBlocks * sizeof(double)) &&
+              dalloc((void **)&S->partB, 2 * kRedBlocks * sizeof(double)) &&
+              dalloc((void **)&S->st, sizeof(CGState));
+    if (ok && !S->ops32.empty())
+        ok = dalloc((void **)&S->w32, S->nglob * sizeof(float)) &&
+             dalloc((void **)&S->s32, S->nglob * sizeof(float)) &&
+             dalloc((void **)&S->x32, S->nglob * sizeof(float)) &&
+             dalloc((void **)&S->p32, S->nn * sizeof(float)) &&
+             dalloc((void **)&S->r32, S->nn * sizeof(float)) &&
+             dalloc((void **)&S->q32, S->nn * sizeof(float)) &&
+             dalloc((void **)&S->dinv32, S->nn * sizeof(float)) &&
+             dalloc((void **)&S->yl32, nloc * sizeof(float)) &&
+             dalloc((void **)&S->st32, sizeof(CGState));
+    if (!ok)
+        return SetError(NKB_ERR_NOMEM, "nkb_sys: device allocation of the CG vectors failed");
+    if (cudaMallocHost(&S->h_st, 3 * sizeof(CGState)) != cudaSuccess)
+        return SetError(NKB_ERR_NOMEM, "nkb_sys: pinned state");
+    std::memset(S->h_st, 0, 3 * sizeof(CGState));
+    return NKB_OK;
+}
+
+// mass and Laplacian parts of the assembled diagonal, computed once per
+// shared system (PreconditionerDiagonal::DiagonalPreconditionerSum with the
+// element diagonals split by lambda)
+static int EnsureDiagParts(nkb_sys *S)
+{
+    SysShared &h = *S->sh;
+    std::lock_guard<std::mutex> lock(h.mu);
+    if (h.d_dM)
+        return NKB_OK;
+    double *dM = nullptr, *dL = nullptr;
+    if (cudaMalloc(&dM, h.nglob * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&dL, h.nglob * sizeof(double)) != cudaSuccess)
+    {
+        cudaFree(dM);
+        return SetError(NKB_ERR_NOMEM, "nkb_sys: split diagonal");
+    }
+    for (size_t c = 0; c < S->ops.size(); ++c)
+    {
+        int rc = HelmholtzDiag(S->ops[c], S->tl + S->off[c], S->stream, S->yl + S->off[c]);
+        if (rc)
+        {
+            cudaFree(dM);
+            cudaFree(dL);
+            return rc;
+        }
+    }
+    k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, S->stream>>>(
+        S->nglob, S->ndir, S->d_aptr, S->d_aidx, nullptr, S->tl, dM, nullptr, nullptr, nullptr);
+    k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, S->stream>>>(
+        S->nglob, S->ndir, S->d_aptr, S->d_aidx, nullptr, S->yl, dL, nullptr, nullptr, nullptr);
+    cudaError_t ce = cudaStreamSynchronize(S->stream);
+    if (ce != cudaSuccess)
+    {
+        cudaFree(dM);
+        cudaFree(dL);
+        return SetError(NKB_ERR_CUDA, "nkb_sys: split diagonal: %s", cudaGetErrorString(ce));
+    }
+    h.d_dM = dM;
+    h.d_dL = dL;
+    h.bytes += 2 * h.nglob * sizeof(double);
+    return NKB_OK;
+}
+
+static bool Busy(const nkb_sys *S)
+{
+    return S->sv.phase != kIdle;
+}
 } // namespace nkb
 
 extern "C" int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **out)
@@ -497,115 +761,169 @@ extern "C" int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **out)
         if (desc->map[i] < 0 || desc->map[i] >= desc->nglob)
             return SetError(NKB_ERR_INVALID, "nkb_sys_create: map[%ld]=%d outside [0,%d)", i,
                             desc->map[i], desc->nglob);
+    if (desc->ops32)
+        for (int c = 0; c < desc->nops; ++c)
+        {
+            const nkb_op *a = desc->ops[c], *b = desc->ops32[c];
+            if (!b || b->optype != NKB_HELMHOLTZ || b->precision != NKB_FP32 ||
+                b->nelmt != a->nelmt || b->nc != a->nc)
+                return SetError(NKB_ERR_INVALID,
+                                "nkb_sys_create: ops32[%d] is not an FP32 twin of ops[%d]", c, c);
+        }
     NKB_CUDA_TRY(cudaSetDevice(desc->device));
-    nkb_sys *S = new nkb_sys();
-    auto fail  = [&](int code) {
-        nkb_sys_destroy(S);
-        return code;
-    };
-    S->device = desc->device;
-    S->nloc   = nloc;
-    S->nglob  = desc->nglob;
-    S->ndir   = desc->ndir;
-    S->nn     = desc->nglob - desc->ndir;
-    long o    = 0;
+
+    auto sh    = std::make_shared<SysShared>();
+    sh->device = desc->device;
+    sh->nloc   = nloc;
+    sh->nglob  = desc->nglob;
+    sh->ndir   = desc->ndir;
+    sh->nn     = desc->nglob - desc->ndir;
+    long o     = 0;
     for (int c = 0; c < desc->nops; ++c)
     {
-        S->ops.push_back(desc->ops[c]);
-        S->off.push_back(o);
+        sh->ops.push_back(desc->ops[c]);
+        if (desc->ops32)
+            sh->ops32.push_back(desc->ops32[c]);
+        sh->off.push_back(o);
         o += long(desc->ops[c]->nelmt) * desc->ops[c]->nc;
     }
-    if (cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&S->ev0) != cudaSuccess || cudaEventCreate(&S->ev1) != cudaSuccess)
-        return fail(SetError(NKB_ERR_CUDA, "nkb_sys_create: stream/event"));
-
     // global -> local CSR for the deterministic assemble
-    std::vector<int> aptr(S->nglob + 1, 0), aidx(nloc);
+    std::vector<int> aptr(sh->nglob + 1, 0), aidx(nloc);
     for (long i = 0; i < nloc; ++i)
         aptr[desc->map[i] + 1]++;
-    for (int g = 0; g < S->nglob; ++g)
+    for (int g = 0; g < sh->nglob; ++g)
         aptr[g + 1] += aptr[g];
     {
         std::vector<int> fill(aptr.begin(), aptr.end() - 1);
         for (long i = 0; i < nloc; ++i)
             aidx[fill[desc->map[i]]++] = int(i);
     }
-    auto dalloc = [&](void **ptr, size_t bytes) -> bool {
-        return cudaMalloc(ptr, std::max<size_t>(bytes, 8)) == cudaSuccess;
+    auto salloc = [&](void **ptr, size_t bytes) -> bool {
+        bytes = std::max<size_t>(bytes, 8);
+        if (cudaMalloc(ptr, bytes) != cudaSuccess)
+            return false;
+        sh->bytes += bytes;
+        return true;
     };
-    bool ok = dalloc((void **)&S->d_map, nloc * sizeof(int)) &&
-              dalloc((void **)&S->d_aptr, (S->nglob + 1) * sizeof(int)) &&
-              dalloc((void **)&S->d_aidx, nloc * sizeof(int)) &&
-              dalloc((void **)&S->d_dinv, S->nn * sizeof(double)) &&
-              dalloc((void **)&S->w, S->nglob * sizeof(double)) &&
-              dalloc((void **)&S->s, S->nglob * sizeof(double)) &&
-              dalloc((void **)&S->x, S->nglob * sizeof(double)) &&
-              dalloc((void **)&S->bglob, S->nglob * sizeof(double)) &&
-              dalloc((void **)&S->p, S->nn * sizeof(double)) &&
-              dalloc((void **)&S->r, S->nn * sizeof(double)) &&
-              dalloc((void **)&S->q, S->nn * sizeof(double)) &&
-              dalloc((void **)&S->yl, nloc * sizeof(double)) &&
-              dalloc((void **)&S->tl, nloc * sizeof(double)) &&
-              dalloc((void **)&S->partA, 2 * kRedBlocks * sizeof(double)) &&
-              dalloc((void **)&S->partB, 2 * kRedBlocks * sizeof(double)) &&
-              dalloc((void **)&S->st, sizeof(CGState));
-    if (!ok)
-        return fail(SetError(NKB_ERR_NOMEM, "nkb_sys_create: device allocation failed"));
-    if (cudaMallocHost(&S->h_st, sizeof(CGState)) != cudaSuccess)
-        return fail(SetError(NKB_ERR_NOMEM, "nkb_sys_create: pinned state"));
-    if (desc->ops32)
-    {
-        for (int c = 0; c < desc->nops; ++c)
-        {
-            const nkb_op *a = desc->ops[c], *b = desc->ops32[c];
-            if (!b || b->optype != NKB_HELMHOLTZ || b->precision != NKB_FP32 ||
-                b->nelmt != a->nelmt || b->nc != a->nc)
-                return fail(SetError(NKB_ERR_INVALID,
-                                     "nkb_sys_create: ops32[%d] is not an FP32 twin of ops[%d]", c,
-                                     c));
-            S->ops32.push_back(desc->ops32[c]);
-        }
-        bool ok32 = dalloc((void **)&S->w32, S->nglob * sizeof(float)) &&
-                    dalloc((void **)&S->s32, S->nglob * sizeof(float)) &&
-                    dalloc((void **)&S->x32, S->nglob * sizeof(float)) &&
-                    dalloc((void **)&S->p32, S->nn * sizeof(float)) &&
-                    dalloc((void **)&S->r32, S->nn * sizeof(float)) &&
-                    dalloc((void **)&S->q32, S->nn * sizeof(float)) &&
-                    dalloc((void **)&S->dinv32, S->nn * sizeof(float)) &&
-                    dalloc((void **)&S->yl32, nloc * sizeof(float)) &&
-                    dalloc((void **)&S->st32, sizeof(CGState));
-        if (!ok32)
-            return fail(SetError(NKB_ERR_NOMEM, "nkb_sys_create: FP32 vectors"));
-    }
-    NKB_CUDA_TRY(cudaMemcpy(S->d_map, desc->map, nloc * sizeof(int), cudaMemcpyHostToDevice));
-    NKB_CUDA_TRY(cudaMemcpy(S->d_aptr, aptr.data(), (S->nglob + 1) * sizeof(int), cudaMemcpyHostToDevice));
-    NKB_CUDA_TRY(cudaMemcpy(S->d_aidx, aidx.data(), nloc * sizeof(int), cudaMemcpyHostToDevice));
+    if (!salloc((void **)&sh->d_map, nloc * sizeof(int)) ||
+        !salloc((void **)&sh->d_aptr, (sh->nglob + 1) * sizeof(int)) ||
+        !salloc((void **)&sh->d_aidx, nloc * sizeof(int)) ||
+        (desc->sign && !salloc((void **)&sh->d_sign, nloc * sizeof(double))))
+        return SetError(NKB_ERR_NOMEM, "nkb_sys_create: device allocation of the map failed");
+    NKB_CUDA_TRY(cudaMemcpy(sh->d_map, desc->map, nloc * sizeof(int), cudaMemcpyHostToDevice));
+    NKB_CUDA_TRY(cudaMemcpy(sh->d_aptr, aptr.data(), (sh->nglob + 1) * sizeof(int),
+                            cudaMemcpyHostToDevice));
+    NKB_CUDA_TRY(cudaMemcpy(sh->d_aidx, aidx.data(), nloc * sizeof(int), cudaMemcpyHostToDevice));
     if (desc->sign)
+        NKB_CUDA_TRY(cudaMemcpy(sh->d_sign, desc->sign, nloc * sizeof(double),
+                                cudaMemcpyHostToDevice));
+
+    nkb_sys *S = new nkb_sys();
+    S->sh      = sh;
+    ViewShared(S);
+    auto fail = [&](int code) {
+        nkb_sys_destroy(S);
+        return code;
+    };
+    int rc = AllocInstance(S);
+    if (rc)
+        return fail(rc);
+    // Jacobi diagonal: element diagonals, assembled (sign^2 = 1), inverted
+    // (PreconditionerDiagonal.cpp:93-125). With one lambda for all operators
+    // the mass and Laplacian parts are kept apart (clones with another lambda
+    // then only recombine them); otherwise each operator's own lambda.
+    bool one_lambda = true;
+    for (const nkb_op *op : S->ops)
+        one_lambda = one_lambda && op->lambda == S->ops[0]->lambda;
+    if (one_lambda)
     {
-        if (!dalloc((void **)&S->d_sign, nloc * sizeof(double)))
-            return fail(SetError(NKB_ERR_NOMEM, "nkb_sys_create: sign"));
-        NKB_CUDA_TRY(cudaMemcpy(S->d_sign, desc->sign, nloc * sizeof(double), cudaMemcpyHostToDevice));
-    }
-    // Jacobi diagonal: element diagonals, assembled, inverted
-    // (PreconditionerDiagonal::DiagonalPreconditionerSum, :93-125)
-    for (size_t c = 0; c < S->ops.size(); ++c)
-    {
-        int rc = HelmholtzDiag(S->ops[c], S->tl + S->off[c], S->stream);
-        if (rc)
+        if ((rc = EnsureDiagParts(S)))
             return fail(rc);
+        k_combine_dinv<<<Blocks(S->nn), kRedThreads, 0, S->stream>>>(
+            S->nn, S->ndir, S->ops[0]->lambda, sh->d_dM, sh->d_dL, S->d_dinv, S->dinv32);
     }
-    // sign^2 = 1: the diagonal sums the raw local entries
-    k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, S->stream>>>(
-        S->nglob, S->ndir, S->d_aptr, S->d_aidx, nullptr, S->tl, S->bglob, nullptr, nullptr, nullptr);
-    k_invert<<<Blocks(S->nn), kRedThreads, 0, S->stream>>>(S->nn, S->ndir, S->bglob, S->d_dinv);
-    if (S->dinv32)
-        k_float_copy<<<Blocks(S->nn), kRedThreads, 0, S->stream>>>(S->nn, S->d_dinv, S->dinv32);
-    NKB_CUDA_TRY(cudaGetLastError());
-    NKB_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    else
+    {
+        for (size_t c = 0; c < S->ops.size(); ++c)
+            if ((rc = HelmholtzDiag(S->ops[c], S->tl + S->off[c], S->stream)))
+                return fail(rc);
+        k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, S->stream>>>(
+            S->nglob, S->ndir, S->d_aptr, S->d_aidx, nullptr, S->tl, S->bglob, nullptr, nullptr,
+            nullptr);
+        k_invert<<<Blocks(S->nn), kRedThreads, 0, S->stream>>>(S->nn, S->ndir, S->bglob, S->d_dinv);
+        if (S->dinv32)
+            k_float_copy<<<Blocks(S->nn), kRedThreads, 0, S->stream>>>(S->nn, S->d_dinv,
+                                                                       S->dinv32);
+    }
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(S->stream) != cudaSuccess)
+        return fail(SetError(NKB_ERR_CUDA, "nkb_sys_create: Jacobi diagonal"));
     *out = S;
     return NKB_OK;
 }
 
+extern "C" int nkb_sys_clone(const nkb_sys *S, nkb_sys **out)
+{
+    ClearError();
+    if (!S || !out)
+        return SetError(NKB_ERR_INVALID, "nkb_sys_clone: NULL argument");
+    *out = nullptr;
+    NKB_CUDA_TRY(cudaSetDevice(S->device));
+    nkb_sys *C = new nkb_sys();
+    C->sh      = S->sh;
+    ViewShared(C);
+    int rc = AllocInstance(C);
+    if (rc == NKB_OK)
+    {
+        C->has_lambda = S->has_lambda;
+        C->lambda     = S->lambda;
+        if (cudaMemcpyAsync(C->d_dinv, S->d_dinv, S->nn * sizeof(double), cudaMemcpyDeviceToDevice,
+                            C->stream) != cudaSuccess ||
+            (C->dinv32 && cudaMemcpyAsync(C->dinv32, S->dinv32, S->nn * sizeof(float),
+                                          cudaMemcpyDeviceToDevice, C->stream) != cudaSuccess) ||
+            cudaStreamSynchronize(C->stream) != cudaSuccess)
+            rc = SetError(NKB_ERR_CUDA, "nkb_sys_clone: copy of the Jacobi diagonal");
+    }
+    if (rc)
+    {
+        nkb_sys_destroy(C);
+        return rc;
+    }
+    *out = C;
+    return NKB_OK;
+}
+
+extern "C" int nkb_sys_set_lambda(nkb_sys *S, double lambda)
+{
+    ClearError();
+    if (!S || !std::isfinite(lambda))
+        return SetError(NKB_ERR_INVALID, "nkb_sys_set_lambda: bad arguments");
+    if (Busy(S))
+        return SetError(NKB_ERR_INVALID, "nkb_sys_set_lambda: a solve is in progress");
+    NKB_CUDA_TRY(cudaSetDevice(S->device));
+    int rc = EnsureDiagParts(S);
+    if (rc)
+        return rc;
+    k_combine_dinv<<<Blocks(S->nn), kRedThreads, 0, S->stream>>>(
+        S->nn, S->ndir, lambda, S->sh->d_dM, S->sh->d_dL, S->d_dinv, S->dinv32);
+    NKB_CUDA_TRY(cudaGetLastError());
+    NKB_CUDA_TRY(cudaStreamSynchronize(S->stream));
+    S->lambda     = lambda;
+    S->has_lambda = true;
+    DropGraphs(S); // the captured launches carry the old lambda
+    return NKB_OK;
+}
+
+extern "C" int nkb_sys_footprint(const nkb_sys *S, size_t *shared_bytes, size_t *instance_bytes)
+{
+    ClearError();
+    if (!S)
+        return SetError(NKB_ERR_INVALID, "nkb_sys_footprint: NULL system");
+    if (shared_bytes)
+        *shared_bytes = S->sh->bytes;
+    if (instance_bytes)
+        *instance_bytes = S->bytes;
+    return NKB_OK;
+}
 extern "C" int nkb_sys_diag_inv(nkb_sys *S, double *diag_inv, int flags, void *stream)
 {
     if (!S || !diag_inv)
@@ -652,129 +970,294 @@ extern "C" int nkb_sys_matvec_local(nkb_sys *S, const double *x_loc, double *y_l
     return Matvec(S, x_loc, y_loc, false, s);
 }
 
+
 namespace nkb
 {
-// FP64 iterative refinement around an FP32 PCG, on the lifted system (bglob
-// already assembled): r = b - A x in FP64, an FP32 PCG solves A d = r to a
-// relative reduction inner_tol (FP64 sums of the dot products), x += d in
-// FP64, until ||r||^2 < tol^2 ||b||^2 (NekLinSysIterCG's criterion). The
-// geometry, the residual, the norms and the solution stay FP64; S->st ends
-// with the FP64 residual and the total inner iteration count.
-static int MixedSolve(nkb_sys *S, const nkb_cg_opts &o, cudaStream_t s, int *outer_out)
+// The solve runs as a sequence of device work blocks; after each block the
+// relevant CG state is copied to pinned host memory and an event recorded.
+// nkb_cg_poll looks at that state once the event has completed and issues the
+// next block, so several systems can be driven concurrently from one host
+// thread (each on its own stream) and nkb_cg_solve is the same machine
+// polled with waits.
+
+static int QueueState(nkb_sys *S, int which)
 {
-    const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
-    const int K   = o.check_interval;
-    const double tol       = std::fmax(o.tol, 1.0e-16);
-    const double inner_tol = o.inner_tol > 0 ? o.inner_tol : 1.0e-5;
-    const int max_outer    = o.max_outer > 0 ? o.max_outer : 40;
-    CGState h0;
+    const CGState *src = which == 0 ? S->st : S->st32;
+    NKB_CUDA_TRY(cudaMemcpyAsync(S->h_st + which, src, sizeof(CGState), cudaMemcpyDeviceToHost,
+                                 S->sv.s));
+    NKB_CUDA_TRY(cudaEventRecord(S->evq, S->sv.s));
+    return NKB_OK;
+}
+
+// h0 -> S->st: a fresh state with the stopping rule (NekLinSysIter.cpp:57)
+static int ResetState(nkb_sys *S)
+{
+    CGState &h0 = S->h_st[2];
     std::memset(&h0, 0, sizeof(h0));
-    h0.tol2  = tol * tol;
-    h0.maxit = o.maxit;
-    NKB_CUDA_TRY(cudaMemcpyAsync(S->st, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
+    const double tol = std::fmax(S->sv.o.tol, 1.0e-16);
+    h0.tol2          = tol * tol;
+    h0.maxit         = S->sv.o.maxit;
+    NKB_CUDA_TRY(cudaMemcpyAsync(S->st, &h0, sizeof(h0), cudaMemcpyHostToDevice, S->sv.s));
+    return NKB_OK;
+}
+
+// x_loc += GlobalToLocal(x) (the Dirichlet part of x is zero), copies back;
+// `fin` (if given) replaces the device state first
+static int Finish(nkb_sys *S, const CGState *fin)
+{
+    SolveCtx &v    = S->sv;
+    cudaStream_t s = v.s;
+    if (fin)
+    {
+        S->h_st[2] = *fin;
+        NKB_CUDA_TRY(cudaMemcpyAsync(S->st, S->h_st + 2, sizeof(CGState), cudaMemcpyHostToDevice, s));
+    }
+    k_global_to_local<<<Blocks(S->nloc), kRedThreads, 0, s>>>(S->nloc, S->d_map, S->d_sign, S->x,
+                                                               S->tl);
+    k_axpy_loc<<<Blocks(S->nloc), kRedThreads, 0, s>>>(S->nloc, 1.0, S->tl, v.dx);
+    S->launches += 2;
+    NKB_CUDA_TRY(cudaEventRecord(S->ev1, s));
+    if (v.flags & NKB_HOST_PTRS)
+        NKB_CUDA_TRY(cudaMemcpyAsync(v.x_user, v.dx, S->nloc * sizeof(double),
+                                     cudaMemcpyDeviceToHost, s));
+    v.phase = kFinishing;
+    return QueueState(S, 0);
+}
+
+static int Begin64(nkb_sys *S)
+{
+    SolveCtx &v    = S->sv;
+    cudaStream_t s = v.s;
+    int rc         = ResetState(S);
+    if (rc)
+        return rc;
+    const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
+    k_init<<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->bglob, S->r, S->x, S->w, S->s, S->p,
+                                       S->q, S->partA);
+    // partA holds (b,b) in [0] and (r,r) in [1]; k_scalars mode 0 reads eps
+    // from partA[1] and rhs from partB[0]
+    k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbA, S->partA, nbA, 0);
+    k_precon<double><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st, S->r, S->w, S->d_dinv,
+                                                 S->partA);
+    if ((rc = Matvec(S, S->w, S->yl, true, s)))
+        return rc;
+    k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
+                                                   S->d_sign, S->yl, S->s, S->w, S->st, S->partB);
+    k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbU, S->partB, nbA, 1);
+    NKB_CUDA_TRY(cudaGetLastError());
+    S->launches += 5 + long(S->ops.size());
+    v.use_graph = v.o.use_graph != 0 && s != cudaStreamLegacy && s != cudaStreamPerThread;
+    if (v.use_graph && (rc = EnsureGraph(S, false, s, v.o.check_interval)))
+        return rc;
+    v.passes     = 0;
+    v.max_passes = v.o.maxit / v.o.check_interval + 2;
+    v.phase      = kRun64;
+    return QueueState(S, 0);
+}
+
+static int Step64(nkb_sys *S)
+{
+    SolveCtx &v = S->sv;
+    if (S->h_st[0].done || v.passes >= v.max_passes)
+        return Finish(S, nullptr);
+    const int K = v.o.check_interval;
+    if (v.use_graph)
+    {
+        NKB_CUDA_TRY(cudaGraphLaunch(S->graph, v.s));
+        S->launches += long(K) * (3 + long(S->ops.size()));
+    }
+    else
+    {
+        for (int k = 0; k < K; ++k)
+        {
+            int rc = Iteration(S, v.s);
+            if (rc)
+                return rc;
+        }
+    }
+    ++v.passes;
+    return QueueState(S, 0);
+}
+
+// Mixed precision: FP32 PCG (operators, vectors, preconditioner in FP32; dot
+// products summed in FP64) with reliable updates. Whenever the iterated FP32
+// residual has dropped by the factor delta since the last update, the FP32
+// correction is folded into the FP64 solution, the true residual b - A x is
+// recomputed with the FP64 operators, and the FP32 recurrence continues from
+// it with its search direction kept (no restart, so the Krylov convergence is
+// preserved). Convergence is decided on the FP64 residual only, with the
+// FP64 criterion eps < tol^2 |b|^2.
+// The FP32 operator's rounding is relative to |A||p|, not |Ap|: on smooth
+// vectors it grows with the condition number, and the true residual can then
+// drift far from the iterated one (the search directions are no longer
+// conjugate). When an update finds |r_true|^2 > kDrift |r_iter|^2 the FP32
+// recurrence restarts from the true residual (iterative refinement) and runs
+// each restarted cycle to the deeper reduction kRestartReduction.
+// The recurrence can also stall (the iterated residual stops falling): after
+// kStallPolls polls without a new minimum (10 % lower) the cycle is ended by a
+// reliable update and a restart.
+constexpr double kDrift            = 2.0;
+constexpr double kRestartReduction = 1.0e-3;
+constexpr int kStallPolls          = 8;
+
+static int BeginMixed(nkb_sys *S)
+{
+    SolveCtx &v    = S->sv;
+    cudaStream_t s = v.s;
+    if (s == cudaStreamLegacy || s == cudaStreamPerThread)
+        return SetError(NKB_ERR_INVALID, "mixed-precision solve needs a created stream");
+    int rc = ResetState(S);
+    if (rc)
+        return rc;
+    const int nbA = Blocks(S->nglob);
     k_init<<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->bglob, S->r, S->x, S->w, S->s, S->p,
                                        S->q, S->partA);
     k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbA, S->partA, nbA, 0);
     S->launches += 2;
-    if (S->graph32 == nullptr || S->graph32_k != K)
-    {
-        if (S->graph32)
-            cudaGraphExecDestroy(S->graph32);
-        S->graph32 = nullptr;
-        cudaGraph_t g;
-        NKB_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        int crc = NKB_OK;
-        for (int k = 0; k < K && !crc; ++k)
-            crc = Iteration32(S, s);
-        cudaError_t ce = cudaStreamEndCapture(s, &g);
-        S->launches -= long(K) * (3 + long(S->ops32.size()));
-        if (crc)
-            return crc;
-        if (ce != cudaSuccess)
-            return SetError(NKB_ERR_CUDA, "mixed CG graph capture: %s", cudaGetErrorString(ce));
-        ce = cudaGraphInstantiate(&S->graph32, g, 0);
-        cudaGraphDestroy(g);
-        if (ce != cudaSuccess)
-            return SetError(NKB_ERR_CUDA, "mixed CG graph instantiate: %s", cudaGetErrorString(ce));
-        S->graph32_k = K;
-    }
-    int total = 0, outer = 0, rc = NKB_OK;
-    CGState h, h32;
-    for (; outer <= max_outer; ++outer)
-    {
-        NKB_CUDA_TRY(cudaMemcpyAsync(&h, S->st, sizeof(h), cudaMemcpyDeviceToHost, s));
-        NKB_CUDA_TRY(cudaStreamSynchronize(s));
-        if (!std::isfinite(h.eps))
-        {
-            h.done   = 1;
-            h.status = NKB_ERR_NONFINITE;
-            break;
-        }
-        if (h.done || h.eps < h.tol2 * h.rhs_mag)
-        {
-            h.done   = 1;
-            h.status = NKB_OK;
-            break;
-        }
-        if (outer == max_outer || total >= o.maxit)
-        {
-            h.done   = 1;
-            h.status = NKB_ERR_NOT_CONVERGED;
-            break;
-        }
-        // inner FP32 PCG on A d = r
+    if ((rc = EnsureGraph(S, true, s, v.o.check_interval)))
+        return rc;
+    v.delta      = v.o.inner_tol > 0 ? std::fmin(v.o.inner_tol, 0.5) : 0.1;
+    v.max_upd    = v.o.max_outer > 0 ? v.o.max_outer : 1000;
+    v.updates    = 0;
+    v.passes     = 0;
+    v.max_passes = v.o.maxit / v.o.check_interval + 2;
+    v.phase      = kMixStart;
+    return QueueState(S, 0);
+}
+
+// FP32 recurrence from r32 (reset: x32 = 0 and a first direction; otherwise
+// a continuation after a reliable update)
+static int Launch32Start(nkb_sys *S, double eps, bool reset, double reduction)
+{
+    SolveCtx &v    = S->sv;
+    cudaStream_t s = v.s;
+    const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
+    if (reset)
         k_init_inner<<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->r, S->r32, S->x32, S->w32,
                                                  S->s32, S->p32, S->q32, S->partA);
-        k_scalars_inner_init<<<1, 1024, 0, s>>>(S->st32, S->partA, nbA, inner_tol * inner_tol,
-                                                o.maxit - total);
-        k_precon<float><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st32, S->r32, S->w32,
-                                                    S->dinv32, S->partA);
-        if ((rc = Matvec32(S, S->w32, S->yl32, s, &S->st32->done)))
-            return rc;
-        k_assemble<float><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
-                                                      S->d_sign, S->yl32, S->s32, S->w32, S->st32,
-                                                      S->partB);
-        k_scalars<<<1, 1024, 0, s>>>(S->st32, S->partA, nbU, S->partB, nbA, 1);
-        S->launches += 6 + long(S->ops32.size());
-        const int max_passes = (o.maxit - total) / K + 2;
-        for (int pass = 0; pass < max_passes; ++pass)
+    k_resume<<<1, 1, 0, s>>>(S->st32, std::fmax(reduction * reduction * eps, v.thr_final),
+                             std::max(v.o.maxit - v.iter_base, 1), reset ? 1 : 0);
+    k_precon<float><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st32, S->r32, S->w32, S->dinv32,
+                                                S->partA);
+    int rc = Matvec32(S, S->w32, S->yl32, s, &S->st32->done);
+    if (rc)
+        return rc;
+    k_assemble<float><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
+                                                  S->d_sign, S->yl32, S->s32, S->w32, S->st32,
+                                                  S->partB);
+    k_scalars<<<1, 1024, 0, s>>>(S->st32, S->partA, nbU, S->partB, nbA, reset ? 1 : 3);
+    NKB_CUDA_TRY(cudaGetLastError());
+    S->launches += (reset ? 5 : 4) + long(S->ops32.size());
+    v.phase     = kRun32;
+    v.cycle_min = eps;
+    v.stall     = 0;
+    return QueueState(S, 1);
+}
+
+static int StepMixStart(nkb_sys *S)
+{
+    SolveCtx &v     = S->sv;
+    const CGState h = S->h_st[0];
+    v.thr_final     = h.tol2 * h.rhs_mag;
+    if (h.done)
+        return Finish(S, nullptr);
+    return Launch32Start(S, h.eps, true, v.delta);
+}
+
+static int StepRun32(nkb_sys *S)
+{
+    SolveCtx &v       = S->sv;
+    const CGState h32 = S->h_st[1];
+    if (!h32.done)
+    {
+        if (h32.eps < 0.9 * v.cycle_min)
         {
-            NKB_CUDA_TRY(cudaMemcpyAsync(&h32, S->st32, sizeof(h32), cudaMemcpyDeviceToHost, s));
-            NKB_CUDA_TRY(cudaStreamSynchronize(s));
-            if (h32.done)
-                break;
-            NKB_CUDA_TRY(cudaGraphLaunch(S->graph32, s));
-            S->launches += long(K) * (3 + long(S->ops32.size()));
+            v.cycle_min = h32.eps;
+            v.stall     = 0;
         }
-        NKB_CUDA_TRY(cudaMemcpyAsync(&h32, S->st32, sizeof(h32), cudaMemcpyDeviceToHost, s));
-        NKB_CUDA_TRY(cudaStreamSynchronize(s));
-        total += std::max(h32.iter, 1);
-        // x += d; r = b - A x and its norm, all FP64
-        k_add_correction<<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->x, S->x32);
-        if ((rc = Matvec(S, S->x, S->yl, true, s)))
-            return rc;
-        k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
-                                                       S->d_sign, S->yl, S->s, nullptr, nullptr,
-                                                       nullptr);
-        k_residual<<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->bglob, S->s, S->r, S->partA);
-        k_scalars_outer<<<1, 1024, 0, s>>>(S->st, S->partA, nbU);
-        S->launches += 4 + long(S->ops.size());
-        NKB_CUDA_TRY(cudaGetLastError());
+        else if (++v.stall >= kStallPolls)
+        {
+            v.force_restart = true;
+        }
     }
-    h.iter = total;
-    NKB_CUDA_TRY(cudaMemcpyAsync(S->st, &h, sizeof(h), cudaMemcpyHostToDevice, s));
-    NKB_CUDA_TRY(cudaStreamSynchronize(s));
-    *outer_out = outer;
-    return NKB_OK;
+    if (!h32.done && !v.force_restart && v.passes < v.max_passes)
+    {
+        NKB_CUDA_TRY(cudaGraphLaunch(S->graph32, v.s));
+        S->launches += long(v.o.check_interval) * (3 + long(S->ops32.size()));
+        ++v.passes;
+        return QueueState(S, 1);
+    }
+    v.last32 = h32;
+    if (h32.status == NKB_ERR_NONFINITE)
+    {
+        CGState fin = S->h_st[0];
+        fin.done    = 1;
+        fin.status  = NKB_ERR_NONFINITE;
+        fin.iter    = v.iter_base + h32.iter;
+        return Finish(S, &fin);
+    }
+    // reliable update: x += x32 (x32 = 0), r = b - A x in FP64, r32 = (float) r
+    cudaStream_t s = v.s;
+    const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
+    k_add_correction<<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->x, S->x32);
+    int rc = Matvec(S, S->x, S->yl, true, s);
+    if (rc)
+        return rc;
+    k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
+                                                   S->d_sign, S->yl, S->s, nullptr, nullptr,
+                                                   nullptr);
+    k_residual<<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->bglob, S->s, S->r, S->r32, S->partA);
+    k_scalars_outer<<<1, 1024, 0, s>>>(S->st, S->partA, nbU);
+    NKB_CUDA_TRY(cudaGetLastError());
+    S->launches += 4 + long(S->ops.size());
+    ++v.updates;
+    v.phase = kUpdate;
+    return QueueState(S, 0);
+}
+
+static int StepUpdate(nkb_sys *S)
+{
+    SolveCtx &v = S->sv;
+    CGState h   = S->h_st[0];
+    bool stop   = true;
+    int status  = NKB_OK;
+    if (!std::isfinite(h.eps))
+        status = NKB_ERR_NONFINITE;
+    else if (h.eps < v.thr_final)
+        status = NKB_OK;
+    else if (v.last32.status == NKB_ERR_NOT_CONVERGED || v.updates >= v.max_upd ||
+             v.iter_base + v.last32.iter >= v.o.maxit ||
+             v.passes >= v.max_passes)
+        status = NKB_ERR_NOT_CONVERGED;
+    else
+        stop = false;
+    if (stop)
+    {
+        h.done   = 1;
+        h.status = status;
+        h.iter   = v.iter_base + v.last32.iter;
+        return Finish(S, &h);
+    }
+    if (v.force_restart || h.eps > kDrift * v.last32.eps)
+    {
+        v.force_restart = false;
+        // the FP32 recurrence has lost track of the true residual: restart it
+        v.iter_base += v.last32.iter;
+        ++v.restarts;
+        return Launch32Start(S, h.eps, true, kRestartReduction);
+    }
+    return Launch32Start(S, h.eps, false, v.delta);
 }
 } // namespace nkb
 
-extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
-                            const nkb_cg_opts *opts, nkb_cg_report *rep, int flags, void *stream)
+extern "C" int nkb_cg_begin(nkb_sys *S, const double *b_loc, double *x_loc,
+                            const nkb_cg_opts *opts, int flags, void *stream)
 {
     ClearError();
     if (!S || !b_loc || !x_loc)
-        return SetError(NKB_ERR_INVALID, "nkb_cg_solve: NULL argument");
+        return SetError(NKB_ERR_INVALID, "nkb_cg_begin: NULL argument");
+    if (Busy(S))
+        return SetError(NKB_ERR_INVALID, "nkb_cg_begin: a solve is already in progress");
     nkb_cg_opts o;
     std::memset(&o, 0, sizeof(o));
     o.tol            = 1e-9;
@@ -790,142 +1273,127 @@ extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
     if (o.check_interval <= 0)
         o.check_interval = 16;
     if (o.mixed && S->ops32.empty())
-        return SetError(NKB_ERR_INVALID, "nkb_cg_solve: mixed precision needs FP32 operators "
+        return SetError(NKB_ERR_INVALID, "nkb_cg_begin: mixed precision needs FP32 operators "
                                          "(nkb_sys_desc.ops32)");
     NKB_CUDA_TRY(cudaSetDevice(S->device));
+    SolveCtx &v = S->sv;
+    v           = SolveCtx();
+    v.o         = o;
+    v.flags     = flags;
     // NULL (or the legacy default stream) -> the system's own stream
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : S->stream;
-    const long nloc = S->nloc;
-
+    v.s              = stream ? static_cast<cudaStream_t>(stream) : S->stream;
+    cudaStream_t s   = v.s;
+    const long nloc  = S->nloc;
     const double *db = b_loc;
-    double *dx       = x_loc;
+    v.x_user         = x_loc;
+    v.dx             = x_loc;
     if (flags & NKB_HOST_PTRS)
     {
-        if (!S->stage && cudaMalloc(&S->stage, 2 * nloc * sizeof(double)) != cudaSuccess)
-            return SetError(NKB_ERR_NOMEM, "nkb_cg_solve: staging buffers");
+        if (!S->stage)
+        {
+            if (cudaMalloc(&S->stage, 2 * nloc * sizeof(double)) != cudaSuccess)
+                return SetError(NKB_ERR_NOMEM, "nkb_cg_begin: staging buffers");
+            S->bytes += 2 * nloc * sizeof(double);
+        }
         NKB_CUDA_TRY(cudaMemcpyAsync(S->stage, b_loc, nloc * sizeof(double), cudaMemcpyHostToDevice, s));
-        NKB_CUDA_TRY(cudaMemcpyAsync(S->stage + nloc, x_loc, nloc * sizeof(double), cudaMemcpyHostToDevice, s));
-        db = S->stage;
-        dx = S->stage + nloc;
+        NKB_CUDA_TRY(cudaMemcpyAsync(S->stage + nloc, x_loc, nloc * sizeof(double),
+                                     cudaMemcpyHostToDevice, s));
+        db   = S->stage;
+        v.dx = S->stage + nloc;
     }
     NKB_CUDA_TRY(cudaEventRecord(S->ev0, s));
     S->launches = 0;
-
     // Dirichlet lifting (GlobalLinSysIterativeFull.cpp:104-164):
     // rhs = b - A x_D (local), gloIn = Assemble(rhs)
-    int rc = Matvec(S, dx, S->yl, false, s);
+    int rc = Matvec(S, v.dx, S->yl, false, s);
+    if (rc == NKB_OK)
+    {
+        k_sub_loc<<<Blocks(nloc), kRedThreads, 0, s>>>(nloc, db, S->yl, S->tl);
+        k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, s>>>(
+            S->nglob, S->ndir, S->d_aptr, S->d_aidx, S->d_sign, S->tl, S->bglob, nullptr, nullptr,
+            nullptr);
+        S->launches += 2 + long(S->ops.size());
+        rc = o.mixed ? BeginMixed(S) : Begin64(S);
+    }
     if (rc)
-        return rc;
-    k_sub_loc<<<Blocks(nloc), kRedThreads, 0, s>>>(nloc, db, S->yl, S->tl);
-    k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, s>>>(
-        S->nglob, S->ndir, S->d_aptr, S->d_aidx, S->d_sign, S->tl, S->bglob, nullptr, nullptr, nullptr);
+        v.phase = kIdle;
+    return rc;
+}
 
-    int outer_done = 0;
-    if (o.mixed)
+extern "C" int nkb_cg_poll(nkb_sys *S, int wait, int *done)
+{
+    ClearError();
+    if (!S || !done)
+        return SetError(NKB_ERR_INVALID, "nkb_cg_poll: NULL argument");
+    *done       = 0;
+    SolveCtx &v = S->sv;
+    if (v.phase == kIdle)
+        return SetError(NKB_ERR_INVALID, "nkb_cg_poll: no solve in progress");
+    if (v.phase == kFinished)
     {
-        if ((rc = MixedSolve(S, o, s, &outer_done)))
-            return rc;
-        goto finish;
+        *done = 1;
+        return NKB_OK;
     }
+    NKB_CUDA_TRY(cudaSetDevice(S->device));
+    if (wait)
     {
-    CGState h0;
-    std::memset(&h0, 0, sizeof(h0));
-    const double tol = std::fmax(o.tol, 1.0e-16); // NekLinSysIter.cpp:57
-    h0.tol2          = tol * tol;
-    h0.maxit         = o.maxit;
-    NKB_CUDA_TRY(cudaMemcpyAsync(S->st, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
-    const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
-    k_init<<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->bglob, S->r, S->x, S->w, S->s, S->p,
-                                       S->q, S->partA);
-    // partA holds (b,b) in [0] and (r,r) in [1]; k_scalars mode 0 reads eps
-    // from partA[1] and rhs from partB[0]
-    k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbA, S->partA, nbA, 0);
-    k_precon<double><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st, S->r, S->w, S->d_dinv, S->partA);
-    if ((rc = Matvec(S, S->w, S->yl, true, s)))
-        return rc;
-    k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
-                                                   S->d_sign, S->yl, S->s, S->w, S->st, S->partB);
-    k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbU, S->partB, nbA, 1);
-    NKB_CUDA_TRY(cudaGetLastError());
-    // lift (ops + sub + assemble), init, scalars, precon, ops, assemble, scalars
-    S->launches += 2 * long(S->ops.size()) + 7;
-
-    const int K = o.check_interval;
-    bool use_graph = o.use_graph != 0;
-    if (use_graph && (S->graph == nullptr || S->graph_k != K))
-    {
-        if (S->graph)
+        const cudaError_t e = cudaEventSynchronize(S->evq);
+        if (e != cudaSuccess)
         {
-            cudaGraphExecDestroy(S->graph);
-            S->graph = nullptr;
-        }
-        if (s != cudaStreamLegacy && s != cudaStreamPerThread)
-        {
-            cudaGraph_t g;
-            NKB_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-            int crc = NKB_OK;
-            for (int k = 0; k < K && !crc; ++k)
-                crc = Iteration(S, s);
-            cudaError_t ce = cudaStreamEndCapture(s, &g);
-            if (crc)
-                return crc;
-            if (ce != cudaSuccess)
-                return SetError(NKB_ERR_CUDA, "nkb_cg_solve: graph capture: %s", cudaGetErrorString(ce));
-            ce = cudaGraphInstantiate(&S->graph, g, 0);
-            cudaGraphDestroy(g);
-            if (ce != cudaSuccess)
-                return SetError(NKB_ERR_CUDA, "nkb_cg_solve: graph instantiate: %s", cudaGetErrorString(ce));
-            S->graph_k = K;
-            S->launches -= long(K) * (3 + long(S->ops.size())); // captured, not launched
-        }
-        else
-        {
-            use_graph = false; // caller stream: launch directly
+            v.phase = kIdle;
+            return SetError(NKB_ERR_CUDA, "nkb_cg_poll: %s", cudaGetErrorString(e));
         }
     }
-    // iterate until the device reports done; each pass runs K iterations
-    // (kernels are no-ops once done is set)
-    const int max_passes = o.maxit / K + 2;
-    for (int pass = 0; pass < max_passes; ++pass)
+    else
     {
-        NKB_CUDA_TRY(cudaMemcpyAsync(S->h_st, S->st, sizeof(CGState), cudaMemcpyDeviceToHost, s));
-        NKB_CUDA_TRY(cudaStreamSynchronize(s));
-        if (S->h_st->done)
+        const cudaError_t q = cudaEventQuery(S->evq);
+        if (q == cudaErrorNotReady)
+            return NKB_OK;
+        if (q != cudaSuccess)
+        {
+            v.phase = kIdle;
+            return SetError(NKB_ERR_CUDA, "nkb_cg_poll: %s", cudaGetErrorString(q));
+        }
+    }
+    int rc = NKB_OK;
+    switch (v.phase)
+    {
+        case kRun64: rc = Step64(S); break;
+        case kMixStart: rc = StepMixStart(S); break;
+        case kRun32: rc = StepRun32(S); break;
+        case kUpdate: rc = StepUpdate(S); break;
+        case kFinishing:
+            v.phase = kFinished;
+            *done   = 1;
             break;
-        if (use_graph)
-        {
-            NKB_CUDA_TRY(cudaGraphLaunch(S->graph, s));
-            S->launches += long(K) * (3 + long(S->ops.size()));
-        }
-        else
-        {
-            for (int k = 0; k < K; ++k)
-                if ((rc = Iteration(S, s)))
-                    return rc;
-        }
+        default: break;
     }
-    }
-finish:
-    NKB_CUDA_TRY(cudaMemcpyAsync(S->h_st, S->st, sizeof(CGState), cudaMemcpyDeviceToHost, s));
-    // x_loc += GlobalToLocal(x) (the Dirichlet part of x is zero)
-    k_global_to_local<<<Blocks(nloc), kRedThreads, 0, s>>>(nloc, S->d_map, S->d_sign, S->x, S->tl);
-    k_axpy_loc<<<Blocks(nloc), kRedThreads, 0, s>>>(nloc, 1.0, S->tl, dx);
-    S->launches += 2;
-    NKB_CUDA_TRY(cudaEventRecord(S->ev1, s));
-    if (flags & NKB_HOST_PTRS)
-        NKB_CUDA_TRY(cudaMemcpyAsync(x_loc, dx, nloc * sizeof(double), cudaMemcpyDeviceToHost, s));
-    NKB_CUDA_TRY(cudaStreamSynchronize(s));
-    const CGState &h = *S->h_st;
+    if (rc)
+        v.phase = kIdle;
+    return rc;
+}
+
+extern "C" int nkb_cg_end(nkb_sys *S, nkb_cg_report *rep)
+{
+    ClearError();
+    if (!S)
+        return SetError(NKB_ERR_INVALID, "nkb_cg_end: NULL system");
+    SolveCtx &v = S->sv;
+    if (v.phase != kFinished)
+        return SetError(NKB_ERR_INVALID, "nkb_cg_end: the solve has not finished (poll until done)");
+    v.phase         = kIdle;
+    const CGState h = S->h_st[0];
     if (rep)
     {
         rep->iterations       = h.iter;
-        rep->outer_iterations = outer_done;
+        rep->outer_iterations = v.updates;
         rep->rel_residual     = std::sqrt(h.eps / h.rhs_mag);
         rep->converged        = (h.done && h.status == NKB_OK) ? 1 : 0;
         float ms              = 0.f;
         cudaEventElapsedTime(&ms, S->ev0, S->ev1);
         rep->device_ms       = ms;
         rep->kernel_launches = S->launches;
+        rep->restarts        = v.restarts;
     }
     if (h.status == NKB_ERR_NONFINITE)
         return SetError(NKB_ERR_NONFINITE, "nkb_cg_solve: non-finite CG scalar at iteration %d", h.iter);
@@ -936,11 +1404,26 @@ finish:
     return NKB_OK;
 }
 
+extern "C" int nkb_cg_solve(nkb_sys *S, const double *b_loc, double *x_loc,
+                            const nkb_cg_opts *opts, nkb_cg_report *rep, int flags, void *stream)
+{
+    int rc = nkb_cg_begin(S, b_loc, x_loc, opts, flags, stream);
+    if (rc)
+        return rc;
+    int done = 0;
+    while (!done)
+        if ((rc = nkb_cg_poll(S, 1, &done)))
+            return rc;
+    return nkb_cg_end(S, rep);
+}
+
 extern "C" int nkb_sys_profile_iteration(nkb_sys *S, int iters, nkb_sys_profile *prof)
 {
     ClearError();
     if (!S || !prof || iters < 1)
         return SetError(NKB_ERR_INVALID, "nkb_sys_profile_iteration: bad arguments");
+    if (Busy(S))
+        return SetError(NKB_ERR_INVALID, "nkb_sys_profile_iteration: a solve is in progress");
     NKB_CUDA_TRY(cudaSetDevice(S->device));
     cudaStream_t s = S->stream;
     const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
@@ -1023,39 +1506,25 @@ extern "C" void nkb_sys_destroy(nkb_sys *S)
     if (!S)
         return;
     cudaSetDevice(S->device);
-    if (S->graph)
-        cudaGraphExecDestroy(S->graph);
-    if (S->graph32)
-        cudaGraphExecDestroy(S->graph32);
+    if (S->stream)
+        cudaStreamSynchronize(S->stream); // a solve may still be in flight
+    if (S->sv.s && S->sv.s != S->stream)
+        cudaStreamSynchronize(S->sv.s);
+    DropGraphs(S);
     for (void *ptr : {(void *)S->w32, (void *)S->s32, (void *)S->x32, (void *)S->p32,
                       (void *)S->r32, (void *)S->q32, (void *)S->dinv32, (void *)S->yl32,
-                      (void *)S->st32})
+                      (void *)S->st32, (void *)S->d_dinv, (void *)S->w, (void *)S->s,
+                      (void *)S->x, (void *)S->bglob, (void *)S->p, (void *)S->r, (void *)S->q,
+                      (void *)S->yl, (void *)S->tl, (void *)S->partA, (void *)S->partB,
+                      (void *)S->st, (void *)S->stage})
         cudaFree(ptr);
-    cudaFree(S->d_map);
-    cudaFree(S->d_sign);
-    cudaFree(S->d_aptr);
-    cudaFree(S->d_aidx);
-    cudaFree(S->d_dinv);
-    cudaFree(S->w);
-    cudaFree(S->s);
-    cudaFree(S->x);
-    cudaFree(S->bglob);
-    cudaFree(S->p);
-    cudaFree(S->r);
-    cudaFree(S->q);
-    cudaFree(S->yl);
-    cudaFree(S->tl);
-    cudaFree(S->partA);
-    cudaFree(S->partB);
-    cudaFree(S->st);
-    cudaFree(S->stage);
     if (S->h_st)
         cudaFreeHost(S->h_st);
-    if (S->ev0)
-        cudaEventDestroy(S->ev0);
-    if (S->ev1)
-        cudaEventDestroy(S->ev1);
+    for (cudaEvent_t e : {S->ev0, S->ev1, S->evq})
+        if (e)
+            cudaEventDestroy(e);
     if (S->stream)
         cudaStreamDestroy(S->stream);
+    S->sh.reset(); // the shared map and diagonal go with the last user
     delete S;
 }

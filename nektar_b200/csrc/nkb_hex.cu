@@ -133,6 +133,72 @@ template <typename T> static int AutotuneHex(nkb_op *op, int *best)
     return NKB_OK;
 }
 
+// Launch shape of the generic kernel (threads per CTA, elements per CTA),
+// timed on the operator's own sizes the same way and cached per (shape,
+// operator, precision, nm, element count). The arithmetic of an element does
+// not depend on the launch shape, so the choice never changes results.
+static std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> g_gen_cache;
+
+template <typename T> static int AutotuneGeneric(nkb_op *op)
+{
+    const auto key = std::make_tuple(op->shape, op->optype, op->precision, op->nm, op->nelmt);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_gen_cache.find(key);
+        if (it != g_gen_cache.end())
+        {
+            op->gen_epb     = it->second.first;
+            op->gen_threads = it->second.second;
+            return NKB_OK;
+        }
+    }
+    if (op->nelmt <= 0)
+        return NKB_OK;
+    const size_t ebyt = GenericSmemBytes(op, int(sizeof(T)));
+    const size_t nmax = size_t(op->nelmt) * size_t(std::max(op->nc, op->nt));
+    T *buf            = nullptr;
+    if (cudaMalloc(&buf, 4 * nmax * sizeof(T)) != cudaSuccess)
+        return SetError(NKB_ERR_NOMEM, "autotune buffers");
+    cudaMemsetAsync(buf, 0, 4 * nmax * sizeof(T), op->stream);
+    float best_ms = 1e30f;
+    int best_e = 0, best_t = 0, rc = NKB_OK;
+    const int threads[3] = {64, 128, 256};
+    const int epbs[4]    = {1, 2, 4, 8};
+    for (int ti = 0; ti < 3 && !rc; ++ti)
+        for (int ei = 0; ei < 4 && !rc; ++ei)
+        {
+            if (ebyt * epbs[ei] > 96 * 1024)
+                continue;
+            op->gen_threads = threads[ti];
+            op->gen_epb     = epbs[ei];
+            T *in = buf, *o0 = buf + nmax, *o1 = buf + 2 * nmax, *o2 = buf + 3 * nmax;
+            if ((rc = LaunchGeneric<T>(op, in, o0, o1, o2, nullptr, nullptr, op->stream)))
+                break;
+            cudaEventRecord(op->ev0, op->stream);
+            for (int it = 0; it < 3 && !rc; ++it)
+                rc = LaunchGeneric<T>(op, in, o0, o1, o2, nullptr, nullptr, op->stream);
+            cudaEventRecord(op->ev1, op->stream);
+            if (rc || cudaEventSynchronize(op->ev1) != cudaSuccess)
+                break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, op->ev0, op->ev1);
+            if (ms < best_ms)
+            {
+                best_ms = ms;
+                best_e  = epbs[ei];
+                best_t  = threads[ti];
+            }
+        }
+    cudaFree(buf);
+    op->gen_epb     = best_e;
+    op->gen_threads = best_t;
+    if (rc)
+        return rc;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_gen_cache[key] = std::make_pair(best_e, best_t);
+    return NKB_OK;
+}
+
 static bool SameTable(const std::vector<double> &a, const std::vector<double> &b)
 {
     return a.size() == b.size() && std::equal(a.begin(), a.end(), b.begin());
@@ -172,7 +238,10 @@ int ChooseKernel(nkb_op *op)
         return SetError(NKB_ERR_UNSUPPORTED,
                         "nkb_op_create: nm=%d nq=(%d,%d,%d) needs %zu bytes of shared memory per "
                         "element", op->nm, op->nq[0], op->nq[1], op->nq[2], GenericSmemBytes(op, eb));
-    return NKB_OK;
+    const char *tune = std::getenv("NKB_GENERIC_TUNE");
+    if (tune && std::strcmp(tune, "0") == 0)
+        return NKB_OK;
+    return op->precision == NKB_FP64 ? AutotuneGeneric<double>(op) : AutotuneGeneric<float>(op);
 }
 
 void FreeKernelData(nkb_op *op)
@@ -182,11 +251,13 @@ void FreeKernelData(nkb_op *op)
 
 template <typename T>
 int LaunchOp(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
-             const double *gsign, cudaStream_t s, const int *skip)
+             const double *gsign, cudaStream_t s, const int *skip, const double *lambda)
 {
     if (op->variant == kVariantHexHelm)
     {
         HexArgs<T> a = MakeHexArgs<T>(op);
+        if (lambda)
+            a.lambda = T(*lambda);
         a.in         = in;
         a.out        = o0;
         a.gmap       = gmap;
@@ -194,12 +265,14 @@ int LaunchOp(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap
         a.skip       = skip;
         return HexLaunchT<T>(op, a, gmap != nullptr, s, op->hex_variant, false);
     }
-    return LaunchGeneric<T>(op, in, o0, o1, o2, gmap, gsign, s, skip);
+    return LaunchGeneric<T>(op, in, o0, o1, o2, gmap, gsign, s, skip, lambda);
 }
 
 template int LaunchOp<double>(const nkb_op *, const double *, double *, double *, double *,
-                              const int *, const double *, cudaStream_t, const int *);
+                              const int *, const double *, cudaStream_t, const int *,
+                              const double *);
 template int LaunchOp<float>(const nkb_op *, const float *, float *, float *, float *,
-                             const int *, const double *, cudaStream_t, const int *);
+                             const int *, const double *, cudaStream_t, const int *,
+                             const double *);
 
 } // namespace nkb

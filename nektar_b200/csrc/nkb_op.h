@@ -36,6 +36,8 @@ struct nkb_op
     // kernel selection (nkb_hex.cu): 0 generic, >0 tuned variant
     int variant     = 0;
     int hex_variant = 0; // tuned Hex kernel variant chosen by the autotuner
+    int gen_epb     = 0; // generic kernel: elements per CTA (0: default)
+    int gen_threads = 0; // generic kernel: threads per CTA (0: default)
     void *kdata = nullptr;
     int *d_err  = nullptr; // device error word (bounded waits that gave up)
 
@@ -50,15 +52,21 @@ namespace nkb
 // generic kernels (nkb_ops.cu)
 template <typename T>
 int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
-                  const double *gsign, cudaStream_t s, const int *skip = nullptr);
+                  const double *gsign, cudaStream_t s, const int *skip = nullptr,
+                  const double *lambda = nullptr);
 // dispatch: tuned kernel if selected, else generic (nkb_hex.cu)
 // skip: optional device flag; when it reads nonzero the kernels return at once
 // (a converged CG keeps its captured graph but stops doing work)
+// lambda: optional host value overriding the operator's own Helmholtz lambda
+// for this launch (systems sharing one operator with different lambdas)
 template <typename T>
 int LaunchOp(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
-             const double *gsign, cudaStream_t s, const int *skip = nullptr);
+             const double *gsign, cudaStream_t s, const int *skip = nullptr,
+             const double *lambda = nullptr);
 int ChooseKernel(nkb_op *op);
 size_t GenericSmemBytes(const nkb_op *op, int elem_bytes);
 void FreeKernelData(nkb_op *op);
-int HelmholtzDiag(const nkb_op *op, double *d_out, cudaStream_t s);
+// element Helmholtz diagonals; with d_stiff the mass part (without lambda)
+// goes to d_out and the Laplacian part to d_stiff, else d_out = lambda M + L
+int HelmholtzDiag(const nkb_op *op, double *d_out, cudaStream_t s, double *d_stiff = nullptr);
 } // namespace nkb

@@ -353,30 +353,128 @@ template <int SHAPE, typename T> __global__ void k_diag(GenArgs<T> a)
         for (int l = threadIdx.x; l < d.nt; l += blockDim.x)
             BW::C(d, a.t, x, wb, u, l);
         __syncthreads();
-        T acc = 0;
+        // mass part sum W u^2 and Laplacian part sum grad u . G' grad u
+        T accm = 0, accl = 0;
         for (int l = threadIdx.x; l < d.nt; l += blockDim.x)
         {
             T q0, q1, q2;
             Grad(d, a.t, u, l, q0, q1, q2);
             const T W = G[l], G00 = G[d.nt + l], G11 = G[2 * d.nt + l], G22 = G[3 * d.nt + l];
             const T G01 = G[4 * d.nt + l], G02 = G[5 * d.nt + l], G12 = G[6 * d.nt + l];
-            T v = a.lambda * W * u[l] * u[l];
-            v   = fma(q0, fma(G00, q0, 2 * (G01 * q1 + G02 * q2)), v);
+            T v = q0 * fma(G00, q0, 2 * (G01 * q1 + G02 * q2));
             v   = fma(q1, fma(G11, q1, 2 * G12 * q2), v);
             v   = fma(q2, G22 * q2, v);
-            acc += v;
+            accm += W * u[l] * u[l];
+            accl += v;
         }
-        red[threadIdx.x] = acc;
+        T *red2           = red + blockDim.x;
+        red[threadIdx.x]  = accm;
+        red2[threadIdx.x] = accl;
         __syncthreads();
         for (int s = blockDim.x / 2; s > 0; s >>= 1)
         {
             if (threadIdx.x < s)
+            {
                 red[threadIdx.x] += red[threadIdx.x + s];
+                red2[threadIdx.x] += red2[threadIdx.x + s];
+            }
             __syncthreads();
         }
         if (threadIdx.x == 0)
-            a.out0[e * d.nc + m] = red[0];
+        {
+            if (a.out1)
+            {
+                a.out0[e * d.nc + m] = red[0];
+                a.out1[e * d.nc + m] = red2[0];
+            }
+            else
+            {
+                a.out0[e * d.nc + m] = fma(a.lambda, red[0], red2[0]);
+            }
+        }
         __syncthreads();
+    }
+}
+
+// Hex element diagonals by sum factorisation. With, per direction d, the
+// tables a_d = B_d^2, c_d = dB_d^2 and x_d = dB_d B_d (dB = D B, the basis
+// derivative at the points; element p, point i at [p*nq + i]):
+//   M_pqr = sum_ijk W a0[p,i] a1[q,j] a2[r,k]
+//   L_pqr = sum_ijk G'00 c0 a1 a2 + G'11 a0 c1 a2 + G'22 a0 a1 c2
+//                   + 2 (G'01 x0 x1 a2 + G'02 x0 a1 x2 + G'12 a0 x1 x2)
+// i.e. seven three-stage contractions of packed geometry fields against
+// products of 1-D tables, the same work as seven inner products, instead of
+// one full operator application per coefficient.
+// tab: [d][kind][nm*nq], kind 0 = a, 1 = c, 2 = x
+__global__ void k_hex_diag(int nm, int nq, const double *__restrict__ tab,
+                           const double *__restrict__ geo, long gstride, long nelmt, double lambda,
+                           double *__restrict__ out0, double *__restrict__ out1)
+{
+    extern __shared__ __align__(16) double sh[];
+    const long e = blockIdx.x;
+    if (e >= nelmt)
+        return;
+    const int nq2 = nq * nq, nq3 = nq2 * nq, nc = nm * nm * nm;
+    double *t1   = sh;                 // [p][k][j]  nm*nq*nq
+    double *t2   = t1 + nm * nq2;      // [p][q][k]  nm*nm*nq
+    double *accM = t2 + nm * nm * nq;  // nc
+    double *accL = accM + nc;          // nc
+    const double *G = geo + e * gstride;
+    for (int m = threadIdx.x; m < nc; m += blockDim.x)
+        accM[m] = accL[m] = 0.0;
+    // (field, table kind per direction, factor, into L)
+    const int field[7]   = {0, 1, 2, 3, 4, 5, 6};
+    const int kind[7][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                            {2, 2, 0}, {2, 0, 2}, {0, 2, 2}};
+    const double fac[7]  = {1, 1, 1, 1, 2, 2, 2};
+    const int tabn       = nm * nq;
+    for (int t = 0; t < 7; ++t)
+    {
+        const double *F  = G + field[t] * nq3;
+        const double *a0 = tab + (0 * 3 + kind[t][0]) * tabn;
+        const double *a1 = tab + (1 * 3 + kind[t][1]) * tabn;
+        const double *a2 = tab + (2 * 3 + kind[t][2]) * tabn;
+        __syncthreads();
+        for (int l = threadIdx.x; l < nm * nq2; l += blockDim.x)
+        {
+            const int p = l / nq2, kj = l - p * nq2; // kj = k*nq + j
+            double s = 0.0;
+            for (int i = 0; i < nq; ++i)
+                s = fma(F[kj * nq + i], a0[p * nq + i], s);
+            t1[l] = s;
+        }
+        __syncthreads();
+        for (int l = threadIdx.x; l < nm * nm * nq; l += blockDim.x)
+        {
+            const int pq = l / nq, k = l - pq * nq, p = pq / nm, q = pq - p * nm;
+            double s = 0.0;
+            for (int j = 0; j < nq; ++j)
+                s = fma(t1[(p * nq + k) * nq + j], a1[q * nq + j], s);
+            t2[l] = s;
+        }
+        __syncthreads();
+        double *acc = t == 0 ? accM : accL;
+        for (int m = threadIdx.x; m < nc; m += blockDim.x)
+        {
+            const int p = m % nm, q = (m / nm) % nm, r = m / (nm * nm);
+            double s = 0.0;
+            for (int k = 0; k < nq; ++k)
+                s = fma(t2[(p * nm + q) * nq + k], a2[r * nq + k], s);
+            acc[m] = fma(fac[t], s, acc[m]);
+        }
+    }
+    __syncthreads();
+    for (int m = threadIdx.x; m < nc; m += blockDim.x)
+    {
+        if (out1)
+        {
+            out0[e * nc + m] = accM[m];
+            out1[e * nc + m] = accL[m];
+        }
+        else
+        {
+            out0[e * nc + m] = fma(lambda, accM[m], accL[m]);
+        }
     }
 }
 
@@ -426,6 +524,9 @@ static int LaunchGenericT(const nkb_op *op, GenArgs<T> a, cudaStream_t s)
     const int es      = ElemSmem(a.d);
     const size_t ebyt = size_t(es) * sizeof(T);
     int epb           = int(std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / ebyt)));
+    if (op->gen_epb > 0)
+        epb = op->gen_epb; // autotuned (checked against the shared-memory limit)
+    const int threads = op->gen_threads > 0 ? op->gen_threads : 128;
     a.epb             = epb;
     const size_t smem = ebyt * epb;
     auto kern         = k_generic<SHAPE, OP, T>;
@@ -439,7 +540,7 @@ static int LaunchGenericT(const nkb_op *op, GenArgs<T> a, cudaStream_t s)
     }
     const long nb = (long(a.nelmt) + epb - 1) / epb;
     if (nb > 0)
-        kern<<<unsigned(nb), 128, smem, s>>>(a);
+        kern<<<unsigned(nb), threads, smem, s>>>(a);
     NKB_CUDA_TRY(cudaGetLastError());
     return NKB_OK;
 }
@@ -459,13 +560,13 @@ template <int OP, typename T> static int LaunchGenericShape(const nkb_op *op, Ge
 
 template <typename T>
 int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
-                  const double *gsign, cudaStream_t s, const int *skip)
+                  const double *gsign, cudaStream_t s, const int *skip, const double *lambda)
 {
     GenArgs<T> a;
     a.d      = MakeDims(op);
     a.t      = MakeTabs<T>(op);
     a.geo    = std::is_same<T, double>::value ? (const T *)op->geo : (const T *)op->geo32;
-    a.lambda = T(op->lambda);
+    a.lambda = T(lambda ? *lambda : op->lambda);
     a.in     = in;
     a.out0   = o0;
     a.out1   = o1;
@@ -490,9 +591,11 @@ int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int 
 }
 
 template int LaunchGeneric<double>(const nkb_op *, const double *, double *, double *, double *,
-                                   const int *, const double *, cudaStream_t, const int *);
+                                   const int *, const double *, cudaStream_t, const int *,
+                                   const double *);
 template int LaunchGeneric<float>(const nkb_op *, const float *, float *, float *, float *,
-                                  const int *, const double *, cudaStream_t, const int *);
+                                  const int *, const double *, cudaStream_t, const int *,
+                                  const double *);
 
 static int Repack(nkb_op *op)
 {
@@ -837,10 +940,55 @@ extern "C" int nkb_op_last_kernel_ms(const nkb_op *op, float *ms)
 
 namespace nkb
 {
-int HelmholtzDiag(const nkb_op *op, double *d_out, cudaStream_t s)
+static int HexDiag(const nkb_op *op, double *d_out, cudaStream_t s, double *d_stiff)
+{
+    const int nm = op->nm, nq = op->nq[0];
+    const size_t tn = size_t(nm) * nq;
+    std::vector<double> tab(9 * tn);
+    for (int d = 0; d < 3; ++d)
+    {
+        const std::vector<double> &B = op->hB[d], &D = op->hD[d]; // D[m*nq + i] = l_m'(z_i)
+        for (int p = 0; p < nm; ++p)
+            for (int i = 0; i < nq; ++i)
+            {
+                double db = 0.0;
+                for (int m = 0; m < nq; ++m)
+                    db += D[size_t(m) * nq + i] * B[size_t(p) * nq + m];
+                const double b = B[size_t(p) * nq + i];
+                tab[(d * 3 + 0) * tn + p * nq + i] = b * b;
+                tab[(d * 3 + 1) * tn + p * nq + i] = db * db;
+                tab[(d * 3 + 2) * tn + p * nq + i] = db * b;
+            }
+    }
+    double *dtab = nullptr;
+    NKB_CUDA_TRY(cudaMallocAsync((void **)&dtab, tab.size() * sizeof(double), s));
+    NKB_CUDA_TRY(cudaMemcpyAsync(dtab, tab.data(), tab.size() * sizeof(double),
+                                 cudaMemcpyHostToDevice, s));
+    const int threads = 256;
+    const size_t smem =
+        (size_t(nm) * nq * nq + size_t(nm) * nm * nq + 2 * size_t(nm) * nm * nm) * sizeof(double);
+    cudaError_t ce = cudaFuncSetAttribute(k_hex_diag, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(smem));
+    if (ce == cudaSuccess && op->nelmt > 0)
+    {
+        k_hex_diag<<<op->nelmt, threads, smem, s>>>(nm, nq, dtab, op->geo, op->gstride, op->nelmt,
+                                                    op->lambda, d_out, d_stiff);
+        ce = cudaGetLastError();
+    }
+    // the host table must outlive the copy: wait before it goes out of scope
+    cudaStreamSynchronize(s);
+    cudaFreeAsync(dtab, s);
+    if (ce != cudaSuccess)
+        return SetError(NKB_ERR_CUDA, "Hex diagonal: %s", cudaGetErrorString(ce));
+    return NKB_OK;
+}
+
+int HelmholtzDiag(const nkb_op *op, double *d_out, cudaStream_t s, double *d_stiff)
 {
     if (op->optype != NKB_HELMHOLTZ)
         return SetError(NKB_ERR_INVALID, "Helmholtz diagonal needs a Helmholtz operator");
+    if (op->shape == NKB_HEX && op->nq[0] == op->nq[1] && op->nq[0] == op->nq[2])
+        return HexDiag(op, d_out, s, d_stiff);
     GenArgs<double> a;
     a.d      = MakeDims(op);
     a.t      = MakeTabs<double>(op);
@@ -848,7 +996,8 @@ int HelmholtzDiag(const nkb_op *op, double *d_out, cudaStream_t s)
     a.lambda = op->lambda;
     a.in     = nullptr;
     a.out0   = d_out;
-    a.out1 = a.out2 = nullptr;
+    a.out1          = d_stiff;
+    a.out2          = nullptr;
     a.gmap          = nullptr;
     a.gsign         = nullptr;
     a.gstride       = op->gstride;
@@ -856,7 +1005,7 @@ int HelmholtzDiag(const nkb_op *op, double *d_out, cudaStream_t s)
     a.epb           = 1;
     a.skip          = nullptr;
     const int threads = 128;
-    size_t smem = size_t(a.d.nc + a.d.nt + 2 * a.d.wsz + threads) * sizeof(double);
+    size_t smem = size_t(a.d.nc + a.d.nt + 2 * a.d.wsz + 2 * threads) * sizeof(double);
     void (*kern)(GenArgs<double>) = op->shape == NKB_HEX     ? k_diag<NKB_HEX, double>
                                     : op->shape == NKB_PRISM ? k_diag<NKB_PRISM, double>
                                                              : k_diag<NKB_TET, double>;

@@ -2,6 +2,10 @@
 input, CUDA-event timing), used for profiling captures:
 
     python -m nektar_b200.opbench --op helmholtz --shape hex --n 24 --p 6 --iters 20
+
+--op matvec times the pieces of one CG iteration of the assembled system
+instead (element Helmholtz with the local<-global gather fused, assemble,
+vector update, scalars), FP64.
 """
 import argparse
 import json
@@ -25,6 +29,17 @@ def main():
     import nektar_b200 as nb
     nm = a.p + 1
     m = nb.BoxMesh(a.shape, a.n, nm, nm + 1, amp=a.amp)
+    if a.op == "matvec":
+        gmap, nglob, ndir = m.assembly()
+        op = nb.Operator("helmholtz", m)
+        op.set_factors(1.0)
+        S = nb.GlobalLinSys([op], gmap, nglob, ndir)
+        S.profile(iters=max(a.warmup, 1))
+        prof = S.profile(iters=a.iters)
+        print(json.dumps({"op": "matvec", "shape": a.shape, "n": a.n, "P": a.p,
+                          "nelmt": m.nelmt, "nglob": nglob, **prof,
+                          "op_GB_s": prof["op_bytes"] / prof["op_ms"] / 1e6}))
+        return
     op = nb.Operator(a.op, m, precision=a.precision)
     dt = torch.float64 if a.precision == "fp64" else torch.float32
     x = torch.rand(op.in_size, dtype=dt, device="cuda")
