@@ -10,6 +10,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <type_traits>
 
 namespace nkb
 {
@@ -427,7 +428,9 @@ enum
 };
 
 // candidate (geometry staging, elements per CTA) of the tuned Hex kernel
-constexpr int kNumHexVariants = 3;
+// 0: TMA-staged geometry; 1, 2: streamed geometry, 1 or 2 elements per CTA;
+// 3: FP64 tensor cores (DMMA, nq <= 8; nkb_hex_mma.cuh)
+constexpr int kNumHexVariants = 4;
 
 template <typename T, int NQ> constexpr int TmaEpb()
 {
@@ -482,11 +485,22 @@ static int HexVariantLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, 
     return NKB_OK;
 }
 
+template <int NM>
+static int HexMmaLaunch(const nkb_op *op, const HexArgs<double> &a, bool gather, cudaStream_t s,
+                        bool set_attr);
+
 template <typename T, int NM>
 static int HexLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStream_t s, int variant,
                      bool set_attr)
 {
     constexpr int NQ = NM + 1;
+    if (variant == 3)
+    {
+        if constexpr (std::is_same<T, double>::value)
+            return HexMmaLaunch<NM>(op, a, gather, s, set_attr);
+        else
+            return SetError(NKB_ERR_UNSUPPORTED, "the DMMA Hex kernel is FP64");
+    }
     switch (variant)
     {
         case 0:
@@ -525,3 +539,5 @@ int HexLaunchT(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStream_t 
 
 
 } // namespace nkb
+
+#include "nkb_hex_mma.cuh"

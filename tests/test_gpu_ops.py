@@ -115,11 +115,12 @@ def test_device_pointer_path_matches_host_path():
 
 
 @pytest.mark.parametrize("n,nm", [(1, 5), (3, 7), (2, 9), (1, 11), (5, 2)])
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 def test_tuned_and_generic_hex_helmholtz_agree(monkeypatch, n, nm, variant):
     """Every variant of the tuned Hex kernel (nkb_hex.cu: TMA-staged or
-    streamed geometry, 1-2 elements per CTA) against the shape-generic
-    kernel, odd element counts included (partially filled last CTA)."""
+    streamed geometry, 1-2 elements per CTA, FP64 tensor cores for nq <= 8)
+    against the shape-generic kernel, odd element counts included (partially
+    filled last CTA)."""
     m = nb.BoxMesh("hex", n, nm, nm + 1, amp=0.05)
     x = np.random.default_rng(nm).uniform(-1, 1, m.nelmt * m.nc)
     monkeypatch.setenv("NKB_HEX_VARIANT", str(variant))
