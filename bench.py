@@ -392,7 +392,7 @@ def run_b200(args, rank, world, local):
         traffic = tr["dram_bytes_per_element"] * mesh.nelmt
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic,
-                "kernel": "k_hex_helm (element Helmholtz, gather fused)",
+                "kernel": op.kernel(gather=True) + ": element Helmholtz, gather fused",
                 "peak_source": peak_src, "kernel_ms": prof["op_ms"],
                 "algorithmic_bytes": prof["op_bytes"], "algorithmic_flops": prof["op_flops"],
                 "fp64_tflops": prof["op_flops"] / (prof["op_ms"] * 1e-3) / 1e12,

@@ -181,6 +181,11 @@ int nkb_op_helmholtz_diag(nkb_op *op, double *diag, int flags, void *stream);
 /* Time in ms of the last nkb_op_apply's kernel on the device (CUDA events). */
 int nkb_op_last_kernel_ms(const nkb_op *op, float *ms);
 
+/* Name of the device kernel the operator runs (the autotuned choice; gather =
+ * 1: the one used when a system gathers its input through the map). For
+ * reports; no reference counterpart. */
+const char *nkb_op_kernel(const nkb_op *op, int gather);
+
 void nkb_op_destroy(nkb_op *op);
 
 /* ---- batched application over many collections --------------------------

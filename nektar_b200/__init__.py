@@ -199,6 +199,10 @@ class Operator:
         else:
             check(fn(self.h, x_ptr, out0, out1, out2, stream))
 
+    def kernel(self, gather=False):
+        """Name of the device kernel the operator runs (autotuned choice)."""
+        return lib().nkb_op_kernel(self.h, int(bool(gather))).decode()
+
     def last_kernel_ms(self):
         ms = ctypes.c_float()
         check(lib().nkb_op_last_kernel_ms(self.h, ctypes.byref(ms)))

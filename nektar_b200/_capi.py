@@ -83,6 +83,7 @@ SIGNATURES = {
     "nkb_op_helmholtz_diag": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "nkb_op_last_kernel_ms": (c_int, [c_void_p, P(c_float)]),
     "nkb_op_destroy": (None, [c_void_p]),
+    "nkb_op_kernel": (c_char_p, [c_void_p, c_int]),
     "nkb_sys_create": (c_int, [P(SysDesc), P(c_void_p)]),
     "nkb_cg_solve": (c_int, [c_void_p, c_void_p, c_void_p, P(CGOpts), P(CGReport), c_int,
                              c_void_p]),

@@ -828,6 +828,20 @@ extern "C" int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **out)
     int rc = AllocInstance(S);
     if (rc)
         return fail(rc);
+    // the Hex kernels' variant for gathered launches, timed with this map
+    NKB_CUDA_TRY(cudaMemsetAsync(S->w, 0, S->nglob * sizeof(double), S->stream));
+    if (S->w32)
+        NKB_CUDA_TRY(cudaMemsetAsync(S->w32, 0, S->nglob * sizeof(float), S->stream));
+    for (size_t c = 0; c < S->ops.size(); ++c)
+    {
+        const int *mp = S->d_map + S->off[c];
+        const double *sg = S->d_sign ? S->d_sign + S->off[c] : nullptr;
+        if ((rc = TuneHexGather(S->ops[c], S->w, S->yl + S->off[c], mp, sg, S->stream)))
+            return fail(rc);
+        if (!S->ops32.empty() &&
+            (rc = TuneHexGather(S->ops32[c], S->w32, S->yl32 + S->off[c], mp, sg, S->stream)))
+            return fail(rc);
+    }
     // Jacobi diagonal: element diagonals, assembled (sign^2 = 1), inverted
     // (PreconditionerDiagonal.cpp:93-125). With one lambda for all operators
     // the mass and Laplacian parts are kept apart (clones with another lambda

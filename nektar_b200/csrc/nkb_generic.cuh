@@ -34,6 +34,24 @@ struct Dims
     int wsz;   // size of each of the two sum-factorisation scratch arrays
 };
 
+// Compile-time sizes of the meshes' standard point sets (nq0 = nm + 1 GLL;
+// Prism nq2 = nm, Tet nq1 = nq2 = nm Gauss-Radau): the stage functions above
+// take either these or the runtime Dims; with these every loop bound, index
+// division and scratch offset is a constant.
+template <int SHAPE, int NM> struct SDims
+{
+    static constexpr int nm    = NM;
+    static constexpr int nq0   = NM + 1;
+    static constexpr int nq1   = SHAPE == NKB_TET ? NM : NM + 1;
+    static constexpr int nq2   = SHAPE == NKB_HEX ? NM + 1 : NM;
+    static constexpr int nc    = SHAPE == NKB_HEX     ? NM * NM * NM
+                                 : SHAPE == NKB_PRISM ? NM * NM * (NM + 1) / 2
+                                                      : NM * (NM + 1) * (NM + 2) / 6;
+    static constexpr int nt    = nq0 * nq1 * nq2;
+    static constexpr int npair = NM * (NM + 1) / 2;
+    static constexpr int wsz   = nq0 * nq0 * nq0 + 2 * nq2 + nq0 * nq0;
+};
+
 template <typename T> struct Tabs
 {
     const T *B0, *B1, *B2;
@@ -67,10 +85,10 @@ template <int SHAPE> struct Bwd;
 
 template <> struct Bwd<NKB_HEX>
 {
-    __device__ static int SizeA(const Dims &d) { return d.nm * d.nm * d.nq0; }
-    __device__ static int SizeB(const Dims &d) { return d.nm * d.nq1 * d.nq0; }
-    template <typename T>
-    __device__ static void A(const Dims &d, const Tabs<T> &t, const T *x, T *wa, int l)
+    template <class D> __device__ static int SizeA(const D &d) { return d.nm * d.nm * d.nq0; }
+    template <class D> __device__ static int SizeB(const D &d) { return d.nm * d.nq1 * d.nq0; }
+    template <class D, typename T>
+    __device__ static void A(const D &d, const Tabs<T> &t, const T *x, T *wa, int l)
     {
         // wa[(r*nm + q)*nq0 + i] = sum_p x[(r*nm+q)*nm + p] B0[p][i]
         int i = l % d.nq0, rq = l / d.nq0;
@@ -80,8 +98,8 @@ template <> struct Bwd<NKB_HEX>
             s = fma(xr[p], t.B0[p * d.nq0 + i], s);
         wa[l] = s;
     }
-    template <typename T>
-    __device__ static void B(const Dims &d, const Tabs<T> &t, const T *, const T *wa, T *wb, int l)
+    template <class D, typename T>
+    __device__ static void B(const D &d, const Tabs<T> &t, const T *, const T *wa, T *wb, int l)
     {
         // wb[(r*nq1 + j)*nq0 + i] = sum_q wa[(r*nm+q)*nq0+i] B1[q][j]
         int i = l % d.nq0, j = (l / d.nq0) % d.nq1, r = l / (d.nq0 * d.nq1);
@@ -90,8 +108,8 @@ template <> struct Bwd<NKB_HEX>
             s = fma(wa[(r * d.nm + q) * d.nq0 + i], t.B1[q * d.nq1 + j], s);
         wb[l] = s;
     }
-    template <typename T>
-    __device__ static void C(const Dims &d, const Tabs<T> &t, const T *, const T *wb, T *u, int l)
+    template <class D, typename T>
+    __device__ static void C(const D &d, const Tabs<T> &t, const T *, const T *wb, T *u, int l)
     {
         int ij = l % (d.nq0 * d.nq1), k = l / (d.nq0 * d.nq1);
         T s = 0;
@@ -103,10 +121,10 @@ template <> struct Bwd<NKB_HEX>
 
 template <> struct Bwd<NKB_PRISM>
 {
-    __device__ static int SizeA(const Dims &d) { return d.nq2 * d.nm * d.nm; }
-    __device__ static int SizeB(const Dims &d) { return d.nq2 * d.nq1 * d.nm; }
-    template <typename T>
-    __device__ static void A(const Dims &d, const Tabs<T> &t, const T *x, T *wa, int l)
+    template <class D> __device__ static int SizeA(const D &d) { return d.nq2 * d.nm * d.nm; }
+    template <class D> __device__ static int SizeB(const D &d) { return d.nq2 * d.nq1 * d.nm; }
+    template <class D, typename T>
+    __device__ static void A(const D &d, const Tabs<T> &t, const T *x, T *wa, int l)
     {
         // wa[(k*nm + p)*nm + q] = sum_{r<nm-p} x[(p,q,r)] B2[(p,r)][k]
         int q = l % d.nm, p = (l / d.nm) % d.nm, k = l / (d.nm * d.nm);
@@ -117,8 +135,8 @@ template <> struct Bwd<NKB_PRISM>
             s = fma(xc[r], t.B2[(row + r) * d.nq2 + k], s);
         wa[l] = s;
     }
-    template <typename T>
-    __device__ static void B(const Dims &d, const Tabs<T> &t, const T *, const T *wa, T *wb, int l)
+    template <class D, typename T>
+    __device__ static void B(const D &d, const Tabs<T> &t, const T *, const T *wa, T *wb, int l)
     {
         // wb[(k*nq1 + j)*nm + p] = sum_q wa[(k*nm+p)*nm+q] B1[q][j]
         int p = l % d.nm, j = (l / d.nm) % d.nq1, k = l / (d.nm * d.nq1);
@@ -128,8 +146,8 @@ template <> struct Bwd<NKB_PRISM>
             s = fma(a[q], t.B1[q * d.nq1 + j], s);
         wb[l] = s;
     }
-    template <typename T>
-    __device__ static void C(const Dims &d, const Tabs<T> &t, const T *x, const T *wb, T *u, int l)
+    template <class D, typename T>
+    __device__ static void C(const D &d, const Tabs<T> &t, const T *x, const T *wb, T *u, int l)
     {
         int i = l % d.nq0, j = (l / d.nq0) % d.nq1, k = l / (d.nq0 * d.nq1);
         const T *b = wb + (k * d.nq1 + j) * d.nm;
@@ -147,10 +165,10 @@ template <> struct Bwd<NKB_PRISM>
 
 template <> struct Bwd<NKB_TET>
 {
-    __device__ static int SizeA(const Dims &d) { return d.nq2 * d.npair; }
-    __device__ static int SizeB(const Dims &d) { return d.nq2 * d.nq1 * d.nm; }
-    template <typename T>
-    __device__ static void A(const Dims &d, const Tabs<T> &t, const T *x, T *wa, int l)
+    template <class D> __device__ static int SizeA(const D &d) { return d.nq2 * d.npair; }
+    template <class D> __device__ static int SizeB(const D &d) { return d.nq2 * d.nq1 * d.nm; }
+    template <class D, typename T>
+    __device__ static void A(const D &d, const Tabs<T> &t, const T *x, T *wa, int l)
     {
         // wa[k*npair + pair(p,q)] = sum_{r<nm-p-q} x[(p,q,r)] B2[(p,q,r)][k]
         int pq = l % d.npair, k = l / d.npair;
@@ -167,8 +185,8 @@ template <> struct Bwd<NKB_TET>
             s = fma(x[m0 + r], t.B2[(m0 + r) * d.nq2 + k], s);
         wa[l] = s;
     }
-    template <typename T>
-    __device__ static void B(const Dims &d, const Tabs<T> &t, const T *, const T *wa, T *wb, int l)
+    template <class D, typename T>
+    __device__ static void B(const D &d, const Tabs<T> &t, const T *, const T *wa, T *wb, int l)
     {
         // wb[(k*nq1 + j)*nm + p] = sum_{q<nm-p} wa[k*npair + pair(p,q)] B1[pair(p,q)][j]
         int p = l % d.nm, j = (l / d.nm) % d.nq1, k = l / (d.nm * d.nq1);
@@ -179,8 +197,8 @@ template <> struct Bwd<NKB_TET>
             s = fma(a[q], t.B1[(pr + q) * d.nq1 + j], s);
         wb[l] = s;
     }
-    template <typename T>
-    __device__ static void C(const Dims &d, const Tabs<T> &t, const T *x, const T *wb, T *u, int l)
+    template <class D, typename T>
+    __device__ static void C(const D &d, const Tabs<T> &t, const T *x, const T *wb, T *u, int l)
     {
         int i = l % d.nq0, j = (l / d.nq0) % d.nq1, k = l / (d.nq0 * d.nq1);
         const T *b = wb + (k * d.nq1 + j) * d.nm;
@@ -207,8 +225,8 @@ template <> struct Bwd<NKB_TET>
 template <int SHAPE> struct Ipr;
 
 // stage A common to all shapes: wa[(k*nq1 + j)*nm + p] = sum_i f[kji] B0[p][i]
-template <typename T>
-__device__ __forceinline__ void IprStageA(const Dims &d, const Tabs<T> &t, const T *f, T *wa, int l)
+template <class D, typename T>
+__device__ __forceinline__ void IprStageA(const D &d, const Tabs<T> &t, const T *f, T *wa, int l)
 {
     int p = l % d.nm, kj = l / d.nm;
     const T *fr = f + kj * d.nq0;
@@ -220,10 +238,10 @@ __device__ __forceinline__ void IprStageA(const Dims &d, const Tabs<T> &t, const
 
 template <> struct Ipr<NKB_HEX>
 {
-    __device__ static int SizeA(const Dims &d) { return d.nq2 * d.nq1 * d.nm; }
-    __device__ static int SizeB(const Dims &d) { return d.nq2 * d.nm * d.nm; }
-    template <typename T>
-    __device__ static void B(const Dims &d, const Tabs<T> &t, const T *wa, T *wb, int l)
+    template <class D> __device__ static int SizeA(const D &d) { return d.nq2 * d.nq1 * d.nm; }
+    template <class D> __device__ static int SizeB(const D &d) { return d.nq2 * d.nm * d.nm; }
+    template <class D, typename T>
+    __device__ static void B(const D &d, const Tabs<T> &t, const T *wa, T *wb, int l)
     {
         // wb[(k*nm + q)*nm + p] = sum_j wa[(k*nq1+j)*nm + p] B1[q][j]
         int p = l % d.nm, q = (l / d.nm) % d.nm, k = l / (d.nm * d.nm);
@@ -232,8 +250,8 @@ template <> struct Ipr<NKB_HEX>
             s = fma(wa[(k * d.nq1 + j) * d.nm + p], t.B1[q * d.nq1 + j], s);
         wb[l] = s;
     }
-    template <typename T>
-    __device__ static T C(const Dims &d, const Tabs<T> &t, const T *wb, int m)
+    template <class D, typename T>
+    __device__ static T C(const D &d, const Tabs<T> &t, const T *wb, int m)
     {
         int pq = m % (d.nm * d.nm), r = m / (d.nm * d.nm);
         T s = 0;
@@ -245,15 +263,15 @@ template <> struct Ipr<NKB_HEX>
 
 template <> struct Ipr<NKB_PRISM>
 {
-    __device__ static int SizeA(const Dims &d) { return d.nq2 * d.nq1 * d.nm; }
-    __device__ static int SizeB(const Dims &d) { return d.nq2 * d.nm * d.nm; }
-    template <typename T>
-    __device__ static void B(const Dims &d, const Tabs<T> &t, const T *wa, T *wb, int l)
+    template <class D> __device__ static int SizeA(const D &d) { return d.nq2 * d.nq1 * d.nm; }
+    template <class D> __device__ static int SizeB(const D &d) { return d.nq2 * d.nm * d.nm; }
+    template <class D, typename T>
+    __device__ static void B(const D &d, const Tabs<T> &t, const T *wa, T *wb, int l)
     {
         Ipr<NKB_HEX>::B(d, t, wa, wb, l);
     }
-    template <typename T>
-    __device__ static T C(const Dims &d, const Tabs<T> &t, const T *wb, int m)
+    template <class D, typename T>
+    __device__ static T C(const D &d, const Tabs<T> &t, const T *wb, int m)
     {
         // m -> (p, q, r), r < nm - p
         int p = 0, rem = m;
@@ -279,11 +297,11 @@ template <> struct Ipr<NKB_PRISM>
 
 template <> struct Ipr<NKB_TET>
 {
-    __device__ static int SizeA(const Dims &d) { return d.nq2 * d.nq1 * d.nm; }
+    template <class D> __device__ static int SizeA(const D &d) { return d.nq2 * d.nq1 * d.nm; }
     // wb holds nq2*npair pair sums followed by the two correction columns c0, c1
-    __device__ static int SizeB(const Dims &d) { return d.nq2 * (d.npair + 2); }
-    template <typename T>
-    __device__ static void B(const Dims &d, const Tabs<T> &t, const T *wa, T *wb, int l)
+    template <class D> __device__ static int SizeB(const D &d) { return d.nq2 * (d.npair + 2); }
+    template <class D, typename T>
+    __device__ static void B(const D &d, const Tabs<T> &t, const T *wa, T *wb, int l)
     {
         const int np = d.nq2 * d.npair;
         if (l < np)
@@ -317,8 +335,8 @@ template <> struct Ipr<NKB_TET>
             wb[l] = s;
         }
     }
-    template <typename T>
-    __device__ static T C(const Dims &d, const Tabs<T> &t, const T *wb, int m)
+    template <class D, typename T>
+    __device__ static T C(const D &d, const Tabs<T> &t, const T *wb, int m)
     {
         int p = 0, rem = m;
         while (rem >= (d.nm - p) * (d.nm - p + 1) / 2)
@@ -361,8 +379,8 @@ template <> struct Ipr<NKB_TET>
 // ---------------------------------------------------------------------------
 // collocation derivatives on the nq0 x nq1 x nq2 grid
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ void Grad(const Dims &d, const Tabs<T> &t, const T *u, int l, T &g0,
+template <class D, typename T>
+__device__ __forceinline__ void Grad(const D &d, const Tabs<T> &t, const T *u, int l, T &g0,
                                      T &g1, T &g2)
 {
     int i = l % d.nq0, j = (l / d.nq0) % d.nq1, k = l / (d.nq0 * d.nq1);
@@ -382,8 +400,8 @@ __device__ __forceinline__ void Grad(const Dims &d, const Tabs<T> &t, const T *u
 }
 
 // sum_a D_a^T v_a at point l
-template <typename T>
-__device__ __forceinline__ T GradT(const Dims &d, const Tabs<T> &t, const T *v0, const T *v1,
+template <class D, typename T>
+__device__ __forceinline__ T GradT(const D &d, const Tabs<T> &t, const T *v0, const T *v1,
                                    const T *v2, int l)
 {
     int i = l % d.nq0, j = (l / d.nq0) % d.nq1, k = l / (d.nq0 * d.nq1);

@@ -37,6 +37,21 @@ namespace nkb
 
 // NKB_KERNEL=generic selects the shape-generic kernels for every operator
 // (used to test both implementations against each other).
+int SmCount(int device)
+{
+    static int counts[64] = {0};
+    if (device < 0 || device >= 64)
+        return 148;
+    if (counts[device] == 0)
+    {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || n <= 0)
+            n = 148;
+        counts[device] = n;
+    }
+    return counts[device];
+}
+
 static bool ForceGeneric()
 {
     const char *v = std::getenv("NKB_KERNEL");
@@ -250,6 +265,73 @@ void FreeKernelData(nkb_op *op)
 }
 
 template <typename T>
+static int TuneHexGatherT(nkb_op *op, const T *xin, T *yl, const int *map, const double *sign,
+                          cudaStream_t s)
+{
+    HexArgs<T> a = MakeHexArgs<T>(op);
+    a.in         = xin;
+    a.out        = yl;
+    a.gmap       = map;
+    a.gsign      = sign;
+    float best_ms = 1e30f;
+    int best = -1, rc = NKB_OK;
+    for (int v = 0; v < kNumHexVariants && !rc; ++v)
+    {
+        if (HexLaunchT<T>(op, a, true, s, v, true) != NKB_OK)
+        {
+            ClearError();
+            continue;
+        }
+        if ((rc = HexLaunchT<T>(op, a, true, s, v, false)))
+            break;
+        cudaEventRecord(op->ev0, s);
+        for (int it = 0; it < 3 && !rc; ++it)
+            rc = HexLaunchT<T>(op, a, true, s, v, false);
+        cudaEventRecord(op->ev1, s);
+        if (rc || cudaEventSynchronize(op->ev1) != cudaSuccess)
+            break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, op->ev0, op->ev1);
+        if (ms < best_ms)
+        {
+            best_ms = ms;
+            best    = v;
+        }
+    }
+    if (rc)
+        return rc;
+    if (best >= 0)
+        op->hex_variant_gather = best;
+    return NKB_OK;
+}
+
+int TuneHexGather(nkb_op *op, const void *xin, void *yl, const int *map, const double *sign,
+                  cudaStream_t s)
+{
+    if (op->variant != kVariantHexHelm || std::getenv("NKB_HEX_VARIANT"))
+        return NKB_OK;
+    return op->precision == NKB_FP64
+               ? TuneHexGatherT<double>(op, static_cast<const double *>(xin),
+                                        static_cast<double *>(yl), map, sign, s)
+               : TuneHexGatherT<float>(op, static_cast<const float *>(xin),
+                                       static_cast<float *>(yl), map, sign, s);
+}
+
+const char *KernelName(const nkb_op *op, bool gather)
+{
+    if (op->variant != kVariantHexHelm)
+        return "k_generic";
+    const int v = (gather && op->hex_variant_gather >= 0) ? op->hex_variant_gather : op->hex_variant;
+    switch (v)
+    {
+        case 0: return "k_hex_helm (TMA-staged geometry)";
+        case 1: return "k_hex_helm (streamed geometry, 1 element per CTA)";
+        case 2: return "k_hex_helm (streamed geometry, 2 elements per CTA)";
+        default: return "k_hex_helm_mma (FP64 tensor cores)";
+    }
+}
+
+template <typename T>
 int LaunchOp(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
              const double *gsign, cudaStream_t s, const int *skip, const double *lambda)
 {
@@ -263,7 +345,8 @@ int LaunchOp(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap
         a.gmap       = gmap;
         a.gsign      = gsign;
         a.skip       = skip;
-        return HexLaunchT<T>(op, a, gmap != nullptr, s, op->hex_variant, false);
+        const int v = (gmap && op->hex_variant_gather >= 0) ? op->hex_variant_gather : op->hex_variant;
+        return HexLaunchT<T>(op, a, gmap != nullptr, s, v, false);
     }
     return LaunchGeneric<T>(op, in, o0, o1, o2, gmap, gsign, s, skip, lambda);
 }
@@ -276,3 +359,8 @@ template int LaunchOp<float>(const nkb_op *, const float *, float *, float *, fl
                              const double *);
 
 } // namespace nkb
+
+extern "C" const char *nkb_op_kernel(const nkb_op *op, int gather)
+{
+    return op ? nkb::KernelName(op, gather != 0) : "";
+}

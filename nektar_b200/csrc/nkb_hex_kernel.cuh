@@ -429,7 +429,8 @@ enum
 
 // candidate (geometry staging, elements per CTA) of the tuned Hex kernel
 // 0: TMA-staged geometry; 1, 2: streamed geometry, 1 or 2 elements per CTA;
-// 3: FP64 tensor cores (DMMA, nq <= 8; nkb_hex_mma.cuh)
+// 3: FP64 tensor cores (DMMA, nq <= 8, FP64 arithmetic for both storage
+//    precisions; nkb_hex_mma.cuh)
 constexpr int kNumHexVariants = 4;
 
 template <typename T, int NQ> constexpr int TmaEpb()
@@ -485,8 +486,8 @@ static int HexVariantLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, 
     return NKB_OK;
 }
 
-template <int NM>
-static int HexMmaLaunch(const nkb_op *op, const HexArgs<double> &a, bool gather, cudaStream_t s,
+template <typename TV, int NM>
+static int HexMmaLaunch(const nkb_op *op, const HexArgs<TV> &a, bool gather, cudaStream_t s,
                         bool set_attr);
 
 template <typename T, int NM>
@@ -495,12 +496,7 @@ static int HexLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStr
 {
     constexpr int NQ = NM + 1;
     if (variant == 3)
-    {
-        if constexpr (std::is_same<T, double>::value)
-            return HexMmaLaunch<NM>(op, a, gather, s, set_attr);
-        else
-            return SetError(NKB_ERR_UNSUPPORTED, "the DMMA Hex kernel is FP64");
-    }
+        return HexMmaLaunch<T, NM>(op, a, gather, s, set_attr);
     switch (variant)
     {
         case 0:

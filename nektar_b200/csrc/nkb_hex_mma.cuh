@@ -1,18 +1,26 @@
 // Hex Helmholtz on the FP64 tensor cores (DMMA, mma.sync m8n8k4 f64) for
-// nq <= 8. One warp per element. Every sum-factorisation contraction is a
+// nq <= 8. One warp per element. The arithmetic is FP64 for both operator
+// precisions; an FP32 operator keeps FP32 storage (coefficients in and out,
+// geometry), which halves its bytes while its rounding stays that of the
+// stored data only. Every sum-factorisation contraction is a
 // 64 x 8 x 8 matrix product over an 8 x 8 x 8 cube (modes and points padded
 // with zeros to 8 per direction): 8 row tiles of 8 x 8 outputs, two k-steps
 // of 4 each, with the 1-D table in the B fragment and the cube rows in the
 // A fragment. Twelve such contractions make one element (BwdTrans 3,
 // gradient 3, transposed gradient 3 accumulated in place, inner product 3),
-// 192 DMMAs; the metric step between them is pointwise. The arithmetic per
+// about 190 DMMAs; the metric step between them is pointwise. Warps are persistent
+// and copy the next element's coefficients into shared memory asynchronously
+// while the current one is computed; the current element's geometry is
+// prefetched into L2 at the start of its turn. The arithmetic per
 // element is the same fused formulation as k_hex_helm:
 //   y = B^T [ lambda W u + sum_a D_a^T (G' grad u)_a ],  u = B x.
 //
 // Shared memory per warp: four cubes, each [c][b][a] at
-// c*68 + b*8 + (a ^ 4*((b >> 1) & 1)): the XOR on a and the c-stride of 68
-// make the A-fragment loads of all three contraction directions free of bank
-// conflicts (a 16-lane phase touches 16 distinct 8-byte bank pairs).
+// c*68 + b*8 + (a ^ 4*((b >> 1) & 1) ^ (c & 4)): the XORs on a and the
+// c-stride of 68 make the A-fragment loads of all three contraction
+// directions, the stores of the a- and c-contractions and the metric step's
+// accesses free of bank conflicts (a 16-lane phase touches 16 distinct 8-byte
+// bank pairs); the b-contraction's stores are 2-way.
 //
 // m8n8k4 f64 fragments (lane = 4 g + t): A (8x4, row) holds A[g][t];
 // B (4x8, col) holds B[t][g]; C/D (8x8) hold C[g][2t], C[g][2t+1].
@@ -25,11 +33,12 @@ namespace nkb
 {
 
 constexpr int kMmaCube  = 8 * 68; // doubles per cube
-constexpr int kMmaWarps = 4;      // warps (elements) per CTA
+constexpr int kMmaWarps = 4;      // warps per CTA (each walks its own elements)
+constexpr int kMmaCubes = 4;      // shared-memory cubes per warp
 
 __device__ __forceinline__ int CubeIdx(int c, int b, int a)
 {
-    return c * 68 + b * 8 + (a ^ ((b & 2) << 1));
+    return c * 68 + b * 8 + (a ^ ((b & 2) << 1) ^ (c & 4));
 }
 
 __device__ __forceinline__ void Dmma(double &c0, double &c1, double a, double b)
@@ -43,14 +52,14 @@ __device__ __forceinline__ void Dmma(double &c0, double &c1, double a, double b)
 // axes (tile = the slower, g = the faster), k and n run along AX.
 // out(rows, n) (+)= sum_k in(rows, k) * B(k, n), B(k, n) in fragments bf[kk]
 // (k = t + 4 kk, n = g).
-template <int AX, bool ACC>
-__device__ __forceinline__ void Contract(const double *__restrict__ in, double *__restrict__ out,
+template <int AX, bool ACC, typename TIN = double>
+__device__ __forceinline__ void Contract(const TIN *__restrict__ in, double *__restrict__ out,
                                          const double (&bf)[2], int g, int t)
 {
 #pragma unroll
     for (int tile = 0; tile < 8; ++tile)
     {
-        int ia0, ia1, io0, io1;
+        int ia0, ia1, io0, io1; // io1 = io0 + 1 when AX == 0
         if (AX == 0) // rows (c = tile, b = g)
         {
             ia0 = CubeIdx(tile, g, t);
@@ -73,15 +82,32 @@ __device__ __forceinline__ void Contract(const double *__restrict__ in, double *
             io1 = CubeIdx(2 * t + 1, tile, g);
         }
         double c0 = 0.0, c1 = 0.0;
-        if (ACC)
+        if (AX == 0)
         {
-            c0 = out[io0];
-            c1 = out[io1];
+            // the pair (2t, 2t+1) is adjacent and 16-byte aligned: one vector access
+            double2 *o2 = reinterpret_cast<double2 *>(out + io0);
+            if (ACC)
+            {
+                const double2 v = *o2;
+                c0              = v.x;
+                c1              = v.y;
+            }
+            Dmma(c0, c1, double(in[ia0]), bf[0]);
+            Dmma(c0, c1, double(in[ia1]), bf[1]);
+            *o2 = make_double2(c0, c1);
         }
-        Dmma(c0, c1, in[ia0], bf[0]);
-        Dmma(c0, c1, in[ia1], bf[1]);
-        out[io0] = c0;
-        out[io1] = c1;
+        else
+        {
+            if (ACC)
+            {
+                c0 = out[io0];
+                c1 = out[io1];
+            }
+            Dmma(c0, c1, double(in[ia0]), bf[0]);
+            Dmma(c0, c1, double(in[ia1]), bf[1]);
+            out[io0] = c0;
+            out[io1] = c1;
+        }
     }
 }
 
@@ -116,115 +142,233 @@ __device__ __forceinline__ void LoadMmaTabs(const HexConst<double, NM, NQ> &c, M
     }
 }
 
-template <int NM, int NQ, bool GATHER>
-__global__ void __launch_bounds__(32 * kMmaWarps)
-    k_hex_helm_mma(HexArgs<double> a, const __grid_constant__ HexConst<double, NM, NQ> c)
+// Coefficients reach shared memory by asynchronous copies (cp.async, no
+// registers held while they are in flight), gathered through the map, one
+// element ahead; the map entries themselves are read two elements ahead.
+__device__ __forceinline__ void CpAsync(double *dst, const double *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(SmemAddr(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void CpAsync(float *dst, const float *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(SmemAddr(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void CpAsyncCommit()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void CpAsyncWaitAll()
+{
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// map entries (or plain offsets) of element e for the lane's 16 cube positions
+template <int NM, bool GATHER, typename TV>
+__device__ __forceinline__ void LoadMap(const HexArgs<TV> &a, long e, int lane, int (&idx)[16])
+{
+    constexpr int NC = NM * NM * NM;
+#pragma unroll
+    for (int s = 0; s < 16; ++s)
+    {
+        const int pos = lane + 32 * s;
+        const int cc = pos >> 6, bb = (pos >> 3) & 7, aa = pos & 7;
+        const int m  = (cc * NM + bb) * NM + aa;
+        const bool real = aa < NM && bb < NM && cc < NM;
+        idx[s]          = real ? (GATHER ? __ldg(a.gmap + e * NC + m) : m) : -1;
+    }
+}
+
+// coefficients of element e into the cube x (real positions only; the padded
+// ones stay zero)
+template <int NM, bool GATHER, typename TV>
+__device__ __forceinline__ void FetchCoeffs(const HexArgs<TV> &a, long e, int lane,
+                                            const int (&idx)[16], TV *x)
+{
+    constexpr int NC = NM * NM * NM;
+#pragma unroll
+    for (int s = 0; s < 16; ++s)
+    {
+        if (idx[s] < 0)
+            continue;
+        const int pos = lane + 32 * s;
+        TV *dst       = x + CubeIdx(pos >> 6, (pos >> 3) & 7, pos & 7);
+        if (!GATHER)
+        {
+            CpAsync(dst, a.in + e * NC + idx[s]);
+        }
+        else if (!a.gsign)
+        {
+            CpAsync(dst, a.in + idx[s]);
+        }
+        else
+        {
+            const int m = ((pos >> 6) * NM + ((pos >> 3) & 7)) * NM + (pos & 7);
+            *dst        = TV(double(__ldg(a.in + idx[s])) * __ldg(a.gsign + e * NC + m));
+        }
+    }
+    CpAsyncCommit();
+}
+
+// Persistent: each warp walks the elements e = warp id, warp id + warps, ...
+// Per warp four cubes in shared memory: x (coefficients, filled
+// asynchronously), c0, c1, c2. The z-gradient and lambda W u never leave
+// registers (the metric step runs in the C-fragment layout of the z
+// contraction, which is also the layout of the first transposed-gradient
+// contraction). Geometry is read with read-only loads in four batches of four
+// points per lane, all loads of a batch issued before any of its stores.
+template <typename TV, int NM, int NQ, bool GATHER>
+__global__ void __launch_bounds__(32 * kMmaWarps, 3)
+    k_hex_helm_mma(HexArgs<TV> a, const __grid_constant__ HexConst<double, NM, NQ> c)
 {
     static_assert(NQ <= 8 && NM < NQ, "the DMMA Hex kernel covers nq <= 8");
     constexpr int NQ2 = NQ * NQ, NQ3 = NQ2 * NQ, NC = NM * NM * NM;
     extern __shared__ __align__(16) double msm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
-    const long e = long(blockIdx.x) * kMmaWarps + warp;
+    const long nwarps = long(gridDim.x) * kMmaWarps;
+    long e            = long(blockIdx.x) * kMmaWarps + warp;
     if (e >= a.nelmt || (a.skip && *a.skip))
         return;
-    double *c0 = msm + warp * 4 * kMmaCube, *c1 = c0 + kMmaCube, *c2 = c1 + kMmaCube,
-           *c3 = c2 + kMmaCube;
-    const double *G = a.geo + e * a.gstride;
-    // the element's geometry is needed only after BwdTrans and the gradient:
-    // start bringing it into L2 now
-    if (lane == 0)
-        BulkPrefetchL2(G, uint32_t(7 * NQ3 * sizeof(double) + 15) & ~15u);
+    double *c0 = msm + warp * kMmaCubes * kMmaCube + kMmaCube, *c1 = c0 + kMmaCube,
+           *c2 = c1 + kMmaCube;
+    TV *xc = reinterpret_cast<TV *>(c0 - kMmaCube); // coefficients, in the vector type
+    const uint32_t gbytes = uint32_t(7 * NQ3 * sizeof(TV) + 15) & ~15u;
 
     MmaTabs<NM, NQ> f;
     LoadMmaTabs<NM, NQ>(c, f, g, t);
+    const double lam = double(a.lambda);
 
-    // coefficients into cube 0 ([r][q][p], zero padded)
-#pragma unroll 4
-    for (int pos = lane; pos < 512; pos += 32)
+    // the padded positions of the coefficient cube stay zero for good
+    for (int pos = lane; pos < kMmaCube; pos += 32)
+        xc[pos] = TV(0);
+    __syncwarp();
+    int idx[16];
+    LoadMap<NM, GATHER, TV>(a, e, lane, idx);
+    FetchCoeffs<NM, GATHER, TV>(a, e, lane, idx, xc);
+    if (e + nwarps < a.nelmt)
+        LoadMap<NM, GATHER, TV>(a, e + nwarps, lane, idx);
+
+    for (; e < a.nelmt; e += nwarps)
     {
-        const int cc = pos >> 6, bb = (pos >> 3) & 7, aa = pos & 7;
-        double v = 0.0;
-        if (aa < NM && bb < NM && cc < NM)
+        const TV *__restrict__ G = a.geo + e * a.gstride;
+        // this element's geometry is read after BwdTrans and the gradient:
+        // bring it into L2 now (a whole element earlier it is evicted again)
+        if (lane == 0)
+            BulkPrefetchL2(G, gbytes);
+        CpAsyncWaitAll();
+        __syncwarp();
+        // BwdTrans: p -> i (x -> c1), q -> j (c1 -> c0), r -> k (c0 -> c1 = u)
+        Contract<0, false, TV>(xc, c1, f.bw[0], g, t);
+        __syncwarp();
+        const long en = e + nwarps;
+        if (en < a.nelmt)
         {
-            const long gi = e * NC + (cc * NM + bb) * NM + aa;
-            if (GATHER)
-            {
-                v = a.in[a.gmap[gi]];
-                if (a.gsign)
-                    v *= a.gsign[gi];
-            }
-            else
-            {
-                v = a.in[gi];
-            }
+            FetchCoeffs<NM, GATHER, TV>(a, en, lane, idx, xc); // x is free again
+            if (en + nwarps < a.nelmt)
+                LoadMap<NM, GATHER, TV>(a, en + nwarps, lane, idx);
         }
-        c0[CubeIdx(cc, bb, aa)] = v;
-    }
-    __syncwarp();
-    // BwdTrans: p -> i, q -> j, r -> k; u in cube 1
-    Contract<0, false>(c0, c1, f.bw[0], g, t);
-    __syncwarp();
-    Contract<1, false>(c1, c0, f.bw[1], g, t);
-    __syncwarp();
-    Contract<2, false>(c0, c1, f.bw[2], g, t);
-    __syncwarp();
-    // reference-space gradient: g0 -> cube 0, g1 -> cube 2, g2 -> cube 3
-    Contract<0, false>(c1, c0, f.dg, g, t);
-    Contract<1, false>(c1, c2, f.dg, g, t);
-    Contract<2, false>(c1, c3, f.dg, g, t);
-    __syncwarp();
-    // metric: v = G' grad u in place of the gradients, f = lambda W u in place of u
-    const double lam = a.lambda;
-#pragma unroll 2
-    for (int q = lane; q < NQ3; q += 32)
-    {
-        const int kk = q / NQ2, jj = (q / NQ) % NQ, ii = q % NQ;
-        const int ci = CubeIdx(kk, jj, ii);
-        const double W = G[q], G00 = G[NQ3 + q], G11 = G[2 * NQ3 + q], G22 = G[3 * NQ3 + q];
-        const double G01 = G[4 * NQ3 + q], G02 = G[5 * NQ3 + q], G12 = G[6 * NQ3 + q];
-        const double x0 = c0[ci], x1 = c2[ci], x2 = c3[ci];
-        c0[ci] = fma(G02, x2, fma(G01, x1, G00 * x0));
-        c2[ci] = fma(G12, x2, fma(G11, x1, G01 * x0));
-        c3[ci] = fma(G22, x2, fma(G12, x1, G02 * x0));
-        c1[ci] = lam * W * c1[ci];
-    }
-    __syncwarp();
-    // f += D_0^T v0 + D_1^T v1 + D_2^T v2 (in place, one direction at a time)
-    Contract<0, true>(c0, c1, f.dt, g, t);
-    __syncwarp();
-    Contract<1, true>(c2, c1, f.dt, g, t);
-    __syncwarp();
-    Contract<2, true>(c3, c1, f.dt, g, t);
-    __syncwarp();
-    // inner product: k -> r (cube 0), j -> q (cube 2), i -> p (to global)
-    Contract<2, false>(c1, c0, f.ip[2], g, t);
-    __syncwarp();
-    Contract<1, false>(c0, c2, f.ip[1], g, t);
-    __syncwarp();
-    double *o = a.out + e * NC;
+        Contract<1, false>(c1, c0, f.bw[1], g, t);
+        __syncwarp();
+        Contract<2, false>(c0, c1, f.bw[2], g, t);
+        __syncwarp();
+        // gradient: g0 -> c0, g1 -> c2, g2 in registers (rows (b = tile, a = g),
+        // columns c = 2t, 2t + 1)
+        Contract<0, false>(c1, c0, f.dg, g, t);
+        Contract<1, false>(c1, c2, f.dg, g, t);
+        double z[8][2];
 #pragma unroll
-    for (int tile = 0; tile < NM; ++tile) // rows (r = tile, q = g), n = p
-    {
-        double y0 = 0.0, y1 = 0.0;
-        Dmma(y0, y1, c2[CubeIdx(tile, g, t)], f.ip[0][0]);
-        Dmma(y0, y1, c2[CubeIdx(tile, g, t + 4)], f.ip[0][1]);
-        if (g < NM)
+        for (int tile = 0; tile < 8; ++tile)
         {
-            if (2 * t < NM)
-                o[(tile * NM + g) * NM + 2 * t] = y0;
-            if (2 * t + 1 < NM)
-                o[(tile * NM + g) * NM + 2 * t + 1] = y1;
+            z[tile][0] = z[tile][1] = 0.0;
+            Dmma(z[tile][0], z[tile][1], c1[CubeIdx(t, tile, g)], f.dg[0]);
+            Dmma(z[tile][0], z[tile][1], c1[CubeIdx(t + 4, tile, g)], f.dg[1]);
+        }
+        __syncwarp();
+        // metric at the lane's 16 points (c = 2t + h, b = tile, a = g):
+        // v0 -> c0, v1 -> c2, v2 -> c1 (over u), z <- lambda W u
+#pragma unroll
+        for (int tb = 0; tb < 8; tb += 2)
+        {
+            double gv[4][7];
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+            {
+                const int tile = tb + (p >> 1), cc = 2 * t + (p & 1);
+                const bool real = cc < NQ && tile < NQ && g < NQ;
+                const int q     = real ? (cc * NQ + tile) * NQ + g : 0;
+#pragma unroll
+                for (int k = 0; k < 7; ++k)
+                    gv[p][k] = real ? double(__ldg(G + k * NQ3 + q)) : 0.0;
+            }
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+            {
+                const int tile = tb + (p >> 1), h = p & 1;
+                const int ci   = CubeIdx(2 * t + h, tile, g);
+                const double x0 = c0[ci], x1 = c2[ci], x2 = z[tile][h];
+                const double W = gv[p][0], G00 = gv[p][1], G11 = gv[p][2], G22 = gv[p][3];
+                const double G01 = gv[p][4], G02 = gv[p][5], G12 = gv[p][6];
+                c0[ci]     = fma(G02, x2, fma(G01, x1, G00 * x0));
+                c2[ci]     = fma(G12, x2, fma(G11, x1, G01 * x0));
+                const double v2 = fma(G22, x2, fma(G12, x1, G02 * x0));
+                z[tile][h] = lam * W * c1[ci];
+                c1[ci]     = v2;
+            }
+        }
+        __syncwarp();
+        // f = lambda W u + D_2^T v2 (registers), then + D_0^T v0 + D_1^T v1 in c1
+#pragma unroll
+        for (int tile = 0; tile < 8; ++tile)
+        {
+            Dmma(z[tile][0], z[tile][1], c1[CubeIdx(t, tile, g)], f.dt[0]);
+            Dmma(z[tile][0], z[tile][1], c1[CubeIdx(t + 4, tile, g)], f.dt[1]);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int tile = 0; tile < 8; ++tile)
+        {
+            c1[CubeIdx(2 * t, tile, g)]     = z[tile][0];
+            c1[CubeIdx(2 * t + 1, tile, g)] = z[tile][1];
+        }
+        __syncwarp();
+        Contract<0, true>(c0, c1, f.dt, g, t);
+        __syncwarp();
+        Contract<1, true>(c2, c1, f.dt, g, t);
+        __syncwarp();
+        // inner product: k -> r (c0), j -> q (c2), i -> p (to global)
+        Contract<2, false>(c1, c0, f.ip[2], g, t);
+        __syncwarp();
+        Contract<1, false>(c0, c2, f.ip[1], g, t);
+        __syncwarp();
+        TV *o = a.out + e * NC;
+#pragma unroll
+        for (int tile = 0; tile < NM; ++tile) // rows (r = tile, q = g), n = p
+        {
+            double y0 = 0.0, y1 = 0.0;
+            Dmma(y0, y1, c2[CubeIdx(tile, g, t)], f.ip[0][0]);
+            Dmma(y0, y1, c2[CubeIdx(tile, g, t + 4)], f.ip[0][1]);
+            if (g < NM)
+            {
+                if (2 * t < NM)
+                    o[(tile * NM + g) * NM + 2 * t] = TV(y0);
+                if (2 * t + 1 < NM)
+                    o[(tile * NM + g) * NM + 2 * t + 1] = TV(y1);
+            }
         }
     }
+    CpAsyncWaitAll(); // nothing may still be copying into shared memory at exit
 }
 
-template <int NM>
-static int HexMmaLaunch(const nkb_op *op, const HexArgs<double> &a, bool gather, cudaStream_t s,
+int SmCount(int device); // multiprocessors of a device (nkb_hex.cu)
+
+template <typename TV, int NM>
+static int HexMmaLaunch(const nkb_op *op, const HexArgs<TV> &a, bool gather, cudaStream_t s,
                         bool set_attr)
 {
     constexpr int NQ   = NM + 1;
-    const size_t bytes = size_t(kMmaWarps) * 4 * kMmaCube * sizeof(double);
+    const size_t bytes = size_t(kMmaWarps) * kMmaCubes * kMmaCube * sizeof(double);
     if constexpr (NQ > 8)
     {
         (void)op;
@@ -232,28 +376,39 @@ static int HexMmaLaunch(const nkb_op *op, const HexArgs<double> &a, bool gather,
         (void)gather;
         (void)s;
         (void)set_attr;
+        (void)bytes;
         return SetError(NKB_ERR_UNSUPPORTED, "the DMMA Hex kernel covers nq <= 8");
     }
     else
     {
         if (set_attr)
         {
-            NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm_mma<NM, NQ, false>,
+            NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm_mma<TV, NM, NQ, false>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               int(bytes)));
-            NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm_mma<NM, NQ, true>,
+            NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm_mma<TV, NM, NQ, true>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               int(bytes)));
             return NKB_OK;
         }
-        const long nb = (long(op->nelmt) + kMmaWarps - 1) / kMmaWarps;
-        if (nb == 0)
+        if (op->nelmt == 0)
             return NKB_OK;
+        // persistent grid: as many CTAs as stay resident, fewer for small operators
+        static int s_per_sm = 0; // resident CTAs per SM of this instantiation
+        if (s_per_sm == 0)
+        {
+            int b = 0;
+            NKB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &b, k_hex_helm_mma<TV, NM, NQ, true>, 32 * kMmaWarps, bytes));
+            s_per_sm = std::max(b, 1);
+        }
+        const long want = (long(op->nelmt) + kMmaWarps - 1) / kMmaWarps;
+        const long nb   = std::min<long>(want, long(s_per_sm) * SmCount(op->device));
         const HexConst<double, NM, NQ> c = MakeHexConst<double, NM, NQ>(op);
         if (gather)
-            k_hex_helm_mma<NM, NQ, true><<<unsigned(nb), 32 * kMmaWarps, bytes, s>>>(a, c);
+            k_hex_helm_mma<TV, NM, NQ, true><<<unsigned(nb), 32 * kMmaWarps, bytes, s>>>(a, c);
         else
-            k_hex_helm_mma<NM, NQ, false><<<unsigned(nb), 32 * kMmaWarps, bytes, s>>>(a, c);
+            k_hex_helm_mma<TV, NM, NQ, false><<<unsigned(nb), 32 * kMmaWarps, bytes, s>>>(a, c);
         NKB_CUDA_TRY(cudaGetLastError());
         return NKB_OK;
     }

@@ -36,6 +36,8 @@ struct nkb_op
     // kernel selection (nkb_hex.cu): 0 generic, >0 tuned variant
     int variant     = 0;
     int hex_variant = 0; // tuned Hex kernel variant chosen by the autotuner
+    int hex_variant_gather = -1; // variant for launches that gather through a
+                                 // map (timed with the system's map; -1: same)
     int gen_epb     = 0; // generic kernel: elements per CTA (0: default)
     int gen_threads = 0; // generic kernel: threads per CTA (0: default)
     void *kdata = nullptr;
@@ -64,6 +66,13 @@ int LaunchOp(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap
              const double *gsign, cudaStream_t s, const int *skip = nullptr,
              const double *lambda = nullptr);
 int ChooseKernel(nkb_op *op);
+// time the Hex variants once more with the local<-global gather a system
+// uses (xin: global vector, yl: local output) and keep the fastest for
+// gathered launches
+int TuneHexGather(nkb_op *op, const void *xin, void *yl, const int *map, const double *sign,
+                  cudaStream_t s);
+// name of the kernel the operator launches (for reports)
+const char *KernelName(const nkb_op *op, bool gather);
 size_t GenericSmemBytes(const nkb_op *op, int elem_bytes);
 void FreeKernelData(nkb_op *op);
 // element Helmholtz diagonals; with d_stiff the mass part (without lambda)

@@ -15,6 +15,7 @@
 // create time in FP64 (the geometric-factor setup stays FP64).
 #include "nkb_internal.h"
 #include "nkb_op.h"
+#include "nkb_generic_kernel.cuh"
 
 #include <cuda_runtime.h>
 
@@ -178,152 +179,6 @@ __global__ void k_pack(PackArgs a)
 // generic kernels
 // ---------------------------------------------------------------------------
 static Dims MakeDims(const nkb_op *op);
-
-enum
-{
-    GK_BWD  = 0,
-    GK_HELM = 1,
-    GK_IP   = 3,
-    GK_PD   = 5,
-    GK_DIAG = 9
-};
-
-// per-element shared memory: x[nc] u[nt] g0 g1 g2 [nt] wa[wsz] wb[wsz]
-__host__ __device__ inline int ElemSmem(const Dims &d)
-{
-    int s = d.nc + 4 * d.nt + 2 * d.wsz;
-    return (s + 1) & ~1;
-}
-
-template <typename T> struct GenArgs
-{
-    Dims d;
-    Tabs<T> t;
-    const T *geo;
-    T lambda;
-    const T *in;
-    T *out0, *out1, *out2;
-    // optional gather of the input from a global vector: in[e*nc+m] = sign * gvec[map]
-    const int *gmap;
-    const double *gsign;
-    long gstride;
-    int nelmt, epb;
-    const int *skip;
-};
-
-#define NKB_STAGE(SIZE, ...)                                                                     \
-    for (int idx = threadIdx.x; idx < ne * (SIZE); idx += blockDim.x)                             \
-    {                                                                                             \
-        const int le = idx / (SIZE);                                                              \
-        const int l  = idx - le * (SIZE);                                                         \
-        T *sm        = smem + le * es;                                                            \
-        T *x = sm, *u = sm + d.nc, *g0 = u + d.nt, *g1 = g0 + d.nt, *g2 = g1 + d.nt;              \
-        T *wa = g2 + d.nt, *wb = wa + d.wsz;                                                      \
-        (void)x;                                                                                  \
-        (void)u;                                                                                  \
-        (void)g0;                                                                                 \
-        (void)g1;                                                                                 \
-        (void)g2;                                                                                 \
-        (void)wa;                                                                                 \
-        (void)wb;                                                                                 \
-        const long e = e0 + le;                                                                   \
-        (void)e;                                                                                  \
-        __VA_ARGS__                                                                               \
-    }                                                                                             \
-    __syncthreads();
-
-template <int SHAPE, int OP, typename T> __global__ void k_generic(GenArgs<T> a)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *smem       = reinterpret_cast<T *>(smem_raw);
-    const Dims &d = a.d;
-    const int es  = ElemSmem(d);
-    const long e0 = long(blockIdx.x) * a.epb;
-    const int ne  = int(min(long(a.epb), long(a.nelmt) - e0));
-    if (ne <= 0 || (a.skip && *a.skip))
-        return;
-    using BW = Bwd<SHAPE>;
-    using IP = Ipr<SHAPE>;
-
-    if (OP == GK_BWD || OP == GK_HELM || OP == GK_DIAG)
-    {
-        if (OP != GK_DIAG)
-        {
-            NKB_STAGE(d.nc, {
-                if (a.gmap)
-                {
-                    const long gi = e * d.nc + l;
-                    const T v = a.in[a.gmap[gi]];
-                    x[l]      = a.gsign ? T(a.gsign[gi]) * v : v;
-                }
-                else
-                {
-                    x[l] = a.in[e * d.nc + l];
-                }
-            })
-        }
-    }
-    else
-    {
-        NKB_STAGE(d.nt, { u[l] = a.in[e * d.nt + l]; })
-    }
-
-    if (OP == GK_BWD || OP == GK_HELM)
-    {
-        NKB_STAGE(BW::SizeA(d), { BW::A(d, a.t, x, wa, l); })
-        NKB_STAGE(BW::SizeB(d), { BW::B(d, a.t, x, wa, wb, l); })
-        NKB_STAGE(d.nt, { BW::C(d, a.t, x, wb, u, l); })
-        if (OP == GK_BWD)
-        {
-            NKB_STAGE(d.nt, { a.out0[e * d.nt + l] = u[l]; })
-            return;
-        }
-    }
-
-    if (OP == GK_PD)
-    {
-        NKB_STAGE(d.nt, {
-            T q0, q1, q2;
-            Grad(d, a.t, u, l, q0, q1, q2);
-            const T *A = a.geo + e * a.gstride + l;
-            const long o = e * d.nt + l;
-            a.out0[o] = fma(A[6 * d.nt], q2, fma(A[3 * d.nt], q1, A[0] * q0));
-            a.out1[o] = fma(A[7 * d.nt], q2, fma(A[4 * d.nt], q1, A[1 * d.nt] * q0));
-            a.out2[o] = fma(A[8 * d.nt], q2, fma(A[5 * d.nt], q1, A[2 * d.nt] * q0));
-        })
-        return;
-    }
-
-    if (OP == GK_IP)
-    {
-        // f = W * in
-        NKB_STAGE(d.nt, { u[l] = u[l] * a.geo[e * a.gstride + l]; })
-    }
-
-    if (OP == GK_HELM)
-    {
-        // v = G' grad u, f = lambda W u
-        NKB_STAGE(d.nt, {
-            T q0, q1, q2;
-            Grad(d, a.t, u, l, q0, q1, q2);
-            const T *G = a.geo + e * a.gstride + l;
-            const T W = G[0], G00 = G[d.nt], G11 = G[2 * d.nt], G22 = G[3 * d.nt];
-            const T G01 = G[4 * d.nt], G02 = G[5 * d.nt], G12 = G[6 * d.nt];
-            g0[l] = fma(G02, q2, fma(G01, q1, G00 * q0));
-            g1[l] = fma(G12, q2, fma(G11, q1, G01 * q0));
-            g2[l] = fma(G22, q2, fma(G12, q1, G02 * q0));
-            wa[l] = a.lambda * W * u[l];
-        })
-        NKB_STAGE(d.nt, { u[l] = wa[l] + GradT(d, a.t, g0, g1, g2, l); })
-    }
-
-    if (OP == GK_HELM || OP == GK_IP)
-    {
-        NKB_STAGE(IP::SizeA(d), { IprStageA(d, a.t, u, wa, l); })
-        NKB_STAGE(IP::SizeB(d), { IP::B(d, a.t, wa, wb, l); })
-        NKB_STAGE(d.nc, { a.out0[e * d.nc + l] = IP::C(d, a.t, wb, l); })
-    }
-}
 
 // Diagonal of the element Helmholtz matrix: for every mode m,
 // diag_m = sum_q lambda W phi_m^2 + grad phi_m . G' grad phi_m,
@@ -518,33 +373,6 @@ size_t GenericSmemBytes(const nkb_op *op, int elem_bytes)
     return size_t(ElemSmem(MakeDims(op))) * elem_bytes;
 }
 
-template <int SHAPE, int OP, typename T>
-static int LaunchGenericT(const nkb_op *op, GenArgs<T> a, cudaStream_t s)
-{
-    const int es      = ElemSmem(a.d);
-    const size_t ebyt = size_t(es) * sizeof(T);
-    int epb           = int(std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / ebyt)));
-    if (op->gen_epb > 0)
-        epb = op->gen_epb; // autotuned (checked against the shared-memory limit)
-    const int threads = op->gen_threads > 0 ? op->gen_threads : 128;
-    a.epb             = epb;
-    const size_t smem = ebyt * epb;
-    auto kern         = k_generic<SHAPE, OP, T>;
-    // raise the dynamic shared-memory limit once per instantiation, before any
-    // stream capture can contain this launch
-    static size_t s_smem_set = 48 * 1024;
-    if (smem > s_smem_set)
-    {
-        NKB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        s_smem_set = smem;
-    }
-    const long nb = (long(a.nelmt) + epb - 1) / epb;
-    if (nb > 0)
-        kern<<<unsigned(nb), threads, smem, s>>>(a);
-    NKB_CUDA_TRY(cudaGetLastError());
-    return NKB_OK;
-}
-
 template <int OP, typename T> static int LaunchGenericShape(const nkb_op *op, GenArgs<T> a, cudaStream_t s)
 {
     switch (op->shape)
@@ -556,6 +384,15 @@ template <int OP, typename T> static int LaunchGenericShape(const nkb_op *op, Ge
         default:
             return LaunchGenericT<NKB_TET, OP, T>(op, a, s);
     }
+}
+
+extern template int LaunchHelmStatic<double>(const nkb_op *, const GenArgs<double> &, cudaStream_t);
+extern template int LaunchHelmStatic<float>(const nkb_op *, const GenArgs<float> &, cudaStream_t);
+
+static bool StaticSizes()
+{
+    const char *v = std::getenv("NKB_GENERIC_STATIC");
+    return !(v && std::strcmp(v, "0") == 0);
 }
 
 template <typename T>
@@ -586,7 +423,15 @@ int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int 
         case NKB_PHYSDERIV:
             return LaunchGenericShape<GK_PD, T>(op, a, s);
         default:
+        {
+            if (StaticSizes())
+            {
+                const int rc = LaunchHelmStatic<T>(op, a, s);
+                if (rc != kNotCovered)
+                    return rc;
+            }
             return LaunchGenericShape<GK_HELM, T>(op, a, s);
+        }
     }
 }
 

@@ -130,3 +130,17 @@ def test_tuned_and_generic_hex_helmholtz_agree(monkeypatch, n, nm, variant):
     generic = nb.Operator("helmholtz", m)
     generic.set_factors(0.3)
     assert rel_l2(tuned(x), generic(x)) < 1e-13
+
+
+@pytest.mark.parametrize("shape,n,nm", [("prism", 2, 4), ("tet", 2, 5), ("prism", 1, 9), ("tet", 1, 11)])
+def test_static_and_runtime_size_generic_helmholtz_agree(monkeypatch, shape, n, nm):
+    """Prism / Tet Helmholtz with compile-time sizes against the same kernel
+    with run-time sizes."""
+    m = nb.BoxMesh(shape, n, nm, nm + 1, amp=0.05)
+    x = np.random.default_rng(nm).uniform(-1, 1, m.nelmt * m.nc)
+    fast = nb.Operator("helmholtz", m)
+    fast.set_factors(0.7)
+    monkeypatch.setenv("NKB_GENERIC_STATIC", "0")
+    slow = nb.Operator("helmholtz", m)
+    slow.set_factors(0.7)
+    assert rel_l2(fast(x), slow(x)) < 1e-13
