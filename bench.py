@@ -253,15 +253,10 @@ def run_b200(args, rank, world, local):
     import torch
     import nektar_b200 as nb
 
+    from nektar_b200 import replicas
     torch.cuda.set_device(local)
     dev = local
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-        pg = dist
+    pg = replicas.init(world, local, "nccl")
 
     mesh = nb.BoxMesh("hex", N_CELLS, NM, NM + 1, amp=AMP, coords=True)
     gmap, nglob, ndir = mesh.assembly()
@@ -296,8 +291,7 @@ def run_b200(args, rank, world, local):
     torch.cuda.synchronize()
 
     def barrier():
-        if pg:
-            pg.barrier()
+        replicas.barrier(pg)
 
     # ---- timed region: K device-resident solves -----------------------------
     reps, lat = [], []
@@ -315,11 +309,8 @@ def run_b200(args, rank, world, local):
         torch.cuda.synchronize()
         barrier()
     ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{dev}")
-    if pg:
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * args.steps / (ms_max / 1e3)
+    ms_max = replicas.max_over_ranks(ms, pg, f"cuda:{dev}")
+    value = replicas.whole_job_rate(args.steps, world, ms_max)
 
     # accuracy of the last solve against the manufactured solution
     x_fp64 = x_dev.cpu().numpy()
@@ -340,10 +331,8 @@ def run_b200(args, rank, world, local):
                           stream=sp)
     e1.record(stream)
     torch.cuda.synchronize()
-    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=f"cuda:{dev}")
-    if pg:
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    e2e = world * args.steps / (float(t.item()) / 1e3)
+    e2e = replicas.whole_job_rate(
+        args.steps, world, replicas.max_over_ranks(e0.elapsed_time(e1), pg, f"cuda:{dev}"))
 
     # ---- mixed precision: FP64 refinement around the FP32 CG, same criterion --
     def solve_mixed():
@@ -363,10 +352,8 @@ def run_b200(args, rank, world, local):
         mreps.append(solve_mixed())
     m1.record(stream)
     torch.cuda.synchronize()
-    t = torch.tensor([m0.elapsed_time(m1)], dtype=torch.float64, device=f"cuda:{dev}")
-    if pg:
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    mixed_value = world * args.steps / (float(t.item()) / 1e3)
+    mixed_value = replicas.whole_job_rate(
+        args.steps, world, replicas.max_over_ranks(m0.elapsed_time(m1), pg, f"cuda:{dev}"))
     xm = x_dev.cpu().numpy()
     mixed = {"value": mixed_value, "unit": "solves/s", "speedup_vs_fp64": mixed_value / value,
              "rel_l2_vs_fp64_solution": float(np.linalg.norm(xm - x_fp64) / np.linalg.norm(x_fp64)),
@@ -444,9 +431,7 @@ def run_b200(args, rank, world, local):
     S.close()
     op.close()
     op32.close()
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    replicas.finish(pg)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
