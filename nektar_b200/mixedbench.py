@@ -91,6 +91,13 @@ def main():
                             stream=s.cuda_stream)
 
     ms_seq = timed(sequential)
+    # each collection alone (same stream, same buffers)
+    for k, op in enumerate(ops):
+        groups[k]["ms"] = timed(lambda k=k, op=op: op.apply_device(
+            x.data_ptr() + 8 * int(offs_in[k]), y.data_ptr() + 8 * int(offs_out[k]),
+            stream=s.cuda_stream))
+        groups[k]["gb_s"] = groups[k]["bytes"] / groups[k]["ms"] / 1e6
+        groups[k]["kernel"] = op.kernel()
     peaks = {}
     try:
         with open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
