@@ -327,7 +327,8 @@ const char *KernelName(const nkb_op *op, bool gather)
         case 0: return "k_hex_helm (TMA-staged geometry)";
         case 1: return "k_hex_helm (streamed geometry, 1 element per CTA)";
         case 2: return "k_hex_helm (streamed geometry, 2 elements per CTA)";
-        default: return "k_hex_helm_mma (FP64 tensor cores)";
+        case 3: return "k_hex_helm_mma (FP64 tensor cores)";
+        default: return "k_hex_helm_mma2 (FP64 tensor cores, two warps per element)";
     }
 }
 

@@ -430,8 +430,9 @@ enum
 // candidate (geometry staging, elements per CTA) of the tuned Hex kernel
 // 0: TMA-staged geometry; 1, 2: streamed geometry, 1 or 2 elements per CTA;
 // 3: FP64 tensor cores (DMMA, nq <= 8, FP64 arithmetic for both storage
-//    precisions; nkb_hex_mma.cuh)
-constexpr int kNumHexVariants = 4;
+//    precisions; nkb_hex_mma.cuh); 4: the same with two warps per element
+//    (nkb_hex_mma2.cuh)
+constexpr int kNumHexVariants = 5;
 
 template <typename T, int NQ> constexpr int TmaEpb()
 {
@@ -489,6 +490,9 @@ static int HexVariantLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, 
 template <typename TV, int NM>
 static int HexMmaLaunch(const nkb_op *op, const HexArgs<TV> &a, bool gather, cudaStream_t s,
                         bool set_attr);
+template <typename TV, int NM>
+static int HexMma2Launch(const nkb_op *op, const HexArgs<TV> &a, bool gather, cudaStream_t s,
+                         bool set_attr);
 
 template <typename T, int NM>
 static int HexLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStream_t s, int variant,
@@ -497,6 +501,8 @@ static int HexLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStr
     constexpr int NQ = NM + 1;
     if (variant == 3)
         return HexMmaLaunch<T, NM>(op, a, gather, s, set_attr);
+    if (variant == 4)
+        return HexMma2Launch<T, NM>(op, a, gather, s, set_attr);
     switch (variant)
     {
         case 0:

@@ -41,6 +41,41 @@ __device__ __forceinline__ int CubeIdx(int c, int b, int a)
     return c * 68 + b * 8 + (a ^ ((b & 2) << 1) ^ (c & 4));
 }
 
+// Cubes of an FP32-storage operator hold floats (half the shared-memory
+// traffic, the operator's arithmetic stays FP64): [c][b][a] at
+// c*72 + b*8 + (a ^ 4*((b >> 2) & 1)), conflict-free for the A-fragment loads
+// of all three directions (32 lanes, 4-byte words).
+constexpr int kMmaCubeF = 8 * 72; // floats per FP32 cube
+
+__device__ __forceinline__ int CubeIdxF(int c, int b, int a)
+{
+    return c * 72 + b * 8 + (a ^ (b & 4));
+}
+
+template <typename TC> __device__ __forceinline__ int CIdx(int c, int b, int a)
+{
+    if constexpr (sizeof(TC) == 8)
+        return CubeIdx(c, b, a);
+    else
+        return CubeIdxF(c, b, a);
+}
+
+// elements per cube of either type
+template <typename TC> constexpr int CubeLen()
+{
+    return sizeof(TC) == 8 ? kMmaCube : kMmaCubeF;
+}
+
+template <typename TC> struct Pair2;
+template <> struct Pair2<double>
+{
+    using type = double2;
+};
+template <> struct Pair2<float>
+{
+    using type = float2;
+};
+
 __device__ __forceinline__ void Dmma(double &c0, double &c1, double a, double b)
 {
     asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
@@ -52,8 +87,8 @@ __device__ __forceinline__ void Dmma(double &c0, double &c1, double a, double b)
 // axes (tile = the slower, g = the faster), k and n run along AX.
 // out(rows, n) (+)= sum_k in(rows, k) * B(k, n), B(k, n) in fragments bf[kk]
 // (k = t + 4 kk, n = g).
-template <int AX, bool ACC, typename TIN = double>
-__device__ __forceinline__ void Contract(const TIN *__restrict__ in, double *__restrict__ out,
+template <int AX, bool ACC, typename TIN = double, typename TOUT = double>
+__device__ __forceinline__ void Contract(const TIN *__restrict__ in, TOUT *__restrict__ out,
                                          const double (&bf)[2], int g, int t)
 {
 #pragma unroll
@@ -62,51 +97,55 @@ __device__ __forceinline__ void Contract(const TIN *__restrict__ in, double *__r
         int ia0, ia1, io0, io1; // io1 = io0 + 1 when AX == 0
         if (AX == 0) // rows (c = tile, b = g)
         {
-            ia0 = CubeIdx(tile, g, t);
-            ia1 = CubeIdx(tile, g, t + 4);
-            io0 = CubeIdx(tile, g, 2 * t);
-            io1 = CubeIdx(tile, g, 2 * t + 1);
+            ia0 = CIdx<TIN>(tile, g, t);
+            ia1 = CIdx<TIN>(tile, g, t + 4);
+            io0 = CIdx<TOUT>(tile, g, 2 * t);
+            io1 = io0 + 1;
         }
         else if (AX == 1) // rows (c = tile, a = g)
         {
-            ia0 = CubeIdx(tile, t, g);
-            ia1 = CubeIdx(tile, t + 4, g);
-            io0 = CubeIdx(tile, 2 * t, g);
-            io1 = CubeIdx(tile, 2 * t + 1, g);
+            ia0 = CIdx<TIN>(tile, t, g);
+            ia1 = CIdx<TIN>(tile, t + 4, g);
+            io0 = CIdx<TOUT>(tile, 2 * t, g);
+            io1 = CIdx<TOUT>(tile, 2 * t + 1, g);
         }
         else // rows (b = tile, a = g)
         {
-            ia0 = CubeIdx(t, tile, g);
-            ia1 = CubeIdx(t + 4, tile, g);
-            io0 = CubeIdx(2 * t, tile, g);
-            io1 = CubeIdx(2 * t + 1, tile, g);
+            ia0 = CIdx<TIN>(t, tile, g);
+            ia1 = CIdx<TIN>(t + 4, tile, g);
+            io0 = CIdx<TOUT>(2 * t, tile, g);
+            io1 = CIdx<TOUT>(2 * t + 1, tile, g);
         }
         double c0 = 0.0, c1 = 0.0;
         if (AX == 0)
         {
-            // the pair (2t, 2t+1) is adjacent and 16-byte aligned: one vector access
-            double2 *o2 = reinterpret_cast<double2 *>(out + io0);
+            // the pair (2t, 2t+1) is adjacent and aligned: one vector access
+            using P2 = typename Pair2<TOUT>::type;
+            P2 *o2   = reinterpret_cast<P2 *>(out + io0);
             if (ACC)
             {
-                const double2 v = *o2;
-                c0              = v.x;
-                c1              = v.y;
+                const P2 v = *o2;
+                c0         = double(v.x);
+                c1         = double(v.y);
             }
             Dmma(c0, c1, double(in[ia0]), bf[0]);
             Dmma(c0, c1, double(in[ia1]), bf[1]);
-            *o2 = make_double2(c0, c1);
+            P2 w;
+            w.x = TOUT(c0);
+            w.y = TOUT(c1);
+            *o2 = w;
         }
         else
         {
             if (ACC)
             {
-                c0 = out[io0];
-                c1 = out[io1];
+                c0 = double(out[io0]);
+                c1 = double(out[io1]);
             }
             Dmma(c0, c1, double(in[ia0]), bf[0]);
             Dmma(c0, c1, double(in[ia1]), bf[1]);
-            out[io0] = c0;
-            out[io1] = c1;
+            out[io0] = TOUT(c0);
+            out[io1] = TOUT(c1);
         }
     }
 }
@@ -193,7 +232,7 @@ __device__ __forceinline__ void FetchCoeffs(const HexArgs<TV> &a, long e, int la
         if (idx[s] < 0)
             continue;
         const int pos = lane + 32 * s;
-        TV *dst       = x + CubeIdx(pos >> 6, (pos >> 3) & 7, pos & 7);
+        TV *dst       = x + CIdx<TV>(pos >> 6, (pos >> 3) & 7, pos & 7);
         if (!GATHER)
         {
             CpAsync(dst, a.in + e * NC + idx[s]);
@@ -219,7 +258,7 @@ __device__ __forceinline__ void FetchCoeffs(const HexArgs<TV> &a, long e, int la
 // contraction). Geometry is read with read-only loads in four batches of four
 // points per lane, all loads of a batch issued before any of its stores.
 template <typename TV, int NM, int NQ, bool GATHER>
-__global__ void __launch_bounds__(32 * kMmaWarps, 3)
+__global__ void __launch_bounds__(32 * kMmaWarps, sizeof(TV) == 8 ? 3 : 4)
     k_hex_helm_mma(HexArgs<TV> a, const __grid_constant__ HexConst<double, NM, NQ> c)
 {
     static_assert(NQ <= 8 && NM < NQ, "the DMMA Hex kernel covers nq <= 8");
@@ -231,9 +270,12 @@ __global__ void __launch_bounds__(32 * kMmaWarps, 3)
     long e            = long(blockIdx.x) * kMmaWarps + warp;
     if (e >= a.nelmt || (a.skip && *a.skip))
         return;
-    double *c0 = msm + warp * kMmaCubes * kMmaCube + kMmaCube, *c1 = c0 + kMmaCube,
-           *c2 = c1 + kMmaCube;
-    TV *xc = reinterpret_cast<TV *>(c0 - kMmaCube); // coefficients, in the vector type
+    // cubes hold the storage type: doubles for an FP64 operator, floats for
+    // an FP32-storage one (the arithmetic is FP64 either way)
+    using TC        = TV;
+    constexpr int CL = CubeLen<TC>();
+    TC *xc = reinterpret_cast<TC *>(msm) + warp * kMmaCubes * CL; // coefficients
+    TC *c0 = xc + CL, *c1 = c0 + CL, *c2 = c1 + CL;
     const uint32_t gbytes = uint32_t(7 * NQ3 * sizeof(TV) + 15) & ~15u;
 
     MmaTabs<NM, NQ> f;
@@ -241,8 +283,8 @@ __global__ void __launch_bounds__(32 * kMmaWarps, 3)
     const double lam = double(a.lambda);
 
     // the padded positions of the coefficient cube stay zero for good
-    for (int pos = lane; pos < kMmaCube; pos += 32)
-        xc[pos] = TV(0);
+    for (int pos = lane; pos < CL; pos += 32)
+        xc[pos] = TC(0);
     __syncwarp();
     int idx[16];
     LoadMap<NM, GATHER, TV>(a, e, lane, idx);
@@ -260,7 +302,7 @@ __global__ void __launch_bounds__(32 * kMmaWarps, 3)
         CpAsyncWaitAll();
         __syncwarp();
         // BwdTrans: p -> i (x -> c1), q -> j (c1 -> c0), r -> k (c0 -> c1 = u)
-        Contract<0, false, TV>(xc, c1, f.bw[0], g, t);
+        Contract<0, false>(xc, c1, f.bw[0], g, t);
         __syncwarp();
         const long en = e + nwarps;
         if (en < a.nelmt)
@@ -282,8 +324,8 @@ __global__ void __launch_bounds__(32 * kMmaWarps, 3)
         for (int tile = 0; tile < 8; ++tile)
         {
             z[tile][0] = z[tile][1] = 0.0;
-            Dmma(z[tile][0], z[tile][1], c1[CubeIdx(t, tile, g)], f.dg[0]);
-            Dmma(z[tile][0], z[tile][1], c1[CubeIdx(t + 4, tile, g)], f.dg[1]);
+            Dmma(z[tile][0], z[tile][1], double(c1[CIdx<TC>(t, tile, g)]), f.dg[0]);
+            Dmma(z[tile][0], z[tile][1], double(c1[CIdx<TC>(t + 4, tile, g)]), f.dg[1]);
         }
         __syncwarp();
         // metric at the lane's 16 points (c = 2t + h, b = tile, a = g):
@@ -306,15 +348,15 @@ __global__ void __launch_bounds__(32 * kMmaWarps, 3)
             for (int p = 0; p < 4; ++p)
             {
                 const int tile = tb + (p >> 1), h = p & 1;
-                const int ci   = CubeIdx(2 * t + h, tile, g);
-                const double x0 = c0[ci], x1 = c2[ci], x2 = z[tile][h];
+                const int ci   = CIdx<TC>(2 * t + h, tile, g);
+                const double x0 = double(c0[ci]), x1 = double(c2[ci]), x2 = z[tile][h];
                 const double W = gv[p][0], G00 = gv[p][1], G11 = gv[p][2], G22 = gv[p][3];
                 const double G01 = gv[p][4], G02 = gv[p][5], G12 = gv[p][6];
-                c0[ci]     = fma(G02, x2, fma(G01, x1, G00 * x0));
-                c2[ci]     = fma(G12, x2, fma(G11, x1, G01 * x0));
+                c0[ci]     = TC(fma(G02, x2, fma(G01, x1, G00 * x0)));
+                c2[ci]     = TC(fma(G12, x2, fma(G11, x1, G01 * x0)));
                 const double v2 = fma(G22, x2, fma(G12, x1, G02 * x0));
-                z[tile][h] = lam * W * c1[ci];
-                c1[ci]     = v2;
+                z[tile][h] = lam * W * double(c1[ci]);
+                c1[ci]     = TC(v2);
             }
         }
         __syncwarp();
@@ -322,15 +364,15 @@ __global__ void __launch_bounds__(32 * kMmaWarps, 3)
 #pragma unroll
         for (int tile = 0; tile < 8; ++tile)
         {
-            Dmma(z[tile][0], z[tile][1], c1[CubeIdx(t, tile, g)], f.dt[0]);
-            Dmma(z[tile][0], z[tile][1], c1[CubeIdx(t + 4, tile, g)], f.dt[1]);
+            Dmma(z[tile][0], z[tile][1], double(c1[CIdx<TC>(t, tile, g)]), f.dt[0]);
+            Dmma(z[tile][0], z[tile][1], double(c1[CIdx<TC>(t + 4, tile, g)]), f.dt[1]);
         }
         __syncwarp();
 #pragma unroll
         for (int tile = 0; tile < 8; ++tile)
         {
-            c1[CubeIdx(2 * t, tile, g)]     = z[tile][0];
-            c1[CubeIdx(2 * t + 1, tile, g)] = z[tile][1];
+            c1[CIdx<TC>(2 * t, tile, g)]     = TC(z[tile][0]);
+            c1[CIdx<TC>(2 * t + 1, tile, g)] = TC(z[tile][1]);
         }
         __syncwarp();
         Contract<0, true>(c0, c1, f.dt, g, t);
@@ -347,8 +389,8 @@ __global__ void __launch_bounds__(32 * kMmaWarps, 3)
         for (int tile = 0; tile < NM; ++tile) // rows (r = tile, q = g), n = p
         {
             double y0 = 0.0, y1 = 0.0;
-            Dmma(y0, y1, c2[CubeIdx(tile, g, t)], f.ip[0][0]);
-            Dmma(y0, y1, c2[CubeIdx(tile, g, t + 4)], f.ip[0][1]);
+            Dmma(y0, y1, double(c2[CIdx<TC>(tile, g, t)]), f.ip[0][0]);
+            Dmma(y0, y1, double(c2[CIdx<TC>(tile, g, t + 4)]), f.ip[0][1]);
             if (g < NM)
             {
                 if (2 * t < NM)
@@ -368,7 +410,7 @@ static int HexMmaLaunch(const nkb_op *op, const HexArgs<TV> &a, bool gather, cud
                         bool set_attr)
 {
     constexpr int NQ   = NM + 1;
-    const size_t bytes = size_t(kMmaWarps) * kMmaCubes * kMmaCube * sizeof(double);
+    const size_t bytes = size_t(kMmaWarps) * kMmaCubes * CubeLen<TV>() * sizeof(TV);
     if constexpr (NQ > 8)
     {
         (void)op;
@@ -415,3 +457,5 @@ static int HexMmaLaunch(const nkb_op *op, const HexArgs<TV> &a, bool gather, cud
 }
 
 } // namespace nkb
+
+#include "nkb_hex_mma2.cuh"

@@ -115,7 +115,7 @@ def test_device_pointer_path_matches_host_path():
 
 
 @pytest.mark.parametrize("n,nm", [(1, 5), (3, 7), (2, 9), (1, 11), (5, 2)])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_tuned_and_generic_hex_helmholtz_agree(monkeypatch, n, nm, variant):
     """Every variant of the tuned Hex kernel (nkb_hex.cu: TMA-staged or
     streamed geometry, 1-2 elements per CTA, FP64 tensor cores for nq <= 8)
