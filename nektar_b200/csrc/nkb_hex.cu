@@ -320,7 +320,15 @@ int TuneHexGather(nkb_op *op, const void *xin, void *yl, const int *map, const d
 const char *KernelName(const nkb_op *op, bool gather)
 {
     if (op->variant != kVariantHexHelm)
+    {
+        const int nm   = op->nm;
+        const bool std = op->nq[0] == nm + 1 &&
+                         ((op->shape == NKB_PRISM && op->nq[1] == nm + 1 && op->nq[2] == nm) ||
+                          (op->shape == NKB_TET && op->nq[1] == nm && op->nq[2] == nm));
+        if (op->optype == NKB_HELMHOLTZ && std && nm >= 2 && nm <= 11)
+            return "k_col_helm (Prism/Tet column kernel)";
         return "k_generic";
+    }
     const int v = (gather && op->hex_variant_gather >= 0) ? op->hex_variant_gather : op->hex_variant;
     switch (v)
     {

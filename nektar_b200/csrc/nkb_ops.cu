@@ -387,11 +387,21 @@ template <int OP, typename T> static int LaunchGenericShape(const nkb_op *op, Ge
 }
 
 extern template int LaunchHelmStatic<double>(const nkb_op *, const GenArgs<double> &, cudaStream_t);
+// Prism / Tet column kernels (nkb_col_kernel.cuh, nkb_col_f64.cu, nkb_col_f32.cu)
+template <typename T> int LaunchColHelm(const nkb_op *op, const GenArgs<T> &a, cudaStream_t s);
+extern template int LaunchColHelm<double>(const nkb_op *, const GenArgs<double> &, cudaStream_t);
+extern template int LaunchColHelm<float>(const nkb_op *, const GenArgs<float> &, cudaStream_t);
 extern template int LaunchHelmStatic<float>(const nkb_op *, const GenArgs<float> &, cudaStream_t);
 
 static bool StaticSizes()
 {
     const char *v = std::getenv("NKB_GENERIC_STATIC");
+    return !(v && std::strcmp(v, "0") == 0);
+}
+
+static bool ColKernels()
+{
+    const char *v = std::getenv("NKB_COL");
     return !(v && std::strcmp(v, "0") == 0);
 }
 
@@ -424,6 +434,12 @@ int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int 
             return LaunchGenericShape<GK_PD, T>(op, a, s);
         default:
         {
+            if (ColKernels())
+            {
+                const int rc = LaunchColHelm<T>(op, a, s);
+                if (rc != kNotCovered)
+                    return rc;
+            }
             if (StaticSizes())
             {
                 const int rc = LaunchHelmStatic<T>(op, a, s);

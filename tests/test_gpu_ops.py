@@ -138,9 +138,61 @@ def test_static_and_runtime_size_generic_helmholtz_agree(monkeypatch, shape, n, 
     with run-time sizes."""
     m = nb.BoxMesh(shape, n, nm, nm + 1, amp=0.05)
     x = np.random.default_rng(nm).uniform(-1, 1, m.nelmt * m.nc)
+    monkeypatch.setenv("NKB_COL", "0")
     fast = nb.Operator("helmholtz", m)
     fast.set_factors(0.7)
+    y_fast = fast(x)  # the switches are read at launch time
     monkeypatch.setenv("NKB_GENERIC_STATIC", "0")
     slow = nb.Operator("helmholtz", m)
     slow.set_factors(0.7)
-    assert rel_l2(fast(x), slow(x)) < 1e-13
+    assert rel_l2(y_fast, slow(x)) < 1e-13
+
+
+@pytest.mark.parametrize("shape,n,nm", [("prism", 2, 3), ("prism", 1, 8), ("prism", 1, 11),
+                                        ("tet", 2, 4), ("tet", 1, 7), ("tet", 1, 11)])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("fp32", 2e-6)])
+def test_column_and_generic_helmholtz_agree(monkeypatch, shape, n, nm, precision, tol):
+    """Prism / Tet column kernels (k direction in registers) against the
+    shape-generic kernel."""
+    import torch
+    m = nb.BoxMesh(shape, n, nm, nm + 1, amp=0.05)
+    x = np.random.default_rng(nm).uniform(-1, 1, m.nelmt * m.nc)
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    xd = torch.tensor(x, dtype=dt, device="cuda")
+
+    def apply(op):
+        yd = torch.empty(m.nelmt * m.nc, dtype=dt, device="cuda")
+        op.apply_device(xd.data_ptr(), yd.data_ptr(),
+                        stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        return yd.double().cpu().numpy()
+
+    col = nb.Operator("helmholtz", m, precision=precision)
+    col.set_factors(1.3)
+    y_col = apply(col)  # the switch is read at launch time
+    monkeypatch.setenv("NKB_COL", "0")
+    gen = nb.Operator("helmholtz", m, precision=precision)
+    gen.set_factors(1.3)
+    assert rel_l2(y_col, apply(gen)) < tol
+
+
+@pytest.mark.parametrize("shape", ["prism", "tet"])
+def test_column_kernel_gathered_in_cg(monkeypatch, shape):
+    """The column kernels' gathered form (inside the CG): a block-diagonal
+    system (every local dof its own global dof) solved with the column and
+    with the generic kernels."""
+    m = nb.BoxMesh(shape, 2, 5, 6, amp=0.05)
+    nloc = m.nelmt * m.nc
+    gmap = np.arange(nloc, dtype=np.int32)
+    b = np.random.default_rng(4).uniform(-1, 1, nloc)
+    op = nb.Operator("helmholtz", m)
+    op.set_factors(2.0)
+    S = nb.GlobalLinSys([op], gmap, nloc, 0)
+    xa, ra = S.solve(b, tol=1e-12)
+    monkeypatch.setenv("NKB_COL", "0")
+    op2 = nb.Operator("helmholtz", m)
+    op2.set_factors(2.0)
+    S2 = nb.GlobalLinSys([op2], gmap, nloc, 0)
+    xb, rb = S2.solve(b, tol=1e-12)
+    assert ra.converged and rb.converged
+    assert rel_l2(xa, xb) < 1e-10
