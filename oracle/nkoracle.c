@@ -781,6 +781,93 @@ void or_helmholtz(int shape, int deformed, int nm, const int *nq, int nelmt,
 }
 
 /* ------------------------------------------------------------------ */
+/* IProductWRTDerivBase                                                */
+/* ------------------------------------------------------------------ */
+
+/* IProductWRTDerivBaseKernels.hpp (Hex / Prism / Tet kernels): the physical
+ * vector field (in0, in1, in2) to reference directions with the derivative
+ * factors df (and, for Prism / Tet, the collapsed-coordinate factors). */
+static void ipd_transform(int shape, int deformed, const int *nq, const double *const *Z,
+                          const double *df, size_t ncol, size_t col0, const double *in0,
+                          const double *in1, const double *in2, double *t0, double *t1,
+                          double *t2)
+{
+    const int nq0 = nq[0], nq1 = nq[1], nq2 = nq[2];
+    double f[9];
+    if (!deformed)
+        for (int d = 0; d < 9; ++d)
+            f[d] = df[d * ncol + col0];
+    for (int k = 0, c = 0; k < nq2; ++k)
+    {
+        const double z2f = 2.0 / (1.0 - Z[2][k]);
+        for (int j = 0; j < nq1; ++j)
+        {
+            const double f3 = (shape == TET) ? 0.5 * (1.0 + Z[1][j]) : 0.0;
+            const double f0 = (shape == TET) ? 2.0 * z2f / (1.0 - Z[1][j]) : 0.0;
+            for (int i = 0; i < nq0; ++i, ++c)
+            {
+                if (deformed)
+                    for (int d = 0; d < 9; ++d)
+                        f[d] = df[d * ncol + col0 + c];
+                const double a = in0[c], b = in1[c], g = in2[c];
+                double v0 = f[0] * a + f[3] * b + f[6] * g;
+                double v1 = f[1] * a + f[4] * b + f[7] * g;
+                double v2 = f[2] * a + f[5] * b + f[8] * g;
+                if (shape == PRISM)
+                {
+                    const double hf1 = 0.5 * (1.0 + Z[0][i]);
+                    v0 *= z2f;
+                    v0 = fma(hf1 * v2, z2f, v0);
+                }
+                else if (shape == TET)
+                {
+                    const double f1 = 0.5 * (1.0 + Z[0][i]);
+                    v0 = fma(v1 + v2, f1, v0);
+                    v0 *= f0;
+                    v1 = fma(v2, f3, v1);
+                    v1 *= z2f;
+                }
+                t0[c] = v0;
+                t1[c] = v1;
+                t2[c] = v2;
+            }
+        }
+    }
+}
+
+/* IProductWRTDerivBase.h fusedKernel3D (:789-825): three inner products,
+ * each with the basis derivative dB in one direction. The three input
+ * fields are consecutive: field f of element e at in + f*nelmt*nt + e*nt. */
+void or_iproduct_deriv(int shape, int deformed, int nm, const int *nq, int nelmt,
+                       const double *const *B, const double *const *dB, const double *const *w,
+                       const double *const *Z, const double *jac, const double *df,
+                       const double *in, double *out)
+{
+    const int nc = or_ncoeffs(shape, nm), nt = nq[0] * nq[1] * nq[2];
+    const size_t ncol = deformed ? (size_t)nelmt * nt : (size_t)nelmt;
+    const size_t field = (size_t)nelmt * nt;
+    double *buf = malloc(sizeof(double) * (3 * (size_t)nt + 2 * wsp_size(nm, nq)));
+    double *t0 = buf, *t1 = buf + nt, *t2 = buf + 2 * nt;
+    double *w0 = buf + 3 * nt, *w1 = w0 + wsp_size(nm, nq);
+    const double *T0[3] = {dB[0], B[1], B[2]};
+    const double *T1[3] = {B[0], dB[1], B[2]};
+    const double *T2[3] = {B[0], B[1], dB[2]};
+    for (int e = 0; e < nelmt; ++e)
+    {
+        const size_t off = (size_t)e * nt;
+        const size_t col0 = deformed ? off : (size_t)e;
+        const double *je = deformed ? jac + off : jac + e;
+        ipd_transform(shape, deformed, nq, Z, df, ncol, col0, in + off, in + field + off,
+                      in + 2 * field + off, t0, t1, t2);
+        double *oe = out + (size_t)e * nc;
+        ip_elem(shape, nm, nq, T0, w, je, deformed, t0, oe, 0, 0, 1.0, w0, w1);
+        ip_elem(shape, nm, nq, T1, w, je, deformed, t1, oe, 0, 1, 1.0, w0, w1);
+        ip_elem(shape, nm, nq, T2, w, je, deformed, t2, oe, 0, 1, 1.0, w0, w1);
+    }
+    free(buf);
+}
+
+/* ------------------------------------------------------------------ */
 /* Assembly map and CG                                                 */
 /* ------------------------------------------------------------------ */
 

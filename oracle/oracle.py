@@ -34,6 +34,7 @@ def lib():
         L.or_bwdtrans.restype = None
         L.or_iproduct.restype = None
         L.or_physderiv.restype = None
+        L.or_iproduct_deriv.restype = None
         L.or_helmholtz.restype = None
         L.or_pcg.restype = ctypes.c_int
         _lib = L
@@ -79,6 +80,19 @@ def physderiv(shape, nq, nelmt, D, Z, df, f, deformed):
                        _p(np.ascontiguousarray(df)), _p(np.ascontiguousarray(f)), _p(o0), _p(o1),
                        _p(o2))
     return o0, o1, o2
+
+
+def iproduct_deriv(shape, nm, nq, nelmt, T, jac, df, f, deformed):
+    """f: the three physical fields consecutively (3 * nelmt * nt values)."""
+    kb, Bp = _arr3(T["b"])
+    kdb, dBp = _arr3(T["db"])
+    kw, Wp = _arr3(T["w"])
+    kz, Zp = _arr3(T["z"])
+    out = np.zeros(nelmt * ncoeffs(shape, nm))
+    lib().or_iproduct_deriv(SHAPES[shape], int(deformed), nm, (ctypes.c_int * 3)(*nq), nelmt,
+                            Bp, dBp, Wp, Zp, _p(np.ascontiguousarray(jac)),
+                            _p(np.ascontiguousarray(df)), _p(np.ascontiguousarray(f)), _p(out))
+    return out
 
 
 def helmholtz(shape, nm, nq, nelmt, T, jac, df, x, lam=1.0, deformed=True, diff_mode=0,

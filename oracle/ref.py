@@ -15,7 +15,7 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 # numbering as LibUtilities::ShapeType / Collections::OperatorType / PointsType / BasisType
 SHAPES = {"tet": 5, "prism": 7, "hex": 8}
-OPS = {"bwdtrans": 0, "helmholtz": 1, "iproduct": 3, "physderiv": 5}
+OPS = {"bwdtrans": 0, "helmholtz": 1, "iproduct": 3, "iproduct_deriv": 4, "physderiv": 5}
 GLL, RADAU_A1, RADAU_A2 = 4, 11, 12
 MOD_A, MOD_B, MOD_C = 4, 5, 6
 

@@ -15,7 +15,8 @@
 //    -> de-interleave with zero padding of the last block:
 //      BwdTrans.h:364-420 (operator3D), IProduct.h:410-491 (operator3D),
 //      PhysDeriv.h:478-571 (operator3D), Helmholtz.h:374-464 (operator3D) and
-//      the fused body Helmholtz.h:549-599 (fusedKernel3D);
+//      the fused body Helmholtz.h:549-599 (fusedKernel3D),
+//      IProductWRTDerivBase.h:592-694 (operator3D) and :789-825 (fusedKernel3D);
 //  * the geometry interleave of CoalescedGeomData.cpp:90-159 (GetJacInterLeave)
 //    and :265-342 (GetDerivFactorsInterLeave);
 //  * the vec_t broadcast of the 1-D tables, Operator.hpp:529-641 (SetUpBdata,
@@ -68,6 +69,7 @@ template <class Dim, class T> struct Array
 #include <MatrixFreeOps/BwdTransKernels.hpp>
 #include <MatrixFreeOps/HelmholtzKernels.hpp>
 #include <MatrixFreeOps/IProductKernels.hpp>
+#include <MatrixFreeOps/IProductWRTDerivBaseKernels.hpp>
 #include <MatrixFreeOps/PhysDerivKernels.hpp>
 
 #ifndef NKREF_SHAPE
@@ -98,6 +100,7 @@ enum
     OP_BWDTRANS  = 0,
     OP_HELMHOLTZ = 1,
     OP_IPRODUCT  = 3,
+    OP_IPRODUCT_DERIV = 4,
     OP_PHYSDERIV = 5
 };
 
@@ -431,6 +434,70 @@ template <bool DEFORMED> void ApplyHelmholtz(const RefOp &o, const Chunk &c, con
     }
 }
 
+// IProductWRTDerivBase.h fusedKernel3D (:789-825): the physical vector field
+// to reference directions (IProductWRTDerivBase3DKernel, with the collapsed
+// factors of Prism/Tet), then three inner products, each with the basis
+// derivative in one direction. The three input fields are consecutive in
+// `in` (field f of element e at in + f*nelmt*nqTot + e*nqTot).
+template <bool DEFORMED>
+void ApplyIProductDeriv(const RefOp &o, const Chunk &c, const double *in, double *out)
+{
+    const int nm = o.nm, nq0 = o.nq[0], nq1 = o.nq[1], nq2 = o.nq[2];
+    const int W  = vec_t::width;
+    constexpr int ndf = 9;
+    std::size_t wsp0Size = 0, wsp1Size = 0, wsp2Size = 0;
+    IProduct3DWorkspace<kShape>(nm, nm, nm, nq0, nq1, nq2, wsp0Size, wsp1Size, wsp2Size);
+    VecV wsp0(wsp0Size), wsp1(wsp1Size), wsp2(std::max<std::size_t>(wsp2Size, nm));
+    VecV tIn0(o.nqTot), tIn1(o.nqTot), tIn2(o.nqTot), t0(o.nqTot), t1(o.nqTot), t2(o.nqTot),
+        tmpOut(o.nmTot);
+    std::vector<double> loc(std::size_t(std::max(o.nmTot, o.nqTot)) * W, 0.0);
+    const std::size_t field = std::size_t(o.nelmt) * o.nqTot;
+    const double *inptr     = in + std::size_t(c.e0) * o.nqTot;
+    double *outptr          = out + std::size_t(c.e0) * o.nmTot;
+    const vec_t *jac_ptr    = c.jac.data();
+    const vec_t *df_ptr     = c.df.data();
+    VecV *tins[3]           = {&tIn0, &tIn1, &tIn2};
+    for (int b = 0; b < c.nBlocks; ++b)
+    {
+        int nreal = std::min(W, c.ne - b * W);
+        for (int f = 0; f < 3; ++f)
+        {
+            std::fill(loc.begin(), loc.end(), 0.0);
+            const double *src = inptr + f * field;
+            std::copy(src, src + std::size_t(nreal) * o.nqTot, loc.data());
+            load_unalign_interleave(loc.data(), o.nqTot, *tins[f]);
+        }
+        IProductWRTDerivBase3DKernel<kShape, DEFORMED>(nq0, nq1, nq2, df_ptr, o.Z[0], o.Z[1],
+                                                       o.Z[2], tIn0, tIn1, tIn2, t0, t1, t2);
+        IProduct3DKernel<kShape, false, false, DEFORMED>(nm, nm, nm, nq0, nq1, nq2, true, t0,
+                                                         o.dbdata[0], o.bdata[1], o.bdata[2],
+                                                         o.w[0], o.w[1], o.w[2], jac_ptr, wsp0,
+                                                         wsp1, wsp2, tmpOut);
+        IProduct3DKernel<kShape, false, true, DEFORMED>(nm, nm, nm, nq0, nq1, nq2, true, t1,
+                                                        o.bdata[0], o.dbdata[1], o.bdata[2],
+                                                        o.w[0], o.w[1], o.w[2], jac_ptr, wsp0,
+                                                        wsp1, wsp2, tmpOut);
+        IProduct3DKernel<kShape, false, true, DEFORMED>(nm, nm, nm, nq0, nq1, nq2, true, t2,
+                                                        o.bdata[0], o.bdata[1], o.dbdata[2],
+                                                        o.w[0], o.w[1], o.w[2], jac_ptr, wsp0,
+                                                        wsp1, wsp2, tmpOut);
+        deinterleave_unalign_store(tmpOut, o.nmTot, loc.data());
+        std::copy(loc.data(), loc.data() + std::size_t(nreal) * o.nmTot, outptr);
+        inptr += std::size_t(W) * o.nqTot;
+        outptr += std::size_t(W) * o.nmTot;
+        if (DEFORMED)
+        {
+            jac_ptr += o.nqTot;
+            df_ptr += std::size_t(ndf) * o.nqTot;
+        }
+        else
+        {
+            ++jac_ptr;
+            df_ptr += ndf;
+        }
+    }
+}
+
 void ApplyChunk(const RefOp &o, const Chunk &c, const double *in, double *o0, double *o1, double *o2)
 {
     if (c.ne == 0)
@@ -451,6 +518,10 @@ void ApplyChunk(const RefOp &o, const Chunk &c, const double *in, double *o0, do
             break;
         case OP_HELMHOLTZ:
             o.deformed ? ApplyHelmholtz<true>(o, c, in, o0) : ApplyHelmholtz<false>(o, c, in, o0);
+            break;
+        case OP_IPRODUCT_DERIV:
+            o.deformed ? ApplyIProductDeriv<true>(o, c, in, o0)
+                       : ApplyIProductDeriv<false>(o, c, in, o0);
             break;
     }
 }

@@ -30,6 +30,8 @@ def test_oracle_matches_golden(path):
         y = O.helmholtz(s, nm, nq, ne, T, g["jac"], g["df"], g["x"], float(g["lam"]), dfm, mode,
                         g["diff"] if mode else None)
         assert rel_l2(y, g["out_" + tag]) < TOL, tag
+    y = O.iproduct_deriv(s, nm, nq, ne, T, g["jac"], g["df"], g["f3"], dfm)
+    assert rel_l2(y, g["out_iproduct_deriv"]) < TOL
 
 
 def _tables(shape, nm, nq0):
@@ -54,6 +56,28 @@ def test_oracle_matches_live_reference(shape, nm):
     y = np.zeros(ne * nc)
     op.apply(x, y)
     yo = O.helmholtz(shape, nm, nq, ne, To, jac, df, x, 0.7, True)
+    assert rel_l2(yo, y) < TOL
+
+
+@pytest.mark.skipif(not ref.available(), reason="reference kernels not built (make -C oracle ref)")
+@pytest.mark.parametrize("shape", ["hex", "prism", "tet"])
+@pytest.mark.parametrize("deformed", [False, True])
+def test_oracle_iproduct_deriv_matches_live_reference(shape, deformed):
+    rng = np.random.default_rng(11 + len(shape) + deformed)
+    nm = 6
+    T, nq = _tables(shape, nm, nm + 1)
+    ne, nt = 11, nq[0] * nq[1] * nq[2]
+    ncol = ne * nt if deformed else ne
+    jac = rng.uniform(0.5, 1.5, ncol)
+    df = rng.uniform(-1, 1, (9, ncol))
+    f = rng.uniform(-1, 1, 3 * ne * nt)
+    To = dict(T)
+    To["w"] = T["ws"]
+    op = ref.RefOp(shape, "iproduct_deriv", nm, nq, ne, To, jac=jac, df=df, deformed=deformed,
+                   nthreads=2)
+    y = np.zeros(ne * O.ncoeffs(shape, nm))
+    op.apply(f, y)
+    yo = O.iproduct_deriv(shape, nm, nq, ne, To, jac, df, f, deformed)
     assert rel_l2(yo, y) < TOL
 
 
