@@ -53,6 +53,7 @@ extern "C" {
 #define NKB_BWDTRANS 0  /* Collections::eBwdTrans */
 #define NKB_HELMHOLTZ 1 /* Collections::eHelmholtz */
 #define NKB_IPRODUCT 3  /* Collections::eIProductWRTBase */
+#define NKB_IPRODUCT_DERIV 4 /* Collections::eIProductWRTDerivBase */
 #define NKB_PHYSDERIV 5 /* Collections::ePhysDeriv */
 
 #define NKB_GLL 4       /* LibUtilities::eGaussLobattoLegendre */
@@ -106,14 +107,16 @@ int nkb_basis(int btype, int nm, int np, const double *z, const double *D, doubl
  *   through OPERATOR_CREATE / GetOperatorFactory (Operator.h:43-54,118-129),
  *   implemented by Helmholtz_MatrixFree (Collections/Helmholtz.cpp:586-761),
  *   BwdTrans_MatrixFree (BwdTrans.cpp:160-243), IProductWRTBase_MatrixFree
- *   (IProductWRTBase.cpp:182-268), PhysDeriv_MatrixFree (PhysDeriv.cpp:272-).
+ *   (IProductWRTBase.cpp:182-268), PhysDeriv_MatrixFree (PhysDeriv.cpp:272-),
+ *   IProductWRTDerivBase_MatrixFree (IProductWRTDerivBase.cpp:276-374).
  */
 typedef struct nkb_op nkb_op;
 
 typedef struct nkb_op_desc
 {
     int shape;    /* NKB_HEX / NKB_PRISM / NKB_TET */
-    int optype;   /* NKB_BWDTRANS / NKB_HELMHOLTZ / NKB_IPRODUCT / NKB_PHYSDERIV */
+    int optype;   /* NKB_BWDTRANS / NKB_HELMHOLTZ / NKB_IPRODUCT / NKB_IPRODUCT_DERIV /
+                     NKB_PHYSDERIV */
     int nm;       /* modes per direction (equal in all directions) */
     int nq[3];    /* points per direction (Tet: nq0, nq0-1, nq0-1; Prism: nq0, nq0, nq0-1) */
     int ptype[3]; /* points type per direction */
@@ -121,7 +124,8 @@ typedef struct nkb_op_desc
     int deformed; /* 1: geometry per quadrature point (eDeformed), 0: per element */
     /* host arrays, reference layouts (see top of file); NULL where the
      * operator does not need them: BwdTrans needs bdata; IProduct bdata, w, jac;
-     * PhysDeriv z, D, df; Helmholtz bdata, w, z, D, jac, df. */
+     * PhysDeriv z, D, df; Helmholtz and IProductWRTDerivBase bdata, w, z, D,
+     * jac, df. */
     const double *bdata[3];
     const double *w[3];
     const double *z[3];
@@ -144,7 +148,10 @@ int nkb_op_set_factors(nkb_op *op, double lambda, int diff_mode, const double *d
 
 /* Replaces Collections::Operator::operator()(in, out0, out1, out2, wsp)
  * (Operator.h:148-152): out0 is overwritten (no accumulate); PhysDeriv
- * writes d/dx, d/dy, d/dz to out0, out1, out2. flags: NKB_HOST_PTRS or
+ * writes d/dx, d/dy, d/dz to out0, out1, out2; IProductWRTDerivBase reads
+ * the three components of its vector field consecutively from in (component
+ * c of element e at in + c*nelmt*ntot + e*ntot; nkb_op_apply3 takes them as
+ * three arrays) and writes out0. flags: NKB_HOST_PTRS or
  * NKB_DEVICE_PTRS; stream: a cudaStream_t (NULL = the legacy default
  * stream), on which the kernel is enqueued. With
  * host pointers the result is in out0.. on return, as the reference's is. */
@@ -165,6 +172,14 @@ int nkb_op_apply(nkb_op *op, const double *in, double *out0, double *out1, doubl
  * NKB_HOST_PTRS path it mirrors. */
 int nkb_op_apply_host_static(nkb_op *op, const double *in, double *out0, double *out1,
                              double *out2, void *stream);
+
+/* IProductWRTDerivBase with its three input fields as separate arrays, as
+ * IProductWRTDerivBase_MatrixFree::operator()(entry0, entry1, entry2, entry3)
+ * takes them for a 3-D coordinate system (IProductWRTDerivBase.cpp:285-318):
+ * out = sum_m (d phi / d x_m, in_m) for every mode phi. flags and stream as
+ * nkb_op_apply. Only for NKB_IPRODUCT_DERIV operators. */
+int nkb_op_apply3(nkb_op *op, const double *in0, const double *in1, const double *in2,
+                  double *out, int flags, void *stream);
 
 /* FP32 variant of nkb_op_apply for NKB_FP32 operators (device pointers). */
 int nkb_op_apply_f32(nkb_op *op, const float *in, float *out0, float *out1, float *out2,

@@ -15,12 +15,12 @@ import numpy as np
 
 from . import _capi as C
 from ._capi import (BWDTRANS, DEVICE_PTRS, DIFF_CONST, DIFF_NONE, DIFF_VAR, FP32, FP64, GLL,
-                    HELMHOLTZ, HEX, HOST_PTRS, IPRODUCT, MODIFIED_A, MODIFIED_B, MODIFIED_C,
+                    HELMHOLTZ, HEX, HOST_PTRS, IPRODUCT, IPRODUCT_DERIV, MODIFIED_A, MODIFIED_B, MODIFIED_C,
                     PHYSDERIV, PRISM, RADAU_A1, RADAU_A2, TET, NektarB200Error, check)
 
 SHAPES = {"hex": HEX, "prism": PRISM, "tet": TET}
 OPTYPES = {"bwdtrans": BWDTRANS, "helmholtz": HELMHOLTZ, "iproduct": IPRODUCT,
-           "physderiv": PHYSDERIV}
+           "iproduct_deriv": IPRODUCT_DERIV, "physderiv": PHYSDERIV}
 WEIGHT_FACTOR = {GLL: 1.0, RADAU_A1: 0.5, RADAU_A2: 0.25}
 
 __all__ = ["Operator", "GlobalLinSys", "BoxMesh", "points", "basis", "shape_tables", "lib",
@@ -190,6 +190,23 @@ class Operator:
         check(lib().nkb_op_apply(self.h, x.ctypes.data, *[None if o is None else o.ctypes.data
                                                            for o in outs], HOST_PTRS, None))
         return tuple(outs[:nout]) if nout > 1 else outs[0]
+
+    def apply3(self, f0, f1, f2):
+        """IProductWRTDerivBase with the vector field as three host arrays
+        (IProductWRTDerivBase_MatrixFree::operator(), synchronous)."""
+        fs = [_f64(f) for f in (f0, f1, f2)]
+        n = self.in_size // 3
+        if self.optype != IPRODUCT_DERIV or any(f.size != n for f in fs):
+            raise ValueError("apply3 takes three fields of %d values of an iproduct_deriv "
+                             "operator" % n)
+        out = np.zeros(self.out_size)
+        check(lib().nkb_op_apply3(self.h, *[f.ctypes.data for f in fs], out.ctypes.data,
+                                  HOST_PTRS, None))
+        return out
+
+    def apply3_device(self, f0_ptr, f1_ptr, f2_ptr, out_ptr, stream=None):
+        """apply3 on device pointers, stream-ordered."""
+        check(lib().nkb_op_apply3(self.h, f0_ptr, f1_ptr, f2_ptr, out_ptr, DEVICE_PTRS, stream))
 
     def apply_device(self, x_ptr, out0, out1=None, out2=None, stream=None):
         """Device pointers (ints); stream-ordered on `stream` (cudaStream_t int)."""

@@ -7,7 +7,7 @@
 //   * OperatorKey (shape, operator type, implementation type, nodal) and a
 //     factory keyed by it (GetOperatorFactory().CreateInstance), with the new
 //     implementation type eB200 registered for Hex/Prism/Tet x BwdTrans,
-//     IProductWRTBase, PhysDeriv, Helmholtz;
+//     IProductWRTBase, IProductWRTDerivBase, PhysDeriv, Helmholtz;
 //   * GlobalLinSysIterativeFullB200: the GlobalLinSysIterativeFull solve.
 //
 // Errors: a failing status from the C ABI throws NekError with the
@@ -59,8 +59,9 @@ enum OperatorType
 {
     eBwdTrans        = NKB_BWDTRANS,
     eHelmholtz       = NKB_HELMHOLTZ,
-    eIProductWRTBase = NKB_IPRODUCT,
-    ePhysDeriv       = NKB_PHYSDERIV
+    eIProductWRTBase      = NKB_IPRODUCT,
+    eIProductWRTDerivBase = NKB_IPRODUCT_DERIV,
+    ePhysDeriv            = NKB_PHYSDERIV
 };
 enum ImplementationType
 {
@@ -297,6 +298,36 @@ private:
     B200OpHandle m_h;
 };
 
+// IProductWRTDerivBase: the vector field's three components in entry0..2,
+// the result in entry3 (IProductWRTDerivBase.cpp:285-318, coordim 3)
+class IProductWRTDerivBase_B200 : public Operator
+{
+public:
+    IProductWRTDerivBase_B200(const CollectionData &d, const FactorMap &)
+        : m_h(d, eIProductWRTDerivBase)
+    {
+        m_in    = m_h.m_in / 3; // per component, as GetInputSize reports it
+        m_out   = m_h.m_out;
+        m_nelmt = unsigned(d.nelmt);
+    }
+    void operator()(const Array1D &entry0, Array1D &entry1, Array1D &entry2, Array1D &entry3,
+                    Array1D &) override
+    {
+        if (entry0.size() < m_in || entry1.size() < m_in || entry2.size() < m_in ||
+            entry3.size() < m_out)
+            throw NekError(NKB_ERR_INVALID, "array smaller than the operator's size");
+        Check(nkb_op_apply3(m_h.get(), entry0.data(), entry1.data(), entry2.data(), entry3.data(),
+                            NKB_HOST_PTRS, nullptr));
+    }
+    void operator()(int, const Array1D &, Array1D &, Array1D &) override
+    {
+        throw NekError(NKB_ERR_INVALID, "Not valid for this operator.");
+    }
+
+private:
+    B200OpHandle m_h;
+};
+
 // Registration of eB200 next to eMatrixFree (the reference registers its
 // implementations the same way, e.g. Helmholtz.cpp:764-783)
 inline bool RegisterB200Operators()
@@ -322,6 +353,12 @@ inline bool RegisterB200Operators()
                 return std::make_shared<PhysDeriv_B200>(d, m);
             },
             "PhysDeriv_B200");
+        f.RegisterCreatorFunction(
+            OperatorKey(s, eIProductWRTDerivBase, eB200, false),
+            [](const CollectionData &d, const FactorMap &m) {
+                return std::make_shared<IProductWRTDerivBase_B200>(d, m);
+            },
+            "IProductWRTDerivBase_B200");
         f.RegisterCreatorFunction(
             OperatorKey(s, eHelmholtz, eB200, false),
             [](const CollectionData &d, const FactorMap &m) {

@@ -49,10 +49,10 @@ namespace
 double Cost(const nkb_op *op)
 {
     const double comps = op->ncomp > 0 ? op->ncomp : 1;
-    const double in    = (op->optype == NKB_BWDTRANS || op->optype == NKB_HELMHOLTZ) ? op->nc : op->nt;
-    const double out   = op->optype == NKB_PHYSDERIV ? 3.0 * op->nt
-                         : (op->optype == NKB_BWDTRANS ? op->nt : op->nc);
-    return double(op->nelmt) * (comps * op->nt + in + out);
+    long in = 0, out = 0;
+    nkb_op_sizes(op, &in, &out);
+    const double nouts = op->optype == NKB_PHYSDERIV ? 3.0 : 1.0;
+    return double(op->nelmt) * comps * op->nt + double(in) + nouts * double(out);
 }
 
 int LaunchAll(nkb_batch *B, const double *in, double *out, cudaStream_t s)
@@ -103,12 +103,12 @@ extern "C" int nkb_batch_create(nkb_op *const *ops, int nops, int nstreams, nkb_
     B->nout = ops[0]->optype == NKB_PHYSDERIV ? 3 : 1;
     for (nkb_op *op : B->ops)
     {
-        const bool coeff_in  = op->optype == NKB_BWDTRANS || op->optype == NKB_HELMHOLTZ;
-        const bool coeff_out = op->optype == NKB_IPRODUCT || op->optype == NKB_HELMHOLTZ;
+        long ni = 0, no = 0;
+        nkb_op_sizes(op, &ni, &no);
         B->in_off.push_back(B->in_size);
         B->out_off.push_back(B->out_size);
-        B->in_size += long(op->nelmt) * (coeff_in ? op->nc : op->nt);
-        B->out_size += long(op->nelmt) * (coeff_out ? op->nc : op->nt) * B->nout;
+        B->in_size += ni;
+        B->out_size += no * B->nout;
     }
     // largest first, each to the least-loaded stream
     B->order.resize(nops);

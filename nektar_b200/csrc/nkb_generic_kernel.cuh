@@ -18,6 +18,7 @@ enum
     GK_BWD  = 0,
     GK_HELM = 1,
     GK_IP   = 3,
+    GK_IPD  = 4,
     GK_PD   = 5,
     GK_DIAG = 9
 };
@@ -39,6 +40,7 @@ template <typename T> struct GenArgs
     const T *geo;
     T lambda;
     const T *in;
+    const T *in1, *in2; // IProductWRTDerivBase: the second and third input fields
     T *out0, *out1, *out2;
     // optional gather of the input from a global vector: in[e*nc+m] = sign * gvec[map]
     const int *gmap;
@@ -100,7 +102,7 @@ template <int SHAPE, int OP, typename T, class D = Dims> __global__ void k_gener
             })
         }
     }
-    else
+    else if (OP != GK_IPD)
     {
         NKB_STAGE(d.nt, { u[l] = a.in[e * d.nt + l]; })
     }
@@ -154,7 +156,23 @@ template <int SHAPE, int OP, typename T, class D = Dims> __global__ void k_gener
         NKB_STAGE(d.nt, { u[l] = wa[l] + GradT(d, a.t, g0, g1, g2, l); })
     }
 
-    if (OP == GK_HELM || OP == GK_IP)
+    if (OP == GK_IPD)
+    {
+        // v_x = sum_m W A[x*3+m] f_m (the packed rows already carry W), then
+        // sum_x D_x^T v_x; dB_x = D_x B_x turns the three inner products of
+        // IProductWRTDerivBase.h:789-825 into one with B.
+        NKB_STAGE(d.nt, {
+            const long o = e * d.nt + l;
+            const T f0 = a.in[o], f1 = a.in1[o], f2 = a.in2[o];
+            const T *P = a.geo + e * a.gstride + l;
+            g0[l] = fma(P[2 * d.nt], f2, fma(P[1 * d.nt], f1, P[0] * f0));
+            g1[l] = fma(P[5 * d.nt], f2, fma(P[4 * d.nt], f1, P[3 * d.nt] * f0));
+            g2[l] = fma(P[8 * d.nt], f2, fma(P[7 * d.nt], f1, P[6 * d.nt] * f0));
+        })
+        NKB_STAGE(d.nt, { u[l] = GradT(d, a.t, g0, g1, g2, l); })
+    }
+
+    if (OP == GK_HELM || OP == GK_IP || OP == GK_IPD)
     {
         NKB_STAGE(IP::SizeA(d), { IprStageA(d, a.t, u, wa, l); })
         NKB_STAGE(IP::SizeB(d), { IP::B(d, a.t, wa, wb, l); })

@@ -187,6 +187,12 @@ template <typename T> static int AutotuneGeneric(nkb_op *op)
             op->gen_threads = threads[ti];
             op->gen_epb     = epbs[ei];
             T *in = buf, *o0 = buf + nmax, *o1 = buf + 2 * nmax, *o2 = buf + 3 * nmax;
+            if (op->optype == NKB_IPRODUCT_DERIV)
+            {
+                // three input fields, one output
+                o0 = buf + 3 * nmax;
+                o1 = o2 = nullptr;
+            }
             if ((rc = LaunchGeneric<T>(op, in, o0, o1, o2, nullptr, nullptr, op->stream)))
                 break;
             cudaEventRecord(op->ev0, op->stream);

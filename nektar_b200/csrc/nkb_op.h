@@ -56,6 +56,12 @@ template <typename T>
 int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
                   const double *gsign, cudaStream_t s, const int *skip = nullptr,
                   const double *lambda = nullptr);
+// the same with IProductWRTDerivBase's three input fields as separate arrays
+// (the one-input form reads them consecutively from `in`)
+template <typename T>
+int LaunchGeneric3(const nkb_op *op, const T *in, const T *in1, const T *in2, T *o0, T *o1, T *o2,
+                   const int *gmap, const double *gsign, cudaStream_t s,
+                   const int *skip = nullptr, const double *lambda = nullptr);
 // dispatch: tuned kernel if selected, else generic (nkb_hex.cu)
 // skip: optional device flag; when it reads nonzero the kernels return at once
 // (a converged CG keeps its captured graph but stops doing work)

@@ -99,7 +99,7 @@ struct PackArgs
     double K[6];                  // d00 d01 d11 d02 d12 d22
     double *geo;                  // packed FP64
     float *geo32;                 // optional FP32 copy
-    int ncomp;                    // 7 Helmholtz, 9 PhysDeriv, 1 IProduct
+    int ncomp;                    // 7 Helmholtz, 9 PhysDeriv / IProductWRTDerivBase, 1 IProduct
     long gstride;                 // element stride of the packed arrays
 };
 
@@ -130,13 +130,16 @@ __global__ void k_pack(PackArgs a)
             f[d] = a.df[d * ncol + col];
         double A[9];
         ShapeRows(a.shape, f, a.z0[i], a.z1[j], a.z2[k], A);
-        if (a.optype == NKB_PHYSDERIV)
+        if (a.optype == NKB_PHYSDERIV || a.optype == NKB_IPRODUCT_DERIV)
         {
+            // IProductWRTDerivBase folds the quadrature weight into the rows
+            const double W = a.optype == NKB_IPRODUCT_DERIV ? J * a.w0[i] * a.w1[j] * a.w2[k] : 1.0;
             for (int c = 0; c < 9; ++c)
             {
-                out[c * nt] = A[c];
+                const double v = a.optype == NKB_IPRODUCT_DERIV ? W * A[c] : A[c];
+                out[c * nt]    = v;
                 if (out32)
-                    out32[c * nt] = float(A[c]);
+                    out32[c * nt] = float(v);
             }
             continue;
         }
@@ -409,12 +412,26 @@ template <typename T>
 int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
                   const double *gsign, cudaStream_t s, const int *skip, const double *lambda)
 {
+    // IProductWRTDerivBase through the one-input entry points: the three
+    // fields lie consecutively in `in`
+    const long field = long(op->nelmt) * op->nt;
+    return LaunchGeneric3<T>(op, in, in + field, in + 2 * field, o0, o1, o2, gmap, gsign, s, skip,
+                             lambda);
+}
+
+template <typename T>
+int LaunchGeneric3(const nkb_op *op, const T *in, const T *in1, const T *in2, T *o0, T *o1, T *o2,
+                   const int *gmap, const double *gsign, cudaStream_t s, const int *skip,
+                   const double *lambda)
+{
     GenArgs<T> a;
     a.d      = MakeDims(op);
     a.t      = MakeTabs<T>(op);
     a.geo    = std::is_same<T, double>::value ? (const T *)op->geo : (const T *)op->geo32;
     a.lambda = T(lambda ? *lambda : op->lambda);
     a.in     = in;
+    a.in1    = in1;
+    a.in2    = in2;
     a.out0   = o0;
     a.out1   = o1;
     a.out2   = o2;
@@ -432,6 +449,8 @@ int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int 
             return LaunchGenericShape<GK_IP, T>(op, a, s);
         case NKB_PHYSDERIV:
             return LaunchGenericShape<GK_PD, T>(op, a, s);
+        case NKB_IPRODUCT_DERIV:
+            return LaunchGenericShape<GK_IPD, T>(op, a, s);
         default:
         {
             if (ColKernels())
@@ -451,6 +470,12 @@ int LaunchGeneric(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int 
     }
 }
 
+template int LaunchGeneric3<double>(const nkb_op *, const double *, const double *,
+                                    const double *, double *, double *, double *, const int *,
+                                    const double *, cudaStream_t, const int *, const double *);
+template int LaunchGeneric3<float>(const nkb_op *, const float *, const float *, const float *,
+                                   float *, float *, float *, const int *, const double *,
+                                   cudaStream_t, const int *, const double *);
 template int LaunchGeneric<double>(const nkb_op *, const double *, double *, double *, double *,
                                    const int *, const double *, cudaStream_t, const int *,
                                    const double *);
@@ -536,7 +561,8 @@ extern "C" int nkb_op_create(const nkb_op_desc *desc, nkb_op **out)
     if (shape != NKB_HEX && shape != NKB_PRISM && shape != NKB_TET)
         return SetError(NKB_ERR_INVALID, "nkb_op_create: unsupported shape %d", shape);
     if (desc->optype != NKB_BWDTRANS && desc->optype != NKB_HELMHOLTZ &&
-        desc->optype != NKB_IPRODUCT && desc->optype != NKB_PHYSDERIV)
+        desc->optype != NKB_IPRODUCT && desc->optype != NKB_IPRODUCT_DERIV &&
+        desc->optype != NKB_PHYSDERIV)
         return SetError(NKB_ERR_INVALID, "nkb_op_create: unsupported operator %d", desc->optype);
     if (nm < 2 || nm > 16 || desc->nelmt < 0)
         return SetError(NKB_ERR_INVALID, "nkb_op_create: nm=%d nelmt=%d out of range", nm,
@@ -562,19 +588,20 @@ extern "C" int nkb_op_create(const nkb_op_desc *desc, nkb_op **out)
                             opt);
         return NKB_OK;
     };
+    const bool weighted = opt == NKB_IPRODUCT || opt == NKB_HELMHOLTZ || opt == NKB_IPRODUCT_DERIV;
+    const bool derived  = opt == NKB_PHYSDERIV || opt == NKB_HELMHOLTZ || opt == NKB_IPRODUCT_DERIV;
     for (int d = 0; d < 3; ++d)
     {
         if (opt != NKB_PHYSDERIV && need(desc->bdata[d], "bdata"))
             return NKB_ERR_INVALID;
-        if ((opt == NKB_IPRODUCT || opt == NKB_HELMHOLTZ) && need(desc->w[d], "w"))
+        if (weighted && need(desc->w[d], "w"))
             return NKB_ERR_INVALID;
-        if ((opt == NKB_PHYSDERIV || opt == NKB_HELMHOLTZ) &&
-            (need(desc->D[d], "D") || need(desc->z[d], "z")))
+        if (derived && (need(desc->D[d], "D") || need(desc->z[d], "z")))
             return NKB_ERR_INVALID;
     }
-    if ((opt == NKB_IPRODUCT || opt == NKB_HELMHOLTZ) && need(desc->jac, "jac"))
+    if (weighted && need(desc->jac, "jac"))
         return NKB_ERR_INVALID;
-    if ((opt == NKB_PHYSDERIV || opt == NKB_HELMHOLTZ) && need(desc->df, "df"))
+    if (derived && need(desc->df, "df"))
         return NKB_ERR_INVALID;
 
     int ndev = 0;
@@ -599,7 +626,9 @@ extern "C" int nkb_op_create(const nkb_op_desc *desc, nkb_op **out)
     }
     op->nc = NumCoeffs(shape, nm);
     op->nt = nq[0] * nq[1] * nq[2];
-    op->ncomp = (opt == NKB_HELMHOLTZ) ? 7 : (opt == NKB_PHYSDERIV ? 9 : (opt == NKB_IPRODUCT ? 1 : 0));
+    op->ncomp = (opt == NKB_HELMHOLTZ)                                    ? 7
+                : (opt == NKB_PHYSDERIV || opt == NKB_IPRODUCT_DERIV) ? 9
+                : (opt == NKB_IPRODUCT ? 1 : 0);
     // element blocks of the packed geometry start on 32-byte boundaries so a
     // bulk (TMA) copy of one element is legal in FP64 and FP32
     op->gstride = (long(op->ncomp) * op->nt + 3) & ~3L;
@@ -704,6 +733,8 @@ extern "C" int nkb_op_sizes(const nkb_op *op, long *in_size, long *out_size)
         out = nt;
     else if (op->optype == NKB_IPRODUCT)
         in = nt;
+    else if (op->optype == NKB_IPRODUCT_DERIV)
+        in = 3 * nt;
     else if (op->optype == NKB_PHYSDERIV)
         in = out = nt;
     if (in_size)
@@ -766,6 +797,49 @@ extern "C" int nkb_op_apply(nkb_op *op, const double *in, double *out0, double *
     }
     NKB_CUDA_TRY(cudaEventRecord(op->ev0, s));
     int rc = LaunchOp<double>(op, in, out0, out1, out2, nullptr, nullptr, s);
+    if (rc)
+        return rc;
+    NKB_CUDA_TRY(cudaEventRecord(op->ev1, s));
+    return NKB_OK;
+}
+
+extern "C" int nkb_op_apply3(nkb_op *op, const double *in0, const double *in1, const double *in2,
+                             double *out, int flags, void *stream)
+{
+    ClearError();
+    if (!op || !in0 || !in1 || !in2 || !out)
+        return SetError(NKB_ERR_INVALID, "nkb_op_apply3: NULL argument");
+    if (op->optype != NKB_IPRODUCT_DERIV)
+        return SetError(NKB_ERR_INVALID, "nkb_op_apply3: operator %d takes one input array",
+                        op->optype);
+    if (op->precision != NKB_FP64)
+        return SetError(NKB_ERR_INVALID, "nkb_op_apply3: needs an FP64 operator");
+    NKB_CUDA_TRY(cudaSetDevice(op->device));
+    cudaStream_t s    = static_cast<cudaStream_t>(stream); // NULL: legacy default stream
+    const long field  = long(op->nelmt) * op->nt;
+    const long nout   = long(op->nelmt) * op->nc;
+    if (flags & NKB_HOST_PTRS)
+    {
+        int rc = EnsureScratch(op, size_t(3 * field + nout) * sizeof(double));
+        if (rc)
+            return rc;
+        double *din         = static_cast<double *>(op->scratch);
+        double *dout        = din + 3 * field;
+        const double *hin[3] = {in0, in1, in2};
+        for (int f = 0; f < 3; ++f)
+            NKB_CUDA_TRY(cudaMemcpyAsync(din + f * field, hin[f], field * sizeof(double),
+                                         cudaMemcpyHostToDevice, s));
+        NKB_CUDA_TRY(cudaEventRecord(op->ev0, s));
+        rc = LaunchGeneric<double>(op, din, dout, nullptr, nullptr, nullptr, nullptr, s);
+        if (rc)
+            return rc;
+        NKB_CUDA_TRY(cudaEventRecord(op->ev1, s));
+        NKB_CUDA_TRY(cudaMemcpyAsync(out, dout, nout * sizeof(double), cudaMemcpyDeviceToHost, s));
+        NKB_CUDA_TRY(cudaStreamSynchronize(s));
+        return NKB_OK;
+    }
+    NKB_CUDA_TRY(cudaEventRecord(op->ev0, s));
+    int rc = LaunchGeneric3<double>(op, in0, in1, in2, out, nullptr, nullptr, nullptr, nullptr, s);
     if (rc)
         return rc;
     NKB_CUDA_TRY(cudaEventRecord(op->ev1, s));

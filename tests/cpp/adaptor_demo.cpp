@@ -1,6 +1,7 @@
 // Drives the C++ Collections mirror (nektar_b200/adaptor/nkb_collections.hpp)
 // the way a Nektar++ Collection would: factory lookup by OperatorKey with the
-// eB200 implementation type, Helmholtz apply with UpdateFactors, then the
+// eB200 implementation type, Helmholtz apply with UpdateFactors, an
+// IProductWRTDerivBase apply with three input fields, then the
 // GlobalLinSysIterativeFull solve. Prints one JSON line. Exit codes: 0 ok,
 // 3 NekError raised (e.g. no CUDA device), 1 other failure.
 #include "../../nektar_b200/adaptor/nkb_collections.hpp"
@@ -71,13 +72,28 @@ int main()
         {
             threw = true; // "Not valid for this operator." as Helmholtz.cpp:604-610
         }
+        // IProductWRTDerivBase: three field components in, coefficients out
+        auto ipd = GetOperatorFactory().CreateInstance(
+            OperatorKey(eHexahedron, eIProductWRTDerivBase, eB200, false), d, f);
+        Array1D f0(ipd->GetInputSize()), f1(f0.size()), f2(f0.size()), g(ipd->GetOutputSize());
+        for (size_t i = 0; i < f0.size(); ++i)
+        {
+            f0[i] = std::cos(0.11 * double(i));
+            f1[i] = std::cos(0.11 * double(i) + 1.0);
+            f2[i] = std::cos(0.11 * double(i) + 2.0);
+        }
+        (*ipd)(f0, f1, f2, g, wsp);
+        double ng = 0.0;
+        for (double v : g)
+            ng += v * v;
         auto helm = std::dynamic_pointer_cast<Helmholtz_B200>(op);
         GlobalLinSysIterativeFullB200 sys({helm}, map, nglob, ndir);
         Array1D b(x), sol(x.size(), 0.0);
         nkb_cg_report r = sys.Solve(b, sol, 1e-10);
-        std::printf("{\"helmholtz_norm2\": %.17g, \"dir_call_threw\": %d, \"cg_iterations\": %d, "
+        std::printf("{\"helmholtz_norm2\": %.17g, \"iproduct_deriv_norm2\": %.17g, "
+                    "\"dir_call_threw\": %d, \"cg_iterations\": %d, "
                     "\"cg_rel_residual\": %.6g, \"nelmt\": %d}\n",
-                    ny, int(threw), r.iterations, r.rel_residual, d.nelmt);
+                    ny, ng, int(threw), r.iterations, r.rel_residual, d.nelmt);
         return 0;
     }
     catch (const NekError &e)

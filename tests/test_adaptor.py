@@ -45,5 +45,10 @@ def test_adaptor_matches_c_abi(tmp_path):
     x = np.sin(0.37 * np.arange(op.in_size))
     ny = float(np.sum(op(x) ** 2))
     assert abs(out["helmholtz_norm2"] - ny) <= 1e-12 * ny
+    ipd = nb.Operator("iproduct_deriv", m)
+    i = np.arange(ipd.in_size // 3)
+    g = ipd.apply3(np.cos(0.11 * i), np.cos(0.11 * i + 1.0), np.cos(0.11 * i + 2.0))
+    ng = float(np.sum(g ** 2))
+    assert abs(out["iproduct_deriv_norm2"] - ng) <= 1e-12 * ng
     assert out["dir_call_threw"] == 1
     assert out["cg_rel_residual"] < 1e-10 and out["cg_iterations"] > 0

@@ -45,7 +45,7 @@ def _desc(**kw):
 
 @pytest.mark.parametrize("kw,msg", [
     ({"shape": 3}, "unsupported shape"),
-    ({"optype": 4}, "unsupported operator"),
+    ({"optype": 6}, "unsupported operator"),  # ePhysInterp1DScaled
     ({"nq": (ctypes.c_int * 3)(4, 4, 5)}, "not homogeneous"),
     ({"precision": 7}, "precision"),
     ({"nm": 1}, "out of range"),

@@ -28,6 +28,7 @@ def test_ops_match_reference_golden(path):
     assert rel_l2(_op("iproduct", g)(g["f"]), g["out_iproduct"]) < TOL64
     d = _op("physderiv", g)(g["f"])
     assert rel_l2(np.stack(d), g["out_physderiv"]) < TOL64
+    assert rel_l2(_op("iproduct_deriv", g)(g["f3"]), g["out_iproduct_deriv"]) < TOL64
     op = _op("helmholtz", g)
     op.set_factors(float(g["lam"]))
     assert rel_l2(op(g["x"]), g["out_helmholtz"]) < TOL64
@@ -71,6 +72,9 @@ def test_ops_match_oracle(shape, n, nm, amp):
     op.set_factors(1.0)
     yo = O.helmholtz(shape, nm, m.nq, m.nelmt, To, m.jac, m.df, x, 1.0, dfm)
     assert rel_l2(op(x), yo) < TOL64
+    f3 = rng.uniform(-1, 1, 3 * m.nelmt * m.nt)
+    yo = O.iproduct_deriv(shape, nm, m.nq, m.nelmt, To, m.jac, m.df, f3, dfm)
+    assert rel_l2(nb.Operator("iproduct_deriv", m)(f3), yo) < TOL64
 
 
 @pytest.mark.parametrize("shape", ["hex", "prism", "tet"])
@@ -196,3 +200,55 @@ def test_column_kernel_gathered_in_cg(monkeypatch, shape):
     xb, rb = S2.solve(b, tol=1e-12)
     assert ra.converged and rb.converged
     assert rel_l2(xa, xb) < 1e-10
+
+
+@pytest.mark.parametrize("shape,nm", [("hex", 7), ("prism", 6), ("tet", 9)])
+def test_iproduct_deriv_three_array_forms_agree(shape, nm):
+    """nkb_op_apply3 (three host arrays, three device arrays) and
+    nkb_op_apply (one array holding the three fields) give one result."""
+    import torch
+    m = nb.BoxMesh(shape, 3, nm, nm + 1, amp=0.05)
+    op = nb.Operator("iproduct_deriv", m)
+    rng = np.random.default_rng(nm)
+    f = rng.uniform(-1, 1, 3 * m.nelmt * m.nt)
+    n = m.nelmt * m.nt
+    y = op(f)
+    assert np.array_equal(op.apply3(f[:n], f[n:2 * n], f[2 * n:]), y)
+    fd = [torch.tensor(f[k * n:(k + 1) * n], device="cuda") for k in (2, 0, 1)]
+    yd = torch.empty(op.out_size, dtype=torch.float64, device="cuda")
+    op.apply3_device(fd[1].data_ptr(), fd[2].data_ptr(), fd[0].data_ptr(), yd.data_ptr(),
+                     stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(yd.cpu().numpy(), y)
+    with pytest.raises(nb.NektarB200Error):
+        nb.Operator("helmholtz", m).apply3_device(fd[0].data_ptr(), fd[1].data_ptr(),
+                                                  fd[2].data_ptr(), yd.data_ptr())
+
+
+@pytest.mark.parametrize("shape", ["hex", "prism", "tet"])
+def test_fp32_iproduct_deriv_matches_oracle(shape):
+    import torch
+    m = nb.BoxMesh(shape, 3, 6, 7, amp=0.05)
+    f = np.random.default_rng(9).uniform(-1, 1, 3 * m.nelmt * m.nt)
+    yo = O.iproduct_deriv(shape, m.nm, m.nq, m.nelmt, _oracle_T(m), m.jac, m.df, f, True)
+    op = nb.Operator("iproduct_deriv", m, precision="fp32")
+    fd = torch.tensor(f, dtype=torch.float32, device="cuda")
+    yd = torch.empty(op.out_size, dtype=torch.float32, device="cuda")
+    op.apply_device(fd.data_ptr(), yd.data_ptr(), stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rel_l2(yd.double().cpu().numpy(), yo) < TOL32
+
+
+@pytest.mark.parametrize("shape,n,nm", [("hex", 12, 7), ("prism", 8, 6), ("tet", 6, 6)])
+def test_iproduct_deriv_of_gradient_is_laplacian(shape, n, nm):
+    """Size-independent identity at larger sizes: the weak Laplacian of
+    Helmholtz with lambda = 0 equals IProductWRTDerivBase applied to
+    PhysDeriv(BwdTrans(x)) (same quadrature, same metric terms)."""
+    m = nb.BoxMesh(shape, n, nm, nm + 1, amp=0.05)
+    x = np.random.default_rng(n).uniform(-1, 1, m.nelmt * m.nc)
+    u = nb.Operator("bwdtrans", m)(x)
+    grad = nb.Operator("physderiv", m)(u)
+    y = nb.Operator("iproduct_deriv", m)(np.concatenate(grad))
+    lap = nb.Operator("helmholtz", m)
+    lap.set_factors(0.0)
+    assert rel_l2(y, lap(x)) < 1e-12
