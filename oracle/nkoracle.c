@@ -781,6 +781,115 @@ void or_helmholtz(int shape, int deformed, int nm, const int *nq, int nelmt,
 }
 
 /* ------------------------------------------------------------------ */
+/* LinearAdvectionDiffusionReaction                                    */
+/* ------------------------------------------------------------------ */
+
+/* LinearAdvectionDiffusionReactionKernels.hpp Advection{Hex,Tet,Prism}Kernel
+ * (:194-278, :280-382, :384-470): bwd += V' . grad_x u from the collocation
+ * derivatives d0..d2, V' per point (vel: three fields, field stride fld) */
+static void advection(int shape, int deformed, const int *nq, const double *const *Z,
+                      const double *df, size_t ncol, size_t col0, const double *vel, size_t fld,
+                      size_t off, const double *d0, const double *d1, const double *d2,
+                      double *bwd)
+{
+    const int nq0 = nq[0], nq1 = nq[1], nq2 = nq[2];
+    double f[9];
+    if (!deformed)
+        for (int d = 0; d < 9; ++d)
+            f[d] = df[d * ncol + col0];
+    for (int k = 0, c = 0; k < nq2; ++k)
+    {
+        const double z2f = 2.0 / (1.0 - Z[2][k]); /* tet h3, prism h1 */
+        for (int j = 0; j < nq1; ++j)
+        {
+            const double h1 = 0.5 * (1.0 + Z[1][j]), h2 = 2.0 / (1.0 - Z[1][j]);
+            for (int i = 0; i < nq0; ++i, ++c)
+            {
+                if (deformed)
+                    for (int d = 0; d < 9; ++d)
+                        f[d] = df[d * ncol + col0 + c];
+                const double h0 = 0.5 * (1.0 + Z[0][i]);
+                double m0 = d0[c], m1 = d1[c], m2 = d2[c];
+                if (shape == TET)
+                {
+                    const double h2h3 = h2 * z2f, h1h3 = h1 * z2f;
+                    m0 = h2h3 * d0[c];
+                    m1 = m0 * h0;
+                    m2 = m1 + d2[c];
+                    m2 = fma(h1h3, d1[c], m2);
+                    m1 = fma(z2f, d1[c], m1);
+                }
+                else if (shape == PRISM)
+                {
+                    m0 = z2f * d0[c];
+                    m2 = h0 * m0 + d2[c];
+                }
+                const double vx = vel[off + c], vy = vel[fld + off + c],
+                             vz = vel[2 * fld + off + c];
+                double t = f[0] * m0;
+                t = fma(f[1], m1, t);
+                t = fma(f[2], m2, t);
+                t = t * vx;
+                double t2 = f[3] * m0;
+                t2 = fma(f[4], m1, t2);
+                t2 = fma(f[5], m2, t2);
+                t = fma(t2, vy, t);
+                t2 = f[6] * m0;
+                t2 = fma(f[7], m1, t2);
+                t2 = fma(f[8], m2, t2);
+                t = fma(t2, vz, t);
+                bwd[c] = bwd[c] + t;
+            }
+        }
+    }
+}
+
+/* LinearAdvectionDiffusionReaction_MatrixFree (Collections
+ * LinearAdvectionDiffusionReaction.cpp:578-723) over the MatrixFree
+ * fusedKernel3D (LinearAdvectionDiffusionReaction.h:608-670). lambda and vel
+ * are the Collections-level eFactorLambda and eVarCoeffVel{X,Y,Z} (three
+ * fields of nelmt*nt values); the operator applies lambda' = -lambda and
+ * V' = (-1/lambda) V:
+ *   out = lambda' (phi, u + V'.grad u) + (grad phi, grad u). */
+void or_linear_adr(int shape, int deformed, int nm, const int *nq, int nelmt,
+                   const double *const *B, const double *const *dB, const double *const *w,
+                   const double *const *D, const double *const *Z, const double *jac,
+                   const double *df, double lambda, const double *vel, const double *in,
+                   double *out)
+{
+    const int nc = or_ncoeffs(shape, nm), nt = nq[0] * nq[1] * nq[2];
+    const size_t ncol = deformed ? (size_t)nelmt * nt : (size_t)nelmt;
+    const size_t fld  = (size_t)nelmt * nt;
+    const double lam  = -1 * lambda, s = -1 / lambda;
+    double *vs  = malloc(sizeof(double) * 3 * fld);
+    double *buf = malloc(sizeof(double) * (6 * (size_t)nt + 2 * wsp_size(nm, nq)));
+    double *bwd = buf, *d0 = buf + nt, *d1 = buf + 2 * nt, *d2 = buf + 3 * nt;
+    double *w0 = buf + 4 * nt, *w1 = w0 + wsp_size(nm, nq);
+    for (size_t i = 0; i < 3 * fld; ++i)
+        vs[i] = s * vel[i];
+    const double *T0[3] = {dB[0], B[1], B[2]};
+    const double *T1[3] = {B[0], dB[1], B[2]};
+    const double *T2[3] = {B[0], B[1], dB[2]};
+    for (int e = 0; e < nelmt; ++e)
+    {
+        const size_t off  = (size_t)e * nt;
+        const size_t col0 = deformed ? off : (size_t)e;
+        const double *je  = deformed ? jac + off : jac + e;
+        double *oe        = out + (size_t)e * nc;
+        bwd_elem(shape, nm, nq, B, in + (size_t)e * nc, bwd, w0, w1);
+        deriv_tensor(nq, D, bwd, d0, d1, d2);
+        advection(shape, deformed, nq, Z, df, ncol, col0, vs, fld, off, d0, d1, d2, bwd);
+        ip_elem(shape, nm, nq, B, w, je, deformed, bwd, oe, 1, 0, lam, w0, w1);
+        diffusion_coeff(shape, deformed, nq, Z, df, ncol, col0, 0, NULL, d0, d1, d2);
+        ip_elem(shape, nm, nq, T0, w, je, deformed, d0, oe, 0, 1, 1.0, w0, w1);
+        ip_elem(shape, nm, nq, T1, w, je, deformed, d1, oe, 0, 1, 1.0, w0, w1);
+        ip_elem(shape, nm, nq, T2, w, je, deformed, d2, oe, 0, 1, 1.0, w0, w1);
+    }
+    free(buf);
+    free(vs);
+}
+
+/* ------------------------------------------------------------------ */
 /* IProductWRTDerivBase                                                */
 /* ------------------------------------------------------------------ */
 

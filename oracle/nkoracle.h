@@ -38,6 +38,14 @@ void or_physderiv(int shape, int deformed, const int *nq, int nelmt, const doubl
  * diff_mode 0 = identity, 1 = constant anisotropic (SetConstVarDiffusion),
  * 2 = per-point variable diffusion filled with the same 6 values
  * (SetVarDiffusion as Collections::Helmholtz_MatrixFree drives it). */
+/* LinearAdvectionDiffusionReaction (LinearAdvectionDiffusionReaction.cpp:578-723,
+ * LinearAdvectionDiffusionReaction.h:608-670): lambda and vel (three fields of
+ * nelmt*nt values) as the Collections operator receives them */
+void or_linear_adr(int shape, int deformed, int nm, const int *nq, int nelmt,
+                   const double *const *B, const double *const *dB, const double *const *w,
+                   const double *const *D, const double *const *Z, const double *jac,
+                   const double *df, double lambda, const double *vel, const double *in,
+                   double *out);
 /* IProductWRTDerivBase (IProductWRTDerivBase.h:592-825): in holds the three
  * physical fields consecutively (field f of element e at in + f*nelmt*nt + e*nt) */
 void or_iproduct_deriv(int shape, int deformed, int nm, const int *nq, int nelmt,

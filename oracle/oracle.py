@@ -35,6 +35,7 @@ def lib():
         L.or_iproduct.restype = None
         L.or_physderiv.restype = None
         L.or_iproduct_deriv.restype = None
+        L.or_linear_adr.restype = None
         L.or_helmholtz.restype = None
         L.or_pcg.restype = ctypes.c_int
         _lib = L
@@ -80,6 +81,22 @@ def physderiv(shape, nq, nelmt, D, Z, df, f, deformed):
                        _p(np.ascontiguousarray(df)), _p(np.ascontiguousarray(f)), _p(o0), _p(o1),
                        _p(o2))
     return o0, o1, o2
+
+
+def linear_adr(shape, nm, nq, nelmt, T, jac, df, lam, vel, x, deformed):
+    """vel: the three velocity fields consecutively (3 * nelmt * nt values),
+    lam the Collections-level lambda (the operator applies -lam)."""
+    kb, Bp = _arr3(T["b"])
+    kdb, dBp = _arr3(T["db"])
+    kw, Wp = _arr3(T["w"])
+    kd, Dp = _arr3(T["D"])
+    kz, Zp = _arr3(T["z"])
+    out = np.zeros(nelmt * ncoeffs(shape, nm))
+    lib().or_linear_adr(SHAPES[shape], int(deformed), nm, (ctypes.c_int * 3)(*nq), nelmt, Bp, dBp,
+                        Wp, Dp, Zp, _p(np.ascontiguousarray(jac)), _p(np.ascontiguousarray(df)),
+                        ctypes.c_double(lam), _p(np.ascontiguousarray(vel)),
+                        _p(np.ascontiguousarray(x)), _p(out))
+    return out
 
 
 def iproduct_deriv(shape, nm, nq, nelmt, T, jac, df, f, deformed):

@@ -15,7 +15,8 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 # numbering as LibUtilities::ShapeType / Collections::OperatorType / PointsType / BasisType
 SHAPES = {"tet": 5, "prism": 7, "hex": 8}
-OPS = {"bwdtrans": 0, "helmholtz": 1, "iproduct": 3, "iproduct_deriv": 4, "physderiv": 5}
+OPS = {"bwdtrans": 0, "helmholtz": 1, "linear_adr": 2, "iproduct": 3, "iproduct_deriv": 4,
+       "physderiv": 5}
 GLL, RADAU_A1, RADAU_A2 = 4, 11, 12
 MOD_A, MOD_B, MOD_C = 4, 5, 6
 
@@ -69,6 +70,9 @@ def lib(isa=None):
         f = getattr(L, "nkref_%s_set_factors" % s)
         f.restype = None
         f.argtypes = [vp, ctypes.c_double, ctypes.c_int, dp, ctypes.c_int]
+        f = getattr(L, "nkref_%s_set_adr" % s)
+        f.restype = None
+        f.argtypes = [vp, ctypes.c_double, dp]
         f = getattr(L, "nkref_%s_apply" % s)
         f.restype = None
         f.argtypes = [vp, dp, dp, dp, dp]
@@ -164,6 +168,12 @@ class RefOp:
             d[:] = var_diff
             isv = 1
         getattr(self.L, "nkref_%s_set_factors" % self.shape)(self.h, float(lam), isc, _dp(d), isv)
+
+    def set_adr(self, lam, vel):
+        """LinearADR factors as the Collections operator takes them: lambda
+        and the three velocity fields (3 * nelmt * nt values)."""
+        self._vel = np.ascontiguousarray(vel, dtype=np.float64)
+        getattr(self.L, "nkref_%s_set_adr" % self.shape)(self.h, float(lam), _dp(self._vel))
 
     def apply(self, x, out0, out1=None, out2=None):
         self._apply(self.h, _dp(x), _dp(out0), None if out1 is None else _dp(out1),

@@ -16,14 +16,19 @@
 //      BwdTrans.h:364-420 (operator3D), IProduct.h:410-491 (operator3D),
 //      PhysDeriv.h:478-571 (operator3D), Helmholtz.h:374-464 (operator3D) and
 //      the fused body Helmholtz.h:549-599 (fusedKernel3D),
-//      IProductWRTDerivBase.h:592-694 (operator3D) and :789-825 (fusedKernel3D);
+//      IProductWRTDerivBase.h:592-694 (operator3D) and :789-825 (fusedKernel3D),
+//      LinearAdvectionDiffusionReaction.h:423-606 (operator3D) and :608-670
+//      (fusedKernel3D);
 //  * the geometry interleave of CoalescedGeomData.cpp:90-159 (GetJacInterLeave)
 //    and :265-342 (GetDerivFactorsInterLeave);
 //  * the vec_t broadcast of the 1-D tables, Operator.hpp:529-641 (SetUpBdata,
 //    SetUpDBdata, SetUpZW, SetUpD). Radau weight scaling is applied by the
 //    caller, which passes already-scaled weights;
 //  * the Helmholtz factor plumbing of Operator.hpp (SetLambda,
-//    SetConstVarDiffusion, SetVarDiffusion) for one collection.
+//    SetConstVarDiffusion, SetVarDiffusion) for one collection;
+//  * the LinearADR factor plumbing of the Collections operator
+//    (LinearAdvectionDiffusionReaction.cpp:578-723: SetLambda(-lambda), the
+//    velocities scaled by -1/lambda and interleaved per block).
 // The element range is split into per-thread collections (one std::thread
 // each), which mirrors MPI ranks each owning a sub-mesh.
 
@@ -70,6 +75,7 @@ template <class Dim, class T> struct Array
 #include <MatrixFreeOps/HelmholtzKernels.hpp>
 #include <MatrixFreeOps/IProductKernels.hpp>
 #include <MatrixFreeOps/IProductWRTDerivBaseKernels.hpp>
+#include <MatrixFreeOps/LinearAdvectionDiffusionReactionKernels.hpp>
 #include <MatrixFreeOps/PhysDerivKernels.hpp>
 
 #ifndef NKREF_SHAPE
@@ -99,6 +105,7 @@ enum
 {
     OP_BWDTRANS  = 0,
     OP_HELMHOLTZ = 1,
+    OP_LINEAR_ADR = 2,
     OP_IPRODUCT  = 3,
     OP_IPRODUCT_DERIV = 4,
     OP_PHYSDERIV = 5
@@ -151,6 +158,7 @@ struct Chunk
     int e0 = 0, ne = 0; // element range of this per-thread collection
     int nBlocks = 0, nPads = 0;
     VecV jac, df; // interleaved geometry
+    VecV advVel;  // LinearADR: interleaved velocities [block][point][dir]
 };
 
 struct RefOp
@@ -434,6 +442,82 @@ template <bool DEFORMED> void ApplyHelmholtz(const RefOp &o, const Chunk &c, con
     }
 }
 
+// LinearAdvectionDiffusionReaction.h fusedKernel3D (:608-670): BwdTrans, the
+// collocation derivatives, bwd += V'.grad u, a lambda'-scaled inner product,
+// then the Laplacian terms as in Helmholtz (no diffusion tensor is set by the
+// Collections operator).
+template <bool DEFORMED> void ApplyLinearADR(const RefOp &o, const Chunk &c, const double *in, double *out)
+{
+    const int nm = o.nm, nq0 = o.nq[0], nq1 = o.nq[1], nq2 = o.nq[2];
+    const int W  = vec_t::width;
+    constexpr int ndf = 9;
+    std::size_t wsp0Size = 0, wsp1Size = 0, wsp2Size = 0;
+    BwdTrans3DWorkspace<kShape>(nm, nm, nm, nq0, nq1, nq2, wsp0Size, wsp1Size);
+    IProduct3DWorkspace<kShape>(nm, nm, nm, nq0, nq1, nq2, wsp0Size, wsp1Size, wsp2Size);
+    VecV wsp0(wsp0Size), wsp1(wsp1Size), wsp2(std::max<std::size_t>(wsp2Size, nm));
+    VecV tmpIn(o.nmTot), tmpOut(o.nmTot), bwd(o.nqTot), deriv0(o.nqTot), deriv1(o.nqTot),
+        deriv2(o.nqTot);
+    std::vector<double> loc(std::size_t(o.nmTot) * W, 0.0);
+    Array<OneD, NekDouble> cvd(const_cast<double *>(o.constVarDiff.data()), 6);
+    Array<OneD, NekDouble> vd[6];
+    for (int i = 0; i < 6; ++i)
+    {
+        vd[i] = Array<OneD, NekDouble>(const_cast<double *>(o.varD[i].data()), o.varD[i].size());
+    }
+    const double *inptr     = in + std::size_t(c.e0) * o.nmTot;
+    double *outptr          = out + std::size_t(c.e0) * o.nmTot;
+    const vec_t *jac_ptr    = c.jac.data();
+    const vec_t *df_ptr     = c.df.data();
+    const vec_t *advVel_ptr = c.advVel.data();
+    for (int b = 0; b < c.nBlocks; ++b)
+    {
+        int nreal     = std::min(W, c.ne - b * W);
+        std::size_t n = std::size_t(nreal) * o.nmTot;
+        std::fill(loc.begin(), loc.end(), 0.0);
+        std::copy(inptr, inptr + n, loc.data());
+        load_unalign_interleave(loc.data(), o.nmTot, tmpIn);
+        BwdTrans3DKernel<kShape>(nm, nm, nm, nq0, nq1, nq2, true, tmpIn, o.bdata[0], o.bdata[1],
+                                 o.bdata[2], wsp0, wsp1, bwd);
+        PhysDerivTensor3DKernel(nq0, nq1, nq2, bwd, o.D[0], o.D[1], o.D[2], deriv0, deriv1, deriv2);
+        Advection3DKernel<kShape, DEFORMED>(nq0, nq1, nq2, advVel_ptr, df_ptr, o.h0, o.h1, o.h2,
+                                            o.h3, deriv0, deriv1, deriv2, bwd);
+        IProduct3DKernel<kShape, true, false, DEFORMED>(nm, nm, nm, nq0, nq1, nq2, true, bwd,
+                                                        o.bdata[0], o.bdata[1], o.bdata[2], o.w[0],
+                                                        o.w[1], o.w[2], jac_ptr, wsp0, wsp1, wsp2,
+                                                        tmpOut, o.lambda);
+        DiffusionCoeff3DKernel<kShape, DEFORMED>(nq0, nq1, nq2, o.isConstVarDiff, cvd, o.isVarDiff,
+                                                 vd[0], vd[1], vd[2], vd[3], vd[4], vd[5], df_ptr,
+                                                 o.h0, o.h1, o.h2, o.h3, deriv0, deriv1, deriv2);
+        IProduct3DKernel<kShape, false, true, DEFORMED>(nm, nm, nm, nq0, nq1, nq2, true, deriv0,
+                                                        o.dbdata[0], o.bdata[1], o.bdata[2],
+                                                        o.w[0], o.w[1], o.w[2], jac_ptr, wsp0,
+                                                        wsp1, wsp2, tmpOut);
+        IProduct3DKernel<kShape, false, true, DEFORMED>(nm, nm, nm, nq0, nq1, nq2, true, deriv1,
+                                                        o.bdata[0], o.dbdata[1], o.bdata[2],
+                                                        o.w[0], o.w[1], o.w[2], jac_ptr, wsp0,
+                                                        wsp1, wsp2, tmpOut);
+        IProduct3DKernel<kShape, false, true, DEFORMED>(nm, nm, nm, nq0, nq1, nq2, true, deriv2,
+                                                        o.bdata[0], o.bdata[1], o.dbdata[2],
+                                                        o.w[0], o.w[1], o.w[2], jac_ptr, wsp0,
+                                                        wsp1, wsp2, tmpOut);
+        deinterleave_unalign_store(tmpOut, o.nmTot, loc.data());
+        std::copy(loc.data(), loc.data() + n, outptr);
+        inptr += std::size_t(W) * o.nmTot;
+        outptr += std::size_t(W) * o.nmTot;
+        advVel_ptr += std::size_t(3) * o.nqTot;
+        if (DEFORMED)
+        {
+            jac_ptr += o.nqTot;
+            df_ptr += std::size_t(ndf) * o.nqTot;
+        }
+        else
+        {
+            ++jac_ptr;
+            df_ptr += ndf;
+        }
+    }
+}
+
 // IProductWRTDerivBase.h fusedKernel3D (:789-825): the physical vector field
 // to reference directions (IProductWRTDerivBase3DKernel, with the collapsed
 // factors of Prism/Tet), then three inner products, each with the basis
@@ -523,6 +607,9 @@ void ApplyChunk(const RefOp &o, const Chunk &c, const double *in, double *o0, do
             o.deformed ? ApplyIProductDeriv<true>(o, c, in, o0)
                        : ApplyIProductDeriv<false>(o, c, in, o0);
             break;
+        case OP_LINEAR_ADR:
+            o.deformed ? ApplyLinearADR<true>(o, c, in, o0) : ApplyLinearADR<false>(o, c, in, o0);
+            break;
     }
 }
 
@@ -594,6 +681,13 @@ extern "C"
             GetHelmholtz3DHalfSpace<kShape>(nq[0], nq[1], nq[2], z0, z1, z2, o->h0, o->h1, o->h2,
                                             o->h3);
         }
+        if (op == OP_LINEAR_ADR)
+        {
+            Array<OneD, const NekDouble> z0(o->z[0].data(), nq[0]), z1(o->z[1].data(), nq[1]),
+                z2(o->z[2].data(), nq[2]);
+            GetLinearAdvectionDiffusionReaction3DHalfSpace<kShape>(nq[0], nq[1], nq[2], z0, z1, z2,
+                                                                   o->h0, o->h1, o->h2, o->h3);
+        }
 #endif
         for (int i = 0; i < 6; ++i)
         {
@@ -624,6 +718,10 @@ extern "C"
             {
                 InterleaveDF(*o, df, c);
             }
+            if (op == OP_LINEAR_ADR)
+            {
+                c.advVel.assign(std::size_t(c.nBlocks) * o->nqTot * 3, vec_t(0.0));
+            }
         }
         return o;
     }
@@ -653,6 +751,42 @@ extern "C"
             for (int i = 0; i < 6; ++i)
             {
                 std::fill(o->varD[i].begin(), o->varD[i].end(), diff[i]);
+            }
+        }
+    }
+
+    // LinearAdvectionDiffusionReaction_MatrixFree::UpdateFactors then
+    // ::UpdateVarcoeffs (LinearAdvectionDiffusionReaction.cpp:578-723):
+    // lambda' = -lambda; the velocities (vel: three fields of nelmt*nqTot
+    // values) scaled by -1/lambda and interleaved as [block][point][dir].
+    void NKREF_FN(_set_adr)(void *h, double lambda, const double *vel)
+    {
+        RefOp *o  = static_cast<RefOp *>(h);
+        o->lambda = -1 * lambda;
+        const double s         = -1 / lambda;
+        const std::size_t fld  = std::size_t(o->nelmt) * o->nqTot;
+        const int W            = vec_t::width;
+        alignas(vec_t::alignment) double tmp[vec_t::width];
+        for (Chunk &c : o->chunks)
+        {
+            c.advVel.resize(std::size_t(c.nBlocks) * o->nqTot * 3);
+            std::size_t cnt = 0;
+            for (int b = 0; b < c.nBlocks; ++b)
+            {
+                for (int q = 0; q < o->nqTot; ++q)
+                {
+                    for (int dir = 0; dir < 3; ++dir, ++cnt)
+                    {
+                        for (int j = 0; j < W; ++j)
+                        {
+                            const int e = b * W + j;
+                            tmp[j]      = (e < c.ne)
+                                              ? s * vel[dir * fld + std::size_t(c.e0 + e) * o->nqTot + q]
+                                              : 0.0;
+                        }
+                        c.advVel[cnt].load(tmp);
+                    }
+                }
             }
         }
     }

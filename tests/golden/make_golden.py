@@ -59,6 +59,7 @@ def make_case(shape, nm, nq0, deformed, seed, ne=3):
     x_rand = rng.uniform(-1.0, 1.0, ne * nc)
     f = rng.uniform(-1.0, 1.0, ne * nt)
     f3 = rng.uniform(-1.0, 1.0, 3 * ne * nt)  # a vector field for IProductWRTDerivBase
+    vel = rng.uniform(-1.0, 1.0, 3 * ne * nt)  # advection velocity for LinearADR
     # the harness takes weights already scaled as MatrixFree SetUpZW scales them
     T = dict(T)
     T["w_raw"], T["w"] = T["w"], T["ws"]
@@ -79,6 +80,11 @@ def make_case(shape, nm, nq0, deformed, seed, ne=3):
     y = np.zeros(ne * nc)
     op.apply(f3, y)
     out["iproduct_deriv"] = y
+    op = ref.RefOp(shape, "linear_adr", nm, nq, ne, T, jac=jac, df=df, deformed=deformed)
+    op.set_adr(1.5, vel)
+    y = np.zeros(ne * nc)
+    op.apply(x, y)
+    out["linear_adr"] = y
     diff = np.array([1.3, 0.2, 0.9, 0.1, -0.3, 1.1])
     for mode, tag in ((0, "helmholtz"), (1, "helmholtz_constdiff"), (2, "helmholtz_vardiff")):
         op = ref.RefOp(shape, "helmholtz", nm, nq, ne, T, jac=jac, df=df, deformed=deformed)
@@ -89,7 +95,7 @@ def make_case(shape, nm, nq0, deformed, seed, ne=3):
         out[tag] = y
     arrays = {"nq": np.array(nq), "nm": np.array(nm), "ne": np.array(ne),
               "deformed": np.array(int(deformed)), "jac": jac, "df": df, "x": x,
-              "x_rand": x_rand, "f": f, "f3": f3, "lam": np.array(1.5), "diff": diff,
+              "x_rand": x_rand, "f": f, "f3": f3, "vel": vel, "lam": np.array(1.5), "diff": diff,
               "ptype": np.array(T["ptype"])}
     for k, src in (("b", "b"), ("db", "db"), ("w", "w_raw"), ("ws", "ws"), ("z", "z"),
                    ("D", "D")):

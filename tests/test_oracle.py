@@ -32,6 +32,8 @@ def test_oracle_matches_golden(path):
         assert rel_l2(y, g["out_" + tag]) < TOL, tag
     y = O.iproduct_deriv(s, nm, nq, ne, T, g["jac"], g["df"], g["f3"], dfm)
     assert rel_l2(y, g["out_iproduct_deriv"]) < TOL
+    y = O.linear_adr(s, nm, nq, ne, T, g["jac"], g["df"], float(g["lam"]), g["vel"], g["x"], dfm)
+    assert rel_l2(y, g["out_linear_adr"]) < TOL
 
 
 def _tables(shape, nm, nq0):
@@ -79,6 +81,35 @@ def test_oracle_iproduct_deriv_matches_live_reference(shape, deformed):
     op.apply(f, y)
     yo = O.iproduct_deriv(shape, nm, nq, ne, To, jac, df, f, deformed)
     assert rel_l2(yo, y) < TOL
+
+
+@pytest.mark.skipif(not ref.available(), reason="reference kernels not built (make -C oracle ref)")
+@pytest.mark.parametrize("shape", ["hex", "prism", "tet"])
+@pytest.mark.parametrize("deformed", [False, True])
+def test_oracle_linear_adr_matches_live_reference(shape, deformed):
+    rng = np.random.default_rng(23 + len(shape) + deformed)
+    nm = 5
+    T, nq = _tables(shape, nm, nm + 1)
+    ne, nt, nc = 10, nq[0] * nq[1] * nq[2], O.ncoeffs(shape, nm)
+    ncol = ne * nt if deformed else ne
+    jac = rng.uniform(0.5, 1.5, ncol)
+    df = rng.uniform(-1, 1, (9, ncol))
+    vel = rng.uniform(-1, 1, 3 * ne * nt)
+    x = rng.uniform(-1, 1, ne * nc)
+    To = dict(T)
+    To["w"] = T["ws"]
+    op = ref.RefOp(shape, "linear_adr", nm, nq, ne, To, jac=jac, df=df, deformed=deformed,
+                   nthreads=2)
+    op.set_adr(0.8, vel)
+    y = np.zeros(ne * nc)
+    op.apply(x, y)
+    yo = O.linear_adr(shape, nm, nq, ne, To, jac, df, 0.8, vel, x, deformed)
+    assert rel_l2(yo, y) < TOL
+    # zero velocity: minus the Helmholtz operator's mass term plus its Laplacian
+    op.set_adr(0.8, np.zeros_like(vel))
+    op.apply(x, y)
+    yh = O.helmholtz(shape, nm, nq, ne, To, jac, df, x, -0.8, deformed)
+    assert rel_l2(y, yh) < TOL
 
 
 def _hex_problem(n, nm, amp, lam):
