@@ -52,6 +52,7 @@ extern "C" {
 
 #define NKB_BWDTRANS 0  /* Collections::eBwdTrans */
 #define NKB_HELMHOLTZ 1 /* Collections::eHelmholtz */
+#define NKB_LINEAR_ADR 2 /* Collections::eLinearAdvectionDiffusionReaction */
 #define NKB_IPRODUCT 3  /* Collections::eIProductWRTBase */
 #define NKB_IPRODUCT_DERIV 4 /* Collections::eIProductWRTDerivBase */
 #define NKB_PHYSDERIV 5 /* Collections::ePhysDeriv */
@@ -108,15 +109,17 @@ int nkb_basis(int btype, int nm, int np, const double *z, const double *D, doubl
  *   implemented by Helmholtz_MatrixFree (Collections/Helmholtz.cpp:586-761),
  *   BwdTrans_MatrixFree (BwdTrans.cpp:160-243), IProductWRTBase_MatrixFree
  *   (IProductWRTBase.cpp:182-268), PhysDeriv_MatrixFree (PhysDeriv.cpp:272-),
- *   IProductWRTDerivBase_MatrixFree (IProductWRTDerivBase.cpp:276-374).
+ *   IProductWRTDerivBase_MatrixFree (IProductWRTDerivBase.cpp:276-374),
+ *   LinearAdvectionDiffusionReaction_MatrixFree
+ *   (LinearAdvectionDiffusionReaction.cpp:548-790).
  */
 typedef struct nkb_op nkb_op;
 
 typedef struct nkb_op_desc
 {
     int shape;    /* NKB_HEX / NKB_PRISM / NKB_TET */
-    int optype;   /* NKB_BWDTRANS / NKB_HELMHOLTZ / NKB_IPRODUCT / NKB_IPRODUCT_DERIV /
-                     NKB_PHYSDERIV */
+    int optype;   /* NKB_BWDTRANS / NKB_HELMHOLTZ / NKB_LINEAR_ADR / NKB_IPRODUCT /
+                     NKB_IPRODUCT_DERIV / NKB_PHYSDERIV */
     int nm;       /* modes per direction (equal in all directions) */
     int nq[3];    /* points per direction (Tet: nq0, nq0-1, nq0-1; Prism: nq0, nq0, nq0-1) */
     int ptype[3]; /* points type per direction */
@@ -124,8 +127,8 @@ typedef struct nkb_op_desc
     int deformed; /* 1: geometry per quadrature point (eDeformed), 0: per element */
     /* host arrays, reference layouts (see top of file); NULL where the
      * operator does not need them: BwdTrans needs bdata; IProduct bdata, w, jac;
-     * PhysDeriv z, D, df; Helmholtz and IProductWRTDerivBase bdata, w, z, D,
-     * jac, df. */
+     * PhysDeriv z, D, df; Helmholtz, LinearADR and IProductWRTDerivBase
+     * bdata, w, z, D, jac, df. */
     const double *bdata[3];
     const double *w[3];
     const double *z[3];
@@ -145,6 +148,23 @@ int nkb_op_create(const nkb_op_desc *desc, nkb_op **op);
  * (d00 d01 d11 d02 d12 d22) from eFactorCoeffD00..D22; NKB_DIFF_VAR fills the
  * per-point tensor with diff as SetVarDiffusion does under eFactorTau. */
 int nkb_op_set_factors(nkb_op *op, double lambda, int diff_mode, const double *diff);
+/* For NKB_LINEAR_ADR it replaces LinearAdvectionDiffusionReaction_MatrixFree::
+ * UpdateFactors (LinearAdvectionDiffusionReaction.cpp:578-590): the operator
+ * applies -lambda (SetLambda(-lambda)); diff_mode must be NKB_DIFF_NONE and
+ * lambda nonzero. Until the first call lambda is 1. */
+
+/* Replaces LinearAdvectionDiffusionReaction_MatrixFree::UpdateVarcoeffs
+ * (LinearAdvectionDiffusionReaction.cpp:598-723): the advection velocities
+ * eVarCoeffVelX/Y/Z, nelmt*ntot values each (host or device pointers per
+ * flags), scaled by -1/lambda with the lambda of the last set_factors, as the
+ * reference scales them when it copies them. So the operator is
+ *   out = lambda' (phi, u + V'.grad u) + (grad phi, grad u),
+ * lambda' = -lambda, V' = -V/lambda at the time of this call. Zero velocity
+ * until the first call. Synchronous: returns when the packed operator data
+ * are updated; with device pointers it first waits for all work on the
+ * device (the arrays may be written on any stream). */
+int nkb_op_set_varcoeffs(nkb_op *op, const double *velx, const double *vely, const double *velz,
+                         int flags);
 
 /* Replaces Collections::Operator::operator()(in, out0, out1, out2, wsp)
  * (Operator.h:148-152): out0 is overwritten (no accumulate); PhysDeriv

@@ -15,11 +15,12 @@ import numpy as np
 
 from . import _capi as C
 from ._capi import (BWDTRANS, DEVICE_PTRS, DIFF_CONST, DIFF_NONE, DIFF_VAR, FP32, FP64, GLL,
-                    HELMHOLTZ, HEX, HOST_PTRS, IPRODUCT, IPRODUCT_DERIV, MODIFIED_A, MODIFIED_B, MODIFIED_C,
+                    HELMHOLTZ, HEX, HOST_PTRS, IPRODUCT, IPRODUCT_DERIV, LINEAR_ADR, MODIFIED_A, MODIFIED_B, MODIFIED_C,
                     PHYSDERIV, PRISM, RADAU_A1, RADAU_A2, TET, NektarB200Error, check)
 
 SHAPES = {"hex": HEX, "prism": PRISM, "tet": TET}
-OPTYPES = {"bwdtrans": BWDTRANS, "helmholtz": HELMHOLTZ, "iproduct": IPRODUCT,
+OPTYPES = {"bwdtrans": BWDTRANS, "helmholtz": HELMHOLTZ, "linear_adr": LINEAR_ADR,
+           "iproduct": IPRODUCT,
            "iproduct_deriv": IPRODUCT_DERIV, "physderiv": PHYSDERIV}
 WEIGHT_FACTOR = {GLL: 1.0, RADAU_A1: 0.5, RADAU_A2: 0.25}
 
@@ -176,9 +177,19 @@ class Operator:
         self.in_size, self.out_size = nin.value, nout.value
 
     def set_factors(self, lam=1.0, diff_mode=DIFF_NONE, diff=None):
-        """Helmholtz_MatrixFree::UpdateFactors: lambda and diffusion tensor."""
+        """Helmholtz_MatrixFree::UpdateFactors: lambda and diffusion tensor
+        (LinearADR: lambda only; the operator applies -lambda)."""
         d = None if diff is None else _f64(diff)
         check(lib().nkb_op_set_factors(self.h, float(lam), diff_mode, _dp(d)))
+
+    def set_varcoeffs(self, velx, vely, velz):
+        """LinearADR advection velocities (UpdateVarcoeffs): host arrays of
+        nelmt * ntot values, or device pointers (ints)."""
+        if all(isinstance(v, int) for v in (velx, vely, velz)):
+            check(lib().nkb_op_set_varcoeffs(self.h, velx, vely, velz, DEVICE_PTRS))
+            return
+        vs = [_f64(v) for v in (velx, vely, velz)]
+        check(lib().nkb_op_set_varcoeffs(self.h, *[v.ctypes.data for v in vs], HOST_PTRS))
 
     def __call__(self, x):
         """Host arrays in, host arrays out (synchronous)."""

@@ -7,7 +7,8 @@
 //   * OperatorKey (shape, operator type, implementation type, nodal) and a
 //     factory keyed by it (GetOperatorFactory().CreateInstance), with the new
 //     implementation type eB200 registered for Hex/Prism/Tet x BwdTrans,
-//     IProductWRTBase, IProductWRTDerivBase, PhysDeriv, Helmholtz;
+//     IProductWRTBase, IProductWRTDerivBase, PhysDeriv, Helmholtz,
+//     LinearAdvectionDiffusionReaction;
 //   * GlobalLinSysIterativeFullB200: the GlobalLinSysIterativeFull solve.
 //
 // Errors: a failing status from the C ABI throws NekError with the
@@ -57,8 +58,9 @@ inline void Check(int rc)
 // numbering of Collections::OperatorType / ImplementationType (Operator.h:62-93)
 enum OperatorType
 {
-    eBwdTrans        = NKB_BWDTRANS,
-    eHelmholtz       = NKB_HELMHOLTZ,
+    eBwdTrans                         = NKB_BWDTRANS,
+    eHelmholtz                        = NKB_HELMHOLTZ,
+    eLinearAdvectionDiffusionReaction = NKB_LINEAR_ADR,
     eIProductWRTBase      = NKB_IPRODUCT,
     eIProductWRTDerivBase = NKB_IPRODUCT_DERIV,
     ePhysDeriv            = NKB_PHYSDERIV
@@ -90,6 +92,13 @@ struct FactorMap
     double tau                  = 0.0;                 // eFactorTau != 0: variable diffusion
 };
 
+// StdRegions::VarCoeffMap subset LinearADR reads: eVarCoeffVelX/Y/Z, one
+// value per quadrature point of the collection
+struct VarCoeffMap
+{
+    Array1D velx, vely, velz;
+};
+
 // what a Collection hands its operator: basis tables, points, geometry
 // (LocalRegions expansions + CoalescedGeomData in the reference)
 struct CollectionData
@@ -115,6 +124,12 @@ public:
     {
         throw NekError(NKB_ERR_INVALID, "This method needs to be re-implemented in derived "
                                         "operator class.");
+    }
+    virtual void UpdateVarcoeffs(VarCoeffMap &)
+    {
+        throw NekError(NKB_ERR_INVALID, "This method needs to be re-implemented in derived "
+                                        "operator class. Make sure it is implemented for the "
+                                        "operator in the .opt file");
     }
     unsigned GetInputSize() const
     {
@@ -298,6 +313,52 @@ private:
     B200OpHandle m_h;
 };
 
+// LinearAdvectionDiffusionReaction (LinearAdvectionDiffusionReaction.cpp:548-790):
+// coefficients in and out; UpdateFactors takes lambda (the operator applies
+// -lambda), UpdateVarcoeffs the advection velocities (scaled by -1/lambda)
+class LinearAdvectionDiffusionReaction_B200 : public Operator
+{
+public:
+    LinearAdvectionDiffusionReaction_B200(const CollectionData &d, const FactorMap &f)
+        : m_h(d, eLinearAdvectionDiffusionReaction),
+          m_nqtot(size_t(d.nelmt) * size_t(d.nq[0]) * size_t(d.nq[1]) * size_t(d.nq[2]))
+    {
+        m_in    = m_h.m_in;
+        m_out   = m_h.m_out;
+        m_nelmt = unsigned(d.nelmt);
+        UpdateFactors(f);
+    }
+    void operator()(const Array1D &input, Array1D &output0, Array1D &, Array1D &,
+                    Array1D &) override
+    {
+        if (input.size() < m_in || output0.size() < m_out)
+            throw NekError(NKB_ERR_INVALID, "array smaller than the operator's size");
+        Check(nkb_op_apply(m_h.get(), input.data(), output0.data(), nullptr, nullptr,
+                           NKB_HOST_PTRS, nullptr));
+    }
+    void operator()(int, const Array1D &, Array1D &, Array1D &) override
+    {
+        throw NekError(NKB_ERR_INVALID, "Not valid for this operator.");
+    }
+    // UpdateFactors (LinearAdvectionDiffusionReaction.cpp:578-590)
+    void UpdateFactors(const FactorMap &f) override
+    {
+        Check(nkb_op_set_factors(m_h.get(), f.lambda, NKB_DIFF_NONE, nullptr));
+    }
+    // UpdateVarcoeffs (LinearAdvectionDiffusionReaction.cpp:598-723)
+    void UpdateVarcoeffs(VarCoeffMap &v) override
+    {
+        if (v.velx.size() < m_nqtot || v.vely.size() < m_nqtot || v.velz.size() < m_nqtot)
+            throw NekError(NKB_ERR_INVALID, "Must define at least one advection velocity");
+        Check(nkb_op_set_varcoeffs(m_h.get(), v.velx.data(), v.vely.data(), v.velz.data(),
+                                   NKB_HOST_PTRS));
+    }
+
+private:
+    B200OpHandle m_h;
+    size_t m_nqtot; // quadrature points of the collection
+};
+
 // IProductWRTDerivBase: the vector field's three components in entry0..2,
 // the result in entry3 (IProductWRTDerivBase.cpp:285-318, coordim 3)
 class IProductWRTDerivBase_B200 : public Operator
@@ -353,6 +414,12 @@ inline bool RegisterB200Operators()
                 return std::make_shared<PhysDeriv_B200>(d, m);
             },
             "PhysDeriv_B200");
+        f.RegisterCreatorFunction(
+            OperatorKey(s, eLinearAdvectionDiffusionReaction, eB200, false),
+            [](const CollectionData &d, const FactorMap &m) {
+                return std::make_shared<LinearAdvectionDiffusionReaction_B200>(d, m);
+            },
+            "LinearAdvectionDiffusionReaction_B200");
         f.RegisterCreatorFunction(
             OperatorKey(s, eIProductWRTDerivBase, eB200, false),
             [](const CollectionData &d, const FactorMap &m) {

@@ -17,6 +17,7 @@ enum
 {
     GK_BWD  = 0,
     GK_HELM = 1,
+    GK_ADR  = 2,
     GK_IP   = 3,
     GK_IPD  = 4,
     GK_PD   = 5,
@@ -84,7 +85,7 @@ template <int SHAPE, int OP, typename T, class D = Dims> __global__ void k_gener
     using BW = Bwd<SHAPE>;
     using IP = Ipr<SHAPE>;
 
-    if (OP == GK_BWD || OP == GK_HELM || OP == GK_DIAG)
+    if (OP == GK_BWD || OP == GK_HELM || OP == GK_ADR || OP == GK_DIAG)
     {
         if (OP != GK_DIAG)
         {
@@ -107,7 +108,7 @@ template <int SHAPE, int OP, typename T, class D = Dims> __global__ void k_gener
         NKB_STAGE(d.nt, { u[l] = a.in[e * d.nt + l]; })
     }
 
-    if (OP == GK_BWD || OP == GK_HELM)
+    if (OP == GK_BWD || OP == GK_HELM || OP == GK_ADR)
     {
         NKB_STAGE(BW::SizeA(d), { BW::A(d, a.t, x, wa, l); })
         NKB_STAGE(BW::SizeB(d), { BW::B(d, a.t, x, wa, wb, l); })
@@ -156,6 +157,26 @@ template <int SHAPE, int OP, typename T, class D = Dims> __global__ void k_gener
         NKB_STAGE(d.nt, { u[l] = wa[l] + GradT(d, a.t, g0, g1, g2, l); })
     }
 
+    if (OP == GK_ADR)
+    {
+        // LinearADR (LinearAdvectionDiffusionReaction.h:608-670): as Helmholtz
+        // with lambda' (u + V'.grad u) for the mass term; the packed rows
+        // 7..9 carry W A V'
+        NKB_STAGE(d.nt, {
+            T q0, q1, q2;
+            Grad(d, a.t, u, l, q0, q1, q2);
+            const T *G = a.geo + e * a.gstride + l;
+            const T W = G[0], G00 = G[d.nt], G11 = G[2 * d.nt], G22 = G[3 * d.nt];
+            const T G01 = G[4 * d.nt], G02 = G[5 * d.nt], G12 = G[6 * d.nt];
+            const T adv = fma(G[9 * d.nt], q2, fma(G[8 * d.nt], q1, G[7 * d.nt] * q0));
+            g0[l] = fma(G02, q2, fma(G01, q1, G00 * q0));
+            g1[l] = fma(G12, q2, fma(G11, q1, G01 * q0));
+            g2[l] = fma(G22, q2, fma(G12, q1, G02 * q0));
+            wa[l] = a.lambda * fma(W, u[l], adv);
+        })
+        NKB_STAGE(d.nt, { u[l] = wa[l] + GradT(d, a.t, g0, g1, g2, l); })
+    }
+
     if (OP == GK_IPD)
     {
         // v_x = sum_m W A[x*3+m] f_m (the packed rows already carry W), then
@@ -172,7 +193,7 @@ template <int SHAPE, int OP, typename T, class D = Dims> __global__ void k_gener
         NKB_STAGE(d.nt, { u[l] = GradT(d, a.t, g0, g1, g2, l); })
     }
 
-    if (OP == GK_HELM || OP == GK_IP || OP == GK_IPD)
+    if (OP == GK_HELM || OP == GK_ADR || OP == GK_IP || OP == GK_IPD)
     {
         NKB_STAGE(IP::SizeA(d), { IprStageA(d, a.t, u, wa, l); })
         NKB_STAGE(IP::SizeB(d), { IP::B(d, a.t, wa, wb, l); })

@@ -30,6 +30,8 @@ struct nkb_op
     float *geo32 = nullptr;
 
     double lambda    = 1.0;
+    double factor_lambda = 1.0; // LinearADR: the caller's eFactorLambda (lambda = -factor_lambda)
+    double *dvel     = nullptr; // LinearADR: V' = (-1/lambda) V on the device, three fields
     int diff_mode    = NKB_DIFF_NONE;
     double diff[6]   = {1, 0, 1, 0, 0, 1};
 

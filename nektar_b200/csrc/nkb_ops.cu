@@ -97,11 +97,20 @@ struct PackArgs
     const double *w0, *w1, *w2;   // scaled weights
     int diff_mode;                // NKB_DIFF_*
     double K[6];                  // d00 d01 d11 d02 d12 d22
+    const double *vel;            // LinearADR: V' = (-1/lambda) V, three fields (or NULL)
     double *geo;                  // packed FP64
     float *geo32;                 // optional FP32 copy
-    int ncomp;                    // 7 Helmholtz, 9 PhysDeriv / IProductWRTDerivBase, 1 IProduct
+    int ncomp;                    // 7 Helmholtz, 10 LinearADR, 9 PhysDeriv /
+                                  // IProductWRTDerivBase, 1 IProduct
     long gstride;                 // element stride of the packed arrays
 };
+
+__global__ void k_scale(double *v, size_t n, double s)
+{
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n;
+         i += size_t(gridDim.x) * blockDim.x)
+        v[i] = s * v[i];
+}
 
 __global__ void k_pack(PackArgs a)
 {
@@ -174,6 +183,22 @@ __global__ void k_pack(PackArgs a)
             out[c * nt] = v[c];
             if (out32)
                 out32[c * nt] = float(v[c]);
+        }
+        if (a.optype == NKB_LINEAR_ADR)
+        {
+            // advection rows W * sum_m A[x*3+m] V'_m: V'.grad_x u = sum_x row_x d_x
+            const long fld = long(a.nelmt) * nt;
+            double V[3]    = {0.0, 0.0, 0.0};
+            if (a.vel)
+                for (int m = 0; m < 3; ++m)
+                    V[m] = a.vel[m * fld + g];
+            for (int x = 0; x < 3; ++x)
+            {
+                const double r = W * fma(A[x * 3 + 2], V[2], fma(A[x * 3 + 1], V[1], A[x * 3] * V[0]));
+                out[(7 + x) * nt] = r;
+                if (out32)
+                    out32[(7 + x) * nt] = float(r);
+            }
         }
     }
 }
@@ -451,6 +476,8 @@ int LaunchGeneric3(const nkb_op *op, const T *in, const T *in1, const T *in2, T 
             return LaunchGenericShape<GK_PD, T>(op, a, s);
         case NKB_IPRODUCT_DERIV:
             return LaunchGenericShape<GK_IPD, T>(op, a, s);
+        case NKB_LINEAR_ADR:
+            return LaunchGenericShape<GK_ADR, T>(op, a, s);
         default:
         {
             if (ColKernels())
@@ -506,6 +533,7 @@ static int Repack(nkb_op *op)
     a.diff_mode = op->diff_mode;
     for (int c = 0; c < 6; ++c)
         a.K[c] = op->diff[c];
+    a.vel     = op->dvel;
     a.geo     = op->geo;
     a.geo32   = op->geo32;
     a.ncomp   = op->ncomp;
@@ -562,7 +590,7 @@ extern "C" int nkb_op_create(const nkb_op_desc *desc, nkb_op **out)
         return SetError(NKB_ERR_INVALID, "nkb_op_create: unsupported shape %d", shape);
     if (desc->optype != NKB_BWDTRANS && desc->optype != NKB_HELMHOLTZ &&
         desc->optype != NKB_IPRODUCT && desc->optype != NKB_IPRODUCT_DERIV &&
-        desc->optype != NKB_PHYSDERIV)
+        desc->optype != NKB_PHYSDERIV && desc->optype != NKB_LINEAR_ADR)
         return SetError(NKB_ERR_INVALID, "nkb_op_create: unsupported operator %d", desc->optype);
     if (nm < 2 || nm > 16 || desc->nelmt < 0)
         return SetError(NKB_ERR_INVALID, "nkb_op_create: nm=%d nelmt=%d out of range", nm,
@@ -588,8 +616,9 @@ extern "C" int nkb_op_create(const nkb_op_desc *desc, nkb_op **out)
                             opt);
         return NKB_OK;
     };
-    const bool weighted = opt == NKB_IPRODUCT || opt == NKB_HELMHOLTZ || opt == NKB_IPRODUCT_DERIV;
-    const bool derived  = opt == NKB_PHYSDERIV || opt == NKB_HELMHOLTZ || opt == NKB_IPRODUCT_DERIV;
+    const bool helm_like = opt == NKB_HELMHOLTZ || opt == NKB_LINEAR_ADR;
+    const bool weighted  = opt == NKB_IPRODUCT || helm_like || opt == NKB_IPRODUCT_DERIV;
+    const bool derived   = opt == NKB_PHYSDERIV || helm_like || opt == NKB_IPRODUCT_DERIV;
     for (int d = 0; d < 3; ++d)
     {
         if (opt != NKB_PHYSDERIV && need(desc->bdata[d], "bdata"))
@@ -625,8 +654,16 @@ extern "C" int nkb_op_create(const nkb_op_desc *desc, nkb_op **out)
         op->ptype[d] = desc->ptype[d];
     }
     op->nc = NumCoeffs(shape, nm);
+    if (opt == NKB_LINEAR_ADR)
+    {
+        // UpdateFactors runs in the reference constructor with the
+        // collection's factors; until set_factors: lambda 1, operator -1
+        op->factor_lambda = 1.0;
+        op->lambda        = -1.0;
+    }
     op->nt = nq[0] * nq[1] * nq[2];
     op->ncomp = (opt == NKB_HELMHOLTZ)                                    ? 7
+                : (opt == NKB_LINEAR_ADR)                                 ? 10
                 : (opt == NKB_PHYSDERIV || opt == NKB_IPRODUCT_DERIV) ? 9
                 : (opt == NKB_IPRODUCT ? 1 : 0);
     // element blocks of the packed geometry start on 32-byte boundaries so a
@@ -699,6 +736,20 @@ extern "C" int nkb_op_set_factors(nkb_op *op, double lambda, int diff_mode, cons
         return SetError(NKB_ERR_INVALID, "nkb_op_set_factors: NULL op");
     if (diff_mode < NKB_DIFF_NONE || diff_mode > NKB_DIFF_VAR || (diff_mode && !diff))
         return SetError(NKB_ERR_INVALID, "nkb_op_set_factors: bad diffusion mode %d", diff_mode);
+    if (op->optype == NKB_LINEAR_ADR)
+    {
+        // LinearAdvectionDiffusionReaction_MatrixFree::UpdateFactors
+        // (LinearAdvectionDiffusionReaction.cpp:578-590): SetLambda(-lambda);
+        // it takes no diffusion tensor
+        if (diff_mode != NKB_DIFF_NONE)
+            return SetError(NKB_ERR_INVALID,
+                            "nkb_op_set_factors: LinearADR takes no diffusion tensor");
+        if (!(lambda != 0.0))
+            return SetError(NKB_ERR_INVALID, "nkb_op_set_factors: LinearADR needs lambda != 0");
+        op->factor_lambda = lambda;
+        op->lambda        = -1 * lambda;
+        return NKB_OK;
+    }
     op->lambda = lambda;
     bool repack = (diff_mode != op->diff_mode);
     if (diff_mode)
@@ -721,6 +772,38 @@ extern "C" int nkb_op_set_factors(nkb_op *op, double lambda, int diff_mode, cons
         return Repack(op);
     }
     return NKB_OK;
+}
+
+extern "C" int nkb_op_set_varcoeffs(nkb_op *op, const double *velx, const double *vely,
+                                    const double *velz, int flags)
+{
+    ClearError();
+    if (!op || !velx || !vely || !velz)
+        return SetError(NKB_ERR_INVALID, "nkb_op_set_varcoeffs: NULL argument");
+    if (op->optype != NKB_LINEAR_ADR)
+        return SetError(NKB_ERR_INVALID, "nkb_op_set_varcoeffs: operator %d takes no velocities",
+                        op->optype);
+    NKB_CUDA_TRY(cudaSetDevice(op->device));
+    const size_t fld = size_t(op->nelmt) * op->nt;
+    if (fld == 0)
+        return NKB_OK;
+    if (!op->dvel && cudaMalloc(&op->dvel, 3 * fld * sizeof(double)) != cudaSuccess)
+        return SetError(NKB_ERR_NOMEM, "nkb_op_set_varcoeffs: velocities (%zu doubles)", 3 * fld);
+    const double *src[3] = {velx, vely, velz};
+    const cudaMemcpyKind kind =
+        (flags & NKB_HOST_PTRS) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    // device arrays may still be written by the caller's streams
+    if (!(flags & NKB_HOST_PTRS))
+        NKB_CUDA_TRY(cudaDeviceSynchronize());
+    for (int d = 0; d < 3; ++d)
+        NKB_CUDA_TRY(cudaMemcpyAsync(op->dvel + d * fld, src[d], fld * sizeof(double), kind,
+                                     op->stream));
+    // LinearAdvectionDiffusionReaction.cpp:662-672: scaled by -1/lambda at
+    // the time of the update
+    const int nb = int(std::min<size_t>((3 * fld + 255) / 256, 148 * 16));
+    k_scale<<<nb, 256, 0, op->stream>>>(op->dvel, 3 * fld, -1 / op->factor_lambda);
+    NKB_CUDA_TRY(cudaGetLastError());
+    return Repack(op);
 }
 
 extern "C" int nkb_op_sizes(const nkb_op *op, long *in_size, long *out_size)
@@ -959,6 +1042,9 @@ extern "C" int nkb_op_helmholtz_diag(nkb_op *op, double *diag, int flags, void *
         return SetError(NKB_ERR_INVALID, "nkb_op_helmholtz_diag: NULL argument");
     if (op->precision != NKB_FP64)
         return SetError(NKB_ERR_INVALID, "nkb_op_helmholtz_diag: needs an FP64 operator");
+    if (op->optype != NKB_HELMHOLTZ)
+        return SetError(NKB_ERR_INVALID, "nkb_op_helmholtz_diag: operator %d is not Helmholtz",
+                        op->optype);
     NKB_CUDA_TRY(cudaSetDevice(op->device));
     cudaStream_t s = static_cast<cudaStream_t>(stream); // NULL: legacy default stream
     const size_t n = size_t(op->nelmt) * op->nc;
@@ -993,6 +1079,7 @@ extern "C" void nkb_op_destroy(nkb_op *op)
     }
     cudaFree(op->djac);
     cudaFree(op->ddf);
+    cudaFree(op->dvel);
     cudaFree(op->geo);
     cudaFree(op->geo32);
     cudaFree(op->scratch);

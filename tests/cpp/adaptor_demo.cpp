@@ -1,7 +1,8 @@
 // Drives the C++ Collections mirror (nektar_b200/adaptor/nkb_collections.hpp)
 // the way a Nektar++ Collection would: factory lookup by OperatorKey with the
 // eB200 implementation type, Helmholtz apply with UpdateFactors, an
-// IProductWRTDerivBase apply with three input fields, then the
+// IProductWRTDerivBase apply with three input fields, a LinearADR apply with
+// UpdateVarcoeffs, then the
 // GlobalLinSysIterativeFull solve. Prints one JSON line. Exit codes: 0 ok,
 // 3 NekError raised (e.g. no CUDA device), 1 other failure.
 #include "../../nektar_b200/adaptor/nkb_collections.hpp"
@@ -86,14 +87,34 @@ int main()
         double ng = 0.0;
         for (double v : g)
             ng += v * v;
+        // LinearAdvectionDiffusionReaction with a velocity field
+        auto adr = GetOperatorFactory().CreateInstance(
+            OperatorKey(eHexahedron, eLinearAdvectionDiffusionReaction, eB200, false), d, f);
+        VarCoeffMap vc;
+        vc.velx.resize(f0.size());
+        vc.vely.resize(f0.size());
+        vc.velz.resize(f0.size());
+        for (size_t i = 0; i < f0.size(); ++i)
+        {
+            vc.velx[i] = 1.0 + 0.1 * std::sin(0.05 * double(i));
+            vc.vely[i] = -0.5;
+            vc.velz[i] = 0.25 * std::cos(0.02 * double(i));
+        }
+        adr->UpdateVarcoeffs(vc);
+        Array1D ya(adr->GetOutputSize());
+        (*adr)(x, ya, e1, e2, wsp);
+        double na = 0.0;
+        for (double v : ya)
+            na += v * v;
         auto helm = std::dynamic_pointer_cast<Helmholtz_B200>(op);
         GlobalLinSysIterativeFullB200 sys({helm}, map, nglob, ndir);
         Array1D b(x), sol(x.size(), 0.0);
         nkb_cg_report r = sys.Solve(b, sol, 1e-10);
         std::printf("{\"helmholtz_norm2\": %.17g, \"iproduct_deriv_norm2\": %.17g, "
+                    "\"linear_adr_norm2\": %.17g, "
                     "\"dir_call_threw\": %d, \"cg_iterations\": %d, "
                     "\"cg_rel_residual\": %.6g, \"nelmt\": %d}\n",
-                    ny, ng, int(threw), r.iterations, r.rel_residual, d.nelmt);
+                    ny, ng, na, int(threw), r.iterations, r.rel_residual, d.nelmt);
         return 0;
     }
     catch (const NekError &e)

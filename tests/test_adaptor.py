@@ -50,5 +50,11 @@ def test_adaptor_matches_c_abi(tmp_path):
     g = ipd.apply3(np.cos(0.11 * i), np.cos(0.11 * i + 1.0), np.cos(0.11 * i + 2.0))
     ng = float(np.sum(g ** 2))
     assert abs(out["iproduct_deriv_norm2"] - ng) <= 1e-12 * ng
+    adr = nb.Operator("linear_adr", m)
+    adr.set_factors(1.5)
+    i = np.arange(m.nelmt * m.nt)
+    adr.set_varcoeffs(1.0 + 0.1 * np.sin(0.05 * i), np.full(i.size, -0.5), 0.25 * np.cos(0.02 * i))
+    na = float(np.sum(adr(x) ** 2))
+    assert abs(out["linear_adr_norm2"] - na) <= 1e-12 * na
     assert out["dir_call_threw"] == 1
     assert out["cg_rel_residual"] < 1e-10 and out["cg_iterations"] > 0

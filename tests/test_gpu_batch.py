@@ -11,8 +11,8 @@ from nektar_b200.mixed_mesh import MixedMesh
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("optype", ["helmholtz", "bwdtrans", "iproduct", "iproduct_deriv",
-                                    "physderiv"])
+@pytest.mark.parametrize("optype", ["helmholtz", "linear_adr", "bwdtrans", "iproduct",
+                                    "iproduct_deriv", "physderiv"])
 def test_batch_equals_collection_by_collection(optype):
     mm = MixedMesh(n=6, ncells=(60, 50, 40), pmin=2, pmax=5, seed=2)
     cols = mm.collections(optype, lam=2.5)

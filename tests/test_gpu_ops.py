@@ -29,6 +29,11 @@ def test_ops_match_reference_golden(path):
     d = _op("physderiv", g)(g["f"])
     assert rel_l2(np.stack(d), g["out_physderiv"]) < TOL64
     assert rel_l2(_op("iproduct_deriv", g)(g["f3"]), g["out_iproduct_deriv"]) < TOL64
+    adr = _op("linear_adr", g)
+    adr.set_factors(float(g["lam"]))
+    n = g["vel"].size // 3
+    adr.set_varcoeffs(g["vel"][:n], g["vel"][n:2 * n], g["vel"][2 * n:])
+    assert rel_l2(adr(g["x"]), g["out_linear_adr"]) < TOL64
     op = _op("helmholtz", g)
     op.set_factors(float(g["lam"]))
     assert rel_l2(op(g["x"]), g["out_helmholtz"]) < TOL64
@@ -75,6 +80,13 @@ def test_ops_match_oracle(shape, n, nm, amp):
     f3 = rng.uniform(-1, 1, 3 * m.nelmt * m.nt)
     yo = O.iproduct_deriv(shape, nm, m.nq, m.nelmt, To, m.jac, m.df, f3, dfm)
     assert rel_l2(nb.Operator("iproduct_deriv", m)(f3), yo) < TOL64
+    vel = rng.uniform(-1, 1, 3 * m.nelmt * m.nt)
+    yo = O.linear_adr(shape, nm, m.nq, m.nelmt, To, m.jac, m.df, 0.7, vel, x, dfm)
+    adr = nb.Operator("linear_adr", m)
+    adr.set_factors(0.7)
+    n = m.nelmt * m.nt
+    adr.set_varcoeffs(vel[:n], vel[n:2 * n], vel[2 * n:])
+    assert rel_l2(adr(x), yo) < TOL64
 
 
 @pytest.mark.parametrize("shape", ["hex", "prism", "tet"])
@@ -252,3 +264,52 @@ def test_iproduct_deriv_of_gradient_is_laplacian(shape, n, nm):
     lap = nb.Operator("helmholtz", m)
     lap.set_factors(0.0)
     assert rel_l2(y, lap(x)) < 1e-12
+
+
+@pytest.mark.parametrize("shape", ["hex", "prism", "tet"])
+def test_linear_adr_factor_semantics(shape):
+    """The reference scales the velocities by -1/lambda when they are set
+    (LinearAdvectionDiffusionReaction.cpp:662-672) and applies -lambda from
+    the last UpdateFactors; zero velocity is minus the Helmholtz mass term."""
+    import torch
+    m = nb.BoxMesh(shape, 3, 5, 6, amp=0.05)
+    To = _oracle_T(m)
+    rng = np.random.default_rng(4)
+    x = rng.uniform(-1, 1, m.nelmt * m.nc)
+    vel = rng.uniform(-1, 1, 3 * m.nelmt * m.nt)
+    n = m.nelmt * m.nt
+    adr = nb.Operator("linear_adr", m)
+    # before any velocities: -lambda M + L, lambda = 1 until set_factors
+    h = nb.Operator("helmholtz", m)
+    h.set_factors(-1.0)
+    assert rel_l2(adr(x), h(x)) < TOL64
+    # velocities scaled with lambda = 2, then lambda changed to 3: V' = -V/2
+    adr.set_factors(2.0)
+    vd = torch.tensor(vel, device="cuda")
+    adr.set_varcoeffs(vd[:n].data_ptr(), vd[n:2 * n].data_ptr(), vd[2 * n:].data_ptr())
+    adr.set_factors(3.0)
+    yo = O.linear_adr(shape, m.nm, m.nq, m.nelmt, To, m.jac, m.df, 3.0, 1.5 * vel, x, True)
+    assert rel_l2(adr(x), yo) < TOL64
+    with pytest.raises(nb.NektarB200Error):
+        adr.set_factors(1.0, nb.DIFF_CONST, np.ones(6))
+    with pytest.raises(nb.NektarB200Error):
+        h.set_varcoeffs(vel[:n], vel[n:2 * n], vel[2 * n:])
+
+
+@pytest.mark.parametrize("shape", ["hex", "prism", "tet"])
+def test_fp32_linear_adr_matches_oracle(shape):
+    import torch
+    m = nb.BoxMesh(shape, 3, 6, 7, amp=0.05)
+    rng = np.random.default_rng(8)
+    x = rng.uniform(-1, 1, m.nelmt * m.nc)
+    vel = rng.uniform(-1, 1, 3 * m.nelmt * m.nt)
+    n = m.nelmt * m.nt
+    yo = O.linear_adr(shape, m.nm, m.nq, m.nelmt, _oracle_T(m), m.jac, m.df, 1.3, vel, x, True)
+    op = nb.Operator("linear_adr", m, precision="fp32")
+    op.set_factors(1.3)
+    op.set_varcoeffs(vel[:n], vel[n:2 * n], vel[2 * n:])
+    xd = torch.tensor(x, dtype=torch.float32, device="cuda")
+    yd = torch.empty(op.out_size, dtype=torch.float32, device="cuda")
+    op.apply_device(xd.data_ptr(), yd.data_ptr(), stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rel_l2(yd.double().cpu().numpy(), yo) < TOL32
