@@ -40,9 +40,14 @@ template <typename T> __device__ __forceinline__ T ColLd(const T *p)
     return __ldg(p);
 }
 
-template <int SHAPE, int NM, typename T, bool GATHER>
+// MODE 0: Helmholtz; 1: Helmholtz with the input gathered from a global
+// vector; 2: LinearADR (lambda (W u + W A V'.grad u) as the mass term, packed
+// rows 7..9)
+template <int SHAPE, int NM, typename T, int MODE>
 __global__ void __launch_bounds__(ColDims<SHAPE, NM>::THREADS) k_col_helm(GenArgs<T> a)
 {
+    constexpr bool GATHER = MODE == 1, ADV = MODE == 2;
+    constexpr int NG      = ADV ? 10 : 7; // packed values per point
     using C          = ColDims<SHAPE, NM>;
     constexpr int Q0 = C::Q0, Q1 = C::Q1, Q2 = C::Q2, NC = C::NC, NT = C::NT, NP = C::NP;
     extern __shared__ __align__(16) unsigned char col_raw[];
@@ -64,7 +69,7 @@ __global__ void __launch_bounds__(ColDims<SHAPE, NM>::THREADS) k_col_helm(GenArg
     const int tid = threadIdx.x;
     const T *G    = a.geo + e * a.gstride;
     if (tid == 0)
-        BulkPrefetchL2(G, uint32_t(7 * NT * sizeof(T) + 15) & ~15u);
+        BulkPrefetchL2(G, uint32_t(NG * NT * sizeof(T) + 15) & ~15u);
 
     for (int l = tid; l < NM * Q0; l += blockDim.x)
         B0[l] = ColLd(a.t.B0 + l);
@@ -295,7 +300,16 @@ __global__ void __launch_bounds__(ColDims<SHAPE, NM>::THREADS) k_col_helm(GenArg
             S0[q] = fma(G02, g2, fma(G01, g1, G00 * g0));
             S1[q] = fma(G12, g2, fma(G11, g1, G01 * g0));
             v2[k] = fma(G22, g2, fma(G12, g1, G02 * g0));
-            f[k]  = lam * W * u[k];
+            if (ADV)
+            {
+                const T adv = fma(ColLd(G + 9 * NT + q), g2,
+                                  fma(ColLd(G + 8 * NT + q), g1, ColLd(G + 7 * NT + q) * g0));
+                f[k] = lam * fma(W, u[k], adv);
+            }
+            else
+            {
+                f[k] = lam * W * u[k];
+            }
         }
     }
     __syncthreads();
@@ -514,9 +528,13 @@ int LaunchColShapeNM(const nkb_op *op, const GenArgs<T> &a, cudaStream_t s, bool
     const size_t smem = size_t(C::SMEM) * sizeof(T);
     if (smem > 200 * 1024)
         return kNotCovered;
-    auto kern = gather ? k_col_helm<SHAPE, NM, T, true> : k_col_helm<SHAPE, NM, T, false>;
-    static size_t s_set[2] = {48 * 1024, 48 * 1024};
-    size_t &set            = s_set[gather ? 1 : 0];
+    const int mode = op->optype == NKB_LINEAR_ADR ? 2 : (gather ? 1 : 0);
+    if (mode == 2 && gather)
+        return kNotCovered;
+    auto kern = mode == 2 ? k_col_helm<SHAPE, NM, T, 2>
+                          : (mode == 1 ? k_col_helm<SHAPE, NM, T, 1> : k_col_helm<SHAPE, NM, T, 0>);
+    static size_t s_set[3] = {48 * 1024, 48 * 1024, 48 * 1024};
+    size_t &set            = s_set[mode];
     if (smem > set)
     {
         NKB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));

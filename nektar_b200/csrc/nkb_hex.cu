@@ -90,11 +90,11 @@ template <typename T> static HexArgs<T> MakeHexArgs(const nkb_op *op)
 // time each candidate on this operator's own data and keep the fastest; the
 // choice is cached per (precision, nm, element count).
 static std::mutex g_tune_mu;
-static std::map<std::tuple<int, int, int>, int> g_tune_cache;
+static std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
 
 template <typename T> static int AutotuneHex(nkb_op *op, int *best)
 {
-    const auto key = std::make_tuple(op->precision, op->nm, op->nelmt);
+    const auto key = std::make_tuple(op->optype, op->precision, op->nm, op->nelmt);
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_cache.find(key);
@@ -229,7 +229,8 @@ int ChooseKernel(nkb_op *op)
 {
     op->variant  = kVariantGeneric;
     const int eb = op->precision == NKB_FP64 ? 8 : 4;
-    if (op->shape == NKB_HEX && op->optype == NKB_HELMHOLTZ && op->nm >= 2 && op->nm <= 11 &&
+    if (op->shape == NKB_HEX && (op->optype == NKB_HELMHOLTZ || op->optype == NKB_LINEAR_ADR) &&
+        op->nm >= 2 && op->nm <= 11 &&
         op->nq[0] == op->nm + 1 && op->nq[1] == op->nq[0] && op->nq[2] == op->nq[0] &&
         SameTable(op->hD[0], op->hD[1]) && SameTable(op->hD[0], op->hD[2]) && !ForceGeneric())
     {
@@ -331,7 +332,8 @@ const char *KernelName(const nkb_op *op, bool gather)
         const bool std = op->nq[0] == nm + 1 &&
                          ((op->shape == NKB_PRISM && op->nq[1] == nm + 1 && op->nq[2] == nm) ||
                           (op->shape == NKB_TET && op->nq[1] == nm && op->nq[2] == nm));
-        if (op->optype == NKB_HELMHOLTZ && std && nm >= 2 && nm <= 11)
+        if ((op->optype == NKB_HELMHOLTZ || op->optype == NKB_LINEAR_ADR) && std && nm >= 2 &&
+            nm <= 11)
             return "k_col_helm (Prism/Tet column kernel)";
         return "k_generic";
     }

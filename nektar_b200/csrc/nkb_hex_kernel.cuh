@@ -30,6 +30,14 @@ template <typename T> struct HexArgs
     const int *skip;    // optional: nonzero -> nothing to do (converged CG)
 };
 
+// kernel modes (the last template argument of the Hex kernels)
+enum
+{
+    kModeLocal  = 0,
+    kModeGather = 1,
+    kModeAdv    = 2
+};
+
 // geometry staging
 enum
 {
@@ -119,10 +127,15 @@ template <typename T, int NQ, int GEO, int EPB> __host__ __device__ constexpr in
     return b < 1 ? 1 : b;
 }
 
-template <typename T, int NM, int NQ, int GEO, int EPB, bool GATHER>
+// MODE: kModeLocal (Helmholtz), kModeGather (Helmholtz, input gathered from
+// a global vector), kModeAdv (LinearADR: lambda (W u + W A V'.grad u) as the
+// mass term, packed rows 7..9)
+template <typename T, int NM, int NQ, int GEO, int EPB, int MODE>
 __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GEO, EPB>()))
     k_hex_helm(HexArgs<T> a, const __grid_constant__ HexConst<T, NM, NQ> c)
 {
+    constexpr bool GATHER = MODE == kModeGather, ADV = MODE == kModeAdv;
+    constexpr int NG      = ADV ? 10 : 7; // packed values per point
     constexpr int NQ2 = NQ * NQ, NQ3 = NQ2 * NQ, NC = NM * NM * NM, NQP = NQ + 1;
     constexpr int NMP = NM + (NM & 1); // coefficient rows padded to an even length
     constexpr int RS  = HexRegion<NQ>(); // element stride of the work regions (even)
@@ -171,12 +184,12 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
 
     // streamed geometry: plane 0 requested before any arithmetic
     const T *Gg = a.geo + (e0 + lec) * GS;
-    T gc[7];
+    T gc[NG];
     if (GEO == kGeoStream && act)
     {
         const int q0 = j * NQ + i;
 #pragma unroll
-        for (int cc = 0; cc < 7; ++cc)
+        for (int cc = 0; cc < NG; ++cc)
             gc[cc] = __ldg(Gg + cc * NQ3 + q0);
     }
 
@@ -290,11 +303,11 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
         for (int k = 0; k < NQ; ++k)
         {
             const int q = (k * NQ + j) * NQ + i;
-            T gn[7];
+            T gn[NG];
             if (GEO == kGeoStream && k + 1 < NQ)
             {
 #pragma unroll
-                for (int cc = 0; cc < 7; ++cc)
+                for (int cc = 0; cc < NG; ++cc)
                     gn[cc] = __ldg(Gg + cc * NQ3 + q + NQ2);
             }
             T g1 = 0, g2 = 0;
@@ -306,7 +319,7 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
 #pragma unroll
             for (int m = 0; m < NQ; ++m)
                 g2 = fma(c.D[k * NQ + m], ur[m], g2);
-            T W, G00, G11, G22, G01, G02, G12;
+            T W, G00, G11, G22, G01, G02, G12, A0 = 0, A1 = 0, A2 = 0;
             if (GEO == kGeoTma)
             {
                 W   = G[q];
@@ -316,6 +329,12 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
                 G01 = G[4 * NQ3 + q];
                 G02 = G[5 * NQ3 + q];
                 G12 = G[6 * NQ3 + q];
+                if (ADV)
+                {
+                    A0 = G[7 * NQ3 + q];
+                    A1 = G[8 * NQ3 + q];
+                    A2 = G[9 * NQ3 + q];
+                }
             }
             else
             {
@@ -326,15 +345,24 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
                 G01 = gc[4];
                 G02 = gc[5];
                 G12 = gc[6];
+                if (ADV)
+                {
+                    A0 = gc[7 % NG];
+                    A1 = gc[8 % NG];
+                    A2 = gc[9 % NG];
+                }
             }
             v0[q]  = fma(G02, g2, fma(G01, g1, G00 * g0));
             v1[q]  = fma(G12, g2, fma(G11, g1, G01 * g0));
             v2r[k] = fma(G22, g2, fma(G12, g1, G02 * g0));
-            fr[k]  = a.lambda * W * ur[k];
+            if (ADV)
+                fr[k] = a.lambda * fma(W, ur[k], fma(A2, g2, fma(A1, g1, A0 * g0)));
+            else
+                fr[k] = a.lambda * W * ur[k];
             if (GEO == kGeoStream && k + 1 < NQ)
             {
 #pragma unroll
-                for (int cc = 0; cc < 7; ++cc)
+                for (int cc = 0; cc < NG; ++cc)
                     gc[cc] = gn[cc];
             }
         }
@@ -459,6 +487,15 @@ template <typename T, int NM, int NQ> static HexConst<T, NM, NQ> MakeHexConst(co
     return c;
 }
 
+// the kernel mode of a launch: gathered Helmholtz, LinearADR (local only; -1
+// if gathered) or local Helmholtz
+inline int HexMode(const nkb_op *op, bool gather)
+{
+    if (op->optype == NKB_LINEAR_ADR)
+        return gather ? -1 : kModeAdv;
+    return gather ? kModeGather : kModeLocal;
+}
+
 template <typename T, int NM, int GEO, int EPB>
 static int HexVariantLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStream_t s,
                             bool set_attr)
@@ -467,11 +504,16 @@ static int HexVariantLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, 
     const size_t bytes = HexSmem<T, NM, NQ, GEO, EPB>(op->gstride);
     if (bytes > 227 * 1024 || HexThreads<NQ, EPB>() > 1024)
         return SetError(NKB_ERR_UNSUPPORTED, "Hex variant needs %zu bytes of shared memory", bytes);
+    const int mode = HexMode(op, gather);
+    if (mode < 0)
+        return SetError(NKB_ERR_UNSUPPORTED, "LinearADR has no gathered Hex kernel");
     if (set_attr)
     {
-        NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm<T, NM, NQ, GEO, EPB, false>,
+        NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm<T, NM, NQ, GEO, EPB, kModeLocal>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
-        NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm<T, NM, NQ, GEO, EPB, true>,
+        NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm<T, NM, NQ, GEO, EPB, kModeGather>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+        NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm<T, NM, NQ, GEO, EPB, kModeAdv>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
         return NKB_OK;
     }
@@ -479,10 +521,13 @@ static int HexVariantLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, 
     if (nb == 0)
         return NKB_OK;
     const HexConst<T, NM, NQ> c = MakeHexConst<T, NM, NQ>(op);
-    if (gather)
-        k_hex_helm<T, NM, NQ, GEO, EPB, true><<<unsigned(nb), HexThreads<NQ, EPB>(), bytes, s>>>(a, c);
+    const unsigned th           = HexThreads<NQ, EPB>();
+    if (mode == kModeGather)
+        k_hex_helm<T, NM, NQ, GEO, EPB, kModeGather><<<unsigned(nb), th, bytes, s>>>(a, c);
+    else if (mode == kModeAdv)
+        k_hex_helm<T, NM, NQ, GEO, EPB, kModeAdv><<<unsigned(nb), th, bytes, s>>>(a, c);
     else
-        k_hex_helm<T, NM, NQ, GEO, EPB, false><<<unsigned(nb), HexThreads<NQ, EPB>(), bytes, s>>>(a, c);
+        k_hex_helm<T, NM, NQ, GEO, EPB, kModeLocal><<<unsigned(nb), th, bytes, s>>>(a, c);
     NKB_CUDA_TRY(cudaGetLastError());
     return NKB_OK;
 }

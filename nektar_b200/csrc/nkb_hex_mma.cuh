@@ -257,10 +257,12 @@ __device__ __forceinline__ void FetchCoeffs(const HexArgs<TV> &a, long e, int la
 // contraction, which is also the layout of the first transposed-gradient
 // contraction). Geometry is read with read-only loads in four batches of four
 // points per lane, all loads of a batch issued before any of its stores.
-template <typename TV, int NM, int NQ, bool GATHER>
+template <typename TV, int NM, int NQ, int MODE>
 __global__ void __launch_bounds__(32 * kMmaWarps, sizeof(TV) == 8 ? 3 : 4)
     k_hex_helm_mma(HexArgs<TV> a, const __grid_constant__ HexConst<double, NM, NQ> c)
 {
+    constexpr bool GATHER = MODE == kModeGather, ADV = MODE == kModeAdv;
+    constexpr int NG      = ADV ? 10 : 7; // packed values per point
     static_assert(NQ <= 8 && NM < NQ, "the DMMA Hex kernel covers nq <= 8");
     constexpr int NQ2 = NQ * NQ, NQ3 = NQ2 * NQ, NC = NM * NM * NM;
     extern __shared__ __align__(16) double msm[];
@@ -276,7 +278,7 @@ __global__ void __launch_bounds__(32 * kMmaWarps, sizeof(TV) == 8 ? 3 : 4)
     constexpr int CL = CubeLen<TC>();
     TC *xc = reinterpret_cast<TC *>(msm) + warp * kMmaCubes * CL; // coefficients
     TC *c0 = xc + CL, *c1 = c0 + CL, *c2 = c1 + CL;
-    const uint32_t gbytes = uint32_t(7 * NQ3 * sizeof(TV) + 15) & ~15u;
+    const uint32_t gbytes = uint32_t(NG * NQ3 * sizeof(TV) + 15) & ~15u;
 
     MmaTabs<NM, NQ> f;
     LoadMmaTabs<NM, NQ>(c, f, g, t);
@@ -333,7 +335,7 @@ __global__ void __launch_bounds__(32 * kMmaWarps, sizeof(TV) == 8 ? 3 : 4)
 #pragma unroll
         for (int tb = 0; tb < 8; tb += 2)
         {
-            double gv[4][7];
+            double gv[4][NG];
 #pragma unroll
             for (int p = 0; p < 4; ++p)
             {
@@ -341,7 +343,7 @@ __global__ void __launch_bounds__(32 * kMmaWarps, sizeof(TV) == 8 ? 3 : 4)
                 const bool real = cc < NQ && tile < NQ && g < NQ;
                 const int q     = real ? (cc * NQ + tile) * NQ + g : 0;
 #pragma unroll
-                for (int k = 0; k < 7; ++k)
+                for (int k = 0; k < NG; ++k)
                     gv[p][k] = real ? double(__ldg(G + k * NQ3 + q)) : 0.0;
             }
 #pragma unroll
@@ -355,7 +357,16 @@ __global__ void __launch_bounds__(32 * kMmaWarps, sizeof(TV) == 8 ? 3 : 4)
                 c0[ci]     = TC(fma(G02, x2, fma(G01, x1, G00 * x0)));
                 c2[ci]     = TC(fma(G12, x2, fma(G11, x1, G01 * x0)));
                 const double v2 = fma(G22, x2, fma(G12, x1, G02 * x0));
-                z[tile][h] = lam * W * double(c1[ci]);
+                if (ADV)
+                {
+                    const double adv = fma(gv[p][9 % NG], x2,
+                                           fma(gv[p][8 % NG], x1, gv[p][7 % NG] * x0));
+                    z[tile][h]       = lam * fma(W, double(c1[ci]), adv);
+                }
+                else
+                {
+                    z[tile][h] = lam * W * double(c1[ci]);
+                }
                 c1[ci]     = TC(v2);
             }
         }
@@ -423,34 +434,34 @@ static int HexMmaLaunch(const nkb_op *op, const HexArgs<TV> &a, bool gather, cud
     }
     else
     {
+        const int mode = HexMode(op, gather);
+        if (mode < 0)
+            return SetError(NKB_ERR_UNSUPPORTED, "LinearADR has no gathered Hex kernel");
+        void (*kerns[3])(HexArgs<TV>, const HexConst<double, NM, NQ>) = {
+            k_hex_helm_mma<TV, NM, NQ, kModeLocal>, k_hex_helm_mma<TV, NM, NQ, kModeGather>,
+            k_hex_helm_mma<TV, NM, NQ, kModeAdv>};
         if (set_attr)
         {
-            NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm_mma<TV, NM, NQ, false>,
-                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              int(bytes)));
-            NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm_mma<TV, NM, NQ, true>,
-                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              int(bytes)));
+            for (auto k : kerns)
+                NKB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  int(bytes)));
             return NKB_OK;
         }
         if (op->nelmt == 0)
             return NKB_OK;
         // persistent grid: as many CTAs as stay resident, fewer for small operators
-        static int s_per_sm = 0; // resident CTAs per SM of this instantiation
-        if (s_per_sm == 0)
+        static int s_per_sm[3] = {0, 0, 0}; // resident CTAs per SM of each mode
+        if (s_per_sm[mode] == 0)
         {
             int b = 0;
-            NKB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &b, k_hex_helm_mma<TV, NM, NQ, true>, 32 * kMmaWarps, bytes));
-            s_per_sm = std::max(b, 1);
+            NKB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kerns[mode],
+                                                                       32 * kMmaWarps, bytes));
+            s_per_sm[mode] = std::max(b, 1);
         }
         const long want = (long(op->nelmt) + kMmaWarps - 1) / kMmaWarps;
-        const long nb   = std::min<long>(want, long(s_per_sm) * SmCount(op->device));
+        const long nb   = std::min<long>(want, long(s_per_sm[mode]) * SmCount(op->device));
         const HexConst<double, NM, NQ> c = MakeHexConst<double, NM, NQ>(op);
-        if (gather)
-            k_hex_helm_mma<TV, NM, NQ, true><<<unsigned(nb), 32 * kMmaWarps, bytes, s>>>(a, c);
-        else
-            k_hex_helm_mma<TV, NM, NQ, false><<<unsigned(nb), 32 * kMmaWarps, bytes, s>>>(a, c);
+        kerns[mode]<<<unsigned(nb), 32 * kMmaWarps, bytes, s>>>(a, c);
         NKB_CUDA_TRY(cudaGetLastError());
         return NKB_OK;
     }

@@ -128,10 +128,12 @@ __device__ __forceinline__ void FetchCoeffs8(const HexArgs<TV> &a, long e, int l
     CpAsyncCommit();
 }
 
-template <typename TV, int NM, int NQ, bool GATHER, bool ISO>
+template <typename TV, int NM, int NQ, int MODE, bool ISO>
 __global__ void __launch_bounds__(64 * kMma2Pairs, 4)
     k_hex_helm_mma2(HexArgs<TV> a, const __grid_constant__ HexConst<double, NM, NQ> c)
 {
+    constexpr bool GATHER = MODE == kModeGather, ADV = MODE == kModeAdv;
+    constexpr int NG      = ADV ? 10 : 7; // packed values per point
     static_assert(NQ <= 8 && NM < NQ, "the DMMA Hex kernel covers nq <= 8");
     constexpr int NQ2 = NQ * NQ, NQ3 = NQ2 * NQ, NC = NM * NM * NM;
     extern __shared__ __align__(16) double msm[];
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(64 * kMma2Pairs, 4)
     double *c0 = msm + pair * kMmaCubes * kMmaCube + kMmaCube, *c1 = c0 + kMmaCube,
            *c2 = c1 + kMmaCube;
     TV *xc = reinterpret_cast<TV *>(c0 - kMmaCube);
-    const uint32_t gbytes = uint32_t(7 * NQ3 * sizeof(TV) + 15) & ~15u;
+    const uint32_t gbytes = uint32_t(NG * NQ3 * sizeof(TV) + 15) & ~15u;
 
     MmaTabs<NM, NQ> f;
     LoadMmaTabs<NM, NQ>(c, f, g, t);
@@ -201,7 +203,7 @@ __global__ void __launch_bounds__(64 * kMma2Pairs, 4)
         for (int i = 0; i < 4; ++i) // batches of the two points (c = 2t, 2t + 1) of one tile
         {
             const int tile = tile0 + i;
-            double gv[2][7];
+            double gv[2][NG];
 #pragma unroll
             for (int hh = 0; hh < 2; ++hh)
             {
@@ -209,7 +211,7 @@ __global__ void __launch_bounds__(64 * kMma2Pairs, 4)
                 const bool real = cc < NQ && tile < NQ && g < NQ;
                 const int q     = real ? (cc * NQ + tile) * NQ + g : 0;
 #pragma unroll
-                for (int k = 0; k < 7; ++k)
+                for (int k = 0; k < NG; ++k)
                     gv[hh][k] = real ? double(__ldg(G + k * NQ3 + q)) : 0.0;
             }
 #pragma unroll
@@ -222,7 +224,16 @@ __global__ void __launch_bounds__(64 * kMma2Pairs, 4)
                 c0[ci]          = fma(G02, x2, fma(G01, x1, G00 * x0));
                 c2[ci]          = fma(G12, x2, fma(G11, x1, G01 * x0));
                 const double v2 = fma(G22, x2, fma(G12, x1, G02 * x0));
-                z[i][hh]        = lam * W * c1[ci];
+                if (ADV)
+                {
+                    const double adv = fma(gv[hh][9 % NG], x2,
+                                           fma(gv[hh][8 % NG], x1, gv[hh][7 % NG] * x0));
+                    z[i][hh]         = lam * fma(W, c1[ci], adv);
+                }
+                else
+                {
+                    z[i][hh] = lam * W * c1[ci];
+                }
                 c1[ci]          = v2;
             }
         }
@@ -281,31 +292,33 @@ static int HexMma2LaunchIso(const nkb_op *op, const HexArgs<TV> &a, bool gather,
 {
     constexpr int NQ   = NM + 1;
     const size_t bytes = size_t(kMma2Pairs) * kMmaCubes * kMmaCube * sizeof(double);
+    const int mode = HexMode(op, gather);
+    if (mode < 0)
+        return SetError(NKB_ERR_UNSUPPORTED, "LinearADR has no gathered Hex kernel");
+    void (*kerns[3])(HexArgs<TV>, const HexConst<double, NM, NQ>) = {
+        k_hex_helm_mma2<TV, NM, NQ, kModeLocal, ISO>, k_hex_helm_mma2<TV, NM, NQ, kModeGather, ISO>,
+        k_hex_helm_mma2<TV, NM, NQ, kModeAdv, ISO>};
     if (set_attr)
     {
-        NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm_mma2<TV, NM, NQ, false, ISO>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
-        NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm_mma2<TV, NM, NQ, true, ISO>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+        for (auto k : kerns)
+            NKB_CUDA_TRY(
+                cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
         return NKB_OK;
     }
     if (op->nelmt == 0)
         return NKB_OK;
-    static int s_per_sm = 0; // resident CTAs per SM of this instantiation
-    if (s_per_sm == 0)
+    static int s_per_sm[3] = {0, 0, 0}; // resident CTAs per SM of each mode
+    if (s_per_sm[mode] == 0)
     {
         int b = 0;
-        NKB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &b, k_hex_helm_mma2<TV, NM, NQ, true, ISO>, 64 * kMma2Pairs, bytes));
-        s_per_sm = std::max(b, 1);
+        NKB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kerns[mode],
+                                                                   64 * kMma2Pairs, bytes));
+        s_per_sm[mode] = std::max(b, 1);
     }
     const long want = (long(op->nelmt) + kMma2Pairs - 1) / kMma2Pairs;
-    const long nb   = std::min<long>(want, long(s_per_sm) * SmCount(op->device));
+    const long nb   = std::min<long>(want, long(s_per_sm[mode]) * SmCount(op->device));
     const HexConst<double, NM, NQ> c = MakeHexConst<double, NM, NQ>(op);
-    if (gather)
-        k_hex_helm_mma2<TV, NM, NQ, true, ISO><<<unsigned(nb), 64 * kMma2Pairs, bytes, s>>>(a, c);
-    else
-        k_hex_helm_mma2<TV, NM, NQ, false, ISO><<<unsigned(nb), 64 * kMma2Pairs, bytes, s>>>(a, c);
+    kerns[mode]<<<unsigned(nb), 64 * kMma2Pairs, bytes, s>>>(a, c);
     NKB_CUDA_TRY(cudaGetLastError());
     return NKB_OK;
 }

@@ -477,6 +477,12 @@ int LaunchGeneric3(const nkb_op *op, const T *in, const T *in1, const T *in2, T 
         case NKB_IPRODUCT_DERIV:
             return LaunchGenericShape<GK_IPD, T>(op, a, s);
         case NKB_LINEAR_ADR:
+            if (ColKernels() && !gmap)
+            {
+                const int rc = LaunchColHelm<T>(op, a, s);
+                if (rc != kNotCovered)
+                    return rc;
+            }
             return LaunchGenericShape<GK_ADR, T>(op, a, s);
         default:
         {

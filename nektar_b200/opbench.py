@@ -41,6 +41,10 @@ def main():
                           "op_GB_s": prof["op_bytes"] / prof["op_ms"] / 1e6}))
         return
     op = nb.Operator(a.op, m, precision=a.precision)
+    if a.op == "linear_adr":
+        op.set_factors(1.0)
+        i = np.arange(m.nelmt * m.nt)
+        op.set_varcoeffs(np.sin(0.01 * i), np.cos(0.01 * i), np.full(i.size, 0.5))
     dt = torch.float64 if a.precision == "fp64" else torch.float32
     x = torch.rand(op.in_size, dtype=dt, device="cuda")
     outs = [torch.empty(op.out_size, dtype=dt, device="cuda")
@@ -56,12 +60,13 @@ def main():
     e1.record(s)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / a.iters
-    ncomp = {"helmholtz": 7, "physderiv": 9, "iproduct": 1, "bwdtrans": 0}[a.op]
+    ncomp = {"helmholtz": 7, "linear_adr": 10, "physderiv": 9, "iproduct_deriv": 9,
+             "iproduct": 1, "bwdtrans": 0}[a.op]
     esz = 8 if a.precision == "fp64" else 4
     byts = m.nelmt * esz * (ncomp * m.nt + (op.in_size + len(outs) * op.out_size) / m.nelmt)
     print(json.dumps({"op": a.op, "shape": a.shape, "n": a.n, "P": a.p, "nelmt": m.nelmt,
-                      "precision": a.precision, "ms": ms, "GB_s": byts / ms / 1e6,
-                      "GDOF_s": m.nelmt * m.nc / ms / 1e6}))
+                      "precision": a.precision, "kernel": op.kernel(), "ms": ms,
+                      "GB_s": byts / ms / 1e6, "GDOF_s": m.nelmt * m.nc / ms / 1e6}))
 
 
 if __name__ == "__main__":

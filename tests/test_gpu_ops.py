@@ -148,6 +148,41 @@ def test_tuned_and_generic_hex_helmholtz_agree(monkeypatch, n, nm, variant):
     assert rel_l2(tuned(x), generic(x)) < 1e-13
 
 
+@pytest.mark.parametrize("n,nm", [(1, 5), (3, 7), (2, 9), (1, 11), (5, 2)])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+def test_hex_kernel_variants_linear_adr_match_oracle(monkeypatch, n, nm, variant):
+    """LinearADR through every variant of the tuned Hex kernel (its advection
+    mode) against the oracle; a variant without room for the three extra
+    geometry rows falls back to the generic kernel."""
+    m = nb.BoxMesh("hex", n, nm, nm + 1, amp=0.05)
+    rng = np.random.default_rng(nm + 100)
+    x = rng.uniform(-1, 1, m.nelmt * m.nc)
+    vel = rng.uniform(-1, 1, 3 * m.nelmt * m.nt)
+    k = m.nelmt * m.nt
+    monkeypatch.setenv("NKB_HEX_VARIANT", str(variant))
+    op = nb.Operator("linear_adr", m)
+    op.set_factors(0.6)
+    op.set_varcoeffs(vel[:k], vel[k:2 * k], vel[2 * k:])
+    yo = O.linear_adr("hex", nm, m.nq, m.nelmt, _oracle_T(m), m.jac, m.df, 0.6, vel, x, True)
+    assert rel_l2(op(x), yo) < TOL64
+
+
+@pytest.mark.parametrize("shape,nm", [("prism", 3), ("prism", 7), ("prism", 11), ("tet", 4),
+                                      ("tet", 8), ("tet", 11)])
+def test_column_kernel_linear_adr_matches_oracle(shape, nm):
+    m = nb.BoxMesh(shape, 2, nm, nm + 1, amp=0.05)
+    rng = np.random.default_rng(nm + 200)
+    x = rng.uniform(-1, 1, m.nelmt * m.nc)
+    vel = rng.uniform(-1, 1, 3 * m.nelmt * m.nt)
+    k = m.nelmt * m.nt
+    op = nb.Operator("linear_adr", m)
+    assert op.kernel().startswith("k_col_helm")
+    op.set_factors(-2.0)
+    op.set_varcoeffs(vel[:k], vel[k:2 * k], vel[2 * k:])
+    yo = O.linear_adr(shape, nm, m.nq, m.nelmt, _oracle_T(m), m.jac, m.df, -2.0, vel, x, True)
+    assert rel_l2(op(x), yo) < TOL64
+
+
 @pytest.mark.parametrize("shape,n,nm", [("prism", 2, 4), ("tet", 2, 5), ("prism", 1, 9), ("tet", 1, 11)])
 def test_static_and_runtime_size_generic_helmholtz_agree(monkeypatch, shape, n, nm):
     """Prism / Tet Helmholtz with compile-time sizes against the same kernel
