@@ -1,0 +1,114 @@
+"""Helmholtz solve of a Nektar++ session on the B200 path, the sequence of
+the reference's Helmholtz3D demo (library/Demos/MultiRegions/Helmholtz3D.cpp):
+
+    forcing f at the quadrature points            (the "Forcing" function)
+    b = -IProductWRTBase(f)                        (ContField::v_HelmSolve,
+                                                    ContField.cpp:797-821)
+    x = Dirichlet values (boundary-constrained projection), zero elsewhere
+    solve (L + lambda M) x = b with the lifting     (GlobalLinSysIterativeFull)
+    u = BwdTrans(x)
+    L_inf, L_2, H_1 errors against "ExactSolution" (ExpList::Linf / L2 / H1)
+
+Every operator application and the CG run on the device through the C ABI
+(nektar_b200.Operator, GlobalLinSys); the host reads the session, builds the
+geometry, the assembly and the Dirichlet values, and evaluates the session's
+functions at the quadrature points.
+
+    python -m nektar_b200.helmsolve session.xml [--tol 1e-13] [--fld out.fld]
+"""
+import argparse
+import json
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class HelmResult:
+    coeffs: np.ndarray  # local coefficients (element-major)
+    phys: np.ndarray  # solution at the quadrature points
+    iterations: int
+    rel_residual: float
+    converged: bool
+    linf: float = None
+    l2: float = None
+    h1: float = None
+    solve_ms: float = None
+
+
+def errors(mesh, u, exact, device=0):
+    """(L_inf, L_2, H_1) of u against exact at the quadrature points:
+    ExpList::Linf, ExpList::L2 and ExpList::H1 (StdExpansion::L2 / H1 per
+    element, integrals with the element's weights and Jacobian; H1 adds the
+    squared L2 norms of the physical derivatives of u - exact)."""
+    import nektar_b200 as nb
+    d = u - exact
+    W = mesh.quad_weights()
+    linf = float(np.max(np.abs(d)))
+    l2sq = float(np.sum(W * d * d))
+    grad = nb.Operator("physderiv", mesh, device=device)(d)
+    h1sq = l2sq + sum(float(np.sum(W * g * g)) for g in grad)
+    return linf, float(np.sqrt(l2sq)), float(np.sqrt(h1sq))
+
+
+def helm_solve(session, device=0, tol=1e-12, maxit=5000, check_interval=16, raise_on_maxit=True):
+    import nektar_b200 as nb
+    from .meshgraph import SessionMesh
+    mesh = SessionMesh(session)
+    if "Lambda" not in session.parameters:
+        raise ValueError("the session defines no Lambda parameter")
+    lam = float(session.parameters["Lambda"])
+    forcing = session.function("Forcing")
+    if forcing is None:
+        raise ValueError("the session defines no Forcing function")
+    f = forcing.evaluate(*mesh.xyz)
+    b_loc = -nb.Operator("iproduct", mesh, device=device)(f)
+    H = nb.Operator("helmholtz", mesh, device=device)
+    H.set_factors(lam)
+    S = nb.GlobalLinSys([H], mesh.gmap, mesh.nglob, mesh.ndir, sign=mesh.sign, device=device)
+    x0 = mesh.dirichlet_local()
+    t0 = time.perf_counter()
+    x, rep = S.solve(b_loc, x0, tol=tol, maxit=maxit, check_interval=check_interval,
+                     raise_on_maxit=raise_on_maxit)
+    ms = (time.perf_counter() - t0) * 1e3
+    u = nb.Operator("bwdtrans", mesh, device=device)(x)
+    res = HelmResult(x, u, rep.iterations, rep.rel_residual, bool(rep.converged), solve_ms=ms)
+    exact = session.function("ExactSolution")
+    if exact is not None:
+        res.linf, res.l2, res.h1 = errors(mesh, u, exact.evaluate(*mesh.xyz), device)
+    res.mesh = mesh
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("session")
+    ap.add_argument("--tol", type=float, default=1e-12)
+    ap.add_argument("--maxit", type=int, default=5000)
+    ap.add_argument("--fld", default=None, help="write the solution as a .fld directory")
+    ap.add_argument("--json", action="store_true")
+    a = ap.parse_args()
+    from .session import read_session
+    s = read_session(a.session)
+    r = helm_solve(s, tol=a.tol, maxit=a.maxit)
+    if a.fld:
+        from .fieldio import write_fld
+        write_fld(a.fld, r.mesh, {"u": r.coeffs})
+    if a.json:
+        print(json.dumps({"session": s.name, "iterations": r.iterations,
+                          "rel_residual": r.rel_residual, "linf": r.linf, "l2": r.l2,
+                          "h1": r.h1, "solve_ms": r.solve_ms}))
+        return
+    print("Solving 3D Helmholtz:")
+    print("  - Lambda        : %g" % s.parameters["Lambda"])
+    print("  - No. modes     : %d" % r.mesh.nm)
+    print("  - CG iterations : %d (relative residual %.3g)" % (r.iterations, r.rel_residual))
+    if r.l2 is not None:
+        print("L infinity error: %g" % r.linf)
+        print("L 2 error:        %g" % r.l2)
+        print("H 1 error:        %g" % r.h1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,123 @@
+"""Session front end on the CPU: the expression grammar, the XML reader,
+hexahedral element frames, the oriented C0 assembly, and - through the
+oracle - the whole discretisation against the reference's recorded errors
+(library/Demos/MultiRegions/Tests/Helmholtz3D_CG_Hex.tst: L2 1.11818e-07,
+Linf 5.66374e-07, tolerance 1e-12, for Helmholtz3D_Hex_P6.xml: the unit cube
+cut into 2^3 hexahedra, NUMMODES 6, Lambda 1, u = sin(pi x/2) sin(pi y/2)
+sin(pi z/2) on the boundary)."""
+import os
+from collections import defaultdict
+
+import numpy as np
+import pytest
+
+from nektar_b200.expr import Expression, ExpressionError, evaluate_parameters
+from nektar_b200.meshgraph import SessionMesh
+from nektar_b200.session import SessionError, read_session, write_hex_box_session
+from oracle import oracle as O
+from tests.session_oracle import oracle_helm_solve
+
+U = "sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)"
+F = "-(Lambda + 3*PI*PI/4)*sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)"
+HEX_L2, HEX_LINF = 1.11818e-07, 5.66374e-07  # Helmholtz3D_CG_Hex.tst
+REF_HEX = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Hex_P6.xml"
+
+
+def test_expression_grammar():
+    assert Expression("-x^2").evaluate(3.0) == -9.0  # '-' applies to the whole term
+    assert Expression("2^3^2").evaluate() == 512.0  # '^' is right associative
+    assert Expression("1 - -x").evaluate(2.0) == 3.0
+    assert Expression("x < 1 && y >= 2 || 0").evaluate(0.5, 2.0) == 1.0
+    assert Expression("fmod(7, 3) + abs(-2) + sqrt(PI_4 * 4 / PI)").evaluate() == 4.0
+    v = Expression(F, {"Lambda": 2.5}).evaluate(0.2, 0.4, 0.6)
+    assert np.isclose(v, -(2.5 + 3 * np.pi ** 2 / 4) * np.prod(np.sin(np.pi / 2 * np.array([.2, .4, .6]))))
+    x = np.linspace(0, 1, 7)
+    assert Expression("x*y").evaluate(x, 2.0).shape == (7,)
+    for bad in ("2*-3", "foo + 1", "awgn(1)", "sin(1, 2)", "(1"):
+        with pytest.raises(ExpressionError):
+            Expression(bad).evaluate()
+    assert evaluate_parameters([("A", "2"), ("B", "A^2 + PI*0")]) == {"A": 2.0, "B": 4.0}
+
+
+def _session(n=2, nm=6, seed=None):
+    return read_session(write_hex_box_session(n, nm, 1.0, U, F, U, shuffle_seed=seed))
+
+
+def test_reader_and_mesh_counts():
+    s = _session(3, 5)
+    assert s.parameters["Lambda"] == 1.0 and s.variables == ["u"]
+    assert len(s.geometry.elements) == 27 and len(s.geometry.vertices) == 64
+    m = SessionMesh(s)
+    assert (m.nglob, m.ndir) == (13 ** 3, 13 ** 3 - 11 ** 3)
+    assert m.jac.shape == (27 * 216,) and m.df.shape == (9, 27 * 216)
+    assert np.isclose(m.quad_weights().sum(), 1.0)  # volume of the unit cube
+
+
+@pytest.mark.parametrize("seed", [None, 1, 2])
+def test_assembly_is_continuous_across_all_relative_orientations(seed):
+    """A random global vector scattered with the map and signs is one
+    continuous function: it takes one value wherever elements share a
+    quadrature point, with element frames rotated at random (seeded)."""
+    m = SessionMesh(_session(3, 6, seed))
+    if seed is not None:
+        assert (m.sign < 0).sum() > 500  # the orientation signs are exercised
+    xg = np.random.default_rng(7).uniform(-1, 1, m.nglob)
+    u = O.bwdtrans("hex", m.nm, m.nq, m.nelmt, m.T["b"], m.sign * xg[m.gmap])
+    vals = defaultdict(list)
+    for p, v in zip(np.round(m.xyz.T, 9), u):
+        vals[tuple(p)].append(v)
+    assert max(max(v) - min(v) for v in vals.values()) < 1e-14
+
+
+def test_dirichlet_projection_is_exact_for_polynomials():
+    """A trace in the discrete space is reproduced by the boundary-constrained
+    projection: quadratic data -> the lifted field equals it on the boundary."""
+    s = read_session(write_hex_box_session(2, 4, 1.0, "x*x + 2*y*z - z", "0", "0", shuffle_seed=3))
+    m = SessionMesh(s)
+    u = O.bwdtrans("hex", m.nm, m.nq, m.nelmt, m.T["b"], m.dirichlet_local())
+    x, y, z = m.xyz
+    on = (np.isclose(x, 0) | np.isclose(x, 1) | np.isclose(y, 0) | np.isclose(y, 1) |
+          np.isclose(z, 0) | np.isclose(z, 1))
+    assert np.abs(u[on] - (x * x + 2 * y * z - z)[on]).max() < 1e-13
+
+
+@pytest.mark.parametrize("seed", [None, 4])
+def test_oracle_solve_reproduces_reference_record(seed):
+    _, linf, l2 = oracle_helm_solve(_session(2, 6, seed))
+    assert abs(l2 - HEX_L2) < 1e-12 and abs(linf - HEX_LINF) < 1e-12
+
+
+@pytest.mark.skipif(not os.path.exists(REF_HEX), reason="reference tree not mounted")
+def test_reference_session_file_reads_and_reproduces_its_record():
+    s = read_session(REF_HEX)
+    assert len(s.geometry.elements) == 8 and s.nummodes == {0: 6}
+    _, linf, l2 = oracle_helm_solve(s)
+    assert abs(l2 - HEX_L2) < 1e-12 and abs(linf - HEX_LINF) < 1e-12
+
+
+def test_reader_rejects_what_the_path_does_not_take():
+    txt = write_hex_box_session(1, 4, 1.0, U, F, U)
+    with pytest.raises(SessionError):
+        read_session(txt.replace('NUMMODES="4"', 'NUMMODES="4,5,6"'))
+    with pytest.raises(SessionError):
+        read_session(txt.replace("</GEOMETRY>", '<CURVED><E ID="0" EDGEID="0" NUMPOINTS="3" '
+                                 'TYPE="PolyEvenlySpaced"> 0 0 0 0.5 0 0 1 0 0 </E></CURVED>'
+                                 "</GEOMETRY>"))
+    s = read_session(txt.replace('<D VAR="u"', '<N VAR="u"'))
+    with pytest.raises(SessionError):
+        SessionMesh(s)
+
+
+def test_fld_round_trip(tmp_path):
+    from nektar_b200.fieldio import read_fld, write_fld
+    s = _session(2, 5, seed=2)
+    m = SessionMesh(s)
+    coeffs = np.random.default_rng(1).uniform(-1, 1, m.nelmt * m.nc)
+    out = str(tmp_path / "sol.fld")
+    write_fld(out, m, {"u": coeffs})
+    assert sorted(os.listdir(out)) == ["Info.xml", "P0000000.fld"]
+    (d,) = read_fld(out)
+    assert d["SHAPE"] == "Hexahedron" and d["NUMMODESPERDIR"] == "UNIORDER:5,5,5"
+    assert d["COMPRESSED"] == "B64Z-LittleEndian" and d["BITSIZE"] == "64"
+    assert d["ids"] == list(range(8)) and d["fields"] == ["u"]
+    assert np.array_equal(d["data"], coeffs)
