@@ -230,11 +230,14 @@ void nkb_op_destroy(nkb_op *op);
  * call: in/out are the concatenated per-collection local vectors in the
  * order given (PhysDeriv: each collection's three derivatives consecutively).
  * The collections run concurrently on nstreams streams (0: 4), largest first,
- * captured once as a CUDA graph per (in, out) pair. */
+ * captured once as a CUDA graph per (in, out) pair. All operators of a batch
+ * share one type and one precision; an FP32 batch is applied with
+ * nkb_batch_apply_f32 (device pointers). */
 typedef struct nkb_batch nkb_batch;
 int nkb_batch_create(nkb_op *const *ops, int nops, int nstreams, nkb_batch **batch);
 int nkb_batch_sizes(const nkb_batch *batch, long *in_size, long *out_size);
 int nkb_batch_apply(nkb_batch *batch, const double *in, double *out, int flags, void *stream);
+int nkb_batch_apply_f32(nkb_batch *batch, const float *in, float *out, void *stream);
 /* device time of the last nkb_batch_apply (waits for it) */
 int nkb_batch_last_ms(nkb_batch *batch, float *ms);
 void nkb_batch_destroy(nkb_batch *batch);

@@ -260,6 +260,7 @@ class Batch:
 
     def __init__(self, ops, nstreams=4):
         self.ops = list(ops)
+        self.precision = self.ops[0].precision
         handles = (ctypes.c_void_p * len(self.ops))(*[o.h.value for o in self.ops])
         h = ctypes.c_void_p()
         check(lib().nkb_batch_create(handles, len(self.ops), int(nstreams), ctypes.byref(h)))
@@ -278,7 +279,11 @@ class Batch:
         return y
 
     def apply_device(self, x_ptr, y_ptr, stream=None):
-        check(lib().nkb_batch_apply(self.h, x_ptr, y_ptr, DEVICE_PTRS, stream))
+        """Device pointers; FP64 or FP32 per the operators' precision."""
+        if self.precision == FP32:
+            check(lib().nkb_batch_apply_f32(self.h, x_ptr, y_ptr, stream))
+        else:
+            check(lib().nkb_batch_apply(self.h, x_ptr, y_ptr, DEVICE_PTRS, stream))
 
     def last_ms(self):
         ms = ctypes.c_float(0.0)

@@ -98,6 +98,7 @@ SIGNATURES = {
     "nkb_batch_create": (c_int, [P(c_void_p), c_int, c_int, P(c_void_p)]),
     "nkb_batch_sizes": (c_int, [c_void_p, P(c_long), P(c_long)]),
     "nkb_batch_apply": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "nkb_batch_apply_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "nkb_batch_last_ms": (c_int, [c_void_p, P(c_float)]),
     "nkb_batch_destroy": (None, [c_void_p]),
     "nkb_cg_begin": (c_int, [c_void_p, c_void_p, c_void_p, P(CGOpts), c_int, c_void_p]),

@@ -25,7 +25,8 @@ using namespace nkb;
 
 struct nkb_batch
 {
-    int device = 0;
+    int device    = 0;
+    int precision = NKB_FP64; // of every operator in the batch
     std::vector<nkb_op *> ops;
     std::vector<long> in_off, out_off;
     long in_size = 0, out_size = 0;
@@ -55,7 +56,7 @@ double Cost(const nkb_op *op)
     return double(op->nelmt) * comps * op->nt + double(in) + nouts * double(out);
 }
 
-int LaunchAll(nkb_batch *B, const double *in, double *out, cudaStream_t s)
+template <typename T> int LaunchAll(nkb_batch *B, const T *in, T *out, cudaStream_t s)
 {
     NKB_CUDA_TRY(cudaEventRecord(B->fork, s));
     for (cudaStream_t w : B->streams)
@@ -63,9 +64,9 @@ int LaunchAll(nkb_batch *B, const double *in, double *out, cudaStream_t s)
     for (int c : B->order)
     {
         const nkb_op *op = B->ops[c];
-        double *o        = out + B->out_off[c];
+        T *o             = out + B->out_off[c];
         const long no    = long(op->nelmt) * (op->optype == NKB_PHYSDERIV ? op->nt : 0);
-        int rc = LaunchOp<double>(op, in + B->in_off[c], o, no ? o + no : nullptr,
+        int rc = LaunchOp<T>(op, in + B->in_off[c], o, no ? o + no : nullptr,
                                   no ? o + 2 * no : nullptr, nullptr, nullptr,
                                   B->streams[B->stream_of[c]]);
         if (rc)
@@ -78,6 +79,40 @@ int LaunchAll(nkb_batch *B, const double *in, double *out, cudaStream_t s)
     }
     return NKB_OK;
 }
+// launch the batch's graph on `run`, capturing it first when (in, out)
+// changed; timed by ev0 / ev1
+template <typename T> int RunGraph(nkb_batch *B, const T *din, T *dout, cudaStream_t run)
+{
+    // one graph per (input, output) pair; re-captured when they change
+    if (!B->graph || B->g_in != din || B->g_out != dout)
+    {
+        if (B->graph)
+            cudaGraphExecDestroy(B->graph);
+        B->graph = nullptr;
+        cudaStream_t cap;
+        NKB_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaGraph_t g;
+        cudaError_t ce = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        int rc         = ce == cudaSuccess ? LaunchAll<T>(B, din, dout, cap) : NKB_OK;
+        cudaError_t ee = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (rc)
+            return rc;
+        if (ce != cudaSuccess || ee != cudaSuccess)
+            return SetError(NKB_ERR_CUDA, "nkb_batch_apply: capture: %s",
+                            cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+        ce = cudaGraphInstantiate(&B->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess)
+            return SetError(NKB_ERR_CUDA, "nkb_batch_apply: instantiate: %s", cudaGetErrorString(ce));
+        B->g_in  = din;
+        B->g_out = dout;
+    }
+    NKB_CUDA_TRY(cudaEventRecord(B->ev0, run));
+    NKB_CUDA_TRY(cudaGraphLaunch(B->graph, run));
+    NKB_CUDA_TRY(cudaEventRecord(B->ev1, run));
+    return NKB_OK;
+}
 } // namespace
 
 extern "C" int nkb_batch_create(nkb_op *const *ops, int nops, int nstreams, nkb_batch **out)
@@ -88,17 +123,19 @@ extern "C" int nkb_batch_create(nkb_op *const *ops, int nops, int nstreams, nkb_
     *out = nullptr;
     for (int c = 0; c < nops; ++c)
     {
-        if (!ops[c] || ops[c]->precision != NKB_FP64)
-            return SetError(NKB_ERR_INVALID, "nkb_batch_create: op %d is not an FP64 operator", c);
-        if (ops[c]->optype != ops[0]->optype || ops[c]->device != ops[0]->device)
-            return SetError(NKB_ERR_INVALID,
-                            "nkb_batch_create: all operators must be of one type on one device");
+        if (!ops[c])
+            return SetError(NKB_ERR_INVALID, "nkb_batch_create: op %d is NULL", c);
+        if (ops[c]->optype != ops[0]->optype || ops[c]->device != ops[0]->device ||
+            ops[c]->precision != ops[0]->precision)
+            return SetError(NKB_ERR_INVALID, "nkb_batch_create: all operators must be of one "
+                                             "type and precision on one device");
     }
     if (nstreams <= 0)
         nstreams = 4;
     nstreams     = std::min(nstreams, nops);
     nkb_batch *B = new nkb_batch();
     B->device    = ops[0]->device;
+    B->precision = ops[0]->precision;
     B->ops.assign(ops, ops + nops);
     B->nout = ops[0]->optype == NKB_PHYSDERIV ? 3 : 1;
     for (nkb_op *op : B->ops)
@@ -160,6 +197,8 @@ extern "C" int nkb_batch_apply(nkb_batch *B, const double *in, double *out, int 
     ClearError();
     if (!B || !in || !out)
         return SetError(NKB_ERR_INVALID, "nkb_batch_apply: NULL argument");
+    if (B->precision != NKB_FP64)
+        return SetError(NKB_ERR_INVALID, "nkb_batch_apply: FP32 batch; use nkb_batch_apply_f32");
     NKB_CUDA_TRY(cudaSetDevice(B->device));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const bool legacy = s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread;
@@ -182,34 +221,9 @@ extern "C" int nkb_batch_apply(nkb_batch *B, const double *in, double *out, int 
         NKB_CUDA_TRY(cudaEventRecord(B->order_ev, s));
         NKB_CUDA_TRY(cudaStreamWaitEvent(run, B->order_ev, 0));
     }
-    // one graph per (input, output) pair; re-captured when they change
-    if (!B->graph || B->g_in != din || B->g_out != dout)
-    {
-        if (B->graph)
-            cudaGraphExecDestroy(B->graph);
-        B->graph = nullptr;
-        cudaStream_t cap;
-        NKB_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-        cudaGraph_t g;
-        cudaError_t ce = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-        int rc         = ce == cudaSuccess ? LaunchAll(B, din, dout, cap) : NKB_OK;
-        cudaError_t ee = cudaStreamEndCapture(cap, &g);
-        cudaStreamDestroy(cap);
-        if (rc)
-            return rc;
-        if (ce != cudaSuccess || ee != cudaSuccess)
-            return SetError(NKB_ERR_CUDA, "nkb_batch_apply: capture: %s",
-                            cudaGetErrorString(ce != cudaSuccess ? ce : ee));
-        ce = cudaGraphInstantiate(&B->graph, g, 0);
-        cudaGraphDestroy(g);
-        if (ce != cudaSuccess)
-            return SetError(NKB_ERR_CUDA, "nkb_batch_apply: instantiate: %s", cudaGetErrorString(ce));
-        B->g_in  = din;
-        B->g_out = dout;
-    }
-    NKB_CUDA_TRY(cudaEventRecord(B->ev0, run));
-    NKB_CUDA_TRY(cudaGraphLaunch(B->graph, run));
-    NKB_CUDA_TRY(cudaEventRecord(B->ev1, run));
+    int rc = RunGraph<double>(B, din, dout, run);
+    if (rc)
+        return rc;
     if (flags & NKB_HOST_PTRS)
     {
         NKB_CUDA_TRY(cudaMemcpyAsync(out, dout, B->out_size * sizeof(double),
@@ -217,6 +231,33 @@ extern "C" int nkb_batch_apply(nkb_batch *B, const double *in, double *out, int 
         NKB_CUDA_TRY(cudaStreamSynchronize(run));
     }
     else if (legacy)
+    {
+        NKB_CUDA_TRY(cudaEventRecord(B->order_ev, run));
+        NKB_CUDA_TRY(cudaStreamWaitEvent(s, B->order_ev, 0));
+    }
+    return NKB_OK;
+}
+
+extern "C" int nkb_batch_apply_f32(nkb_batch *B, const float *in, float *out, void *stream)
+{
+    ClearError();
+    if (!B || !in || !out)
+        return SetError(NKB_ERR_INVALID, "nkb_batch_apply_f32: NULL argument");
+    if (B->precision != NKB_FP32)
+        return SetError(NKB_ERR_INVALID, "nkb_batch_apply_f32: FP64 batch; use nkb_batch_apply");
+    NKB_CUDA_TRY(cudaSetDevice(B->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const bool legacy = s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread;
+    cudaStream_t run  = legacy ? B->own : s;
+    if (legacy)
+    {
+        NKB_CUDA_TRY(cudaEventRecord(B->order_ev, s));
+        NKB_CUDA_TRY(cudaStreamWaitEvent(run, B->order_ev, 0));
+    }
+    int rc = RunGraph<float>(B, in, out, run);
+    if (rc)
+        return rc;
+    if (legacy)
     {
         NKB_CUDA_TRY(cudaEventRecord(B->order_ev, run));
         NKB_CUDA_TRY(cudaStreamWaitEvent(s, B->order_ev, 0));

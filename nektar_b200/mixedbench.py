@@ -4,7 +4,7 @@ each and 10000 cells split into 6 tets each (110000 elements), P drawn in
 {2..10} per cell, curved by the box map, coefficients uniform in [-1, 1].
 One collection per (shape, P), all applied by one batched call.
 
-    python -m nektar_b200.mixedbench [--iters 10] [--cpu]
+    python -m nektar_b200.mixedbench [--iters 10] [--cpu] [--precision fp32]
 
 Prints one JSON line: local GDOF/s of the batched apply (device time, CUDA
 events), the same collections applied one after another on one stream, the
@@ -30,6 +30,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--streams", type=int, default=4)
     ap.add_argument("--cpu", action="store_true", help="time the reference CPU kernels too")
+    ap.add_argument("--precision", default="fp64", choices=("fp64", "fp32"))
     a = ap.parse_args()
     import torch
 
@@ -40,11 +41,12 @@ def main():
     ops, groups, cpu_s, cpu_threads = [], [], 0.0, None
     t_setup = time.perf_counter()
     for (shape, p, cells), m in zip(mm.groups, mm.meshes()):
-        op = nb.Operator("helmholtz", m)
+        op = nb.Operator("helmholtz", m, precision=a.precision)
         op.set_factors(1.0)
         ops.append(op)
+        esz = 8 if a.precision == "fp64" else 4
         groups.append({"shape": shape, "P": p, "elements": m.nelmt, "dofs": m.nelmt * m.nc,
-                       "bytes": m.nelmt * 8 * (7 * m.nt + 2 * m.nc)})
+                       "bytes": m.nelmt * esz * (7 * m.nt + 2 * m.nc)})
         if a.cpu:
             from oracle import ref
             cpu_threads = len(os.sched_getaffinity(0))
@@ -64,8 +66,10 @@ def main():
     B = nb.Batch(ops, nstreams=a.streams)
     dofs = sum(g["dofs"] for g in groups)
     byts = sum(g["bytes"] for g in groups)
-    x = torch.rand(B.in_size, dtype=torch.float64, device="cuda") * 2 - 1
-    y = torch.empty(B.out_size, dtype=torch.float64, device="cuda")
+    dt = torch.float64 if a.precision == "fp64" else torch.float32
+    esz = 8 if a.precision == "fp64" else 4
+    x = torch.rand(B.in_size, dtype=dt, device="cuda") * 2 - 1
+    y = torch.empty(B.out_size, dtype=dt, device="cuda")
     s = torch.cuda.Stream()
     torch.cuda.synchronize()
 
@@ -87,14 +91,14 @@ def main():
 
     def sequential():
         for k, op in enumerate(ops):
-            op.apply_device(x.data_ptr() + 8 * int(offs_in[k]), y.data_ptr() + 8 * int(offs_out[k]),
-                            stream=s.cuda_stream)
+            op.apply_device(x.data_ptr() + esz * int(offs_in[k]),
+                            y.data_ptr() + esz * int(offs_out[k]), stream=s.cuda_stream)
 
     ms_seq = timed(sequential)
     # each collection alone (same stream, same buffers)
     for k, op in enumerate(ops):
         groups[k]["ms"] = timed(lambda k=k, op=op: op.apply_device(
-            x.data_ptr() + 8 * int(offs_in[k]), y.data_ptr() + 8 * int(offs_out[k]),
+            x.data_ptr() + esz * int(offs_in[k]), y.data_ptr() + esz * int(offs_out[k]),
             stream=s.cuda_stream))
         groups[k]["gb_s"] = groups[k]["bytes"] / groups[k]["ms"] / 1e6
         groups[k]["kernel"] = op.kernel()
@@ -111,7 +115,7 @@ def main():
         "workload": "%d^3 grid: %d hex cells, %d cells -> 2 prisms, %d cells -> 6 tets, P %d..%d "
                     "per cell, curved" % (a.n, *a.cells, a.pmin, a.pmax),
         "elements": int(sum(g["elements"] for g in groups)), "collections": len(groups),
-        "local_dofs": int(dofs), "algorithmic_bytes": int(byts),
+        "precision": a.precision, "local_dofs": int(dofs), "algorithmic_bytes": int(byts),
         "batched": {"ms": ms_batch, "gdof_s": dofs / ms_batch / 1e6,
                     "gb_s": byts / ms_batch / 1e6, "hbm_frac": byts / ms_batch / 1e6 / hbm,
                     "streams": a.streams},

@@ -50,3 +50,33 @@ def test_batch_device_pointers_and_regraph():
         assert np.array_equal(yd.cpu().numpy(), ref)
     assert B.last_ms() > 0
     B.close()
+
+
+@pytest.mark.parametrize("optype", ["helmholtz", "linear_adr", "iproduct_deriv"])
+def test_fp32_batch_equals_collection_by_collection(optype):
+    """FP32 operators in one batch (the FP32 variant of the mixed-element
+    launch): the same bits as each collection applied alone."""
+    import torch
+    mm = MixedMesh(n=6, ncells=(60, 50, 40), pmin=2, pmax=6, seed=3)
+    ops = []
+    for m in mm.meshes():
+        op = nb.Operator(optype, m, precision="fp32")
+        if optype != "iproduct_deriv":
+            op.set_factors(1.5)
+        ops.append(op)
+    B = nb.Batch(ops, nstreams=3)
+    x = torch.rand(B.in_size, dtype=torch.float32, device="cuda") * 2 - 1
+    y = torch.empty(B.out_size, dtype=torch.float32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    B.apply_device(x.data_ptr(), y.data_ptr(), stream=s)
+    ref = torch.empty_like(y)
+    oi = oo = 0
+    for op in ops:
+        op.apply_device(x[oi:].data_ptr(), ref[oo:].data_ptr(), stream=s)
+        oi += op.in_size
+        oo += op.out_size
+    torch.cuda.synchronize()
+    assert torch.equal(y, ref)
+    with pytest.raises(nb.NektarB200Error):
+        B(np.zeros(B.in_size))  # host FP64 entry point refuses an FP32 batch
+    B.close()
