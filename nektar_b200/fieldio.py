@@ -75,34 +75,40 @@ def _write_xml(root, path):
 
 
 def write_fld(path, mesh, fields, metadata=None):
-    """Write fields {name: local coefficients (nelmt*ncoeffs)} of a session
-    mesh (one shape and order) as the directory `path`."""
+    """Write fields {name: local coefficients (the mesh's concatenated local
+    vector)} of a session mesh as the directory `path`: one ELEMENTS block
+    per collection (shape and order), as GetFieldDefinitions groups them."""
     names = list(fields)
-    # field by field, element by element (ExpList::AppendFieldData per field)
-    data = np.concatenate([np.asarray(fields[n], dtype=np.float64).reshape(-1) for n in names])
     if os.path.isdir(path):
         shutil.rmtree(path)
     elif os.path.exists(path):
         os.remove(path)
     os.makedirs(path)
-    ids = list(mesh.elem_ids)  # in the order their data follows
     root = ET.Element("NEKTAR")
     _metadata(root, metadata)
-    el = ET.SubElement(root, "ELEMENTS")
-    el.set("FIELDS", ",".join(names))
-    el.set("SHAPE", SHAPE_NAMES[mesh.shape])
-    el.set("BASIS", ",".join(BASIS_NAMES[mesh.shape]))
-    el.set("NUMMODESPERDIR", "UNIORDER:%d,%d,%d" % (mesh.nm, mesh.nm, mesh.nm))
-    el.set("ID", seq_string(ids))
-    el.set("COMPRESSED", "B64Z-LittleEndian")
-    el.set("BITSIZE", "64")
-    el.text = encode(data)
+    all_ids = []
+    for ci, col in enumerate(mesh.collections):
+        lo, hi = int(mesh.offsets[ci]), int(mesh.offsets[ci + 1])
+        # field by field, element by element (ExpList::AppendFieldData per field)
+        data = np.concatenate([np.asarray(fields[n], dtype=np.float64).reshape(-1)[lo:hi]
+                               for n in names])
+        ids = list(col.elem_ids)  # in the order their data follows
+        all_ids += ids
+        el = ET.SubElement(root, "ELEMENTS")
+        el.set("FIELDS", ",".join(names))
+        el.set("SHAPE", SHAPE_NAMES[col.shape])
+        el.set("BASIS", ",".join(BASIS_NAMES[col.shape]))
+        el.set("NUMMODESPERDIR", "UNIORDER:%d,%d,%d" % (col.nm, col.nm, col.nm))
+        el.set("ID", seq_string(ids))
+        el.set("COMPRESSED", "B64Z-LittleEndian")
+        el.set("BITSIZE", "64")
+        el.text = encode(data)
     _write_xml(root, os.path.join(path, "P0000000.fld"))
     info = ET.Element("NEKTAR")
     _metadata(info, metadata)
     part = ET.SubElement(info, "Partition")
     part.set("FileName", "P0000000.fld")
-    part.text = seq_string(ids)
+    part.text = seq_string(all_ids)
     _write_xml(info, os.path.join(path, "Info.xml"))
 
 

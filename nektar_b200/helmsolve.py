@@ -47,8 +47,10 @@ def errors(mesh, u, exact, device=0):
     W = mesh.quad_weights()
     linf = float(np.max(np.abs(d)))
     l2sq = float(np.sum(W * d * d))
-    grad = nb.Operator("physderiv", mesh, device=device)(d)
-    h1sq = l2sq + sum(float(np.sum(W * g * g)) for g in grad)
+    h1sq = l2sq
+    for col, dc, Wc in zip(mesh.collections, mesh.split(d, "phys"), mesh.split(W, "phys")):
+        for gr in nb.Operator("physderiv", col, device=device)(dc):
+            h1sq += float(np.sum(Wc * gr * gr))
     return linf, float(np.sqrt(l2sq)), float(np.sqrt(h1sq))
 
 
@@ -63,16 +65,22 @@ def helm_solve(session, device=0, tol=1e-12, maxit=5000, check_interval=16, rais
     if forcing is None:
         raise ValueError("the session defines no Forcing function")
     f = forcing.evaluate(*mesh.xyz)
-    b_loc = -nb.Operator("iproduct", mesh, device=device)(f)
-    H = nb.Operator("helmholtz", mesh, device=device)
-    H.set_factors(lam)
-    S = nb.GlobalLinSys([H], mesh.gmap, mesh.nglob, mesh.ndir, sign=mesh.sign, device=device)
+    cols = mesh.collections
+    b_loc = -np.concatenate([nb.Operator("iproduct", c, device=device)(fc)
+                             for c, fc in zip(cols, mesh.split(f, "phys"))])
+    Hs = []
+    for c in cols:
+        H = nb.Operator("helmholtz", c, device=device)
+        H.set_factors(lam)
+        Hs.append(H)
+    S = nb.GlobalLinSys(Hs, mesh.gmap, mesh.nglob, mesh.ndir, sign=mesh.sign, device=device)
     x0 = mesh.dirichlet_local()
     t0 = time.perf_counter()
     x, rep = S.solve(b_loc, x0, tol=tol, maxit=maxit, check_interval=check_interval,
                      raise_on_maxit=raise_on_maxit)
     ms = (time.perf_counter() - t0) * 1e3
-    u = nb.Operator("bwdtrans", mesh, device=device)(x)
+    u = np.concatenate([nb.Operator("bwdtrans", c, device=device)(xc)
+                        for c, xc in zip(cols, mesh.split(x))])
     res = HelmResult(x, u, rep.iterations, rep.rel_residual, bool(rep.converged), solve_ms=ms)
     exact = session.function("ExactSolution")
     if exact is not None:
@@ -102,7 +110,7 @@ def main():
         return
     print("Solving 3D Helmholtz:")
     print("  - Lambda        : %g" % s.parameters["Lambda"])
-    print("  - No. modes     : %d" % r.mesh.nm)
+    print("  - No. modes     : %s" % ",".join(str(c.nm) for c in r.mesh.collections))
     print("  - CG iterations : %d (relative residual %.3g)" % (r.iterations, r.rel_residual))
     if r.l2 is not None:
         print("L infinity error: %g" % r.linf)

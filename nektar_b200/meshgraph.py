@@ -1,52 +1,152 @@
 """Mesh graph of a session for the B200 path: element frames, geometric
-factors at the quadrature points, the C0 local -> global map with
-Dirichlet degrees of freedom first, and the Dirichlet values.
+factors at the quadrature points, the C0 local -> global map with Dirichlet
+degrees of freedom first, and the Dirichlet values, for meshes of
+hexahedra, prisms and tetrahedra (one operator collection per shape and
+order, as the reference groups them).
 
-Hexahedra, as the reference sets them up:
+Element frames follow the reference's geometry classes: the element lists
+its faces in a fixed order, local edges are the faces' shared edges, local
+vertices follow the edge chain (HexGeom::SetUpLocalEdges / Vertices,
+SpatialDomains/HexGeom.cpp:200-430; PrismGeom.cpp:185-391; TetGeom.cpp:
+113-308). Standard-region vertices:
 
-* local frame: HexGeom::SetUpLocalEdges / SetUpLocalVertices
-  (SpatialDomains/HexGeom.cpp:200-430). The element lists its faces bottom,
-  four sides, top; local edges are the faces' shared edges in a fixed
-  order; local vertices follow the edge chain. Vertex v0 is xi = (-1,-1,-1),
-  v1 (+1,-1,-1), v2 (+1,+1,-1), v3 (-1,+1,-1), v4..v7 the same at xi3 = +1;
-* geometry: the straight-sided map is trilinear in the vertices (the
-  two-mode coordinate expansion of Geometry3D); jac and df as GeomFactors
-  defines them (GeomFactors.cpp:248-477), df[k*3+j] = d xi_j / d x_k, in the
-  Collections layout (9, nelmt*nt);
-* coefficients: Modified_A in each direction, mode (p, q, r) at
-  p + nm (q + nm r); index 0 / 1 are the vertex modes at xi = -1 / +1,
-  indices >= 2 the bubbles.
+    hex    v0..v3 = (-1,-1,-1) (1,-1,-1) (1,1,-1) (-1,1,-1), v4..v7 the same at +1
+    prism  v0..v3 as the hex, v4 = (-1,-1,1), v5 = (-1,1,1)
+    tet    v0 = (-1,-1,-1), v1 = (1,-1,-1), v2 = (-1,1,-1), v3 = (-1,-1,1)
 
-Continuity (the role of AssemblyMapCG, AssemblyMapCG.cpp:1322-2300): a local
-mode is a vertex, edge, face or interior mode by how many of its indices are
-bubbles. Edge modes are numbered along the edge from its lower to its higher
-global vertex id; mode p of an element edge running the other way gets the
-sign (-1)^p (the bubble phi_p(-xi) = (-1)^p phi_p(xi)). Face modes are
-numbered in a frame anchored at the face's lowest global vertex, first axis
-towards the lower of its two neighbours; an element face frame maps to it by
-a transposition and two reflections, which permute the (a, b) mode indices
-and give the sign (-1)^(a s_a + b s_b). Any consistent choice gives the same
-discrete space as the reference's, hence the same solution.
+Geometry: straight-sided maps, linear in the vertex coordinates through
+the vertex shape functions (the two-mode coordinate expansion), evaluated at
+the collapsed quadrature points mapped to the standard region; jac = det
+dx/dxi and df[k*3+j] = d xi_j / d x_k in the Collections layout (GeomFactors
+.cpp:248-477).
 
-Dirichlet values follow ExpList::FwdTransBndConstrained on the boundary
-faces (QuadExp.cpp:67-170, SegExp.cpp:81-180): vertex modes take the point
-values, edge bubbles the L2 projection (edge quadrature) of the remainder
-after the vertex modes, face bubbles the L2 projection (face quadrature and
-surface Jacobian) of the remainder after vertex and edge modes. The result
-is independent of the face's parametrisation for the symmetric GLL points.
+Continuity (AssemblyMapCG, AssemblyMapCG.cpp:1322-2300): each shape's modes
+are split into vertex, edge, face and interior modes by the reference's maps
+(StdHexExp / StdPrismExp / StdTetExp GetVertexMap,
+GetEdgeInteriorToElementMap, GetTraceInteriorToElementMap; e.g.
+StdTetExp.cpp:1075-1700, StdPrismExp.cpp:942-1760). Edge modes are numbered
+along the edge from its lower to its higher global vertex id; mode k of an
+element edge running the other way gets (-1)^k. Quadrilateral face modes
+(a, b) are numbered in a frame anchored at the face's lowest global vertex,
+first axis towards the lower of its neighbours; an element's face frame maps
+to it by a transposition and reflections (sign (-1)^(a s_a + b s_b)).
+Triangular faces have only two admissible relative orientations (the
+collapsed apex shared, the other axis possibly reflected): modes are numbered
+from the lower of the two base vertices, and a reflected element face gets
+(-1)^a; a mesh whose neighbouring triangles disagree on the apex is
+rejected, as the reference requires compatible collapsed directions.
+
+Dirichlet values (ExpList::FwdTransBndConstrained on the boundary faces,
+QuadExp.cpp:67-170, TriExp.cpp, SegExp.cpp:81-180): vertex modes take the
+point values, edge bubbles the L2 projection of the remainder at GLL points
+along the edge, face bubbles the L2 projection of the remainder with the
+face's quadrature (GLL x GLL, or GLL x Gauss-Radau on a triangle) and
+surface Jacobian. On hexahedral boundaries this is the reference's result.
+On triangular boundary faces the reference instead interpolates the data of
+the two collapsed-direction edges from the Radau points to GLL points
+before projecting (so the apex value is extrapolated) and writes the faces'
+results one after another; that is not restated, so Prism/Tet solves agree
+with the reference's to the accuracy of that interpolation, not to rounding.
 """
 import numpy as np
 
 from . import shape_tables
 from .session import SessionError
 
-# local vertex index of the corner (a, b, c) in {0, 1}^3 (xi = 2a - 1, ...)
-HEX_CORNER = {(0, 0, 0): 0, (1, 0, 0): 1, (1, 1, 0): 2, (0, 1, 0): 3,
-              (0, 0, 1): 4, (1, 0, 1): 5, (1, 1, 1): 6, (0, 1, 1): 7}
-HEX_CORNER_XI = np.array([[2 * a - 1, 2 * b - 1, 2 * c - 1]
-                          for (a, b, c), _ in sorted(HEX_CORNER.items(), key=lambda kv: kv[1])],
-                         dtype=np.float64)
+# ---------------------------------------------------------------------------
+# standard-region vertices, vertex shape functions, collapsed -> standard
+# ---------------------------------------------------------------------------
+STD_VERTS = {
+    "hex": np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                     [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], dtype=np.float64),
+    "prism": np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                       [-1, -1, 1], [-1, 1, 1]], dtype=np.float64),
+    "tet": np.array([[-1, -1, -1], [1, -1, -1], [-1, 1, -1], [-1, -1, 1]], dtype=np.float64),
+}
+NVERTS = {"hex": 8, "prism": 6, "tet": 4}
+NFACES = {"hex": 6, "prism": 5, "tet": 4}
+FACE_KINDS = {"hex": "QQQQQQ", "prism": "QTQTQ", "tet": "TTTT"}
 
+
+def shape_functions(shape, xi):
+    """N (npts, nv) and dN/dxi (npts, nv, 3) of the straight-sided map."""
+    x1, x2, x3 = xi[:, 0], xi[:, 1], xi[:, 2]
+    h = lambda v: 0.5 * (1.0 + v)  # noqa: E731
+    m = lambda v: 0.5 * (1.0 - v)  # noqa: E731
+    n = xi.shape[0]
+    if shape == "hex":
+        s = STD_VERTS["hex"]
+        fac = 0.5 * (1.0 + xi[:, None, :] * s[None, :, :])
+        N = fac.prod(axis=2)
+        dN = np.empty((n, 8, 3))
+        for j in range(3):
+            d = fac.copy()
+            d[:, :, j] = 0.5 * s[None, :, j]
+            dN[:, :, j] = d.prod(axis=2)
+        return N, dN
+    if shape == "prism":
+        la, lb, lc = -0.5 * (x1 + x3), h(x1), h(x3)
+        m0, m1 = m(x2), h(x2)
+        N = np.stack([la * m0, lb * m0, lb * m1, la * m1, lc * m0, lc * m1], axis=1)
+        dla = np.array([-0.5, 0.0, -0.5])
+        dlb = np.array([0.5, 0.0, 0.0])
+        dlc = np.array([0.0, 0.0, 0.5])
+        dm0 = np.array([0.0, -0.5, 0.0])
+        dm1 = np.array([0.0, 0.5, 0.0])
+        dN = np.empty((n, 6, 3))
+        for v, (l, dl, mm, dmm) in enumerate(((la, dla, m0, dm0), (lb, dlb, m0, dm0),
+                                               (lb, dlb, m1, dm1), (la, dla, m1, dm1),
+                                               (lc, dlc, m0, dm0), (lc, dlc, m1, dm1))):
+            dN[:, v, :] = dl[None, :] * mm[:, None] + l[:, None] * dmm[None, :]
+        return N, dN
+    if shape == "tet":
+        N = np.stack([-0.5 * (1.0 + x1 + x2 + x3), h(x1), h(x2), h(x3)], axis=1)
+        dN = np.broadcast_to(np.array([[-0.5, -0.5, -0.5], [0.5, 0, 0], [0, 0.5, 0], [0, 0, 0.5]]),
+                             (n, 4, 3)).copy()
+        return N, dN
+    raise SessionError("unsupported shape %r" % shape)
+
+
+def collapsed_to_standard(shape, e1, e2, e3):
+    """Standard-region coordinates of collapsed coordinates (the Duffy maps
+    of StdPrismExp / StdTetExp)."""
+    if shape == "hex":
+        return e1, e2, e3
+    if shape == "prism":
+        return 0.5 * (1 + e1) * (1 - e3) - 1, e2, e3
+    return 0.25 * (1 + e1) * (1 - e2) * (1 - e3) - 1, 0.5 * (1 + e2) * (1 - e3) - 1, e3
+
+
+def element_geometry(shape, X, z):
+    """jac (nelmt*nt,), df (9, nelmt*nt), coordinates (3, nelmt*nt) of
+    straight-sided elements with vertex coordinates X (nelmt, nv, 3) at the
+    collapsed tensor points z = (z0, z1, z2) (point q = (k nq1 + j) nq0 + i)."""
+    e1, e2, e3 = np.meshgrid(z[0], z[1], z[2], indexing="ij")  # [i, j, k]
+    e = [a.transpose(2, 1, 0).reshape(-1) for a in (e1, e2, e3)]
+    xi = np.stack(collapsed_to_standard(shape, *e), axis=1)
+    N, dN = shape_functions(shape, xi)
+    x = np.einsum("pc,ecd->edp", N, X)
+    J = np.einsum("pcj,ecd->epdj", dN, X)  # J[e, p, d, j] = d x_d / d xi_j
+    det = np.linalg.det(J)
+    if np.any(det <= 0):
+        raise SessionError("element with a non-positive Jacobian")
+    inv = np.linalg.inv(J)  # d xi_j / d x_k at [e, p, j, k]
+    ne, nt = X.shape[0], xi.shape[0]
+    df = np.empty((9, ne * nt))
+    for k in range(3):
+        for j in range(3):
+            df[k * 3 + j] = inv[:, :, j, k].reshape(-1)
+    return det.reshape(-1), df, x.transpose(1, 0, 2).reshape(3, -1)
+
+
+def hex_geometry(X, z):
+    """element_geometry for hexahedra at the same points in every direction."""
+    return element_geometry("hex", X, (z, z, z))
+
+
+# ---------------------------------------------------------------------------
+# local frames (reference geometry classes)
+# ---------------------------------------------------------------------------
 
 def _shared_edge(fa, fb, faces, what):
     common = [e for e in faces[fa][1] if e in faces[fb][1]]
@@ -55,131 +155,249 @@ def _shared_edge(fa, fb, faces, what):
     return common[0]
 
 
-def hex_local_vertices(geom, eid):
-    """Global vertex ids v0..v7 of hexahedron eid in its local order
-    (HexGeom::SetUpLocalEdges, HexGeom.cpp:200-339, and
-    HexGeom::SetUpLocalVertices, HexGeom.cpp:341-430)."""
-    shape, F = geom.elements[eid]
-    if shape != "hex" or len(F) != 6:
-        raise SessionError("element %d is not a hexahedron" % eid)
-    for f in F:
-        if geom.faces[f][0] != "Q":
-            raise SessionError("hexahedron %d has a non-quadrilateral face" % eid)
-    faces = geom.faces
-    e = [None] * 12
-    for f in range(1, 5):
-        e[f - 1] = _shared_edge(F[0], F[f], faces, "bottom")
-    e[4] = _shared_edge(F[1], F[4], faces, "vertical")
-    for f in range(1, 4):
-        e[f + 4] = _shared_edge(F[f], F[f + 1], faces, "vertical")
-    for f in range(1, 5):
-        e[f + 7] = _shared_edge(F[5], F[f], faces, "top")
-    E = [geom.edges[k] for k in e]
-
-    def chain(first, second, nxt):
-        a, b = E[first]
-        if a in E[second]:
-            v = [b, a]
-        elif b in E[second]:
-            v = [a, b]
+def _chain(E, first, second, nxt, eid):
+    a, b = E[first]
+    if a in E[second]:
+        v = [b, a]
+    elif b in E[second]:
+        v = [a, b]
+    else:
+        raise SessionError("edges of element %d do not connect" % eid)
+    for k in nxt:
+        x, y = E[k]
+        if x == v[-1]:
+            v.append(y)
+        elif y == v[-1]:
+            v.append(x)
         else:
             raise SessionError("edges of element %d do not connect" % eid)
-        for k in nxt:
-            x, y = E[k]
-            if x == v[-1]:
-                v.append(y)
-            elif y == v[-1]:
-                v.append(x)
-            else:
-                raise SessionError("edges of element %d do not connect" % eid)
+    return v
+
+
+def _other_end(edge, v, eid):
+    a, b = edge
+    if a == v:
+        return b
+    if b == v:
+        return a
+    raise SessionError("edges of element %d do not connect" % eid)
+
+
+def local_vertices(geom, eid):
+    """Global vertex ids of element eid in its local order."""
+    shape, F = geom.elements[eid]
+    faces = geom.faces
+    if len(F) != NFACES[shape]:
+        raise SessionError("element %d has %d faces" % (eid, len(F)))
+    for f, kind in zip(F, FACE_KINDS[shape]):
+        if faces[f][0] != kind:
+            raise SessionError("face %d of %s %d is not a %s" % (f, shape, eid,
+                               "quadrilateral" if kind == "Q" else "triangle"))
+    if shape == "hex":  # HexGeom.cpp:200-430
+        e = [None] * 12
+        for f in range(1, 5):
+            e[f - 1] = _shared_edge(F[0], F[f], faces, "bottom")
+        e[4] = _shared_edge(F[1], F[4], faces, "vertical")
+        for f in range(1, 4):
+            e[f + 4] = _shared_edge(F[f], F[f + 1], faces, "vertical")
+        for f in range(1, 5):
+            e[f + 7] = _shared_edge(F[5], F[f], faces, "top")
+        E = [geom.edges[k] for k in e]
+        return _chain(E, 0, 1, (1, 2), eid) + _chain(E, 8, 9, (9, 10), eid)
+    if shape == "prism":  # PrismGeom.cpp:185-391
+        e = [None] * 9
+        for f in range(1, 5):
+            e[f - 1] = _shared_edge(F[0], F[f], faces, "bottom")
+        e[4] = _shared_edge(F[1], F[4], faces, "vertical")
+        for f in range(1, 4):
+            e[f + 4] = _shared_edge(F[f], F[f + 1], faces, "vertical")
+        e[8] = _shared_edge(F[2], F[4], faces, "top")
+        E = [geom.edges[k] for k in e]
+        v = _chain(E, 0, 1, (1, 2), eid)
+        a, b = E[8]
+        if a in E[4]:
+            v += [a, b]
+        elif b in E[4]:
+            v += [b, a]
+        else:
+            raise SessionError("edges of element %d do not connect" % eid)
         return v
-
-    return chain(0, 1, (1, 2)) + chain(8, 9, (9, 10))
-
-
-def hex_geometry(X, z):
-    """jac (nelmt*nt,), df (9, nelmt*nt) and coordinates (3, nelmt*nt) of
-    trilinear hexahedra with corner coordinates X (nelmt, 8, 3) at the tensor
-    points z (each direction the same, point q = (k nq + j) nq + i)."""
-    nq = len(z)
-    xi = np.stack(np.meshgrid(z, z, z, indexing="ij"), axis=-1)  # [i, j, k, dir]
-    xi = xi.transpose(2, 1, 0, 3).reshape(-1, 3)  # q = (k nq + j) nq + i
-    s = HEX_CORNER_XI  # (8, 3)
-    fac = 0.5 * (1.0 + xi[:, None, :] * s[None, :, :])  # (nt, 8, 3)
-    N = fac.prod(axis=2)  # (nt, 8)
-    dN = np.empty((xi.shape[0], 8, 3))
-    for j in range(3):
-        d = fac.copy()
-        d[:, :, j] = 0.5 * s[None, :, j]
-        dN[:, :, j] = d.prod(axis=2)
-    x = np.einsum("pc,ecd->edp", N, X)  # (nelmt, 3, nt)
-    J = np.einsum("pcj,ecd->epdj", dN, X)  # J[e, p, d, j] = d x_d / d xi_j
-    det = np.linalg.det(J)
-    if np.any(det <= 0):
-        raise SessionError("element with a non-positive Jacobian")
-    inv = np.linalg.inv(J)  # inv[e, p, j, k] = d xi_j / d x_k
-    ne, nt = X.shape[0], xi.shape[0]
-    df = np.empty((9, ne * nt))
-    for k in range(3):
-        for j in range(3):
-            df[k * 3 + j] = inv[:, :, j, k].reshape(-1)
-    coords = x.transpose(1, 0, 2).reshape(3, -1)
-    return det.reshape(-1), df, coords
+    # tet, TetGeom.cpp:113-308
+    e = [None] * 6
+    for f in range(1, 4):
+        e[f - 1] = _shared_edge(F[0], F[f], faces, "bottom")
+    e[3] = _shared_edge(F[1], F[3], faces, "vertical")
+    e[4] = _shared_edge(F[1], F[2], faces, "vertical")
+    e[5] = _shared_edge(F[2], F[3], faces, "vertical")
+    E = [geom.edges[k] for k in e]
+    v = _chain(E, 0, 1, (1,), eid)
+    v.append(_other_end(E[3], v[0], eid))
+    return v
 
 
-def _modA(T):
-    """(nm, nq) Modified_A table of direction 0 and its raw weights / points."""
-    nq = len(T["z"][0])
-    return np.asarray(T["b"][0]).reshape(-1, nq), np.asarray(T["w"][0]), np.asarray(T["z"][0])
+def hex_local_vertices(geom, eid):
+    return local_vertices(geom, eid)
+
+
+# ---------------------------------------------------------------------------
+# mode maps
+# ---------------------------------------------------------------------------
+
+def mode_index(shape, nm):
+    """(p, q, r) -> local coefficient index (StdHexExp ordering p fastest;
+    StdPrismExp::GetMode, StdPrismExp.cpp:1947-1956; StdTetExp::GetMode,
+    StdTetExp.cpp:1864-1893)."""
+    if shape == "hex":
+        return lambda p, q, r: p + nm * (q + nm * r)
+    if shape == "prism":
+        Q = R = nm - 1
+        return lambda p, q, r: r + q * (R + 1 - p) + (Q + 1) * (p * R + 1 - (p - 2) * (p - 1) // 2)
+
+    def tet(I, J, K):
+        cnt = 0
+        for i in range(I):
+            cnt += (nm - i) * (nm - i + 1) // 2
+        for j in range(J):
+            cnt += nm - I - j
+        return cnt + K
+    return tet
+
+
+def topology(shape, nm):
+    """Vertex modes, edges (start, end, [(mode, k)]) and faces (kind, frame,
+    [(mode, a, b)]) of a shape at nm modes per direction. Quadrilateral frames
+    are (origin, end of axis a, end of axis b); triangular frames (origin, end
+    of axis a, apex)."""
+    G = mode_index(shape, nm)
+    K = range(2, nm)
+    if shape == "hex":
+        verts = [G(0, 0, 0), G(1, 0, 0), G(1, 1, 0), G(0, 1, 0), G(0, 0, 1), G(1, 0, 1),
+                 G(1, 1, 1), G(0, 1, 1)]
+        edges = [(0, 1, [(G(k, 0, 0), k) for k in K]), (1, 2, [(G(1, k, 0), k) for k in K]),
+                 (3, 2, [(G(k, 1, 0), k) for k in K]), (0, 3, [(G(0, k, 0), k) for k in K]),
+                 (0, 4, [(G(0, 0, k), k) for k in K]), (1, 5, [(G(1, 0, k), k) for k in K]),
+                 (2, 6, [(G(1, 1, k), k) for k in K]), (3, 7, [(G(0, 1, k), k) for k in K]),
+                 (4, 5, [(G(k, 0, 1), k) for k in K]), (5, 6, [(G(1, k, 1), k) for k in K]),
+                 (7, 6, [(G(k, 1, 1), k) for k in K]), (4, 7, [(G(0, k, 1), k) for k in K])]
+        faces = [("Q", (0, 1, 3), [(G(a, b, 0), a, b) for b in K for a in K]),
+                 ("Q", (0, 1, 4), [(G(a, 0, b), a, b) for b in K for a in K]),
+                 ("Q", (1, 2, 5), [(G(1, a, b), a, b) for b in K for a in K]),
+                 ("Q", (3, 2, 7), [(G(a, 1, b), a, b) for b in K for a in K]),
+                 ("Q", (0, 3, 4), [(G(0, a, b), a, b) for b in K for a in K]),
+                 ("Q", (4, 5, 7), [(G(a, b, 1), a, b) for b in K for a in K])]
+    elif shape == "prism":  # StdPrismExp.cpp:942-1760
+        verts = [G(0, 0, 0), G(1, 0, 0), G(1, 1, 0), G(0, 1, 0), G(0, 0, 1), G(0, 1, 1)]
+        edges = [(0, 1, [(G(k, 0, 0), k) for k in K]), (1, 2, [(G(1, k, 0), k) for k in K]),
+                 (3, 2, [(G(k, 1, 0), k) for k in K]), (0, 3, [(G(0, k, 0), k) for k in K]),
+                 (0, 4, [(G(0, 0, k), k) for k in K]), (1, 4, [(G(1, 0, k - 1), k) for k in K]),
+                 (2, 5, [(G(1, 1, k - 1), k) for k in K]), (3, 5, [(G(0, 1, k), k) for k in K]),
+                 (4, 5, [(G(0, k, 1), k) for k in K])]
+        tri = lambda q: [(G(a, q, b), a, b) for a in K for b in range(1, nm - a)]  # noqa: E731
+        faces = [("Q", (0, 1, 3), [(G(a, b, 0), a, b) for b in K for a in K]),
+                 ("T", (0, 1, 4), tri(0)),
+                 ("Q", (1, 2, 4), [(G(1, a, b - 1), a, b) for b in K for a in K]),
+                 ("T", (3, 2, 5), tri(1)),
+                 ("Q", (0, 3, 4), [(G(0, a, b), a, b) for b in K for a in K])]
+    else:  # tet, StdTetExp.cpp:1075-1700
+        verts = [G(0, 0, 0), G(1, 0, 0), G(0, 1, 0), G(0, 0, 1)]
+        edges = [(0, 1, [(G(k, 0, 0), k) for k in K]), (1, 2, [(G(1, k - 1, 0), k) for k in K]),
+                 (0, 2, [(G(0, k, 0), k) for k in K]), (0, 3, [(G(0, 0, k), k) for k in K]),
+                 (1, 3, [(G(1, 0, k - 1), k) for k in K]), (2, 3, [(G(0, 1, k - 1), k) for k in K])]
+        faces = [("T", (0, 1, 2), [(G(a, b, 0), a, b) for a in K for b in range(1, nm - a)]),
+                 ("T", (0, 1, 3), [(G(a, 0, b), a, b) for a in K for b in range(1, nm - a)]),
+                 ("T", (1, 2, 3), [(G(1, a - 1, b), a, b) for a in K for b in range(1, nm - a)]),
+                 ("T", (0, 2, 3), [(G(0, a, b), a, b) for a in K for b in range(1, nm - a)])]
+    return verts, edges, faces
+
+
+def ncoeffs(shape, nm):
+    return {"hex": nm ** 3, "prism": nm * nm * (nm + 1) // 2,
+            "tet": nm * (nm + 1) * (nm + 2) // 6}[shape]
+
+
+def _tables_1d(nm):
+    """Modified_A at nm+1 GLL points and Modified_B at nm Gauss-Radau (1, 0)
+    points with the raw weights (the face expansions' tables)."""
+    import nektar_b200 as nb
+    zg, wg, Dg = nb.points(nb.GLL, nm + 1)
+    A, _ = nb.basis(nb.MODIFIED_A, nm, zg, Dg)
+    zr, wr, Dr = nb.points(nb.RADAU_A1, nm)
+    Bt, _ = nb.basis(nb.MODIFIED_B, nm, zr, Dr)
+    Bt = np.asarray(Bt).reshape(-1, nm)
+    rows, i = {}, 0
+    for p in range(nm):
+        for q in range(nm - p):
+            rows[(p, q)] = Bt[i]
+            i += 1
+    return np.asarray(A).reshape(nm, nm + 1), zg, wg, rows, zr, wr * 0.5
+
+
+# ---------------------------------------------------------------------------
+# collections and the mesh
+# ---------------------------------------------------------------------------
+
+class Collection:
+    """One operator collection: elements of one shape and order, with the
+    attributes nektar_b200.Operator takes."""
+
+    def __init__(self, geom, shape, nm, eids):
+        self.shape, self.nm, self.elem_ids = shape, nm, list(eids)
+        self.nelmt = len(self.elem_ids)
+        self.T, self.nq = shape_tables(shape, nm, nm + 1)
+        self.nt = self.nq[0] * self.nq[1] * self.nq[2]
+        self.nc = ncoeffs(shape, nm)
+        self.deformed = True
+        self.lverts = np.array([local_vertices(geom, e) for e in self.elem_ids], dtype=np.int64)
+        self.X = np.array([[geom.vertices[v] for v in row] for row in self.lverts])
+        self.jac, self.df, self.xyz = element_geometry(
+            shape, self.X, tuple(np.asarray(z) for z in self.T["z"]))
+
+    def quad_weights(self):
+        """Integration weights jac * w0 w1 w2 at every quadrature point (the
+        collapsed directions' Gauss-Radau weights carry the Duffy factor)."""
+        w = [np.asarray(v) for v in self.T["ws"]]
+        wq = np.einsum("k,j,i->kji", w[2], w[1], w[0]).reshape(-1)
+        return self.jac * np.tile(wq, self.nelmt)
 
 
 class SessionMesh:
-    """The hexahedral mesh of a session with the attributes the operators take
-    (shape, nm, nq, nt, nc, nelmt, T, jac, df, deformed) plus coordinates of
-    the quadrature points, the assembly and the Dirichlet data."""
+    """The mesh of a session: collections (one per shape and order, in the
+    order of the domain's composites), the assembly over the concatenated
+    local coefficient vector and the Dirichlet data. With a single
+    collection the object also carries that collection's attributes, so it
+    can be handed to nektar_b200.Operator directly."""
 
     def __init__(self, session, var=None):
         g = session.geometry
         self.session = session
         self.var = var or (session.variables[0] if session.variables else "u")
-        eids, nms = [], set()
+        groups = {}
         for c in g.domain:
             letter, ids = g.composites[c]
             if letter not in ("H", "R", "A", "P"):
                 raise SessionError("domain composite %d does not hold elements" % c)
             if c not in session.nummodes:
                 raise SessionError("no expansion defined on composite %d" % c)
-            nms.add(session.nummodes[c])
-            eids.extend(ids)
-        shapes = {g.elements[e][0] for e in eids}
-        if shapes != {"hex"}:
-            raise SessionError("only hexahedral meshes are supported, found %s" % sorted(shapes))
-        if len(nms) != 1:
-            raise SessionError("one expansion order per mesh is supported")
-        self.shape, self.nm = "hex", nms.pop()
-        self.elem_ids = eids
-        self.nelmt = len(eids)
-        self.T, self.nq = shape_tables("hex", self.nm, self.nm + 1)
-        self.nt = self.nq[0] * self.nq[1] * self.nq[2]
-        self.nc = self.nm ** 3
-        self.deformed = True
-        self.lverts = np.array([hex_local_vertices(g, e) for e in eids], dtype=np.int64)
-        self.X = np.array([[g.vertices[v] for v in row] for row in self.lverts])
-        self.jac, self.df, self.xyz = hex_geometry(self.X, np.asarray(self.T["z"][0]))
+            for e in ids:
+                shape = g.elements[e][0]
+                groups.setdefault((shape, session.nummodes[c]), []).append(e)
+        order = {"hex": 0, "prism": 1, "tet": 2}
+        self.collections = [Collection(g, s, nm, ids) for (s, nm), ids in
+                            sorted(groups.items(), key=lambda kv: (order[kv[0][0]], kv[0][1]))]
+        self.offsets = np.cumsum([0] + [c.nelmt * c.nc for c in self.collections])
+        self.nloc = int(self.offsets[-1])
+        if len(self.collections) == 1:
+            c = self.collections[0]
+            for k in ("shape", "nm", "nq", "nt", "nc", "nelmt", "T", "deformed", "jac", "df",
+                      "elem_ids", "lverts", "X"):
+                setattr(self, k, getattr(c, k))
+        self.xyz = np.concatenate([c.xyz for c in self.collections], axis=1)
         self._assemble()
 
     # ------------------------------------------------------------------ #
-    def _classify(self):
-        """Per local mode of a hexahedron: kind (0 vertex, 1 edge, 2 face,
-        3 interior) and the indices that say where it lives."""
-        nm = self.nm
-        p, q, r = np.meshgrid(np.arange(nm), np.arange(nm), np.arange(nm), indexing="ij")
-        p, q, r = (a.transpose(2, 1, 0).reshape(-1) for a in (p, q, r))  # index p + nm(q + nm r)
-        return np.stack([p, q, r], axis=1)
-
     def _dirichlet_faces(self):
         g, s = self.session.geometry, self.session
-        faces = set()
+        self._face_bc = {}
         for rid, comps in s.boundary_regions.items():
             conds = [bc for bc in s.boundary_conditions.get(rid, []) if bc.var == self.var]
             if not conds:
@@ -193,194 +411,241 @@ class SessionMesh:
                 if letter not in ("F", "Q", "T"):
                     raise SessionError("boundary composite %d does not hold faces" % c)
                 for f in ids:
-                    faces.add(f)
                     self._face_bc[f] = bc
-        return faces
 
     def _assemble(self):
-        g, nm = self.session.geometry, self.nm
-        modes = self._classify()
-        bub = modes >= 2
-        kind = bub.sum(axis=1)
-        self._face_bc = {}
-        dir_faces = self._dirichlet_faces()
-        # boundary face keys (sorted vertex ids) -> face id
-        def face_verts(f):
-            return tuple(sorted({v for e in g.faces[f][1] for v in g.edges[e]}))
-        dir_keys = {face_verts(f): f for f in dir_faces}
-        nb = nm - 2
-        entities = {}  # key -> (kind, size)
-        refs = []  # per element, per local mode: (entity key, offset, sign)
-        for el in range(self.nelmt):
-            V = self.lverts[el]
-            row = []
-            for m in range(self.nc):
-                idx = modes[m]
-                k = kind[m]
-                if k == 0:
-                    key = ("v", int(V[HEX_CORNER[tuple(idx)]]))
-                    row.append((key, 0, 1.0))
-                elif k == 1:
-                    d = int(np.nonzero(bub[m])[0][0])
-                    lo, hi = list(idx), list(idx)
-                    lo[d], hi[d] = 0, 1
-                    ga, gb = int(V[HEX_CORNER[tuple(lo)]]), int(V[HEX_CORNER[tuple(hi)]])
+        g = self.session.geometry
+        self._dirichlet_faces()
+        entities = {}  # key -> size
+        tri_frame = {}  # triangle key -> (apex, origin) of its canonical frame
+        gm, sg = [], []
+        for col in self.collections:
+            nm, nb = col.nm, col.nm - 2
+            verts, edges, faces = topology(col.shape, nm)
+            nbt = (nm - 3) * (nm - 2) // 2  # interior modes of a triangle
+            all_modes = set(verts)
+            for _, _, lst in edges:
+                all_modes.update(m for m, _ in lst)
+            for _, _, lst in faces:
+                all_modes.update(m for m, _, _ in lst)
+            interior = [m for m in range(col.nc) if m not in all_modes]
+            for el in range(col.nelmt):
+                V = [int(v) for v in col.lverts[el]]
+                key_of = [None] * col.nc
+                for lv, m in enumerate(verts):
+                    key_of[m] = (("v", V[lv]), 0, 1.0)
+                    entities.setdefault(("v", V[lv]), 1)
+                for a, b, lst in edges:
+                    ga, gb = V[a], V[b]
                     key = ("e", min(ga, gb), max(ga, gb))
-                    mode = int(idx[d])
-                    sign = (-1.0) ** mode if ga > gb else 1.0
-                    row.append((key, mode - 2, sign))
-                elif k == 2:
-                    d1, d2 = (int(v) for v in np.nonzero(bub[m])[0])
-
-                    def corner(a1, a2):
-                        c = list(idx)
-                        c[d1], c[d2] = a1, a2
-                        return int(V[HEX_CORNER[tuple(c)]])
-                    cids = {(0, 0): corner(0, 0), (1, 0): corner(1, 0), (0, 1): corner(0, 1),
-                            (1, 1): corner(1, 1)}
-                    key = ("f",) + tuple(sorted(cids.values()))
-                    (aO, bO) = min(cids, key=lambda c: cids[c])
-                    n1 = cids[(1 - aO, bO)]  # neighbour along element axis 1
-                    n2 = cids[(aO, 1 - bO)]  # neighbour along element axis 2
-                    s1 = 1 if aO == 0 else -1
-                    s2 = 1 if bO == 0 else -1
-                    m1, m2 = int(idx[d1]), int(idx[d2])
-                    sign = float((s1 ** m1) * (s2 ** m2))
-                    ca, cb = (m1, m2) if n1 < n2 else (m2, m1)
-                    row.append((key, (ca - 2) * nb + (cb - 2), sign))
-                else:
-                    key = ("i", el)
-                    off = ((int(idx[2]) - 2) * nb + (int(idx[1]) - 2)) * nb + (int(idx[0]) - 2)
-                    row.append((key, off, 1.0))
-                size = {0: 1, 1: nb, 2: nb * nb, 3: nb ** 3}[k]
-                entities.setdefault(key, size)
-            refs.append(row)
+                    entities.setdefault(key, nb)
+                    for m, k in lst:
+                        key_of[m] = (key, k - 2, (-1.0) ** k if ga > gb else 1.0)
+                for kind, frame, lst in faces:
+                    if kind == "Q":
+                        o, ea, eb = (V[i] for i in frame)
+                        quad = self._quad_of(col.shape, frame, V)  # corner opposite o
+                        cid = {(0, 0): o, (1, 0): ea, (0, 1): eb, (1, 1): quad}
+                        key = ("f",) + tuple(sorted(cid.values()))
+                        entities.setdefault(key, nb * nb)
+                        aO, bO = min(cid, key=lambda c: cid[c])
+                        n1, n2 = cid[(1 - aO, bO)], cid[(aO, 1 - bO)]
+                        s1 = 1 if aO == 0 else -1
+                        s2 = 1 if bO == 0 else -1
+                        for m, a, b in lst:
+                            ca, cb = (a, b) if n1 < n2 else (b, a)
+                            key_of[m] = (key, (ca - 2) * nb + (cb - 2), float(s1 ** a * s2 ** b))
+                    else:
+                        o, ea, apex = (V[i] for i in frame)
+                        key = ("t",) + tuple(sorted((o, ea, apex)))
+                        entities.setdefault(key, nbt)
+                        if key not in tri_frame:
+                            tri_frame[key] = (apex, min(o, ea))
+                        capex, corigin = tri_frame[key]
+                        if capex != apex:
+                            raise SessionError(
+                                "triangular face %s: neighbouring elements collapse it towards "
+                                "different vertices (%d, %d)" % (key[1:], capex, apex))
+                        refl = o != corigin
+                        for pos, (m, a, b) in enumerate(lst):
+                            key_of[m] = (key, pos, (-1.0) ** a if refl else 1.0)
+                for pos, m in enumerate(interior):
+                    key_of[m] = (("i", len(gm), el), pos, 1.0)
+                entities.setdefault(("i", len(gm), el), len(interior))
+                gm.append(key_of)
+        self._tri_frame = tri_frame
         # Dirichlet entities: the vertices, edges and faces of Dirichlet faces
         dir_ent = set()
-        for fv in dir_keys:
-            dir_ent.add(("f",) + fv)
-        for f in dir_faces:
-            for e in g.faces[f][1]:
+        for f in self._face_bc:
+            kind, es = g.faces[f]
+            vs = sorted({v for e in es for v in g.edges[e]})
+            dir_ent.add(("f" if kind == "Q" else "t",) + tuple(vs))
+            for e in es:
                 a, b = g.edges[e]
-                dir_ent.add(("e", min(a, b), max(a, b)))
-                dir_ent.add(("v", a))
-                dir_ent.add(("v", b))
-        order = {"v": 0, "e": 1, "f": 2, "i": 3}
-        keys = sorted(entities, key=lambda k: (k not in dir_ent, order[k[0]], k[1:]))
-        base, n = {}, 0
-        ndir = 0
+                dir_ent.update({("e", min(a, b), max(a, b)), ("v", a), ("v", b)})
+        missing = [k for k in dir_ent if k not in entities]
+        if missing:
+            raise SessionError("boundary faces that belong to no element: %s" % missing[:3])
+        rank = {"v": 0, "e": 1, "f": 2, "t": 3, "i": 4}
+        keys = sorted(entities, key=lambda k: (k not in dir_ent, rank[k[0]], k[1:]))
+        base, n, ndir = {}, 0, 0
         for k in keys:
             base[k] = n
             n += entities[k]
             if k in dir_ent:
                 ndir = n
         self.nglob, self.ndir = n, ndir
-        gmap = np.empty(self.nelmt * self.nc, dtype=np.int32)
-        sign = np.empty(self.nelmt * self.nc)
-        for el, row in enumerate(refs):
-            for m, (key, off, sg) in enumerate(row):
-                gmap[el * self.nc + m] = base[key] + off
-                sign[el * self.nc + m] = sg
+        gmap = np.empty(self.nloc, dtype=np.int32)
+        sign = np.empty(self.nloc)
+        i = 0
+        for key_of in gm:
+            for key, off, s in key_of:
+                gmap[i] = base[key] + off
+                sign[i] = s
+                i += 1
         self.gmap, self.sign = gmap, sign
-        self._base, self._entities = base, entities
-        self._dir_ent = dir_ent
-        self._dir_keys = dir_keys
+        self._base, self._entities, self._dir_ent = base, entities, dir_ent
+
+    @staticmethod
+    def _quad_of(shape, frame, V):
+        """The corner of a quadrilateral face opposite its frame origin."""
+        opposite = {("hex", (0, 1, 3)): 2, ("hex", (0, 1, 4)): 5, ("hex", (1, 2, 5)): 6,
+                    ("hex", (3, 2, 7)): 6, ("hex", (0, 3, 4)): 7, ("hex", (4, 5, 7)): 6,
+                    ("prism", (0, 1, 3)): 2, ("prism", (1, 2, 4)): 5, ("prism", (0, 3, 4)): 5}
+        return V[opposite[(shape, tuple(frame))]]
 
     # ------------------------------------------------------------------ #
     def dirichlet_values(self, time=0.0):
         """Global Dirichlet coefficients (ndir,) by the boundary-constrained
-        projection of the boundary values on each Dirichlet face."""
+        projection of the boundary values."""
         g = self.session.geometry
-        B, w, z = _modA(self.T)
-        nm, nb = self.nm, self.nm - 2
+        nms = {c.nm for c in self.collections}
+        if len(nms) != 1:
+            raise SessionError("Dirichlet data with several expansion orders is not supported")
+        nm = nms.pop()
+        nb = nm - 2
+        A, zg, wg, Brow, zr, wr = _tables_1d(nm)
         out = np.zeros(self.ndir)
         P = lambda v: np.asarray(g.vertices[v], dtype=np.float64)  # noqa: E731
-        bc_of = {}
-        for fv, f in self._dir_keys.items():
-            bc_of[fv] = self._face_bc[f]
-        # vertices and edges take the condition of one face that holds them
         ent_bc = {}
-        for fv, bc in bc_of.items():
-            for v in fv:
-                ent_bc.setdefault(("v", v), bc)
         for f, bc in self._face_bc.items():
             for e in g.faces[f][1]:
                 a, b = g.edges[e]
+                ent_bc.setdefault(("v", a), bc)
+                ent_bc.setdefault(("v", b), bc)
                 ent_bc.setdefault(("e", min(a, b), max(a, b)), bc)
         vals = {}
         for key, bc in ent_bc.items():
             if key[0] == "v":
                 x = P(key[1])
-                out[self._base[key]] = bc.value.evaluate(x[0], x[1], x[2], time)
-                vals[key] = out[self._base[key]]
-        # edges: 1-D constrained projection along lo -> hi
-        M1 = (B[2:] * w) @ B[2:].T
+                vals[key[1]] = out[self._base[key]] = bc.value.evaluate(x[0], x[1], x[2], time)
+        M1 = (A[2:] * wg) @ A[2:].T
         for key, bc in ent_bc.items():
-            if key[0] != "e":
+            if key[0] != "e" or nb == 0:
                 continue
             xa, xb = P(key[1]), P(key[2])
-            x = np.outer(0.5 * (1 - z), xa) + np.outer(0.5 * (1 + z), xb)
+            x = np.outer(0.5 * (1 - zg), xa) + np.outer(0.5 * (1 + zg), xb)
             f = bc.value.evaluate(x[:, 0], x[:, 1], x[:, 2], time)
-            c0, c1 = f[0], f[-1]
-            rem = f - c0 * B[0] - c1 * B[1]
-            # the edge Jacobian (length / 2) scales both sides alike
-            c = np.linalg.solve(M1, (B[2:] * w) @ rem) if nb > 0 else np.zeros(0)
+            rem = f - f[0] * A[0] - f[-1] * A[1]
             o = self._base[key]
-            out[o:o + nb] = c
-        # faces: 2-D constrained projection in the canonical face frame
-        for fv, bc in bc_of.items():
-            key = ("f",) + fv
-            f = self._dir_keys[fv]
-            cyc = self._face_cycle(f)
-            i0 = int(np.argmin(cyc))
-            O = cyc[i0]
-            nA, nB = cyc[(i0 + 1) % 4], cyc[(i0 - 1) % 4]
-            if nA > nB:
-                nA, nB = nB, nA
-            AB = cyc[(i0 + 2) % 4]
-            XO, XA, XB, XAB = P(O), P(nA), P(nB), P(AB)
-            za, zb = np.meshgrid(z, z, indexing="ij")  # [a, b]
-            Na = [0.5 * (1 - za), 0.5 * (1 + za)]
-            Nb = [0.5 * (1 - zb), 0.5 * (1 + zb)]
-            x = (Na[0] * Nb[0])[..., None] * XO + (Na[1] * Nb[0])[..., None] * XA + \
-                (Na[0] * Nb[1])[..., None] * XB + (Na[1] * Nb[1])[..., None] * XAB
-            dxa = (0.5 * Nb[0])[..., None] * (XA - XO) + (0.5 * Nb[1])[..., None] * (XAB - XB)
-            dxb = (0.5 * Na[0])[..., None] * (XB - XO) + (0.5 * Na[1])[..., None] * (XAB - XA)
-            J = np.linalg.norm(np.cross(dxa, dxb), axis=-1)
-            vals_f = bc.value.evaluate(x[..., 0], x[..., 1], x[..., 2], time)
-            # boundary part: vertex modes, then the four edges' bubbles
-            ub = (vals[("v", O)] * np.outer(B[0], B[0]) + vals[("v", nA)] * np.outer(B[1], B[0])
-                  + vals[("v", nB)] * np.outer(B[0], B[1]) + vals[("v", AB)] * np.outer(B[1], B[1]))
+            out[o:o + nb] = np.linalg.solve(M1, (A[2:] * wg) @ rem)
 
-            def edge_coeffs(a, b):
-                k = ("e", min(a, b), max(a, b))
-                c = out[self._base[k]:self._base[k] + nb].copy()
-                if a > b:  # face direction runs against the edge's numbering
-                    c *= (-1.0) ** np.arange(2, nm)
-                return c
-            for (a, b, side, along) in ((O, nA, 0, "a"), (nB, AB, 1, "a"), (O, nB, 0, "b"),
-                                        (nA, AB, 1, "b")):
-                c = edge_coeffs(a, b)
-                prof = c @ B[2:]  # bubble sum along the edge, (nq,)
-                if along == "a":
-                    ub = ub + np.outer(prof, B[side])
-                else:
-                    ub = ub + np.outer(B[side], prof)
-            W = np.outer(w, w) * J
-            Bi = B[2:]
-            rhs = np.einsum("ai,bj,ij->ab", Bi, Bi, W * (vals_f - ub)).reshape(-1)
-            M2 = np.einsum("ai,ci,bj,dj,ij->abcd", Bi, Bi, Bi, Bi, W).reshape(nb * nb, nb * nb)
-            c = np.linalg.solve(M2, rhs) if nb > 0 else np.zeros(0)
-            o = self._base[key]
-            out[o:o + nb * nb] = c
+        def edge_coeffs(a, b):
+            k = ("e", min(a, b), max(a, b))
+            c = out[self._base[k]:self._base[k] + nb].copy()
+            if a > b:  # face direction runs against the edge's numbering
+                c *= (-1.0) ** np.arange(2, nm)
+            return c
+
+        for f, bc in self._face_bc.items():
+            kind, es = g.faces[f]
+            if nb == 0:
+                continue
+            if kind == "Q":
+                self._quad_face(f, bc, time, out, vals, edge_coeffs, A, zg, wg, nm)
+            else:
+                self._tri_face(f, bc, time, out, vals, edge_coeffs, A, zg, wg, Brow, zr, wr, nm)
         return out
 
+    def _quad_face(self, f, bc, time, out, vals, edge_coeffs, A, z, w, nm):
+        g = self.session.geometry
+        nb = nm - 2
+        cyc = self._face_cycle(f)
+        i0 = int(np.argmin(cyc))
+        O = cyc[i0]
+        nA, nB = cyc[(i0 + 1) % 4], cyc[(i0 - 1) % 4]
+        if nA > nB:
+            nA, nB = nB, nA
+        AB = cyc[(i0 + 2) % 4]
+        P = lambda v: np.asarray(g.vertices[v], dtype=np.float64)  # noqa: E731
+        XO, XA, XB, XAB = P(O), P(nA), P(nB), P(AB)
+        za, zb = np.meshgrid(z, z, indexing="ij")
+        Na = [0.5 * (1 - za), 0.5 * (1 + za)]
+        Nb = [0.5 * (1 - zb), 0.5 * (1 + zb)]
+        x = (Na[0] * Nb[0])[..., None] * XO + (Na[1] * Nb[0])[..., None] * XA + \
+            (Na[0] * Nb[1])[..., None] * XB + (Na[1] * Nb[1])[..., None] * XAB
+        dxa = (0.5 * Nb[0])[..., None] * (XA - XO) + (0.5 * Nb[1])[..., None] * (XAB - XB)
+        dxb = (0.5 * Na[0])[..., None] * (XB - XO) + (0.5 * Na[1])[..., None] * (XAB - XA)
+        J = np.linalg.norm(np.cross(dxa, dxb), axis=-1)
+        fv = bc.value.evaluate(x[..., 0], x[..., 1], x[..., 2], time)
+        ub = (vals[O] * np.outer(A[0], A[0]) + vals[nA] * np.outer(A[1], A[0])
+              + vals[nB] * np.outer(A[0], A[1]) + vals[AB] * np.outer(A[1], A[1]))
+        for (a, b, side, along) in ((O, nA, 0, "a"), (nB, AB, 1, "a"), (O, nB, 0, "b"),
+                                    (nA, AB, 1, "b")):
+            prof = edge_coeffs(a, b) @ A[2:]
+            ub = ub + (np.outer(prof, A[side]) if along == "a" else np.outer(A[side], prof))
+        W = np.outer(w, w) * J
+        Bi = A[2:]
+        rhs = np.einsum("ai,bj,ij->ab", Bi, Bi, W * (fv - ub)).reshape(-1)
+        M2 = np.einsum("ai,ci,bj,dj,ij->abcd", Bi, Bi, Bi, Bi, W).reshape(nb * nb, nb * nb)
+        key = ("f",) + tuple(sorted(cyc))
+        o = self._base[key]
+        out[o:o + nb * nb] = np.linalg.solve(M2, rhs)
+
+    def _tri_face(self, f, bc, time, out, vals, edge_coeffs, A, zs, ws, Brow, zt, wt, nm):
+        """Constrained projection on a triangle in its canonical frame
+        (origin, end of axis a, apex): modes phi_p(s) psi_pq(t), the apex
+        vertex mode psi_01(t) (the collapsed-vertex fix of StdTriExp)."""
+        g = self.session.geometry
+        vs = sorted({v for e in g.faces[f][1] for v in g.edges[e]})
+        key = ("t",) + tuple(vs)
+        apex, O = self._tri_frame[key]
+        E = [v for v in vs if v not in (apex, O)][0]
+        P = lambda v: np.asarray(g.vertices[v], dtype=np.float64)  # noqa: E731
+        XO, XE, XC = P(O), P(E), P(apex)
+        S, T = np.meshgrid(zs, zt, indexing="ij")  # [i (s), j (t)]
+        xa = 0.5 * (1 + S) * (1 - T) - 1
+        xb = T
+        x = (-0.5 * (xa + xb))[..., None] * XO + (0.5 * (1 + xa))[..., None] * XE + \
+            (0.5 * (1 + xb))[..., None] * XC
+        J = np.linalg.norm(np.cross(0.5 * (XE - XO), 0.5 * (XC - XO)))
+        fv = bc.value.evaluate(x[..., 0], x[..., 1], x[..., 2], time)
+        phi = A  # (nm, nq_s)
+        ub = (vals[O] * np.outer(phi[0], Brow[(0, 0)]) + vals[E] * np.outer(phi[1], Brow[(1, 0)])
+              + vals[apex] * np.outer(np.ones_like(zs), Brow[(0, 1)]))
+        for k, c in zip(range(2, nm), edge_coeffs(O, E)):
+            ub = ub + c * np.outer(phi[k], Brow[(k, 0)])
+        for k, c in zip(range(2, nm), edge_coeffs(O, apex)):
+            ub = ub + c * np.outer(phi[0], Brow[(0, k)])
+        for k, c in zip(range(2, nm), edge_coeffs(E, apex)):
+            ub = ub + c * np.outer(phi[1], Brow[(1, k - 1)])
+        modes = [(a, b) for a in range(2, nm) for b in range(1, nm - a)]
+        if not modes:
+            return
+        F = np.stack([np.outer(phi[a], Brow[(a, b)]) for a, b in modes])  # (nmodes, s, t)
+        W = np.outer(ws, wt) * J
+        rhs = np.einsum("mij,ij->m", F, W * (fv - ub))
+        M = np.einsum("mij,nij,ij->mn", F, F, W)
+        o = self._base[key]
+        out[o:o + len(modes)] = np.linalg.solve(M, rhs)
+
     def _face_cycle(self, f):
-        """The 4 global vertex ids of face f in cyclic order."""
+        """The global vertex ids of face f in cyclic order."""
         g = self.session.geometry
         es = [g.edges[e] for e in g.faces[f][1]]
         cyc = [es[0][0], es[0][1]]
-        while len(cyc) < 4:
+        n = len(es)
+        while len(cyc) < n:
             last = cyc[-1]
             for a, b in es:
                 if a == last and b not in cyc:
@@ -397,13 +662,18 @@ class SessionMesh:
         """Local coefficient vector holding the Dirichlet values (zeros
         elsewhere), the x_loc a solve takes for the lifting."""
         dv = self.dirichlet_values(time)
-        x = np.zeros(self.nelmt * self.nc)
+        x = np.zeros(self.nloc)
         mask = self.gmap < self.ndir
         x[mask] = self.sign[mask] * dv[self.gmap[mask]]
         return x
 
     def quad_weights(self):
-        """W = jac * w0 w1 w2 at every quadrature point (integration weights)."""
-        w = [np.asarray(v) for v in self.T["w"]]
-        wq = np.einsum("k,j,i->kji", w[2], w[1], w[0]).reshape(-1)
-        return self.jac * np.tile(wq, self.nelmt)
+        return np.concatenate([c.quad_weights() for c in self.collections])
+
+    def split(self, vec, per="coeff"):
+        """Per-collection views of a concatenated local (coeff) or physical
+        (phys) vector."""
+        if per == "coeff":
+            return [vec[self.offsets[i]:self.offsets[i + 1]] for i in range(len(self.collections))]
+        off = np.cumsum([0] + [c.nelmt * c.nt for c in self.collections])
+        return [vec[off[i]:off[i + 1]] for i in range(len(self.collections))]

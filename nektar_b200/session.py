@@ -380,3 +380,122 @@ def write_hex_box_session(n, nummodes, lam, dirichlet, forcing, exact, lengths=(
               "  </CONDITIONS>", "</NEKTAR>"]
     return "\n".join(lines) + "\n"
 
+
+def write_box_session(shape, n, nummodes, lam, dirichlet, forcing, exact, shuffle_seed=None):
+    """XML text of a session on the unit cube cut into n^3 cells, each a
+    hexahedron, two prisms (triangles in the x-z plane, extruded along y) or
+    six tetrahedra (the cell split along its main diagonal), with Dirichlet
+    data on all six sides. Elements list their faces in the order of the
+    reference's geometry classes; a triangle lists its edges starting with
+    the one between its two lowest vertex ids, which is what TetGeom expects
+    of a face's first edge; every tetrahedron has its vertices in increasing
+    id (v0 and v1 swapped where that would invert it), so neighbouring
+    triangles collapse towards the same vertex. shuffle_seed (hexahedra:
+    random frames, see write_hex_box_session; prisms and tetrahedra: random
+    edge directions and quadrilateral edge lists)."""
+    if shape == "hex":
+        return write_hex_box_session(n, nummodes, lam, dirichlet, forcing, exact,
+                                     shuffle_seed=shuffle_seed)
+    # "hexprism": hexahedra for x < 1/2, prisms for x > 1/2 (two collections)
+    rng = np.random.default_rng(shuffle_seed) if shuffle_seed is not None else None
+    N = n + 1
+    vid = lambda i, j, k: (k * N + j) * N + i  # noqa: E731
+    coords = {vid(i, j, k): (i / n, j / n, k / n) for k in range(N) for j in range(N)
+              for i in range(N)}
+    edges, emap, faces, fmap = [], {}, [], {}
+
+    def edge(a, b):
+        key = (min(a, b), max(a, b))
+        if key not in emap:
+            emap[key] = len(edges)
+            edges.append((b, a) if rng is not None and rng.integers(2) else (a, b))
+        return emap[key]
+
+    def face(cyc):
+        key = tuple(sorted(cyc))
+        if key not in fmap:
+            if len(cyc) == 3:
+                lo = sorted(cyc)[:2]
+                rest = [v for v in cyc if v not in lo][0]
+                es = [edge(lo[0], lo[1]), edge(lo[1], rest), edge(rest, lo[0])]
+            else:
+                es = [edge(cyc[m], cyc[(m + 1) % 4]) for m in range(4)]
+                if rng is not None:
+                    r = int(rng.integers(4))
+                    es = es[r:] + es[:r]
+            fmap[key] = len(faces)
+            faces.append(("T" if len(cyc) == 3 else "Q", es))
+        return fmap[key]
+
+    elems = []
+    for k in range(n):
+        for j in range(n):
+            for i in range(n):
+                c = lambda a, b, cc: vid(i + a, j + b, k + cc)  # noqa: E731
+                if shape == "hexprism" and 2 * i < n:
+                    v = [c(0, 0, 0), c(1, 0, 0), c(1, 1, 0), c(0, 1, 0), c(0, 0, 1), c(1, 0, 1),
+                         c(1, 1, 1), c(0, 1, 1)]
+                    elems.append(("H", [face([v[0], v[1], v[2], v[3]]), face([v[0], v[1], v[5], v[4]]),
+                                        face([v[1], v[2], v[6], v[5]]), face([v[3], v[2], v[6], v[7]]),
+                                        face([v[0], v[3], v[7], v[4]]), face([v[4], v[5], v[6], v[7]])]))
+                elif shape in ("prism", "hexprism"):
+                    for v in ([c(0, 0, 0), c(1, 0, 0), c(1, 1, 0), c(0, 1, 0), c(0, 0, 1), c(0, 1, 1)],
+                              [c(1, 0, 1), c(0, 0, 1), c(0, 1, 1), c(1, 1, 1), c(1, 0, 0), c(1, 1, 0)]):
+                        elems.append(("R", [face([v[0], v[1], v[2], v[3]]), face([v[0], v[1], v[4]]),
+                                            face([v[1], v[2], v[5], v[4]]), face([v[3], v[2], v[5]]),
+                                            face([v[0], v[3], v[5], v[4]])]))
+                else:
+                    import itertools
+                    for perm in itertools.permutations(range(3)):
+                        pos = [0, 0, 0]
+                        path = [c(0, 0, 0)]
+                        for ax in perm[:2]:
+                            pos[ax] = 1
+                            path.append(c(*pos))
+                        path.append(c(1, 1, 1))
+                        v = sorted(path)
+                        X = np.array([coords[x] for x in v])
+                        if np.linalg.det(np.array([X[1] - X[0], X[2] - X[0], X[3] - X[0]])) < 0:
+                            v[0], v[1] = v[1], v[0]
+                        elems.append(("A", [face([v[0], v[1], v[2]]), face([v[0], v[1], v[3]]),
+                                            face([v[1], v[2], v[3]]), face([v[0], v[2], v[3]])]))
+    bnd = {s_: [] for s_ in range(6)}
+    for fid, (kind, es) in enumerate(faces):
+        vs = {x for ed in es for x in edges[ed]}
+        ijk = [(x % N, (x // N) % N, x // (N * N)) for x in vs]
+        for side, (ax, val) in enumerate(((2, 0), (1, 0), (0, n), (1, n), (0, 0), (2, n))):
+            if all(t[ax] == val for t in ijk):
+                bnd[side].append(fid)
+    lines = ['<?xml version="1.0" encoding="utf-8" ?>', "<NEKTAR>",
+             '  <GEOMETRY DIM="3" SPACE="3">', "    <VERTEX>"]
+    lines += ['      <V ID="%d">%.17g %.17g %.17g</V>' % ((v,) + coords[v]) for v in sorted(coords)]
+    lines += ["    </VERTEX>", "    <EDGE>"]
+    lines += ['      <E ID="%d"> %d %d </E>' % (e, a, b) for e, (a, b) in enumerate(edges)]
+    lines += ["    </EDGE>", "    <FACE>"]
+    lines += ['      <%s ID="%d"> %s </%s>' % (kd, f, " ".join(map(str, es)), kd)
+              for f, (kd, es) in enumerate(faces)]
+    lines += ["    </FACE>", "    <ELEMENT>"]
+    lines += ['      <%s ID="%d"> %s </%s>' % (t, e, " ".join(map(str, fs)), t)
+              for e, (t, fs) in enumerate(elems)]
+    # one domain composite per element type (C[0], C[7], ...), boundary sides C[1-6]
+    kinds = sorted({t for t, _ in elems}, key="HRA".index)
+    cids = {t: (0 if m == 0 else 6 + m) for m, t in enumerate(kinds)}
+    lines += ["    </ELEMENT>", "    <COMPOSITE>"]
+    lines += ['      <C ID="%d"> %s[%s] </C>' % (cids[t], t, _seq([e for e, (tt, _) in enumerate(elems)
+                                                                 if tt == t])) for t in kinds]
+    lines += ['      <C ID="%d"> F[%s] </C>' % (s_ + 1, _seq(bnd[s_])) for s_ in range(6)]
+    dom = ",".join(str(cids[t]) for t in kinds)
+    lines += ["    </COMPOSITE>", "    <DOMAIN> C[%s] </DOMAIN>" % dom, "  </GEOMETRY>",
+              "  <EXPANSIONS>",
+              '    <E COMPOSITE="C[%s]" NUMMODES="%d" FIELDS="u" TYPE="MODIFIED" />' % (dom, nummodes),
+              "  </EXPANSIONS>", "  <CONDITIONS>", "    <PARAMETERS>",
+              "      <P> Lambda = %.17g </P>" % lam, "    </PARAMETERS>",
+              '    <VARIABLES> <V ID="0"> u </V> </VARIABLES>',
+              '    <BOUNDARYREGIONS> <B ID="0"> C[1-6] </B> </BOUNDARYREGIONS>',
+              "    <BOUNDARYCONDITIONS>", '      <REGION REF="0">',
+              '        <D VAR="u" VALUE="%s" />' % dirichlet, "      </REGION>",
+              "    </BOUNDARYCONDITIONS>",
+              '    <FUNCTION NAME="Forcing"> <E VAR="u" VALUE="%s" /> </FUNCTION>' % forcing,
+              '    <FUNCTION NAME="ExactSolution"> <E VAR="u" VALUE="%s" /> </FUNCTION>' % exact,
+              "  </CONDITIONS>", "</NEKTAR>"]
+    return "\n".join(lines) + "\n"
