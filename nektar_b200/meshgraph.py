@@ -336,6 +336,15 @@ def _tables_1d(nm):
 # collections and the mesh
 # ---------------------------------------------------------------------------
 
+def _interp_matrix(zfrom, zto):
+    """Lagrange interpolation from the points zfrom to the points zto
+    (LibUtilities::Interp1D)."""
+    n = len(zfrom)
+    Vf = np.polynomial.legendre.legvander(zfrom, n - 1)
+    Vt = np.polynomial.legendre.legvander(zto, n - 1)
+    return Vt @ np.linalg.inv(Vf)
+
+
 class Collection:
     """One operator collection: elements of one shape and order, with the
     attributes nektar_b200.Operator takes."""
@@ -658,14 +667,189 @@ class SessionMesh:
                 raise SessionError("face %d is not a closed cycle" % f)
         return cyc
 
-    def dirichlet_local(self, time=0.0):
+    def dirichlet_local(self, time=0.0, consistent=False):
         """Local coefficient vector holding the Dirichlet values (zeros
-        elsewhere), the x_loc a solve takes for the lifting."""
-        dv = self.dirichlet_values(time)
+        elsewhere), the x_loc a solve takes for the lifting.
+
+        By default built as ContField::v_ImposeDirichletConditions builds it
+        in a serial run (ContField.cpp:557-613): every Dirichlet boundary
+        face, in boundary-region, composite and listed order, projects the
+        data with its own expansion's FwdTransBndConstrained in its own frame
+        and writes the result into its element's local coefficients, later
+        faces overwriting shared vertex and edge modes (the max-abs merge of
+        :602 only acts across partitions). On a triangle
+        (TriExp::v_FwdTransBndConstrained) the data of edges 1 and 2 are
+        interpolated from the Gauss-Radau points to GLL points before their
+        1-D projection and edge 2 is written last, so the apex value is the
+        extrapolation along edge 2. consistent=True instead takes one global
+        value per Dirichlet dof (dirichlet_values)."""
         x = np.zeros(self.nloc)
         mask = self.gmap < self.ndir
-        x[mask] = self.sign[mask] * dv[self.gmap[mask]]
+        if consistent:
+            dv = self.dirichlet_values(time)
+            x[mask] = self.sign[mask] * dv[self.gmap[mask]]
+            return x
+        owner = self._face_owners()
+        g, s = self.session.geometry, self.session
+        written, src = np.zeros(self.nloc, dtype=bool), {}
+        for f in self._boundary_face_order():
+            if f not in self._face_bc:
+                continue
+            vals = self._face_values(f, self._face_bc[f], time)
+            lo, hi = owner[f]
+            gm, sg = self.gmap[lo:hi], self.sign[lo:hi]
+            for i, gd in enumerate(gm):
+                if gd in vals:
+                    x[lo + i] = sg[i] * vals[gd]
+                    written[lo + i] = True
+                    src[int(gd)] = lo + i  # the last write of each dof
+        # local copies of Dirichlet dofs on elements that touch the boundary
+        # only at an edge or vertex take the last written copy's value
+        # (AssemblyMapCG.cpp:1925-2010, the copyLocalDirDofs of :609-613)
+        for k in np.nonzero(mask & ~written)[0]:
+            j = src[int(self.gmap[k])]
+            x[k] = x[j] * self.sign[j] * self.sign[k]
         return x
+
+    def _boundary_face_order(self):
+        """Dirichlet faces in the order of the reference's boundary expansions:
+        regions in id order; within a region its composites in id order, the
+        faces grouped by expansion type (basis and regular / deformed
+        geometry) in order of first appearance, listed order within a group
+        (ExpList's CompositeMap constructor, ExpList.cpp:1436-1462)."""
+        g, s = self.session.geometry, self.session
+        P = lambda v: np.asarray(g.vertices[v], dtype=np.float64)  # noqa: E731
+        out = []
+        for rid in sorted(s.boundary_regions):
+            groups = {}
+            for c in sorted(s.boundary_regions[rid]):
+                if c not in g.composites:
+                    continue
+                for f in g.composites[c][1]:
+                    kind = g.faces[f][0]
+                    regular = True
+                    if kind == "Q":  # a parallelogram has a constant Jacobian
+                        cyc = [P(v) for v in self._face_cycle(f)]
+                        regular = bool(np.allclose(cyc[0] + cyc[2], cyc[1] + cyc[3],
+                                                   rtol=0, atol=1e-12))
+                    groups.setdefault((kind, regular), []).append(f)
+            for lst in groups.values():  # dicts keep first-appearance order
+                out.extend(lst)
+        return out
+
+    def _face_owners(self):
+        """Local coefficient range of the element that owns each boundary face."""
+        g = self.session.geometry
+        out = {}
+        for ci, col in enumerate(self.collections):
+            base = int(self.offsets[ci])
+            for el, eid in enumerate(col.elem_ids):
+                for f in g.elements[eid][1]:
+                    if f in self._face_bc:
+                        out[f] = (base + el * col.nc, base + (el + 1) * col.nc)
+        return out
+
+    def _face_values(self, f, bc, time):
+        """{global dof: value} of the Dirichlet face f's boundary-constrained
+        projection, as the face's own expansion computes it."""
+        g = self.session.geometry
+        nm = self.collections[0].nm
+        nb = nm - 2
+        A, zg, wg, Brow, zr, wr = _tables_1d(nm)
+        P = lambda v: np.asarray(g.vertices[v], dtype=np.float64)  # noqa: E731
+        kind, es = g.faces[f]
+        E = [g.edges[e] for e in es]
+        # the face's own frame: vertex j starts edge j (TriGeom / QuadGeom)
+        fv = []
+        for j in range(len(E)):
+            a, b = E[j]
+            nxt = E[(j + 1) % len(E)]
+            fv.append(a if b in nxt else b)
+        vals = {}
+        M1 = (A[2:] * wg) @ A[2:].T
+
+        def proj1d(data):
+            c = np.zeros(nm)
+            c[0], c[1] = data[0], data[-1]
+            if nb:
+                rem = data - c[0] * A[0] - c[1] * A[1]
+                c[2:] = np.linalg.solve(M1, (A[2:] * wg) @ rem)
+            return c
+
+        def put_edge(a, b, c):
+            key = ("e", min(a, b), max(a, b))
+            o = self._base[key]
+            cc = c[2:] * ((-1.0) ** np.arange(2, nm) if a > b else 1.0)
+            for k in range(nb):
+                vals[o + k] = cc[k]
+
+        bcv = lambda x: bc.value.evaluate(x[..., 0], x[..., 1], x[..., 2], time)  # noqa: E731
+        if kind == "Q":
+            # symmetric GLL points: the same polynomial in every frame
+            for v in fv:
+                vals[self._base[("v", v)]] = float(bcv(P(v)))
+            for j in range(4):
+                a, b = fv[j], fv[(j + 1) % 4]
+                x = np.outer(0.5 * (1 - zg), P(a)) + np.outer(0.5 * (1 + zg), P(b))
+                put_edge(a, b, proj1d(bcv(x)))
+            if nb:
+                out = np.zeros(self.ndir)
+                for gd, v in vals.items():
+                    out[gd] = v
+                vtab = {v: vals[self._base[("v", v)]] for v in fv}
+
+                def ec(a, b):
+                    k = ("e", min(a, b), max(a, b))
+                    c = out[self._base[k]:self._base[k] + nb].copy()
+                    return c * ((-1.0) ** np.arange(2, nm)) if a > b else c
+                self._quad_face(f, bc, time, out, vtab, ec, A, zg, wg, nm)
+                key = ("f",) + tuple(sorted(fv))
+                o = self._base[key]
+                for k in range(nb * nb):
+                    vals[o + k] = out[o + k]
+            return vals
+        # triangle in its own frame: v0 -> v1 along s, apex v2 along t
+        v0, v1, v2 = fv
+        X0, X1, X2 = P(v0), P(v1), P(v2)
+        S, T = np.meshgrid(zg, zr, indexing="ij")
+        xa = 0.5 * (1 + S) * (1 - T) - 1
+        x = (-0.5 * (xa + T))[..., None] * X0 + (0.5 * (1 + xa))[..., None] * X1 + \
+            (0.5 * (1 + T))[..., None] * X2
+        data = bcv(x)  # [s, t]
+        I = _interp_matrix(zr, zg)  # Gauss-Radau -> GLL
+        c0 = proj1d(data[:, 0])
+        c1 = proj1d(I @ data[-1, :])
+        c2 = proj1d(I @ data[0, :])
+        vtab = {v0: c2[0], v1: c1[0], v2: c2[1]}  # edge 2 written last
+        vtab[v1] = c1[0]
+        for v, val in vtab.items():
+            vals[self._base[("v", v)]] = val
+        put_edge(v0, v1, c0)
+        put_edge(v1, v2, c1)
+        put_edge(v0, v2, c2)
+        key = ("t",) + tuple(sorted(fv))
+        capex, corigin = self._tri_frame[key]
+        if capex != v2:
+            raise SessionError("boundary triangle %d collapses towards %d, its element towards %d"
+                               % (f, v2, capex))
+        modes = [(a, b) for a in range(2, nm) for b in range(1, nm - a)]
+        if modes:
+            phi = A
+            ub = (vtab[v0] * np.outer(phi[0], Brow[(0, 0)]) + vtab[v1] * np.outer(phi[1], Brow[(1, 0)])
+                  + vtab[v2] * np.outer(np.ones_like(zg), Brow[(0, 1)]))
+            for k in range(2, nm):
+                ub = ub + c0[k] * np.outer(phi[k], Brow[(k, 0)]) \
+                    + c2[k] * np.outer(phi[0], Brow[(0, k)]) + c1[k] * np.outer(phi[1], Brow[(1, k - 1)])
+            F = np.stack([np.outer(phi[a], Brow[(a, b)]) for a, b in modes])
+            J = np.linalg.norm(np.cross(0.5 * (X1 - X0), 0.5 * (X2 - X0)))
+            W = np.outer(wg, wr) * J
+            c = np.linalg.solve(np.einsum("mij,nij,ij->mn", F, F, W),
+                                np.einsum("mij,ij->m", F, W * (data - ub)))
+            refl = v0 != corigin
+            o = self._base[key]
+            for pos, (a, b) in enumerate(modes):
+                vals[o + pos] = c[pos] * ((-1.0) ** a if refl else 1.0)
+        return vals
 
     def quad_weights(self):
         return np.concatenate([c.quad_weights() for c in self.collections])

@@ -386,11 +386,13 @@ def write_box_session(shape, n, nummodes, lam, dirichlet, forcing, exact, shuffl
     hexahedron, two prisms (triangles in the x-z plane, extruded along y) or
     six tetrahedra (the cell split along its main diagonal), with Dirichlet
     data on all six sides. Elements list their faces in the order of the
-    reference's geometry classes; a triangle lists its edges starting with
-    the one between its two lowest vertex ids, which is what TetGeom expects
-    of a face's first edge; every tetrahedron has its vertices in increasing
-    id (v0 and v1 swapped where that would invert it), so neighbouring
-    triangles collapse towards the same vertex. shuffle_seed (hexahedra:
+    reference's geometry classes; every tetrahedron has its vertices in
+    increasing id (v0 and v1 swapped where that would invert it), so
+    neighbouring triangles collapse towards the same vertex and each face's
+    first edge is the one TetGeom expects; a triangle lists its edges
+    origin -> end of axis a -> apex of the element that first uses it, so
+    that its own frame (TriGeom: vertex j starts edge j) collapses towards the
+    element's apex. shuffle_seed (hexahedra:
     random frames, see write_hex_box_session; prisms and tetrahedra: random
     edge directions and quadrilateral edge lists)."""
     if shape == "hex":
@@ -415,9 +417,9 @@ def write_box_session(shape, n, nummodes, lam, dirichlet, forcing, exact, shuffl
         key = tuple(sorted(cyc))
         if key not in fmap:
             if len(cyc) == 3:
-                lo = sorted(cyc)[:2]
-                rest = [v for v in cyc if v not in lo][0]
-                es = [edge(lo[0], lo[1]), edge(lo[1], rest), edge(rest, lo[0])]
+                # (origin, end of axis a, apex): the triangle's own frame has
+                # its vertex 2 where the element collapses it
+                es = [edge(cyc[0], cyc[1]), edge(cyc[1], cyc[2]), edge(cyc[2], cyc[0])]
             else:
                 es = [edge(cyc[m], cyc[(m + 1) % 4]) for m in range(4)]
                 if rng is not None:

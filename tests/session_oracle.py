@@ -33,15 +33,28 @@ def oracle_helm_solve(session, mesh=None):
             np.add.at(G, (gm[e][:, None], gm[e][None, :]), sg[e][:, None] * K[e] * sg[e][None, :])
         b_loc.append(-O.iproduct(c.shape, c.nm, c.nq, ne, To["b"], To["w"], c.jac, fc, True))
     b_loc = np.concatenate(b_loc)
+    # lifting with the local Dirichlet values element by element, as
+    # GlobalLinSysIterativeFull::v_Solve does (GlobalLinSysIterativeFull.cpp:114-164)
+    xdl = m.dirichlet_local()
+    r_loc = b_loc - _apply_blocks(m, lam, xdl)
     b = np.zeros(m.nglob)
-    np.add.at(b, m.gmap, m.sign * b_loc)
-    xd = m.dirichlet_values()
+    np.add.at(b, m.gmap, m.sign * r_loc)
     nd = m.ndir
-    xg = np.concatenate([xd, np.linalg.solve(G[nd:, nd:], b[nd:] - G[nd:, :nd] @ xd)])
-    xl = m.sign * xg[m.gmap]
+    xg = np.concatenate([np.zeros(nd), np.linalg.solve(G[nd:, nd:], b[nd:])])
+    xl = xdl + m.sign * xg[m.gmap]
     for c, xc in zip(m.collections, m.split(xl)):
         us.append(O.bwdtrans(c.shape, c.nm, c.nq, c.nelmt, c.T["b"], xc))
     u = np.concatenate(us)
     ue = session.function("ExactSolution").evaluate(*m.xyz)
     W = m.quad_weights()
     return xl, float(np.max(np.abs(u - ue))), float(np.sqrt(np.sum(W * (u - ue) ** 2)))
+
+
+def _apply_blocks(m, lam, x_loc):
+    """Element Helmholtz operators of every collection on a local vector."""
+    out = []
+    for c, xc in zip(m.collections, m.split(x_loc)):
+        To = dict(c.T)
+        To["w"] = c.T["ws"]
+        out.append(O.helmholtz(c.shape, c.nm, c.nq, c.nelmt, To, c.jac, c.df, xc, lam, True))
+    return np.concatenate(out)
