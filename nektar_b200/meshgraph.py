@@ -37,16 +37,17 @@ from the lower of the two base vertices, and a reflected element face gets
 rejected, as the reference requires compatible collapsed directions.
 
 Dirichlet values (ExpList::FwdTransBndConstrained on the boundary faces,
-QuadExp.cpp:67-170, TriExp.cpp, SegExp.cpp:81-180): vertex modes take the
-point values, edge bubbles the L2 projection of the remainder at GLL points
-along the edge, face bubbles the L2 projection of the remainder with the
-face's quadrature (GLL x GLL, or GLL x Gauss-Radau on a triangle) and
-surface Jacobian. On hexahedral boundaries this is the reference's result.
-On triangular boundary faces the reference instead interpolates the data of
-the two collapsed-direction edges from the Radau points to GLL points
-before projecting (so the apex value is extrapolated) and writes the faces'
-results one after another; that is not restated, so Prism/Tet solves agree
-with the reference's to the accuracy of that interpolation, not to rounding.
+QuadExp.cpp:67-170, TriExp::v_FwdTransBndConstrained, SegExp.cpp:81-180):
+vertex modes take the point values, edge bubbles the constrained L2
+projection at GLL points along the edge, face bubbles the constrained L2
+projection with the face's quadrature (GLL x GLL, or GLL x Gauss-Radau on a
+triangle) and surface Jacobian. A triangle works in its own frame and
+interpolates the data of its edges 1 and 2 from the Gauss-Radau points to
+GLL points first, so its apex value is an extrapolation. The local Dirichlet
+vector a solve takes is built as the reference builds it
+(dirichlet_local): face by face into each face's element, later faces
+overwriting, then copied to elements that only touch the boundary; with it
+the reference's Hex, Prism and Tet regression errors are reproduced.
 """
 import numpy as np
 
