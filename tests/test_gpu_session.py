@@ -1,7 +1,6 @@
 """Session solves on the device (operators and CG through the C ABI) against
 the reference's recorded errors for Helmholtz3D_CG_Hex.tst (L2 1.11818e-07,
 Linf 5.66374e-07, tolerance 1e-12) and against the oracle's dense solve."""
-import numpy as np
 import pytest
 
 from nektar_b200.helmsolve import helm_solve

@@ -5,7 +5,6 @@ It stages through one static 32 MiB device array instead of cudaMalloc'd
 buffers. Checked through the C ABI against nkb_op_apply with host pointers on
 two calls in a row (the array keeps the previous call's contents). Collected
 last so that a run stopping at the first failure has run every other test."""
-import ctypes
 
 import numpy as np
 import pytest
