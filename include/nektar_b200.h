@@ -56,6 +56,7 @@ extern "C" {
 #define NKB_IPRODUCT 3  /* Collections::eIProductWRTBase */
 #define NKB_IPRODUCT_DERIV 4 /* Collections::eIProductWRTDerivBase */
 #define NKB_PHYSDERIV 5 /* Collections::ePhysDeriv */
+#define NKB_DENSE_BLOCK 64 /* per-element dense matrices (no Collections counterpart) */
 
 #define NKB_GLL 4       /* LibUtilities::eGaussLobattoLegendre */
 #define NKB_RADAU_A1 11 /* LibUtilities::eGaussRadauMAlpha1Beta0 */
@@ -142,6 +143,14 @@ typedef struct nkb_op_desc
 /* Replaces OPERATOR_CREATE(...)::create + the MatrixFree constructors
  * (Helmholtz.cpp:713-760 etc.): uploads tables, packs the geometry. */
 int nkb_op_create(const nkb_op_desc *desc, nkb_op **op);
+
+/* Per-element dense operator y_e = M_e x_e: nelmt blocks of n x n FP64
+ * matrices (host, row-major, element after element), e.g. the Schur
+ * complements of a statically condensed Helmholtz system
+ * (GlobalLinSysIterativeStaticCond.cpp). It applies, gathers and feeds a CG
+ * system's Jacobi preconditioner (its diagonal) like a Helmholtz operator;
+ * in and out are nelmt*n values. n <= 6144. */
+int nkb_op_create_dense(int n, int nelmt, const double *mats, int device, nkb_op **op);
 
 /* Replaces Helmholtz_MatrixFree::UpdateFactors (Helmholtz.cpp:615-691):
  * lambda (eFactorLambda); diff_mode NKB_DIFF_CONST with diff =
@@ -252,7 +261,7 @@ typedef struct nkb_sys nkb_sys;
 typedef struct nkb_sys_desc
 {
     int nops;             /* Helmholtz operators (collections), in local-space order */
-    nkb_op *const *ops;   /* FP64 Helmholtz operators */
+    nkb_op *const *ops;   /* FP64 Helmholtz (or NKB_DENSE_BLOCK) operators */
     nkb_op *const *ops32; /* optional FP32 twins for mixed precision (or NULL) */
     long nloc;            /* local coefficients = sum of nelmt*ncoeffs */
     int nglob;            /* global coefficients, Dirichlet ones first */

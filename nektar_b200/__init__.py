@@ -302,6 +302,54 @@ class Batch:
             pass
 
 
+class DenseOperator:
+    """Per-element dense operator y_e = M_e x_e (nkb_op_create_dense): mats
+    (nelmt, n, n) FP64, e.g. the Schur complements of static condensation.
+    Usable wherever a Helmholtz Operator is (GlobalLinSys, apply)."""
+
+    def __init__(self, mats, device=0):
+        mats = np.ascontiguousarray(mats, dtype=np.float64)
+        self.nelmt, n, n2 = mats.shape
+        if n != n2:
+            raise ValueError("blocks must be square")
+        self.n, self.precision, self.optype = n, FP64, C.DENSE_BLOCK
+        h = ctypes.c_void_p()
+        check(lib().nkb_op_create_dense(n, self.nelmt, mats.ctypes.data, device, ctypes.byref(h)))
+        self.h = h
+        self.in_size = self.out_size = self.nelmt * n
+
+    def __call__(self, x):
+        x = _f64(x)
+        if x.size != self.in_size:
+            raise ValueError("input size %d != %d" % (x.size, self.in_size))
+        y = np.zeros(self.out_size)
+        check(lib().nkb_op_apply(self.h, x.ctypes.data, y.ctypes.data, None, None, HOST_PTRS,
+                                 None))
+        return y
+
+    def apply_device(self, x_ptr, y_ptr, stream=None):
+        check(lib().nkb_op_apply(self.h, x_ptr, y_ptr, None, None, DEVICE_PTRS, stream))
+
+    def kernel(self, gather=False):
+        return lib().nkb_op_kernel(self.h, int(bool(gather))).decode()
+
+    def last_kernel_ms(self):
+        ms = ctypes.c_float()
+        check(lib().nkb_op_last_kernel_ms(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().nkb_op_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class GlobalLinSys:
     """GlobalLinSysIterativeFull + PreconditionerDiagonal + NekLinSysIterCG."""
 
@@ -310,7 +358,7 @@ class GlobalLinSys:
         FP32 twins (same meshes) enabling the mixed-precision solve."""
         self.ops = list(ops)
         self.ops32 = None if ops32 is None else list(ops32)
-        self.nloc = int(sum(o.nelmt * ncoeffs(o.shape, o.nm) for o in self.ops))
+        self.nloc = int(sum(o.in_size for o in self.ops))
         self.nglob, self.ndir = int(nglob), int(ndir)
         gmap = np.ascontiguousarray(gmap, dtype=np.int32)
         sign = None if sign is None else _f64(sign)

@@ -26,6 +26,7 @@ NKB_ERR_NO_DEVICE = -7
 
 TET, PRISM, HEX = 5, 7, 8
 BWDTRANS, HELMHOLTZ, LINEAR_ADR, IPRODUCT, IPRODUCT_DERIV, PHYSDERIV = 0, 1, 2, 3, 4, 5
+DENSE_BLOCK = 64
 GLL, RADAU_A1, RADAU_A2 = 4, 11, 12
 MODIFIED_A, MODIFIED_B, MODIFIED_C = 4, 5, 6
 FP64, FP32 = 0, 1
@@ -79,6 +80,7 @@ SIGNATURES = {
     "nkb_op_apply_f32": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "nkb_op_apply_host_static": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                          c_void_p]),
+    "nkb_op_create_dense": (c_int, [c_int, c_int, c_void_p, c_int, P(c_void_p)]),
     "nkb_op_set_varcoeffs": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "nkb_op_apply3": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "nkb_op_sizes": (c_int, [c_void_p, P(c_long), P(c_long)]),

@@ -748,7 +748,8 @@ extern "C" int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **out)
     for (int c = 0; c < desc->nops; ++c)
     {
         const nkb_op *op = desc->ops[c];
-        if (!op || op->optype != NKB_HELMHOLTZ || op->precision != NKB_FP64)
+        if (!op || (op->optype != NKB_HELMHOLTZ && op->optype != NKB_DENSE_BLOCK) ||
+            op->precision != NKB_FP64)
             return SetError(NKB_ERR_INVALID, "nkb_sys_create: op %d is not an FP64 Helmholtz op", c);
         nloc += long(op->nelmt) * op->nc;
     }

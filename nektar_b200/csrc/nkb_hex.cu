@@ -326,6 +326,8 @@ int TuneHexGather(nkb_op *op, const void *xin, void *yl, const int *map, const d
 
 const char *KernelName(const nkb_op *op, bool gather)
 {
+    if (op->optype == NKB_DENSE_BLOCK)
+        return "k_dense_gemv (per-element dense blocks)";
     if (op->variant != kVariantHexHelm)
     {
         const int nm   = op->nm;
@@ -352,6 +354,13 @@ template <typename T>
 int LaunchOp(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
              const double *gsign, cudaStream_t s, const int *skip, const double *lambda)
 {
+    if (op->optype == NKB_DENSE_BLOCK)
+    {
+        if (!std::is_same<T, double>::value)
+            return SetError(NKB_ERR_UNSUPPORTED, "dense operators are FP64");
+        return LaunchDense(op, reinterpret_cast<const double *>(in), reinterpret_cast<double *>(o0),
+                           gmap, gsign, s, skip);
+    }
     if (op->variant == kVariantHexHelm)
     {
         HexArgs<T> a = MakeHexArgs<T>(op);

@@ -64,6 +64,10 @@ template <typename T>
 int LaunchGeneric3(const nkb_op *op, const T *in, const T *in1, const T *in2, T *o0, T *o1, T *o2,
                    const int *gmap, const double *gsign, cudaStream_t s,
                    const int *skip = nullptr, const double *lambda = nullptr);
+// per-element dense operators (nkb_dense.cu)
+int LaunchDense(const nkb_op *op, const double *in, double *out, const int *gmap,
+                const double *gsign, cudaStream_t s, const int *skip);
+int DenseDiag(const nkb_op *op, double *d, cudaStream_t s, double *stiff);
 // dispatch: tuned kernel if selected, else generic (nkb_hex.cu)
 // skip: optional device flag; when it reads nonzero the kernels return at once
 // (a converged CG keeps its captured graph but stops doing work)

@@ -1009,6 +1009,8 @@ static int HexDiag(const nkb_op *op, double *d_out, cudaStream_t s, double *d_st
 
 int HelmholtzDiag(const nkb_op *op, double *d_out, cudaStream_t s, double *d_stiff)
 {
+    if (op->optype == NKB_DENSE_BLOCK)
+        return DenseDiag(op, d_out, s, d_stiff);
     if (op->optype != NKB_HELMHOLTZ)
         return SetError(NKB_ERR_INVALID, "Helmholtz diagonal needs a Helmholtz operator");
     if (op->shape == NKB_HEX && op->nq[0] == op->nq[1] && op->nq[0] == op->nq[2])
@@ -1048,7 +1050,7 @@ extern "C" int nkb_op_helmholtz_diag(nkb_op *op, double *diag, int flags, void *
         return SetError(NKB_ERR_INVALID, "nkb_op_helmholtz_diag: NULL argument");
     if (op->precision != NKB_FP64)
         return SetError(NKB_ERR_INVALID, "nkb_op_helmholtz_diag: needs an FP64 operator");
-    if (op->optype != NKB_HELMHOLTZ)
+    if (op->optype != NKB_HELMHOLTZ && op->optype != NKB_DENSE_BLOCK)
         return SetError(NKB_ERR_INVALID, "nkb_op_helmholtz_diag: operator %d is not Helmholtz",
                         op->optype);
     NKB_CUDA_TRY(cudaSetDevice(op->device));
