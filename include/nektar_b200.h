@@ -152,6 +152,15 @@ int nkb_op_create(const nkb_op_desc *desc, nkb_op **op);
  * in and out are nelmt*n values. n <= 6144. */
 int nkb_op_create_dense(int n, int nelmt, const double *mats, int device, nkb_op **op);
 
+/* The same with rows x cols blocks (in nelmt*cols, out nelmt*rows values,
+ * cols <= 6144): the per-element maps of a statically condensed solve around
+ * its CG, i.e. the right-hand side condensation F_b - K_bi K_ii^-1 F_i and the
+ * interior back substitution of GlobalLinSysStaticCond::v_Solve
+ * (GlobalLinSysStaticCond.cpp:98-227), with a low-energy basis change folded
+ * in. Not usable as a CG system's operator. */
+int nkb_op_create_dense_rect(int rows, int cols, int nelmt, const double *mats, int device,
+                             nkb_op **op);
+
 /* Replaces Helmholtz_MatrixFree::UpdateFactors (Helmholtz.cpp:615-691):
  * lambda (eFactorLambda); diff_mode NKB_DIFF_CONST with diff =
  * (d00 d01 d11 d02 d12 d22) from eFactorCoeffD00..D22; NKB_DIFF_VAR fills the
@@ -330,6 +339,18 @@ int nkb_sys_clone(const nkb_sys *sys, nkb_sys **clone);
  * its solves, Jacobi diagonal rebuilt from the split mass / Laplacian
  * diagonal, computed once per shared system). */
 int nkb_sys_set_lambda(nkb_sys *sys, double lambda);
+
+/* Block-Jacobi preconditioner: replaces PreconditionerBlock::v_DoPreconditioner
+ * (MultiRegions/PreconditionerBlock.cpp:813-852) and the block step of
+ * PreconditionerLowEnergy::v_DoPreconditioner (PreconditionerLowEnergy.cpp
+ * :915-933). Block b covers the non-Dirichlet dofs bidx[bptr[b]..bptr[b+1])
+ * (indices counted from the first non-Dirichlet dof, 1..256 per block, no
+ * dof in two blocks); binv holds the blocks' inverses one after another, each
+ * n*n doubles column-major (for the symmetric blocks of an SPD system either
+ * order). Dofs outside every block keep the Jacobi step. Host arrays, copied;
+ * set once per system, before any clone; FP64 solves only. */
+int nkb_sys_set_blocks(nkb_sys *sys, int nblk, const int *bptr, const int *bidx,
+                       const double *binv);
 
 /* Device bytes: shared by all clones (map, CSR, sign, split diagonal) and
  * owned by this instance (vectors, state, staging). Operators not included. */

@@ -181,6 +181,7 @@ class Operator:
         (LinearADR: lambda only; the operator applies -lambda)."""
         d = None if diff is None else _f64(diff)
         check(lib().nkb_op_set_factors(self.h, float(lam), diff_mode, _dp(d)))
+        self.lam = float(lam)
 
     def set_varcoeffs(self, velx, vely, velz):
         """LinearADR advection velocities (UpdateVarcoeffs): host arrays of
@@ -303,20 +304,21 @@ class Batch:
 
 
 class DenseOperator:
-    """Per-element dense operator y_e = M_e x_e (nkb_op_create_dense): mats
-    (nelmt, n, n) FP64, e.g. the Schur complements of static condensation.
-    Usable wherever a Helmholtz Operator is (GlobalLinSys, apply)."""
+    """Per-element dense operator y_e = M_e x_e (nkb_op_create_dense[_rect]):
+    mats (nelmt, rows, cols) FP64, e.g. the Schur complements of static
+    condensation. Square ones are usable wherever a Helmholtz Operator is
+    (GlobalLinSys, apply)."""
 
     def __init__(self, mats, device=0):
         mats = np.ascontiguousarray(mats, dtype=np.float64)
-        self.nelmt, n, n2 = mats.shape
-        if n != n2:
-            raise ValueError("blocks must be square")
-        self.n, self.precision, self.optype = n, FP64, C.DENSE_BLOCK
+        self.nelmt, rows, cols = mats.shape
+        self.n, self.rows, self.cols = cols, rows, cols
+        self.precision, self.optype = FP64, C.DENSE_BLOCK
         h = ctypes.c_void_p()
-        check(lib().nkb_op_create_dense(n, self.nelmt, mats.ctypes.data, device, ctypes.byref(h)))
+        check(lib().nkb_op_create_dense_rect(rows, cols, self.nelmt, mats.ctypes.data, device,
+                                             ctypes.byref(h)))
         self.h = h
-        self.in_size = self.out_size = self.nelmt * n
+        self.in_size, self.out_size = self.nelmt * cols, self.nelmt * rows
 
     def __call__(self, x):
         x = _f64(x)
@@ -453,6 +455,18 @@ class GlobalLinSys:
     def set_lambda(self, lam):
         """Helmholtz lambda of this system's solves (overrides the operators')."""
         check(lib().nkb_sys_set_lambda(self.h, float(lam)))
+
+    def set_blocks(self, blocks):
+        """Block-Jacobi preconditioner (nkb_sys_set_blocks): a list of
+        (dofs, inverse) pairs, dofs the global indices (>= ndir) of one block
+        and inverse its n x n inverse. Dofs outside every block keep Jacobi."""
+        idx = [np.asarray(d, dtype=np.int64) - self.ndir for d, _ in blocks]
+        ptr = np.zeros(len(blocks) + 1, dtype=np.int32)
+        ptr[1:] = np.cumsum([i.size for i in idx])
+        bidx = np.ascontiguousarray(np.concatenate(idx), dtype=np.int32)
+        binv = np.concatenate([np.asarray(m, dtype=np.float64).T.ravel() for _, m in blocks])
+        check(lib().nkb_sys_set_blocks(self.h, len(blocks), ptr.ctypes.data_as(C.ip),
+                                       bidx.ctypes.data_as(C.ip), _dp(binv)))
 
     def footprint(self):
         """(shared bytes, instance bytes) of device memory held by the system."""

@@ -81,6 +81,7 @@ SIGNATURES = {
     "nkb_op_apply_host_static": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                          c_void_p]),
     "nkb_op_create_dense": (c_int, [c_int, c_int, c_void_p, c_int, P(c_void_p)]),
+    "nkb_op_create_dense_rect": (c_int, [c_int, c_int, c_int, c_void_p, c_int, P(c_void_p)]),
     "nkb_op_set_varcoeffs": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "nkb_op_apply3": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "nkb_op_sizes": (c_int, [c_void_p, P(c_long), P(c_long)]),
@@ -108,6 +109,7 @@ SIGNATURES = {
     "nkb_cg_end": (c_int, [c_void_p, P(CGReport)]),
     "nkb_sys_clone": (c_int, [c_void_p, P(c_void_p)]),
     "nkb_sys_set_lambda": (c_int, [c_void_p, c_double]),
+    "nkb_sys_set_blocks": (c_int, [c_void_p, c_int, ip, ip, dp]),
     "nkb_sys_footprint": (c_int, [c_void_p, P(c_size_t), P(c_size_t)]),
     "nkb_geom_nelmt": (c_long, [P(GeomRequest)]),
     "nkb_geom_fill": (c_int, [P(GeomRequest), dp, dp, dp]),

@@ -124,6 +124,90 @@ __global__ void k_precon(int nn, int ndir, const CGState *st, const T *__restric
     BlockSum2(rw, rr, part);
 }
 
+// Block-Jacobi step (PreconditionerBlock::v_DoPreconditioner,
+// PreconditionerBlock.cpp; PreconditionerLowEnergy::v_DoPreconditioner,
+// PreconditionerLowEnergy.cpp:915-933): for every block b of dofs idx_b, w_b =
+// M_b^-1 r_b, replacing the diagonal step's w there. One warp per block and
+// a grid of one CTA per 8 blocks (all blocks in flight at once: the step is
+// latency-bound, a few MB of blocks), the inverse stored column-major so a
+// warp's lanes read consecutive rows. The change of (r,w) goes to per-CTA
+// partials that k_scalars adds to (r,w) in a fixed order.
+constexpr int kBlockMax     = 256; // largest block (rows)
+constexpr int kBlockWarps   = kRedThreads / 32;
+constexpr int kBlockGridMax = 8192;
+
+__global__ void __launch_bounds__(kRedThreads)
+    k_block_precon(int nblk, int ndir, const CGState *st, const int *__restrict__ bptr,
+                   const int *__restrict__ bidx, const long *__restrict__ boff,
+                   const double *__restrict__ bmat, const double *__restrict__ r,
+                   double *__restrict__ w, double *part)
+{
+    if (st->done)
+        return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double corr = 0.0;
+    for (int b = blockIdx.x * kBlockWarps + warp; b < nblk; b += gridDim.x * kBlockWarps)
+    {
+        const int o = bptr[b], n = bptr[b + 1] - o;
+        const int *idx = bidx + o;
+        const double *M = bmat + boff[b];
+        // rows i0 + lane; columns in chunks of 32 whose r values sit one per
+        // lane (shuffled to all), so a chunk's 32 loads per lane and its r
+        // gather are in flight together (the step is latency-bound)
+        for (int i0 = 0; i0 < n; i0 += 32)
+        {
+            const int i   = i0 + lane;
+            const bool ir = i < n;
+            double acc = 0.0, ri = 0.0, wold = 0.0;
+            long gi = 0;
+            for (int j0 = 0; j0 < n; j0 += 32)
+            {
+                const int jl = j0 + lane;
+                long gj      = 0;
+                double rj    = 0.0, wj = 0.0;
+                if (jl < n)
+                {
+                    gj = long(ndir) + idx[jl];
+                    rj = r[idx[jl]];
+                    if (j0 == i0)
+                        wj = w[gj];
+                }
+                double m[32];
+#pragma unroll
+                for (int u = 0; u < 32; ++u)
+                    m[u] = (ir && j0 + u < n) ? __ldg(M + long(j0 + u) * n + i) : 0.0;
+#pragma unroll
+                for (int u = 0; u < 32; ++u)
+                    acc = fma(m[u], __shfl_sync(0xffffffffu, rj, u), acc);
+                if (j0 == i0) // this lane's own row i = jl
+                {
+                    ri   = rj;
+                    wold = wj;
+                    gi   = gj;
+                }
+            }
+            if (ir)
+            {
+                corr += ri * (acc - wold);
+                w[gi] = acc;
+            }
+        }
+    }
+    __shared__ double red[kBlockWarps];
+    corr = WarpSum(corr);
+    if (lane == 0)
+        red[warp] = corr;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double t = 0.0;
+        for (int k = 0; k < kBlockWarps; ++k)
+            t += red[k];
+        part[2 * blockIdx.x]     = t;
+        part[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
 template <typename T>
 __global__ void k_assemble(int nglob, int ndir, const int *__restrict__ aptr,
                            const int *__restrict__ aidx, const double *__restrict__ sign,
@@ -183,12 +267,15 @@ __device__ double ReducePart(const double *part, int nb, int which)
 // mode 1: first direction:  rho = (r,w) partA[0], mu = (s,w) partB[0]; alpha = rho/mu
 // mode 2: iteration:        rho_new, eps from partA, mu from partB
 // mode 3: restart of the recurrence after a reliable update (mixed precision)
+// partC (nbC > 0): the block preconditioner's corrections of (r,w)
 __global__ void k_scalars(CGState *st, const double *partA, int nbA, const double *partB, int nbB,
-                          int mode)
+                          int mode, const double *partC = nullptr, int nbC = 0)
 {
     if (st->done)
         return;
-    const double a0 = ReducePart(partA, nbA, 0);
+    double a0 = ReducePart(partA, nbA, 0);
+    if (nbC)
+        a0 += ReducePart(partC, nbC, 0);
     const double a1 = ReducePart(partA, nbA, 1);
     const double b0 = ReducePart(partB, nbB, 0);
     if (threadIdx.x != 0)
@@ -426,6 +513,12 @@ struct SysShared
     int *d_map = nullptr, *d_aptr = nullptr, *d_aidx = nullptr;
     double *d_sign = nullptr;
     double *d_dM = nullptr, *d_dL = nullptr; // nglob each
+    // optional block-Jacobi preconditioner (nkb_sys_set_blocks): blocks of
+    // non-Dirichlet dofs with their inverses; other dofs keep Jacobi
+    int nblk = 0;
+    int *d_bptr = nullptr, *d_bidx = nullptr;
+    long *d_boff = nullptr;
+    double *d_bmat = nullptr;
     size_t bytes = 0;
     std::mutex mu; // guards the lazy split diagonal
 
@@ -433,7 +526,8 @@ struct SysShared
     {
         cudaSetDevice(device);
         for (void *p : {(void *)d_map, (void *)d_aptr, (void *)d_aidx, (void *)d_sign,
-                        (void *)d_dM, (void *)d_dL})
+                        (void *)d_dM, (void *)d_dL, (void *)d_bptr, (void *)d_bidx,
+                        (void *)d_boff, (void *)d_bmat})
             cudaFree(p);
     }
 };
@@ -490,6 +584,8 @@ struct nkb_sys
     double *w = nullptr, *s = nullptr, *x = nullptr, *p = nullptr, *r = nullptr, *q = nullptr;
     double *bglob = nullptr, *yl = nullptr, *tl = nullptr;
     double *partA = nullptr, *partB = nullptr;
+    double *partC = nullptr; // block preconditioner partials (2 per CTA)
+    int nbC       = 0;
     CGState *st = nullptr;
     CGState *h_st = nullptr; // pinned [3]: FP64 state, FP32 state, state to write
     cudaGraphExec_t graph = nullptr;
@@ -567,18 +663,41 @@ static int Iteration32(nkb_sys *S, cudaStream_t s)
     return NKB_OK;
 }
 
+// the block step after the diagonal one (k_update / k_precon)
+static void BlockPrecon(nkb_sys *S, cudaStream_t s)
+{
+    const SysShared &h = *S->sh;
+    if (!h.nblk)
+        return;
+    k_block_precon<<<S->nbC, kRedThreads, 0, s>>>(h.nblk, S->ndir, S->st, h.d_bptr, h.d_bidx,
+                                                  h.d_boff, h.d_bmat, S->r, S->w, S->partC);
+    ++S->launches;
+}
+
+static int BlockGrid(int nblk)
+{
+    return std::max(1, std::min((nblk + kBlockWarps - 1) / kBlockWarps, kBlockGridMax));
+}
+
+// kernels of one FP64 iteration
+static long IterationLaunches(const nkb_sys *S)
+{
+    return 3 + long(S->ops.size()) + (S->sh->nblk ? 1 : 0);
+}
+
 static int Iteration(nkb_sys *S, cudaStream_t s)
 {
     const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
     S->launches += 3 + long(S->ops.size());
     k_update<double><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st, S->p, S->q, S->x, S->r,
                                                  S->w, S->s, S->d_dinv, S->partA);
+    BlockPrecon(S, s);
     int rc = Matvec(S, S->w, S->yl, true, s, &S->st->done);
     if (rc)
         return rc;
     k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
                                                    S->d_sign, S->yl, S->s, S->w, S->st, S->partB);
-    k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbU, S->partB, nbA, 2);
+    k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbU, S->partB, nbA, 2, S->partC, S->nbC);
     NKB_CUDA_TRY(cudaGetLastError());
     return NKB_OK;
 }
@@ -681,6 +800,11 @@ static int AllocInstance(nkb_sys *S)
              dalloc((void **)&S->dinv32, S->nn * sizeof(float)) &&
              dalloc((void **)&S->yl32, nloc * sizeof(float)) &&
              dalloc((void **)&S->st32, sizeof(CGState));
+    if (ok && S->sh->nblk)
+    {
+        S->nbC = BlockGrid(S->sh->nblk);
+        ok     = dalloc((void **)&S->partC, 2 * size_t(S->nbC) * sizeof(double));
+    }
     if (!ok)
         return SetError(NKB_ERR_NOMEM, "nkb_sys: device allocation of the CG vectors failed");
     if (cudaMallocHost(&S->h_st, 3 * sizeof(CGState)) != cudaSuccess)
@@ -749,7 +873,7 @@ extern "C" int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **out)
     {
         const nkb_op *op = desc->ops[c];
         if (!op || (op->optype != NKB_HELMHOLTZ && op->optype != NKB_DENSE_BLOCK) ||
-            op->precision != NKB_FP64)
+            op->precision != NKB_FP64 || (op->optype == NKB_DENSE_BLOCK && op->nc != op->nt))
             return SetError(NKB_ERR_INVALID, "nkb_sys_create: op %d is not an FP64 Helmholtz op", c);
         nloc += long(op->nelmt) * op->nc;
     }
@@ -928,6 +1052,90 @@ extern "C" int nkb_sys_set_lambda(nkb_sys *S, double lambda)
     return NKB_OK;
 }
 
+extern "C" int nkb_sys_set_blocks(nkb_sys *S, int nblk, const int *bptr, const int *bidx,
+                                  const double *binv)
+{
+    ClearError();
+    if (!S || nblk < 1 || !bptr || !bidx || !binv)
+        return SetError(NKB_ERR_INVALID, "nkb_sys_set_blocks: bad arguments");
+    if (Busy(S))
+        return SetError(NKB_ERR_INVALID, "nkb_sys_set_blocks: a solve is in progress");
+    SysShared &h = *S->sh;
+    if (S->sh.use_count() > 1)
+        return SetError(NKB_ERR_INVALID, "nkb_sys_set_blocks: set the blocks before cloning");
+    if (h.nblk)
+        return SetError(NKB_ERR_INVALID, "nkb_sys_set_blocks: blocks already set");
+    if (bptr[0] != 0)
+        return SetError(NKB_ERR_INVALID, "nkb_sys_set_blocks: bptr[0] = %d", bptr[0]);
+    std::vector<long> boff(nblk);
+    std::vector<char> seen(S->nn, 0);
+    long tot = 0;
+    for (int b = 0; b < nblk; ++b)
+    {
+        const int n = bptr[b + 1] - bptr[b];
+        if (n < 1 || n > kBlockMax)
+            return SetError(NKB_ERR_INVALID, "nkb_sys_set_blocks: block %d has %d rows (1..%d)", b,
+                            n, kBlockMax);
+        for (int j = bptr[b]; j < bptr[b + 1]; ++j)
+        {
+            if (bidx[j] < 0 || bidx[j] >= S->nn || seen[bidx[j]])
+                return SetError(NKB_ERR_INVALID,
+                                "nkb_sys_set_blocks: index %d of block %d outside [0,%d) or "
+                                "in two blocks",
+                                bidx[j], b, S->nn);
+            seen[bidx[j]] = 1;
+        }
+        boff[b] = tot;
+        tot += long(n) * n;
+    }
+    const long nidx = bptr[nblk];
+    NKB_CUDA_TRY(cudaSetDevice(S->device));
+    int *dp = nullptr, *di = nullptr;
+    long *dof = nullptr;
+    double *dm = nullptr;
+    auto release = [&]() {
+        cudaFree(dp);
+        cudaFree(di);
+        cudaFree(dof);
+        cudaFree(dm);
+    };
+    if (cudaMalloc(&dp, (nblk + 1) * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&di, nidx * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&dof, nblk * sizeof(long)) != cudaSuccess ||
+        cudaMalloc(&dm, tot * sizeof(double)) != cudaSuccess)
+    {
+        release();
+        return SetError(NKB_ERR_NOMEM, "nkb_sys_set_blocks: %ld doubles of blocks", tot);
+    }
+    if (cudaMemcpy(dp, bptr, (nblk + 1) * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(di, bidx, nidx * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dof, boff.data(), nblk * sizeof(long), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dm, binv, tot * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    {
+        release();
+        return SetError(NKB_ERR_CUDA, "nkb_sys_set_blocks: upload");
+    }
+    double *pc   = nullptr;
+    const int nc = BlockGrid(nblk);
+    if (cudaMalloc(&pc, 2 * size_t(nc) * sizeof(double)) != cudaSuccess)
+    {
+        release();
+        return SetError(NKB_ERR_NOMEM, "nkb_sys_set_blocks: partials");
+    }
+    S->partC = pc;
+    S->nbC   = nc;
+    S->bytes += 2 * size_t(nc) * sizeof(double);
+    h.d_bptr = dp;
+    h.d_bidx = di;
+    h.d_boff = dof;
+    h.d_bmat = dm;
+    h.nblk   = nblk;
+    h.bytes += (nblk + 1) * sizeof(int) + nidx * sizeof(int) + nblk * sizeof(long) +
+               tot * sizeof(double);
+    DropGraphs(S); // graphs captured so far lack the block step
+    return NKB_OK;
+}
+
 extern "C" int nkb_sys_footprint(const nkb_sys *S, size_t *shared_bytes, size_t *instance_bytes)
 {
     ClearError();
@@ -1054,11 +1262,12 @@ static int Begin64(nkb_sys *S)
     k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbA, S->partA, nbA, 0);
     k_precon<double><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st, S->r, S->w, S->d_dinv,
                                                  S->partA);
+    BlockPrecon(S, s);
     if ((rc = Matvec(S, S->w, S->yl, true, s)))
         return rc;
     k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
                                                    S->d_sign, S->yl, S->s, S->w, S->st, S->partB);
-    k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbU, S->partB, nbA, 1);
+    k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbU, S->partB, nbA, 1, S->partC, S->nbC);
     NKB_CUDA_TRY(cudaGetLastError());
     S->launches += 5 + long(S->ops.size());
     v.use_graph = v.o.use_graph != 0 && s != cudaStreamLegacy && s != cudaStreamPerThread;
@@ -1079,7 +1288,7 @@ static int Step64(nkb_sys *S)
     if (v.use_graph)
     {
         NKB_CUDA_TRY(cudaGraphLaunch(S->graph, v.s));
-        S->launches += long(K) * (3 + long(S->ops.size()));
+        S->launches += long(K) * IterationLaunches(S);
     }
     else
     {
@@ -1290,6 +1499,8 @@ extern "C" int nkb_cg_begin(nkb_sys *S, const double *b_loc, double *x_loc,
     if (o.mixed && S->ops32.empty())
         return SetError(NKB_ERR_INVALID, "nkb_cg_begin: mixed precision needs FP32 operators "
                                          "(nkb_sys_desc.ops32)");
+    if (o.mixed && S->sh->nblk)
+        return SetError(NKB_ERR_UNSUPPORTED, "nkb_cg_begin: the block preconditioner is FP64 only");
     NKB_CUDA_TRY(cudaSetDevice(S->device));
     SolveCtx &v = S->sv;
     v           = SolveCtx();
@@ -1531,7 +1742,7 @@ extern "C" void nkb_sys_destroy(nkb_sys *S)
                       (void *)S->st32, (void *)S->d_dinv, (void *)S->w, (void *)S->s,
                       (void *)S->x, (void *)S->bglob, (void *)S->p, (void *)S->r, (void *)S->q,
                       (void *)S->yl, (void *)S->tl, (void *)S->partA, (void *)S->partB,
-                      (void *)S->st, (void *)S->stage})
+                      (void *)S->partC, (void *)S->st, (void *)S->stage})
         cudaFree(ptr);
     if (S->h_st)
         cudaFreeHost(S->h_st);

@@ -1,4 +1,4 @@
-// Per-element dense operators: y_e = M_e x_e for nelmt blocks of n x n
+// Per-element dense operators: y_e = M_e x_e for nelmt blocks of rows x cols
 // matrices. Used for the statically condensed (boundary) system of
 // GlobalLinSysIterativeStaticCond (MultiRegions/GlobalLinSysIterativeStaticCond
 // .cpp, GlobalLinSysStaticCond.cpp: the Schur complement of each element's
@@ -26,35 +26,35 @@ constexpr int kDenseThreads = 256;
 
 template <bool GATHER>
 __global__ void __launch_bounds__(kDenseThreads)
-    k_dense_gemv(const double *__restrict__ M, int n, long nelmt, const double *__restrict__ x,
-                 const int *__restrict__ gmap, const double *__restrict__ gsign,
-                 double *__restrict__ y, const int *skip)
+    k_dense_gemv(const double *__restrict__ M, int rows, int cols, long nelmt,
+                 const double *__restrict__ x, const int *__restrict__ gmap,
+                 const double *__restrict__ gsign, double *__restrict__ y, const int *skip)
 {
     extern __shared__ double xs[];
     const long e = blockIdx.x;
     if (e >= nelmt || (skip && *skip))
         return;
-    for (int j = threadIdx.x; j < n; j += blockDim.x)
+    for (int j = threadIdx.x; j < cols; j += blockDim.x)
     {
-        const long l = e * n + j;
+        const long l = e * cols + j;
         if (GATHER)
             xs[j] = gsign ? gsign[l] * x[gmap[l]] : x[gmap[l]];
         else
             xs[j] = x[l];
     }
     __syncthreads();
-    const double *Me = M + e * long(n) * n;
+    const double *Me = M + e * long(rows) * cols;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int i = warp; i < n; i += kDenseThreads / 32)
+    for (int i = warp; i < rows; i += kDenseThreads / 32)
     {
-        const double *row = Me + long(i) * n;
+        const double *row = Me + long(i) * cols;
         double s = 0.0;
-        for (int j = lane; j < n; j += 32)
+        for (int j = lane; j < cols; j += 32)
             s = fma(__ldg(row + j), xs[j], s);
         for (int o = 16; o; o >>= 1)
             s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0)
-            y[e * n + i] = s;
+            y[e * rows + i] = s;
     }
 }
 
@@ -77,13 +77,14 @@ int LaunchDense(const nkb_op *op, const double *in, double *out, const int *gmap
 {
     if (op->nelmt == 0)
         return NKB_OK;
+    // rows = op->nt outputs and cols = op->nc inputs per element
     const size_t smem = size_t(op->nc) * sizeof(double);
     if (gmap)
         k_dense_gemv<true><<<unsigned(op->nelmt), kDenseThreads, smem, s>>>(
-            op->geo, op->nc, op->nelmt, in, gmap, gsign, out, skip);
+            op->geo, op->nt, op->nc, op->nelmt, in, gmap, gsign, out, skip);
     else
         k_dense_gemv<false><<<unsigned(op->nelmt), kDenseThreads, smem, s>>>(
-            op->geo, op->nc, op->nelmt, in, nullptr, nullptr, out, skip);
+            op->geo, op->nt, op->nc, op->nelmt, in, nullptr, nullptr, out, skip);
     NKB_CUDA_TRY(cudaGetLastError());
     return NKB_OK;
 }
@@ -93,6 +94,8 @@ int LaunchDense(const nkb_op *op, const double *in, double *out, const int *gmap
 int DenseDiag(const nkb_op *op, double *d, cudaStream_t s, double *stiff)
 {
     const long tot = long(op->nelmt) * op->nc;
+    if (op->nc != op->nt)
+        return SetError(NKB_ERR_INVALID, "diagonal of non-square dense blocks");
     if (tot == 0)
         return NKB_OK;
     const int nb = int(std::min<long>((tot + 255) / 256, 148L * 16));
@@ -108,15 +111,15 @@ int DenseDiag(const nkb_op *op, double *d, cudaStream_t s, double *stiff)
 
 using namespace nkb;
 
-extern "C" int nkb_op_create_dense(int n, int nelmt, const double *mats, int device,
-                                   nkb_op **out)
+extern "C" int nkb_op_create_dense_rect(int rows, int cols, int nelmt, const double *mats,
+                                        int device, nkb_op **out)
 {
     ClearError();
-    if (!out || (!mats && nelmt > 0) || n < 1 || nelmt < 0)
+    if (!out || (!mats && nelmt > 0) || rows < 1 || cols < 1 || nelmt < 0)
         return SetError(NKB_ERR_INVALID, "nkb_op_create_dense: bad arguments");
     *out = nullptr;
-    if (size_t(n) * sizeof(double) > 48 * 1024)
-        return SetError(NKB_ERR_UNSUPPORTED, "nkb_op_create_dense: blocks of %d rows", n);
+    if (size_t(cols) * sizeof(double) > 48 * 1024)
+        return SetError(NKB_ERR_UNSUPPORTED, "nkb_op_create_dense: blocks of %d columns", cols);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return SetError(NKB_ERR_NO_DEVICE, "nkb_op_create_dense: no CUDA device");
@@ -126,7 +129,8 @@ extern "C" int nkb_op_create_dense(int n, int nelmt, const double *mats, int dev
     nkb_op *op    = new nkb_op();
     op->optype    = NKB_DENSE_BLOCK;
     op->nelmt     = nelmt;
-    op->nc = op->nt = n;
+    op->nc        = cols;
+    op->nt        = rows;
     op->precision = NKB_FP64;
     op->device    = device;
     op->lambda    = 1.0;
@@ -140,7 +144,7 @@ extern "C" int nkb_op_create_dense(int n, int nelmt, const double *mats, int dev
     if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess ||
         cudaMemset(op->d_err, 0, sizeof(int)) != cudaSuccess)
         return fail(SetError(NKB_ERR_CUDA, "nkb_op_create_dense: error word"));
-    const size_t bytes = size_t(nelmt) * n * n * sizeof(double);
+    const size_t bytes = size_t(nelmt) * rows * cols * sizeof(double);
     if (bytes)
     {
         if (cudaMalloc(&op->geo, bytes) != cudaSuccess)
@@ -150,4 +154,10 @@ extern "C" int nkb_op_create_dense(int n, int nelmt, const double *mats, int dev
     }
     *out = op;
     return NKB_OK;
+}
+
+extern "C" int nkb_op_create_dense(int n, int nelmt, const double *mats, int device,
+                                   nkb_op **out)
+{
+    return nkb_op_create_dense_rect(n, n, nelmt, mats, device, out);
 }

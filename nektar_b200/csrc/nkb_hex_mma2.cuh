@@ -161,6 +161,10 @@ __global__ void __launch_bounds__(64 * kMma2Pairs, 4)
 
     for (int pos = lane + 32 * h; pos < kMmaCube; pos += 64)
         xc[pos] = TV(0);
+    // the zero fill interleaves the two warps' positions, the fetch splits them
+    // in halves: without this barrier a late zero store of one warp can land
+    // on a coefficient the other warp's copy has already written
+    PairSync(pair);
     int idx[8];
     LoadMap8<NM, GATHER, TV>(a, e, lane, h, idx);
     FetchCoeffs8<NM, GATHER, TV>(a, e, lane, h, idx, xc);

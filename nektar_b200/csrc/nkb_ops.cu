@@ -826,6 +826,8 @@ extern "C" int nkb_op_sizes(const nkb_op *op, long *in_size, long *out_size)
         in = 3 * nt;
     else if (op->optype == NKB_PHYSDERIV)
         in = out = nt;
+    else if (op->optype == NKB_DENSE_BLOCK)
+        out = nt; // rows per element; nc columns
     if (in_size)
         *in_size = in;
     if (out_size)

@@ -14,10 +14,28 @@ element by element:
 The CG on the condensed system runs on the device exactly as the full one
 does (gather fused into the operator, deterministic CSR assemble, Jacobi on
 diag(S), graphs), with the Schur blocks as per-element dense operators
-(nkb_op_create_dense, an HBM-bound batched GEMV). The element matrices are
-taken from the device Helmholtz operators (applied to unit vectors) and the
-condensation and the back substitution are done on the host with numpy, as
-the reference builds its condensed matrices on the host.
+(nkb_op_create_dense, an HBM-bound batched GEMV); the right-hand side
+condensation and the back substitution around it are per-element dense maps
+on the device too (nkb_op_create_dense_rect). The element matrices are taken
+from the device Helmholtz operators (applied to unit vectors) and condensed
+on the host with numpy, as the reference builds its condensed matrices on the
+host.
+
+Preconditioners of the condensed system (the reference's Preconditioner
+classes for GlobalLinSysIterativeStaticCond):
+
+  "diagonal"   PreconditionerDiagonal: Jacobi on the assembled diag(S).
+  "block"      PreconditionerBlock::BlockPreconditionerCG
+               (PreconditionerBlock.cpp:123-420): the assembled S restricted
+               to each mesh edge's and face's interior modes, inverted; the
+               vertex modes keep Jacobi.
+  "lowenergy"  PreconditionerLowEnergy (PreconditionerLowEnergy.cpp): the
+               boundary space is changed to the low-energy basis of the
+               reference element, S~ = R S R^T per element
+               (v_TransformedSchurCompl), the CG runs on S~ with the block
+               step of "block" built from S~, and the solution is mapped back
+               with R^T (v_DoTransformCoeffsFromLowEnergy). Hexahedral meshes
+               of one order.
 """
 import time
 
@@ -52,6 +70,119 @@ def element_matrices(op):
     return K
 
 
+def reference_helmholtz(shape, nm, lam):
+    """Helmholtz matrix L + lam M of the element the LowEnergy transform is
+    built on (PreconditionerLowEnergy::SetUpReferenceElements,
+    PreconditionerLowEnergy.cpp:1662-1760; CreateRefHexGeom 1575-1660): the
+    unit cube [0,1]^3, Modified_A with nm modes at nm+1 GLL points in every
+    direction. Built from the 1-D mass and stiffness matrices (the map from
+    [-1,1] to [0,1] scales them by 1/2 and 2)."""
+    if shape != "hex":
+        raise NotImplementedError("low-energy reference element: hexahedra only")
+    import nektar_b200 as nb
+    z, w, D = nb.points(nb.GLL, nm + 1)
+    b, db = nb.basis(nb.MODIFIED_A, nm, z, D)
+    B, dB = np.asarray(b).reshape(nm, nm + 1), np.asarray(db).reshape(nm, nm + 1)
+    M = 0.5 * (B * w) @ B.T
+    L = 2.0 * (dB * w) @ dB.T
+    k3 = lambda a, b, c: np.kron(a, np.kron(b, c))  # noqa: E731  (r, q, p): p fastest
+    return lam * k3(M, M, M) + k3(M, M, L) + k3(M, L, M) + k3(L, M, M)
+
+
+def _entities(shape, nm, bm):
+    """Positions (in the boundary-mode order bm) of each vertex, edge and face
+    of a shape, and which vertices each edge and face has."""
+    verts, edges, faces = topology(shape, nm)
+    pos = {int(m): k for k, m in enumerate(bm)}
+    V = [pos[m] for m in verts]
+    E = [np.array([pos[m] for m, _ in lst], dtype=np.int64) for _, _, lst in edges]
+    F = [np.array([pos[m] for m, _, _ in lst], dtype=np.int64) for _, _, lst in faces]
+    ev = [(a, b) for a, b, _ in edges]
+    adj = {}
+    for a, b in ev:
+        adj.setdefault(a, set()).add(b)
+        adj.setdefault(b, set()).add(a)
+    fv = []
+    for kind, (o, a, c), _ in faces:
+        if kind == "T":
+            fv.append({o, a, c})
+        else:  # the fourth corner is joined to both ends of the frame's axes
+            d = (adj[a] & adj[c]) - {o}
+            fv.append({o, a, c} | d)
+    return V, E, F, ev, fv
+
+
+def lowenergy_transform(shape, nm, S):
+    """R of Expansion3D::v_BuildTransformationMatrix (Expansion3D.cpp
+    :2229-2600) from the reference element's Schur complement S (boundary
+    modes in sorted order): unit diagonal; for each vertex v,
+    R[v, ef] = -S[v, ef] S[ef, ef]^-1 over the interior modes of its three
+    edges and three faces; for each edge e, R[e, f] = -S[e, f] S[f, f]^-1 over
+    the interior modes of its two faces."""
+    bm, _ = boundary_interior(shape, nm)
+    V, E, F, ev, fv = _entities(shape, nm, bm)
+    R = np.eye(bm.size)
+    for v, pv in enumerate(V):
+        cols = np.concatenate([E[e] for e, (a, b) in enumerate(ev) if v in (a, b)] +
+                              [F[f] for f in range(len(F)) if v in fv[f]])
+        if cols.size:
+            R[pv, cols] = -S[pv, cols] @ np.linalg.inv(S[np.ix_(cols, cols)])
+    for e, (a, b) in enumerate(ev):
+        cols = np.concatenate([F[f] for f in range(len(F)) if a in fv[f] and b in fv[f]])
+        if E[e].size and cols.size:
+            R[np.ix_(E[e], cols)] = -S[np.ix_(E[e], cols)] @ np.linalg.inv(S[np.ix_(cols, cols)])
+    return R
+
+
+def entity_blocks(parts, bmap, bsign, ndir):
+    """Assembled blocks of the condensed matrices (parts' "S") over the
+    interior modes of every mesh edge and face without Dirichlet dofs, as
+    PreconditionerBlock::BlockPreconditionerCG and the LowEnergy block step
+    gather them (PreconditionerLowEnergy.cpp:568-760): sign_i sign_j S_e[i, j]
+    summed over the elements sharing the entity, rows in global dof order.
+    Returns [(global dofs, inverse)], blocks of one dof left to Jacobi."""
+    groups = {}
+    ob = 0
+    for p in parts:
+        ne, nbm = p["ne"], p["bm"].size
+        gb = bmap[ob:ob + ne * nbm].reshape(ne, nbm)
+        sb = bsign[ob:ob + ne * nbm].reshape(ne, nbm)
+        ob += ne * nbm
+        _, E, F, _, _ = _entities(p["shape"], p["nm"], p["bm"])
+        er = np.arange(ne)[:, None]
+        for L in E + F:
+            n = L.size
+            if n < 2:
+                continue
+            order = np.argsort(gb[:, L], axis=1)
+            idx = L[order]
+            G = gb[er, idx]
+            sg = sb[er, idx]
+            dirm = G < ndir
+            if (dirm.any(axis=1) != dirm.all(axis=1)).any():
+                raise ValueError("an edge or face has Dirichlet and free dofs")
+            keep = ~dirm[:, 0]
+            sub = p["S"][er[keep][:, :, None], idx[keep][:, :, None], idx[keep][:, None, :]]
+            sub = sub * (sg[keep][:, :, None] * sg[keep][:, None, :])
+            g = groups.setdefault(n, ([], [], []))
+            g[0].append(G[keep, 0])
+            g[1].append(G[keep])
+            g[2].append(sub)
+    blocks = []
+    for n in sorted(groups):
+        keys = np.concatenate(groups[n][0])
+        G = np.concatenate(groups[n][1])
+        sub = np.concatenate(groups[n][2])
+        uk, first, inv = np.unique(keys, return_index=True, return_inverse=True)
+        if (G != G[first][inv]).any():
+            raise ValueError("entities with a shared first dof differ")
+        acc = np.zeros((uk.size, n, n))
+        np.add.at(acc, inv, sub)
+        for dofs, Minv in zip(G[first], np.linalg.inv(acc)):
+            blocks.append((dofs, Minv))
+    return blocks
+
+
 def condense(K, bm, im):
     """(S, C, Kii_inv, Kib) of element matrices: S = Kbb - C Kib, C = Kbi Kii^-1."""
     Kbb = K[:, bm][:, :, bm]
@@ -62,14 +193,49 @@ def condense(K, bm, im):
     return Kbb - C @ Kib, C, Kii_inv, Kib
 
 
+def solve_maps(C, Kii_inv, Kib, bm, im, R=None):
+    """Per-element matrices of the two steps around the condensed CG
+    (GlobalLinSysStaticCond::v_Solve, GlobalLinSysStaticCond.cpp:98-227):
+
+      W (nb x nc):        b~ = R (b_b - C b_i)          from the local b_e
+      V (nc x (nb + ni)): x_b = R^T x~,
+                          x_i = Kii^-1 b_i - Kii^-1 Kib R^T x~
+                                                        from [x~_e, b_i,e]
+
+    with R the low-energy transform (identity if None); V's rows are in the
+    element's local mode order."""
+    ne, nbm, ni = C.shape
+    nc = nbm + ni
+    R = np.eye(nbm) if R is None else R
+    W = np.zeros((ne, nbm, nc))
+    W[:, :, bm] = R
+    W[:, :, im] = -(R @ C)
+    V = np.zeros((ne, nc, nbm + ni))
+    V[:, bm, :nbm] = R.T
+    V[:, im, :nbm] = -(Kii_inv @ (Kib @ R.T))
+    V[:, im, nbm:] = Kii_inv
+    return W, V
+
+
 class StaticCondSys:
     """Statically condensed Helmholtz system over Helmholtz collection
-    operators (Operator) with the C0 map of the full local space."""
+    operators (Operator) with the C0 map of the full local space. The set-up
+    (element matrices, condensation, low-energy transform, blocks) runs on the
+    host; a solve is three device steps: the right-hand side condensation
+    (per-element dense W), the CG on the condensed system, and the interior
+    back substitution (per-element dense V)."""
 
-    def __init__(self, ops, gmap, nglob, ndir, sign=None, device=0, matrices=None):
+    def __init__(self, ops, gmap, nglob, ndir, sign=None, device=0, matrices=None,
+                 precon="diagonal", lam=None):
+        """precon: "diagonal", "block" or "lowenergy"; lam: the operators'
+        Helmholtz lambda, which the low-energy reference element uses
+        (default: the one last given to the operators' set_factors)."""
         import nektar_b200 as nb
+        if precon not in ("diagonal", "block", "lowenergy"):
+            raise ValueError("precon %r" % (precon,))
         t0 = time.perf_counter()
         self.ops = list(ops)
+        self.precon = precon
         self.parts = []
         gmap = np.asarray(gmap)
         sign = np.ones(gmap.size) if sign is None else np.asarray(sign, dtype=np.float64)
@@ -85,7 +251,7 @@ class StaticCondSys:
             bglob.append(gm[:, bm].ravel())
             bsign.append(sg[:, bm].ravel())
             self.parts.append(dict(nc=nc, ne=ne, bm=bm, im=im, S=S, C=C, Kii_inv=Kii_inv,
-                                   Kib=Kib, off=off))
+                                   Kib=Kib, off=off, shape=op.shape, nm=op.nm, R=None))
             off += ne * nc
         self.nloc = off
         bglob = np.concatenate(bglob)
@@ -99,42 +265,84 @@ class StaticCondSys:
         self.bsign = np.concatenate(bsign)
         self.nglob_b, self.ndir = int(ids.size), int(ndir)
         self.nglob = int(nglob)
-        self.setup_s = time.perf_counter() - t0
-        self.dense = [nb.DenseOperator(p["S"], device=device) for p in self.parts]
+        if precon == "lowenergy":
+            if lam is None:
+                lam = getattr(self.ops[0], "lam", None)
+            if lam is None:
+                raise ValueError("lowenergy needs the Helmholtz lambda")
+            Rs = {}
+            for p in self.parts:
+                key = (p["shape"], p["nm"])
+                if key not in Rs:
+                    Kr = reference_helmholtz(p["shape"], p["nm"], float(lam))
+                    Sr = condense(Kr[None], p["bm"], p["im"])[0][0]
+                    Rs[key] = lowenergy_transform(p["shape"], p["nm"], Sr)
+                R = Rs[key]
+                p["R"], p["Rinv"] = R, np.linalg.inv(R)
+                p["S"] = R @ p["S"] @ R.T  # v_TransformedSchurCompl
+        blocks = None
+        if precon != "diagonal":
+            blocks = entity_blocks(self.parts, self.bmap, self.bsign, self.ndir)
+        self.nblocks = 0 if blocks is None else len(blocks)
+        self.dense, self.W, self.V = [], [], []
+        for p in self.parts:
+            W, V = solve_maps(p.pop("C"), p.pop("Kii_inv"), p.pop("Kib"), p["bm"], p["im"],
+                              p["R"])
+            self.W.append(nb.DenseOperator(W, device=device))
+            del W
+            self.V.append(nb.DenseOperator(V, device=device))
+            del V
+            self.dense.append(nb.DenseOperator(p.pop("S"), device=device))
         self.sys = nb.GlobalLinSys(self.dense, self.bmap, self.nglob_b, self.ndir,
                                    sign=self.bsign, device=device)
+        if blocks:
+            self.sys.set_blocks(blocks)
+        self.setup_s = time.perf_counter() - t0
+
+    def _parts_of(self, v):
+        for p in self.parts:
+            yield p, v[p["off"]:p["off"] + p["ne"] * p["nc"]].reshape(p["ne"], p["nc"])
 
     def condense_rhs(self, b_loc):
-        out = []
-        for p in self.parts:
-            b = np.asarray(b_loc[p["off"]:p["off"] + p["ne"] * p["nc"]]).reshape(p["ne"], p["nc"])
-            out.append((b[:, p["bm"]] - np.einsum("ebi,ei->eb", p["C"], b[:, p["im"]])).ravel())
-        return np.concatenate(out)
+        """Condensed (and, for lowenergy, transformed) boundary right-hand
+        side, element by element (device)."""
+        b = np.asarray(b_loc, dtype=np.float64)
+        return np.concatenate([W(be.ravel()) for W, (_, be) in zip(self.W, self._parts_of(b))])
 
     def solve(self, b_loc, x_loc=None, tol=1e-9, maxit=5000, check_interval=16,
               raise_on_maxit=True):
         """Local rhs and local Dirichlet values -> local solution, report
         (the report's iterations and device time are the condensed CG's)."""
-        x_loc = np.zeros(self.nloc) if x_loc is None else np.asarray(x_loc, dtype=np.float64)
-        xb0 = np.concatenate([x_loc[p["off"]:p["off"] + p["ne"] * p["nc"]]
-                              .reshape(p["ne"], p["nc"])[:, p["bm"]].ravel() for p in self.parts])
-        xb, rep = self.sys.solve(self.condense_rhs(b_loc), xb0, tol=tol, maxit=maxit,
+        b = np.asarray(b_loc, dtype=np.float64)
+        xb0 = []
+        if x_loc is None:
+            xb0 = np.zeros(self.bmap.size)
+        else:
+            ob = 0
+            for p, xe in self._parts_of(np.asarray(x_loc, dtype=np.float64)):
+                ne, nbm = p["ne"], p["bm"].size
+                xe = xe[:, p["bm"]]
+                if p["R"] is not None:
+                    # v_DoTransformCoeffsToLowEnergy (R^-T x) of the Dirichlet
+                    # values; the Dirichlet modes transform among themselves
+                    free = self.bmap[ob:ob + ne * nbm].reshape(ne, nbm) >= self.ndir
+                    xe = xe @ p["Rinv"]
+                    xe[free] = 0.0
+                xb0.append(xe.ravel())
+                ob += ne * nbm
+            xb0 = np.concatenate(xb0)
+        xb, rep = self.sys.solve(self.condense_rhs(b), xb0, tol=tol, maxit=maxit,
                                  check_interval=check_interval, raise_on_maxit=raise_on_maxit)
         x = np.empty(self.nloc)
         ob = 0
-        for p in self.parts:
-            ne, nc, nbm = p["ne"], p["nc"], p["bm"].size
-            b = np.asarray(b_loc[p["off"]:p["off"] + ne * nc]).reshape(ne, nc)
-            xbe = xb[ob:ob + ne * nbm].reshape(ne, nbm)
-            xie = np.einsum("eij,ej->ei", p["Kii_inv"],
-                            b[:, p["im"]] - np.einsum("eib,eb->ei", p["Kib"], xbe))
-            xe = x[p["off"]:p["off"] + ne * nc].reshape(ne, nc)
-            xe[:, p["bm"]] = xbe
-            xe[:, p["im"]] = xie
+        for V, (p, be) in zip(self.V, self._parts_of(b)):
+            ne, nbm = p["ne"], p["bm"].size
+            z = np.concatenate([xb[ob:ob + ne * nbm].reshape(ne, nbm), be[:, p["im"]]], axis=1)
+            x[p["off"]:p["off"] + ne * p["nc"]] = V(z.ravel())
             ob += ne * nbm
         return x, rep
 
     def close(self):
         self.sys.close()
-        for d in self.dense:
+        for d in self.dense + self.W + self.V:
             d.close()

@@ -348,3 +348,19 @@ def test_fp32_linear_adr_matches_oracle(shape):
     op.apply_device(xd.data_ptr(), yd.data_ptr(), stream=torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     assert rel_l2(yd.double().cpu().numpy(), yo) < TOL32
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+def test_hex_kernel_variants_are_repeatable(monkeypatch, variant):
+    """Repeated applications of every Hex variant to one input give the same
+    bits: a race between the warps of an element (a shared-memory store
+    landing after another warp's copy) shows up as an occasional wrong
+    element, which a one-shot comparison can miss."""
+    m = nb.BoxMesh("hex", 16, 7, 8, amp=0.05)
+    x = np.random.default_rng(11).uniform(-1, 1, m.nelmt * m.nc)
+    monkeypatch.setenv("NKB_HEX_VARIANT", str(variant))
+    op = nb.Operator("helmholtz", m)
+    op.set_factors(1.0)
+    y0 = op(x)
+    bad = sum(not np.array_equal(op(x), y0) for _ in range(150))
+    assert bad == 0

@@ -57,3 +57,67 @@ def test_condensed_solve_on_mixed_session():
     xs, _ = StaticCondSys(ops, mesh.gmap, mesh.nglob, mesh.ndir, sign=mesh.sign).solve(
         b, x0, tol=1e-13)
     assert rel_l2(xs, xf) < 1e-9
+
+
+@pytest.mark.parametrize("precon", ["block", "lowenergy"])
+def test_block_and_lowenergy_preconditioned_solves(precon):
+    m = nb.BoxMesh("hex", 4, 7, 8, amp=0.05)
+    gmap, nglob, ndir = m.assembly()
+    op = nb.Operator("helmholtz", m)
+    op.set_factors(1.0)
+    b = np.random.default_rng(1).uniform(-1, 1, m.nelmt * m.nc)
+    xf, rf = nb.GlobalLinSys([op], gmap, nglob, ndir).solve(b, tol=1e-12)
+    xd, rd = StaticCondSys([op], gmap, nglob, ndir).solve(b, tol=1e-12)
+    sc = StaticCondSys([op], gmap, nglob, ndir, precon=precon)
+    assert sc.nblocks > 0
+    xs, rs = sc.solve(b, tol=1e-12)
+    assert rel_l2(xs, xf) < 1e-9
+    if precon == "lowenergy":
+        assert rs.iterations * 4 < rd.iterations
+    else:
+        assert rs.iterations < rd.iterations
+    sc.close()
+
+
+def test_lowenergy_solve_on_rotated_hex_session():
+    """Rotated element frames (signs in the map) and Dirichlet data: the
+    low-energy condensed solve reproduces the full solve."""
+    from nektar_b200.meshgraph import SessionMesh
+    from nektar_b200.session import read_session, write_hex_box_session
+    U = "sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)"
+    F = "-(Lambda + 3*PI*PI/4)*sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)"
+    s = read_session(write_hex_box_session(3, 6, 1.5, U, F, U, shuffle_seed=4))
+    mesh = SessionMesh(s)
+    c = mesh.collections[0]
+    H = nb.Operator("helmholtz", c)
+    H.set_factors(1.5)
+    f = s.function("Forcing").evaluate(*mesh.xyz)
+    b = -nb.Operator("iproduct", c)(f)
+    x0 = mesh.dirichlet_local()
+    xf, rf = nb.GlobalLinSys([H], mesh.gmap, mesh.nglob, mesh.ndir, sign=mesh.sign).solve(
+        b, x0, tol=1e-13)
+    sc = StaticCondSys([H], mesh.gmap, mesh.nglob, mesh.ndir, sign=mesh.sign, precon="lowenergy")
+    xs, rs = sc.solve(b, x0, tol=1e-13)
+    assert rel_l2(xs, xf) < 1e-9
+    assert rs.iterations * 4 < rf.iterations
+
+
+def test_set_blocks_rejects_bad_blocks():
+    m = nb.BoxMesh("hex", 2, 4, 5, amp=0.0)
+    gmap, nglob, ndir = m.assembly()
+    op = nb.Operator("helmholtz", m)
+    op.set_factors(1.0)
+    sys_ = nb.GlobalLinSys([op], gmap, nglob, ndir)
+    eye = np.eye(2)
+    with pytest.raises(nb.NektarB200Error):  # a dof in two blocks
+        sys_.set_blocks([(np.array([ndir, ndir + 1]), eye), (np.array([ndir + 1, ndir + 2]), eye)])
+    with pytest.raises(nb.NektarB200Error):  # a Dirichlet dof
+        sys_.set_blocks([(np.array([ndir - 1, ndir]), eye)])
+    sys_.set_blocks([(np.array([ndir, ndir + 1]), eye)])
+    with pytest.raises(nb.NektarB200Error):  # set twice
+        sys_.set_blocks([(np.array([ndir + 2, ndir + 3]), eye)])
+    # identity blocks on two dofs: still converges to the same solution
+    b = np.random.default_rng(3).uniform(-1, 1, m.nelmt * m.nc)
+    xb, _ = sys_.solve(b, tol=1e-12)
+    xj, _ = nb.GlobalLinSys([op], gmap, nglob, ndir).solve(b, tol=1e-12)
+    assert rel_l2(xb, xj) < 1e-9

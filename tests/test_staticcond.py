@@ -59,3 +59,184 @@ def test_condensed_system_reproduces_full_solution():
     scale = np.abs(xg).max()  # two dense solves agree to rounding times the conditioning
     assert np.abs(xg[gm[:, bm]] - xbl).max() < 1e-10 * scale
     assert np.abs(xg[gm[:, im]] - xil).max() < 1e-10 * scale
+
+
+def test_reference_helmholtz_energy():
+    """The low-energy reference element is the unit cube: the constant
+    function has energy lambda, the function x has 1 + lambda / 3."""
+    from nektar_b200.meshgraph import topology
+    from nektar_b200.staticcond import reference_helmholtz
+    lam, nm = 2.5, 6
+    K = reference_helmholtz("hex", nm, lam)
+    assert np.abs(K - K.T).max() < 1e-13
+    verts = topology("hex", nm)[0]
+    one = np.zeros(nm ** 3)
+    one[verts] = 1.0
+    x = np.zeros(nm ** 3)
+    x[[verts[i] for i in (1, 2, 5, 6)]] = 1.0  # the vertices at x = 1
+    assert abs(one @ K @ one - lam) < 1e-12
+    assert abs(x @ K @ x - (1.0 + lam / 3.0)) < 1e-12
+
+
+def test_lowenergy_transform_decouples_reference_element():
+    """R S of the reference element has no coupling of a vertex to the
+    interior modes of its edges and faces, nor of an edge to its faces."""
+    from nektar_b200.staticcond import (_entities, lowenergy_transform, reference_helmholtz)
+    nm = 6
+    bm, im = boundary_interior("hex", nm)
+    S = condense(reference_helmholtz("hex", nm, 1.0)[None], bm, im)[0][0]
+    R = lowenergy_transform("hex", nm, S)
+    V, E, F, ev, fv = _entities("hex", nm, bm)
+    RS = R @ S
+    assert np.allclose(np.diag(R), 1.0)
+    for v, pv in enumerate(V):
+        cols = np.concatenate([E[e] for e, (a, b) in enumerate(ev) if v in (a, b)] +
+                              [F[f] for f in range(6) if v in fv[f]])
+        assert np.abs(RS[pv, cols]).max() < 1e-12 * np.abs(S).max()
+    for e, (a, b) in enumerate(ev):
+        cols = np.concatenate([F[f] for f in range(6) if a in fv[f] and b in fv[f]])
+        assert np.abs(RS[np.ix_(E[e], cols)]).max() < 1e-12 * np.abs(S).max()
+
+
+def _rotated_hex_condensed(nm=5, n=3, lam=1.3):
+    """Condensed matrices of a hex session with rotated element frames (so
+    the map carries signs), from the oracle's element matrices."""
+    from nektar_b200.meshgraph import SessionMesh
+    from nektar_b200.session import read_session, write_hex_box_session
+    s = read_session(write_hex_box_session(n, nm, lam, "x", "0", "x", shuffle_seed=4))
+    mesh = SessionMesh(s)
+    c = mesh.collections[0]
+    T = dict(c.T)
+    T["w"] = c.T["ws"]
+    ne, nc = c.nelmt, nm ** 3
+    K = np.zeros((ne, nc, nc))
+    for j in range(nc):
+        x = np.zeros(ne * nc)
+        x[j::nc] = 1.0
+        K[:, :, j] = O.helmholtz("hex", nm, c.nq, ne, T, c.jac, c.df, x, lam,
+                                 c.deformed).reshape(ne, nc)
+    bm, im = boundary_interior("hex", nm)
+    S, C, Kii_inv, Kib = condense(K, bm, im)
+    gm = np.asarray(mesh.gmap).reshape(ne, nc)
+    sg = np.asarray(mesh.sign, dtype=np.float64).reshape(ne, nc)
+    ids = np.unique(gm[:, bm])
+    renum = np.full(mesh.nglob, -1)
+    renum[ids] = np.arange(ids.size)
+    return dict(S=S, bm=bm, im=im, ne=ne, nm=nm, lam=lam, shape="hex",
+                bmap=renum[gm[:, bm]].ravel(), bsign=sg[:, bm].ravel(), nb=ids.size,
+                ndir=mesh.ndir, K=K, C=C, Kii_inv=Kii_inv, Kib=Kib, gm=gm, sg=sg,
+                nglob=mesh.nglob)
+
+
+def _assemble(mats, bmap, bsign, nb):
+    ne, n, _ = mats.shape
+    G = np.zeros((nb, nb))
+    gm, sg = bmap.reshape(ne, n), bsign.reshape(ne, n)
+    for e in range(ne):
+        np.add.at(G, (gm[e][:, None], gm[e][None, :]), sg[e][:, None] * sg[e][None, :] * mats[e])
+    return G
+
+
+def test_lowenergy_basis_is_conforming():
+    """The condensed system solved in the low-energy basis (S~ = R S R^T per
+    element, right-hand side R b, solution R^T x~) gives the solution of the
+    original condensed system: the reference-element transform is the same
+    function space on a mesh whose elements meet in rotated frames."""
+    from nektar_b200.staticcond import lowenergy_transform, reference_helmholtz
+    d = _rotated_hex_condensed()
+    S, ne, nd = d["S"], d["ne"], d["ndir"]
+    nbm = d["bm"].size
+    Sr = condense(reference_helmholtz("hex", d["nm"], d["lam"])[None], d["bm"], d["im"])[0][0]
+    R = lowenergy_transform("hex", d["nm"], Sr)
+    rng = np.random.default_rng(7)
+    gm, sg = d["bmap"].reshape(ne, nbm), d["bsign"].reshape(ne, nbm)
+    xg = np.zeros(d["nb"])
+    xg[:nd] = rng.uniform(-1, 1, nd)           # Dirichlet values
+    b_loc = rng.uniform(-1, 1, (ne, nbm))
+    x0 = np.where(gm < nd, sg * xg[gm], 0.0)   # local Dirichlet values
+
+    def solve(mats, b, x0l):
+        G = _assemble(mats, d["bmap"], d["bsign"], d["nb"])
+        r = np.zeros(d["nb"])
+        np.add.at(r, gm.ravel(), (sg * (b - np.einsum("eij,ej->ei", mats, x0l))).ravel())
+        x = np.zeros(d["nb"])
+        x[nd:] = np.linalg.solve(G[nd:, nd:], r[nd:])
+        return x0l + sg * x[gm]
+
+    x_ref = solve(S, b_loc, x0)
+    xt0 = x0 @ np.linalg.inv(R)
+    xt0[gm >= nd] = 0.0
+    x_le = solve(R @ S @ R.T, b_loc @ R.T, xt0) @ R
+    assert np.abs(x_le - x_ref).max() < 1e-10 * np.abs(x_ref).max()
+
+
+def _precon_matrix(blocks, diag, nd):
+    """Dense preconditioner: inverse blocks, Jacobi elsewhere (free dofs)."""
+    M = np.diag(1.0 / diag)
+    for dofs, inv in blocks:
+        f = np.asarray(dofs) - nd
+        M[np.ix_(f, f)] = inv
+    return M
+
+
+def test_block_and_lowenergy_preconditioners_condition_number():
+    """Condition numbers of the preconditioned condensed systems: Block
+    below Jacobi, LowEnergy well below both (the order of the reference's
+    Diagonal / Block / LowEnergy preconditioners)."""
+    from nektar_b200.staticcond import (entity_blocks, lowenergy_transform, reference_helmholtz)
+    d = _rotated_hex_condensed(nm=6, n=3)
+    nd = d["ndir"]
+    Sr = condense(reference_helmholtz("hex", d["nm"], d["lam"])[None], d["bm"], d["im"])[0][0]
+    R = lowenergy_transform("hex", d["nm"], Sr)
+    kappa = {}
+    for name, S in (("jacobi", d["S"]), ("block", d["S"]), ("lowenergy", R @ d["S"] @ R.T)):
+        A = _assemble(S, d["bmap"], d["bsign"], d["nb"])[nd:, nd:]
+        if name == "jacobi":
+            M = np.diag(1.0 / np.diag(A))
+        else:
+            part = dict(S=S, ne=d["ne"], bm=d["bm"], shape="hex", nm=d["nm"])
+            blocks = entity_blocks([part], d["bmap"], d["bsign"], nd)
+            M = _precon_matrix(blocks, np.diag(A), nd)
+            for dofs, inv in blocks:  # each block is the assembled matrix's own block
+                f = np.asarray(dofs) - nd
+                assert np.allclose(np.linalg.inv(inv), A[np.ix_(f, f)], rtol=1e-10, atol=1e-12)
+        L = np.linalg.cholesky(M)
+        ev = np.linalg.eigvalsh(L.T @ A @ L)
+        kappa[name] = ev[-1] / ev[0]
+    assert kappa["block"] < kappa["jacobi"]
+    assert kappa["lowenergy"] < 0.25 * kappa["block"]
+
+
+def test_solve_maps_reproduce_full_solution():
+    """The per-element maps around the condensed CG (W: condensed and
+    low-energy transformed right-hand side; V: back to the local modes with
+    the interior back substitution) give the full system's solution."""
+    from nektar_b200.staticcond import lowenergy_transform, reference_helmholtz, solve_maps
+    d = _rotated_hex_condensed(nm=5, n=2)
+    ne, nd, nc = d["ne"], d["ndir"], d["nm"] ** 3
+    nbm = d["bm"].size
+    gm, sg = d["gm"], d["sg"]
+    rng = np.random.default_rng(5)
+    b_loc = rng.uniform(-1, 1, (ne, nc))
+    G = np.zeros((d["nglob"], d["nglob"]))
+    for e in range(ne):
+        np.add.at(G, (gm[e][:, None], gm[e][None, :]), sg[e][:, None] * sg[e][None, :] * d["K"][e])
+    bg = np.zeros(d["nglob"])
+    np.add.at(bg, gm.ravel(), (sg * b_loc).ravel())
+    xg = np.zeros(d["nglob"])
+    xg[nd:] = np.linalg.solve(G[nd:, nd:], bg[nd:])
+    x_full = sg * xg[gm]
+    Sr = condense(reference_helmholtz("hex", d["nm"], d["lam"])[None], d["bm"], d["im"])[0][0]
+    for R in (None, lowenergy_transform("hex", d["nm"], Sr)):
+        W, V = solve_maps(d["C"], d["Kii_inv"], d["Kib"], d["bm"], d["im"], R)
+        St = d["S"] if R is None else R @ d["S"] @ R.T
+        bt = np.einsum("ebc,ec->eb", W, b_loc)
+        A = _assemble(St, d["bmap"], d["bsign"], d["nb"])
+        gb, sb = d["bmap"].reshape(ne, nbm), d["bsign"].reshape(ne, nbm)
+        r = np.zeros(d["nb"])
+        np.add.at(r, gb.ravel(), (sb * bt).ravel())
+        xt = np.zeros(d["nb"])
+        xt[nd:] = np.linalg.solve(A[nd:, nd:], r[nd:])
+        z = np.concatenate([sb * xt[gb], b_loc[:, d["im"]]], axis=1)
+        x = np.einsum("ecz,ez->ec", V, z)
+        assert np.abs(x - x_full).max() < 1e-10 * np.abs(x_full).max()
