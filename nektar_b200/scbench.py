@@ -1,5 +1,5 @@
 """Static condensation against the full matrix-free solve on one GPU:
-curved hex box, P, random right-hand side, zero Dirichlet data; the full
+curved box of hexahedra, prisms or tetrahedra, P, random right-hand side, zero Dirichlet data; the full
 solve with Jacobi, the condensed one with each preconditioner asked for
 (diagonal, block, lowenergy).
 
@@ -25,32 +25,45 @@ def main():
     ap.add_argument("--p", type=int, default=6)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--precon", default="diagonal,block,lowenergy")
+    ap.add_argument("--shape", default="hex", choices=["hex", "prism", "tet"])
     a = ap.parse_args()
     import nektar_b200 as nb
     from nektar_b200.staticcond import StaticCondSys, element_matrices
     nm = a.p + 1
-    m = nb.BoxMesh("hex", a.n, nm, nm + 1, amp=0.05)
-    gmap, nglob, ndir = m.assembly()
-    op = nb.Operator("helmholtz", m)
-    op.set_factors(1.0)
-    b = np.random.default_rng(0).uniform(-1, 1, m.nelmt * m.nc)
-    full = nb.GlobalLinSys([op], gmap, nglob, ndir)
+    if a.shape == "hex":
+        m = nb.BoxMesh("hex", a.n, nm, nm + 1, amp=0.05)
+        gmap, nglob, ndir = m.assembly()
+        sign, colls, what = None, [m], "curved hex box"
+    else:  # straight-sided box session (the box assembly covers hexes only)
+        from nektar_b200.meshgraph import SessionMesh
+        from nektar_b200.session import read_session, write_box_session
+        m = SessionMesh(read_session(write_box_session(a.shape, a.n, nm, 1.0, "0", "0", "0")))
+        gmap, nglob, ndir, sign = m.gmap, m.nglob, m.ndir, m.sign
+        colls, what = m.collections, "%s box session" % a.shape
+    ops = []
+    for c in colls:
+        op = nb.Operator("helmholtz", c)
+        op.set_factors(1.0)
+        ops.append(op)
+    nloc = sum(o.in_size for o in ops)
+    b = np.random.default_rng(0).uniform(-1, 1, nloc)
+    full = nb.GlobalLinSys(ops, gmap, nglob, ndir, sign=sign)
     full.solve(b, tol=a.tol)  # warm (graphs)
     t0 = time.perf_counter()
     xf, rf = full.solve(b, tol=a.tol)
     full_wall = time.perf_counter() - t0
     t0 = time.perf_counter()
-    K = [element_matrices(op)]  # shared by the condensed systems
+    K = [element_matrices(o) for o in ops]  # shared by the condensed systems
     t_mats = time.perf_counter() - t0
     out = {
-        "workload": "%d^3 curved hex, P=%d, CG to %g" % (a.n, a.p, a.tol),
+        "workload": "%d^3 %s, P=%d, CG to %g" % (a.n, what, a.p, a.tol),
         "nglob": nglob, "element_matrices_s": t_mats,
         "full": {"precon": "diagonal", "iterations": rf.iterations, "device_ms": rf.device_ms,
                  "ms_per_iteration": rf.device_ms / max(rf.iterations, 1),
                  "solve_wall_s": full_wall},
     }
     for pc in a.precon.split(","):
-        sc = StaticCondSys([op], gmap, nglob, ndir, matrices=K, precon=pc)
+        sc = StaticCondSys(ops, gmap, nglob, ndir, sign=sign, matrices=K, precon=pc)
         sc.solve(b, tol=a.tol)
         t0 = time.perf_counter()
         xs, rs = sc.solve(b, tol=a.tol)
@@ -59,7 +72,7 @@ def main():
         d(np.zeros(d.in_size))
         ms = d.last_kernel_ms()
         nbm = sc.parts[0]["bm"].size
-        dense_bytes = m.nelmt * (nbm * nbm + 2 * nbm) * 8
+        dense_bytes = sc.parts[0]["ne"] * (nbm * nbm + 2 * nbm) * 8
         out["static_condensation_" + pc] = {
             "iterations": rs.iterations, "device_ms": rs.device_ms,
             "ms_per_iteration": rs.device_ms / max(rs.iterations, 1),

@@ -34,8 +34,9 @@ classes for GlobalLinSysIterativeStaticCond):
                reference element, S~ = R S R^T per element
                (v_TransformedSchurCompl), the CG runs on S~ with the block
                step of "block" built from S~, and the solution is mapped back
-               with R^T (v_DoTransformCoeffsFromLowEnergy). Hexahedral meshes
-               of one order.
+               with R^T (v_DoTransformCoeffsFromLowEnergy). Hexahedra,
+               tetrahedra and prisms (the prism's transform assembled from the
+               hexahedron's and the tetrahedron's), one order.
 """
 import time
 
@@ -70,23 +71,55 @@ def element_matrices(op):
     return K
 
 
-def reference_helmholtz(shape, nm, lam):
-    """Helmholtz matrix L + lam M of the element the LowEnergy transform is
-    built on (PreconditionerLowEnergy::SetUpReferenceElements,
-    PreconditionerLowEnergy.cpp:1662-1760; CreateRefHexGeom 1575-1660): the
-    unit cube [0,1]^3, Modified_A with nm modes at nm+1 GLL points in every
-    direction. Built from the 1-D mass and stiffness matrices (the map from
-    [-1,1] to [0,1] scales them by 1/2 and 2)."""
-    if shape != "hex":
-        raise NotImplementedError("low-energy reference element: hexahedra only")
+# vertices of the reference elements the LowEnergy transform is built on
+# (PreconditionerLowEnergy::CreateRefHexGeom / CreateRefTetGeom,
+# PreconditionerLowEnergy.cpp:1489-1661): the unit cube and the regular
+# tetrahedron of edge 2
+_S3, _S6 = 3.0 ** 0.5, 6.0 ** 0.5
+REFERENCE_VERTICES = {
+    "hex": [[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1],
+            [0, 1, 1]],
+    "tet": [[-1, -1 / _S3, -1 / _S6], [1, -1 / _S3, -1 / _S6], [0, 2 / _S3, -1 / _S6],
+            [0, 0, 3 / _S6]],
+}
+
+
+def reference_geometry(shape, nm):
+    """(T, nq, jac, df) of the reference element at nm modes and nm+1 points
+    (GLL, and Gauss-Radau in collapsed directions, as SetUpReferenceElements
+    sets up its bases, PreconditionerLowEnergy.cpp:1662-1760)."""
+    from . import shape_tables
+    from .meshgraph import element_geometry
+    if shape not in REFERENCE_VERTICES:
+        raise NotImplementedError("low-energy reference element: %s" % shape)
+    T, nq = shape_tables(shape, nm, nm + 1)
+    X = np.asarray(REFERENCE_VERTICES[shape], dtype=np.float64)[None]
+    jac, df, _ = element_geometry(shape, X, tuple(np.asarray(z) for z in T["z"]))
+    return T, nq, jac, df
+
+
+def reference_helmholtz(shape, nm, lam, device=0):
+    """Helmholtz matrix L + lam M of the reference element (above). The cube's
+    is built on the host from the 1-D mass and stiffness matrices (the map
+    from [-1,1] to [0,1] scales them by 1/2 and 2); the tetrahedron's is a
+    one-element device operator applied to unit vectors."""
     import nektar_b200 as nb
-    z, w, D = nb.points(nb.GLL, nm + 1)
-    b, db = nb.basis(nb.MODIFIED_A, nm, z, D)
-    B, dB = np.asarray(b).reshape(nm, nm + 1), np.asarray(db).reshape(nm, nm + 1)
-    M = 0.5 * (B * w) @ B.T
-    L = 2.0 * (dB * w) @ dB.T
-    k3 = lambda a, b, c: np.kron(a, np.kron(b, c))  # noqa: E731  (r, q, p): p fastest
-    return lam * k3(M, M, M) + k3(M, M, L) + k3(M, L, M) + k3(L, M, M)
+    if shape == "hex":
+        z, w, D = nb.points(nb.GLL, nm + 1)
+        b, db = nb.basis(nb.MODIFIED_A, nm, z, D)
+        B, dB = np.asarray(b).reshape(nm, nm + 1), np.asarray(db).reshape(nm, nm + 1)
+        M = 0.5 * (B * w) @ B.T
+        L = 2.0 * (dB * w) @ dB.T
+        k3 = lambda a, b, c: np.kron(a, np.kron(b, c))  # noqa: E731  (r, q, p): p fastest
+        return lam * k3(M, M, M) + k3(M, M, L) + k3(M, L, M) + k3(L, M, M)
+    T, nq, jac, df = reference_geometry(shape, nm)
+    op = nb.Operator("helmholtz", shape=shape, nm=nm, nq=nq, nelmt=1, T=T, jac=jac, df=df,
+                     deformed=True, device=device)
+    try:
+        op.set_factors(lam)
+        return element_matrices(op)[0]
+    finally:
+        op.close()
 
 
 def _entities(shape, nm, bm):
@@ -132,6 +165,93 @@ def lowenergy_transform(shape, nm, S):
         if E[e].size and cols.size:
             R[np.ix_(E[e], cols)] = -S[np.ix_(E[e], cols)] @ np.linalg.inv(S[np.ix_(cols, cols)])
     return R
+
+
+# Correspondence tables of PreconditionerLowEnergy::ReSetTetMaxRMat and
+# ReSetPrismMaxRMat (PreconditionerLowEnergy.cpp:2043-2315): which vertex,
+# edge and face of the reference hexahedron (or tetrahedron) lends its
+# transform entries to which vertex, edge and face of the tetrahedron (or
+# prism), in the shapes' standard vertex / edge / face numbering.
+_TET_FROM_HEX_VE = ([[0, 0, 0], [1, 1, 1], [2, 2, 2], [4, 5, 6]],   # hex vertex
+                    [[0, 3, 4], [0, 1, 5], [1, 2, 6], [4, 5, 6]],   # hex edge
+                    [[0, 2, 3], [0, 1, 4], [1, 2, 5], [3, 4, 5]])   # tet edge
+_PRISM_FROM_HEX_VE = ([[0, 0, 0], [1, 1, 1], [2, 2, 2], [3, 3, 3], [4, 5, 5], [6, 7, 7]],
+                      [[0, 3, 4], [0, 1, 5], [1, 2, 6], [2, 3, 7], [4, 5, 9], [6, 7, 11]],
+                      [[0, 3, 4], [0, 1, 5], [1, 2, 6], [2, 3, 7], [4, 5, 8], [6, 7, 8]])
+_PRISM_FROM_HEX_VF = ([[0, 0], [1, 1], [4, 5], [2, 2], [3, 3], [6, 7]],   # hex vertex
+                      [[0, 4], [0, 2], [4, 2], [0, 2], [0, 4], [2, 4]],   # hex face
+                      [[0, 0], [1, 1], [4, 4], [2, 2], [3, 3], [5, 5]],   # prism vertex
+                      [[0, 4], [0, 2], [4, 2], [0, 2], [0, 4], [2, 4]])   # prism face
+_PRISM_FROM_HEX_EF = ([[0], [1, 1], [2], [3, 3], [4], [5], [6], [7], [9, 11]],   # hex edge
+                      [[0], [0, 2], [0], [0, 4], [4], [2], [2], [4], [2, 4]],    # hex face
+                      [[0], [1, 1], [2], [3, 3], [4], [5], [6], [7], [8, 8]],    # prism edge
+                      [[0], [0, 2], [0], [0, 4], [4], [2], [2], [4], [2, 4]])    # prism face
+_PRISM_FROM_TET_VF = ([0, 1, 3, 1, 0, 3], [1] * 6, [0, 1, 4, 2, 3, 5], [1, 1, 1, 3, 3, 3])
+_PRISM_FROM_TET_EF = ([0, 3, 4, 0, 4, 3], [1] * 6, [0, 4, 5, 2, 6, 7], [1, 1, 1, 3, 3, 3])
+
+
+def _maps(shape, nm):
+    bm, _ = boundary_interior(shape, nm)
+    V, E, F, _, _ = _entities(shape, nm, bm)
+    return bm.size, V, E, F
+
+
+def lowenergy_transforms(shapes, nm, lam, device=0, reference=None):
+    """R per shape for a mesh with the given shapes at nm modes, as
+    SetUpReferenceElements (PreconditionerLowEnergy.cpp:1662-1876) sets them
+    up: prisms bring in the hexahedron and the tetrahedron; with a
+    hexahedron present the tetrahedron's vertex-edge entries come from the
+    hexahedron's (ReSetTetMaxRMat), and the prism's transform is assembled
+    from the hexahedron's (quadrilateral faces, vertex-edge) and the
+    tetrahedron's (triangular faces) entries (ReSetPrismMaxRMat) instead of
+    from a prism reference element. reference(shape, nm, lam) gives the
+    reference element's matrix (default reference_helmholtz)."""
+    if reference is None:
+        reference = lambda sh, n, lm: reference_helmholtz(sh, n, lm, device)  # noqa: E731
+    need = set(shapes)
+    if "prism" in need:
+        need |= {"hex", "tet"}
+    Rs = {}
+    for shape in ("hex", "tet"):
+        if shape in need:
+            bm, im = boundary_interior(shape, nm)
+            Sr = condense(reference(shape, nm, lam)[None], bm, im)[0][0]
+            Rs[shape] = lowenergy_transform(shape, nm, Sr)
+    if "hex" in Rs and "tet" in Rs:
+        _, Vh, Eh, _ = _maps("hex", nm)
+        _, Vt, Et, _ = _maps("tet", nm)
+        R = Rs["tet"].copy()
+        hv, he, te = _TET_FROM_HEX_VE
+        for v in range(4):
+            for e in range(3):
+                R[Vt[v], Et[te[v][e]]] = Rs["hex"][Vh[hv[v][e]], Eh[he[v][e]]]
+        Rs["tet"] = R
+    if "prism" in need:
+        H, T = Rs["hex"], Rs["tet"]
+        _, Vh, Eh, Fh = _maps("hex", nm)
+        _, Vt, Et, Ft = _maps("tet", nm)
+        nbp, Vp, Ep, Fp = _maps("prism", nm)
+        R = np.eye(nbp)
+        hv, he, pe = _PRISM_FROM_HEX_VE
+        for v in range(6):
+            for e in range(3):
+                R[Vp[v], Ep[pe[v][e]]] = H[Vh[hv[v][e]], Eh[he[v][e]]]
+        hv, hf, pv, pf = _PRISM_FROM_HEX_VF
+        for v in range(6):
+            for f in range(2):
+                R[Vp[pv[v][f]], Fp[pf[v][f]]] = H[Vh[hv[v][f]], Fh[hf[v][f]]]
+        he, hf, pe, pf = _PRISM_FROM_HEX_EF
+        for e in range(9):
+            for f in range(len(he[e])):
+                R[np.ix_(Ep[pe[e][f]], Fp[pf[e][f]])] = H[np.ix_(Eh[he[e][f]], Fh[hf[e][f]])]
+        tv, tf, pv, pf = _PRISM_FROM_TET_VF
+        for v in range(6):
+            R[Vp[pv[v]], Fp[pf[v]]] = T[Vt[tv[v]], Ft[tf[v]]]
+        te, tf, pe, pf = _PRISM_FROM_TET_EF
+        for e in range(6):
+            R[np.ix_(Ep[pe[e]], Fp[pf[e]])] = T[np.ix_(Et[te[e]], Ft[tf[e]])]
+        Rs["prism"] = R
+    return {k: v for k, v in Rs.items() if k in shapes}
 
 
 def entity_blocks(parts, bmap, bsign, ndir):
@@ -270,14 +390,13 @@ class StaticCondSys:
                 lam = getattr(self.ops[0], "lam", None)
             if lam is None:
                 raise ValueError("lowenergy needs the Helmholtz lambda")
-            Rs = {}
+            nms = {p["nm"] for p in self.parts}
+            if len(nms) != 1:
+                raise NotImplementedError("lowenergy: collections of one order only")
+            Rs = lowenergy_transforms({p["shape"] for p in self.parts}, nms.pop(), float(lam),
+                                      device)
             for p in self.parts:
-                key = (p["shape"], p["nm"])
-                if key not in Rs:
-                    Kr = reference_helmholtz(p["shape"], p["nm"], float(lam))
-                    Sr = condense(Kr[None], p["bm"], p["im"])[0][0]
-                    Rs[key] = lowenergy_transform(p["shape"], p["nm"], Sr)
-                R = Rs[key]
+                R = Rs[p["shape"]]
                 p["R"], p["Rinv"] = R, np.linalg.inv(R)
                 p["S"] = R @ p["S"] @ R.T  # v_TransformedSchurCompl
         blocks = None
@@ -318,18 +437,17 @@ class StaticCondSys:
         if x_loc is None:
             xb0 = np.zeros(self.bmap.size)
         else:
-            ob = 0
             for p, xe in self._parts_of(np.asarray(x_loc, dtype=np.float64)):
-                ne, nbm = p["ne"], p["bm"].size
                 xe = xe[:, p["bm"]]
                 if p["R"] is not None:
-                    # v_DoTransformCoeffsToLowEnergy (R^-T x) of the Dirichlet
-                    # values; the Dirichlet modes transform among themselves
-                    free = self.bmap[ob:ob + ne * nbm].reshape(ne, nbm) >= self.ndir
+                    # v_CoeffsFwdTransform of the whole local boundary vector
+                    # (R^-T x, GlobalLinSysStaticCond.cpp:166-172): the lifting
+                    # then equals R (b - S x) and the result x + R^T (G d~), so
+                    # local Dirichlet values that differ between elements (the
+                    # reference's boundary projection allows that) never
+                    # reach the free modes
                     xe = xe @ p["Rinv"]
-                    xe[free] = 0.0
                 xb0.append(xe.ravel())
-                ob += ne * nbm
             xb0 = np.concatenate(xb0)
         xb, rep = self.sys.solve(self.condense_rhs(b), xb0, tol=tol, maxit=maxit,
                                  check_interval=check_interval, raise_on_maxit=raise_on_maxit)
