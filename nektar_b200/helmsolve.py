@@ -15,6 +15,14 @@ geometry, the assembly and the Dirichlet values, and evaluates the session's
 functions at the quadrature points.
 
     python -m nektar_b200.helmsolve session.xml [--tol 1e-13] [--fld out.fld]
+        [-I GlobalSysSoln=IterativeStaticCond] [-I Preconditioner=LowEnergyBlock]
+
+The linear solver follows the session's SOLVERINFO (or -I overrides, as the
+reference's command line takes them): GlobalSysSoln IterativeFull (the
+default here) or IterativeStaticCond, Preconditioner Diagonal (default),
+Block or LowEnergyBlock (static condensation only). The reference's direct
+solvers (DirectFull, DirectStaticCond, ...) map to the iterative solve of the
+same system, whose solution they share to the solver tolerance.
 """
 import argparse
 import json
@@ -54,9 +62,36 @@ def errors(mesh, u, exact, device=0):
     return linf, float(np.sqrt(l2sq)), float(np.sqrt(h1sq))
 
 
-def helm_solve(session, device=0, tol=1e-12, maxit=5000, check_interval=16, raise_on_maxit=True):
+SOLVERS = {"IterativeFull": "full", "DirectFull": "full", "XxtFull": "full", "PETScFull": "full",
+           "IterativeStaticCond": "staticcond", "DirectStaticCond": "staticcond",
+           "XxtStaticCond": "staticcond", "PETScStaticCond": "staticcond"}
+PRECONS = {"Diagonal": "diagonal", "Block": "block", "LowEnergyBlock": "lowenergy"}
+
+
+def linear_solver(solver_info):
+    """(solver, preconditioner) of a session's SOLVERINFO: GlobalSysSoln and
+    Preconditioner (MultiRegions GlobalLinSys / Preconditioner factories)."""
+    sol = solver_info.get("GlobalSysSoln", "IterativeFull")
+    pre = solver_info.get("Preconditioner", "Diagonal")
+    if sol not in SOLVERS:
+        raise ValueError("GlobalSysSoln %s is not supported" % sol)
+    if pre not in PRECONS:
+        raise ValueError("Preconditioner %s is not supported" % pre)
+    solver, precon = SOLVERS[sol], PRECONS[pre]
+    if solver == "full" and precon != "diagonal":
+        raise ValueError("Preconditioner %s needs GlobalSysSoln IterativeStaticCond" % pre)
+    return solver, precon
+
+
+def helm_solve(session, device=0, tol=1e-12, maxit=5000, check_interval=16, raise_on_maxit=True,
+               solver_info=None):
+    """solver_info: overrides of the session's SOLVERINFO (GlobalSysSoln,
+    Preconditioner)."""
     import nektar_b200 as nb
     from .meshgraph import SessionMesh
+    info = dict(session.solver_info)
+    info.update(solver_info or {})
+    solver, precon = linear_solver(info)
     mesh = SessionMesh(session)
     if "Lambda" not in session.parameters:
         raise ValueError("the session defines no Lambda parameter")
@@ -73,7 +108,12 @@ def helm_solve(session, device=0, tol=1e-12, maxit=5000, check_interval=16, rais
         H = nb.Operator("helmholtz", c, device=device)
         H.set_factors(lam)
         Hs.append(H)
-    S = nb.GlobalLinSys(Hs, mesh.gmap, mesh.nglob, mesh.ndir, sign=mesh.sign, device=device)
+    if solver == "full":
+        S = nb.GlobalLinSys(Hs, mesh.gmap, mesh.nglob, mesh.ndir, sign=mesh.sign, device=device)
+    else:
+        from .staticcond import StaticCondSys
+        S = StaticCondSys(Hs, mesh.gmap, mesh.nglob, mesh.ndir, sign=mesh.sign, device=device,
+                          precon=precon, lam=lam)
     x0 = mesh.dirichlet_local()
     t0 = time.perf_counter()
     x, rep = S.solve(b_loc, x0, tol=tol, maxit=maxit, check_interval=check_interval,
@@ -82,6 +122,7 @@ def helm_solve(session, device=0, tol=1e-12, maxit=5000, check_interval=16, rais
     u = np.concatenate([nb.Operator("bwdtrans", c, device=device)(xc)
                         for c, xc in zip(cols, mesh.split(x))])
     res = HelmResult(x, u, rep.iterations, rep.rel_residual, bool(rep.converged), solve_ms=ms)
+    res.solver, res.precon = solver, precon
     exact = session.function("ExactSolution")
     if exact is not None:
         res.linf, res.l2, res.h1 = errors(mesh, u, exact.evaluate(*mesh.xyz), device)
@@ -96,21 +137,26 @@ def main():
     ap.add_argument("--maxit", type=int, default=5000)
     ap.add_argument("--fld", default=None, help="write the solution as a .fld directory")
     ap.add_argument("--json", action="store_true")
+    ap.add_argument("-I", dest="info", action="append", default=[],
+                    help="SOLVERINFO override PROPERTY=VALUE")
     a = ap.parse_args()
     from .session import read_session
     s = read_session(a.session)
-    r = helm_solve(s, tol=a.tol, maxit=a.maxit)
+    over = dict(kv.split("=", 1) for kv in a.info)
+    r = helm_solve(s, tol=a.tol, maxit=a.maxit, solver_info=over)
     if a.fld:
         from .fieldio import write_fld
         write_fld(a.fld, r.mesh, {"u": r.coeffs})
     if a.json:
-        print(json.dumps({"session": s.name, "iterations": r.iterations,
+        print(json.dumps({"session": s.name, "solver": r.solver, "precon": r.precon,
+                          "iterations": r.iterations,
                           "rel_residual": r.rel_residual, "linf": r.linf, "l2": r.l2,
                           "h1": r.h1, "solve_ms": r.solve_ms}))
         return
     print("Solving 3D Helmholtz:")
     print("  - Lambda        : %g" % s.parameters["Lambda"])
     print("  - No. modes     : %s" % ",".join(str(c.nm) for c in r.mesh.collections))
+    print("  - Solver        : %s, %s" % (r.solver, r.precon))
     print("  - CG iterations : %d (relative residual %.3g)" % (r.iterations, r.rel_residual))
     if r.l2 is not None:
         print("L infinity error: %g" % r.linf)

@@ -59,3 +59,26 @@ def test_device_solve_reproduces_polynomial_solution(shape):
     s = read_session(write_box_session(shape, 4, 5, 2.0, UQ, FQ, UQ, shuffle_seed=6))
     r = helm_solve(s, tol=1e-13, maxit=3000)
     assert r.linf < 1e-10 and r.l2 < 1e-11
+
+
+@pytest.mark.parametrize("precon", ["Diagonal", "Block", "LowEnergyBlock"])
+def test_static_condensation_solvers_reproduce_reference_record(precon):
+    """-I GlobalSysSoln=IterativeStaticCond -I Preconditioner=...: the
+    condensed solves give the Hex record's errors as the full solve does."""
+    s = read_session(write_hex_box_session(2, 6, 1.0, U, F, U, shuffle_seed=4))
+    info = {"GlobalSysSoln": "IterativeStaticCond", "Preconditioner": precon}
+    r = helm_solve(s, tol=1e-14, maxit=2000, raise_on_maxit=False, solver_info=info)
+    assert (r.solver, r.precon) == ("staticcond", {"Diagonal": "diagonal", "Block": "block",
+                                                   "LowEnergyBlock": "lowenergy"}[precon])
+    assert abs(r.l2 - HEX_L2) < 1e-12 and abs(r.linf - HEX_LINF) < 1e-12
+
+
+@pytest.mark.parametrize("shape", ["prism", "tet", "hexprism"])
+def test_lowenergy_session_solve_matches_full_solve(shape):
+    s = read_session(write_box_session(shape, 2, 6, 1.0, U, F, U, shuffle_seed=3))
+    rf = helm_solve(s, tol=1e-14, maxit=3000, raise_on_maxit=False)
+    info = {"GlobalSysSoln": "IterativeStaticCond", "Preconditioner": "LowEnergyBlock"}
+    rl = helm_solve(s, tol=1e-14, maxit=3000, raise_on_maxit=False, solver_info=info)
+    assert rel_l2(rl.coeffs, rf.coeffs) < 1e-10
+    assert abs(rl.l2 - rf.l2) < 1e-9 * rf.l2
+    assert rl.iterations * 3 < rf.iterations

@@ -203,3 +203,15 @@ def test_fld_mixed_mesh_has_one_block_per_collection(tmp_path):
     assert [b["SHAPE"] for b in blocks] == ["Hexahedron", "Prism"]
     assert blocks[1]["BASIS"] == "Modified_A,Modified_A,Modified_B"
     assert np.array_equal(np.concatenate([b["data"] for b in blocks]), coeffs)
+
+
+def test_linear_solver_from_solver_info():
+    from nektar_b200.helmsolve import linear_solver
+    assert linear_solver({}) == ("full", "diagonal")
+    assert linear_solver({"GlobalSysSoln": "IterativeStaticCond",
+                          "Preconditioner": "LowEnergyBlock"}) == ("staticcond", "lowenergy")
+    assert linear_solver({"GlobalSysSoln": "DirectStaticCond"}) == ("staticcond", "diagonal")
+    with pytest.raises(ValueError):
+        linear_solver({"GlobalSysSoln": "IterativeFull", "Preconditioner": "Block"})
+    with pytest.raises(ValueError):
+        linear_solver({"Preconditioner": "FullLinearSpace"})
