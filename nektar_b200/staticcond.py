@@ -305,10 +305,10 @@ def entity_blocks(parts, bmap, bsign, ndir):
 
 def condense(K, bm, im):
     """(S, C, Kii_inv, Kib) of element matrices: S = Kbb - C Kib, C = Kbi Kii^-1."""
-    Kbb = K[:, bm][:, :, bm]
-    Kbi = K[:, bm][:, :, im]
-    Kib = K[:, im][:, :, bm]
-    Kii_inv = np.linalg.inv(K[:, im][:, :, im])
+    Kbb = K[:, bm[:, None], bm]
+    Kbi = K[:, bm[:, None], im]
+    Kib = K[:, im[:, None], bm]
+    Kii_inv = np.linalg.inv(K[:, im[:, None], im])
     C = Kbi @ Kii_inv
     return Kbb - C @ Kib, C, Kii_inv, Kib
 
