@@ -234,6 +234,27 @@ __global__ void k_assemble(int nglob, int ndir, const int *__restrict__ aptr,
         BlockSum2(sw, 0.0, part);
 }
 
+// the Jacobi diagonal: element diagonals summed per global dof, leaving out
+// local modes whose sign is 0 (a mode a lower-order neighbour lacks,
+// PreconditionerDiagonal::DiagonalPreconditionerSum, PreconditionerDiagonal.cpp
+// :104-117)
+__global__ void k_assemble_diag(int nglob, const int *__restrict__ aptr,
+                                const int *__restrict__ aidx, const double *__restrict__ sign,
+                                const double *__restrict__ loc, double *__restrict__ glob)
+{
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nglob; g += gridDim.x * blockDim.x)
+    {
+        double acc = 0.0;
+        for (int k = aptr[g]; k < aptr[g + 1]; ++k)
+        {
+            const int l = aidx[k];
+            if (!sign || sign[l] != 0.0)
+                acc += loc[l];
+        }
+        glob[g] = acc;
+    }
+}
+
 __global__ void k_global_to_local(long nloc, const int *__restrict__ map,
                                   const double *__restrict__ sign, const double *__restrict__ glob,
                                   double *__restrict__ loc)
@@ -839,10 +860,12 @@ static int EnsureDiagParts(nkb_sys *S)
             return rc;
         }
     }
-    k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, S->stream>>>(
-        S->nglob, S->ndir, S->d_aptr, S->d_aidx, nullptr, S->tl, dM, nullptr, nullptr, nullptr);
-    k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, S->stream>>>(
-        S->nglob, S->ndir, S->d_aptr, S->d_aidx, nullptr, S->yl, dL, nullptr, nullptr, nullptr);
+    k_assemble_diag<<<Blocks(S->nglob), kRedThreads, 0, S->stream>>>(S->nglob, S->d_aptr,
+                                                                     S->d_aidx, S->d_sign, S->tl,
+                                                                     dM);
+    k_assemble_diag<<<Blocks(S->nglob), kRedThreads, 0, S->stream>>>(S->nglob, S->d_aptr,
+                                                                     S->d_aidx, S->d_sign, S->yl,
+                                                                     dL);
     cudaError_t ce = cudaStreamSynchronize(S->stream);
     if (ce != cudaSuccess)
     {
@@ -967,8 +990,8 @@ extern "C" int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **out)
             (rc = TuneHexGather(S->ops32[c], S->w32, S->yl32 + S->off[c], mp, sg, S->stream)))
             return fail(rc);
     }
-    // Jacobi diagonal: element diagonals, assembled (sign^2 = 1), inverted
-    // (PreconditionerDiagonal.cpp:93-125). With one lambda for all operators
+    // Jacobi diagonal: element diagonals, assembled (modes of sign 0 left
+    // out), inverted (PreconditionerDiagonal.cpp:93-125). With one lambda for all operators
     // the mass and Laplacian parts are kept apart (clones with another lambda
     // then only recombine them); otherwise each operator's own lambda.
     bool one_lambda = true;
@@ -986,9 +1009,8 @@ extern "C" int nkb_sys_create(const nkb_sys_desc *desc, nkb_sys **out)
         for (size_t c = 0; c < S->ops.size(); ++c)
             if ((rc = HelmholtzDiag(S->ops[c], S->tl + S->off[c], S->stream)))
                 return fail(rc);
-        k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, S->stream>>>(
-            S->nglob, S->ndir, S->d_aptr, S->d_aidx, nullptr, S->tl, S->bglob, nullptr, nullptr,
-            nullptr);
+        k_assemble_diag<<<Blocks(S->nglob), kRedThreads, 0, S->stream>>>(
+            S->nglob, S->d_aptr, S->d_aidx, S->d_sign, S->tl, S->bglob);
         k_invert<<<Blocks(S->nn), kRedThreads, 0, S->stream>>>(S->nn, S->ndir, S->bglob, S->d_dinv);
         if (S->dinv32)
             k_float_copy<<<Blocks(S->nn), kRedThreads, 0, S->stream>>>(S->nn, S->d_dinv,

@@ -423,16 +423,38 @@ class SessionMesh:
                 for f in ids:
                     self._face_bc[f] = bc
 
+    def _entity_orders(self):
+        """Lowest order (modes) of the elements sharing each edge and face:
+        with variable order an edge or face carries only the modes of its
+        lowest-order element (AssemblyMapCG.cpp:1330-1375)."""
+        low = {}
+        for col in self.collections:
+            _, edges, faces = topology(col.shape, col.nm)
+            for el in range(col.nelmt):
+                V = [int(v) for v in col.lverts[el]]
+                keys = [("e", min(V[a], V[b]), max(V[a], V[b])) for a, b, _ in edges]
+                for kind, frame, _ in faces:
+                    if kind == "Q":
+                        cs = {V[i] for i in frame} | {self._quad_of(col.shape, frame, V)}
+                        keys.append(("f",) + tuple(sorted(cs)))
+                    else:
+                        keys.append(("t",) + tuple(sorted(V[i] for i in frame)))
+                for k in keys:
+                    low[k] = min(low.get(k, col.nm), col.nm)
+        return low
+
     def _assemble(self):
         g = self.session.geometry
         self._dirichlet_faces()
+        low = self._entity_orders()
+        self.variable_order = len({c.nm for c in self.collections}) > 1
         entities = {}  # key -> size
         tri_frame = {}  # triangle key -> (apex, origin) of its canonical frame
+        tri_pos = {}  # order -> {(a, b): position among a triangle's interior modes}
         gm, sg = [], []
         for col in self.collections:
             nm, nb = col.nm, col.nm - 2
             verts, edges, faces = topology(col.shape, nm)
-            nbt = (nm - 3) * (nm - 2) // 2  # interior modes of a triangle
             all_modes = set(verts)
             for _, _, lst in edges:
                 all_modes.update(m for m, _ in lst)
@@ -448,27 +470,41 @@ class SessionMesh:
                 for a, b, lst in edges:
                     ga, gb = V[a], V[b]
                     key = ("e", min(ga, gb), max(ga, gb))
-                    entities.setdefault(key, nb)
+                    lo = low[key]
+                    entities.setdefault(key, lo - 2)
                     for m, k in lst:
-                        key_of[m] = (key, k - 2, (-1.0) ** k if ga > gb else 1.0)
+                        if k < lo:
+                            key_of[m] = (key, k - 2, (-1.0) ** k if ga > gb else 1.0)
+                        else:  # a mode the lower-order neighbour lacks: sign 0
+                            key_of[m] = (("v", ga), 0, 0.0)
                 for kind, frame, lst in faces:
                     if kind == "Q":
                         o, ea, eb = (V[i] for i in frame)
                         quad = self._quad_of(col.shape, frame, V)  # corner opposite o
                         cid = {(0, 0): o, (1, 0): ea, (0, 1): eb, (1, 1): quad}
                         key = ("f",) + tuple(sorted(cid.values()))
-                        entities.setdefault(key, nb * nb)
+                        lb = low[key] - 2
+                        entities.setdefault(key, lb * lb)
                         aO, bO = min(cid, key=lambda c: cid[c])
                         n1, n2 = cid[(1 - aO, bO)], cid[(aO, 1 - bO)]
                         s1 = 1 if aO == 0 else -1
                         s2 = 1 if bO == 0 else -1
                         for m, a, b in lst:
                             ca, cb = (a, b) if n1 < n2 else (b, a)
-                            key_of[m] = (key, (ca - 2) * nb + (cb - 2), float(s1 ** a * s2 ** b))
+                            if ca - 2 < lb and cb - 2 < lb:
+                                key_of[m] = (key, (ca - 2) * lb + (cb - 2),
+                                             float(s1 ** a * s2 ** b))
+                            else:
+                                key_of[m] = (("v", o), 0, 0.0)
                     else:
                         o, ea, apex = (V[i] for i in frame)
                         key = ("t",) + tuple(sorted((o, ea, apex)))
-                        entities.setdefault(key, nbt)
+                        lo = low[key]
+                        entities.setdefault(key, (lo - 3) * (lo - 2) // 2)
+                        if lo not in tri_pos:
+                            tri_pos[lo] = {ab: i for i, ab in enumerate(
+                                (a, b) for a in range(2, lo) for b in range(1, lo - a))}
+                        tp = tri_pos[lo]
                         if key not in tri_frame:
                             tri_frame[key] = (apex, min(o, ea))
                         capex, corigin = tri_frame[key]
@@ -477,8 +513,11 @@ class SessionMesh:
                                 "triangular face %s: neighbouring elements collapse it towards "
                                 "different vertices (%d, %d)" % (key[1:], capex, apex))
                         refl = o != corigin
-                        for pos, (m, a, b) in enumerate(lst):
-                            key_of[m] = (key, pos, (-1.0) ** a if refl else 1.0)
+                        for m, a, b in lst:
+                            if (a, b) in tp:
+                                key_of[m] = (key, tp[(a, b)], (-1.0) ** a if refl else 1.0)
+                            else:
+                                key_of[m] = (("v", o), 0, 0.0)
                 for pos, m in enumerate(interior):
                     key_of[m] = (("i", len(gm), el), pos, 1.0)
                 entities.setdefault(("i", len(gm), el), len(interior))
@@ -531,7 +570,8 @@ class SessionMesh:
         g = self.session.geometry
         nms = {c.nm for c in self.collections}
         if len(nms) != 1:
-            raise SessionError("Dirichlet data with several expansion orders is not supported")
+            raise SessionError("consistent Dirichlet values with several expansion orders are "
+                               "not supported (dirichlet_local takes them)")
         nm = nms.pop()
         nb = nm - 2
         A, zg, wg, Brow, zr, wr = _tables_1d(nm)
@@ -696,11 +736,13 @@ class SessionMesh:
         for f in self._boundary_face_order():
             if f not in self._face_bc:
                 continue
-            vals = self._face_values(f, self._face_bc[f], time)
-            lo, hi = owner[f]
+            lo, hi, nm = owner[f]
+            vals = self._face_values(f, self._face_bc[f], time, nm)
             gm, sg = self.gmap[lo:hi], self.sign[lo:hi]
             for i, gd in enumerate(gm):
-                if gd in vals:
+                # modes a lower-order neighbour lacks (sign 0) end up zero and
+                # are no source for other copies (AssemblyMapCG.cpp:1940-1957)
+                if gd in vals and sg[i] != 0.0:
                     x[lo + i] = sg[i] * vals[gd]
                     written[lo + i] = True
                     src[int(gd)] = lo + i  # the last write of each dof
@@ -747,14 +789,15 @@ class SessionMesh:
             for el, eid in enumerate(col.elem_ids):
                 for f in g.elements[eid][1]:
                     if f in self._face_bc:
-                        out[f] = (base + el * col.nc, base + (el + 1) * col.nc)
+                        out[f] = (base + el * col.nc, base + (el + 1) * col.nc, col.nm)
         return out
 
-    def _face_values(self, f, bc, time):
+    def _face_values(self, f, bc, time, nm):
         """{global dof: value} of the Dirichlet face f's boundary-constrained
-        projection, as the face's own expansion computes it."""
+        projection, as the face's own expansion (nm modes, its element's)
+        computes it; an edge shared with lower-order elements keeps its
+        lower modes only."""
         g = self.session.geometry
-        nm = self.collections[0].nm
         nb = nm - 2
         A, zg, wg, Brow, zr, wr = _tables_1d(nm)
         P = lambda v: np.asarray(g.vertices[v], dtype=np.float64)  # noqa: E731
@@ -777,11 +820,15 @@ class SessionMesh:
                 c[2:] = np.linalg.solve(M1, (A[2:] * wg) @ rem)
             return c
 
+        full = {}  # (a, b) -> the edge's coefficients along a -> b, all nm modes
+
         def put_edge(a, b, c):
             key = ("e", min(a, b), max(a, b))
             o = self._base[key]
+            full[(a, b)] = c[2:]
+            full[(b, a)] = c[2:] * (-1.0) ** np.arange(2, nm)
             cc = c[2:] * ((-1.0) ** np.arange(2, nm) if a > b else 1.0)
-            for k in range(nb):
+            for k in range(min(nb, self._entities[key])):
                 vals[o + k] = cc[k]
 
         bcv = lambda x: bc.value.evaluate(x[..., 0], x[..., 1], x[..., 2], time)  # noqa: E731
@@ -800,9 +847,7 @@ class SessionMesh:
                 vtab = {v: vals[self._base[("v", v)]] for v in fv}
 
                 def ec(a, b):
-                    k = ("e", min(a, b), max(a, b))
-                    c = out[self._base[k]:self._base[k] + nb].copy()
-                    return c * ((-1.0) ** np.arange(2, nm)) if a > b else c
+                    return full[(a, b)]
                 self._quad_face(f, bc, time, out, vtab, ec, A, zg, wg, nm)
                 key = ("f",) + tuple(sorted(fv))
                 o = self._base[key]

@@ -8,7 +8,8 @@ Follows the reference readers section by section:
   (:1240-1325), v_ReadFaces (:1327-1469), v_ReadElements3D (:1718-2054),
   ReadComposites (:2056-), ReadDomain (:1144-1238);
 * expansions: MeshGraph::ReadExpansionInfo (MeshGraph.cpp:3102-) for the
-  `TYPE="MODIFIED"` form with one NUMMODES for all directions;
+  `TYPE="MODIFIED"` form with one NUMMODES for all directions, per domain
+  composite (different composites may have different orders);
 * parameters, solver info, variables, functions: SessionReader.cpp
   ReadParameters (:1785-1867), ReadSolverInfo (:1869-1941), ReadVariables
   (:2172-2250), ReadFunctions (:2252-2475);
@@ -379,6 +380,46 @@ def write_hex_box_session(n, nummodes, lam, dirichlet, forcing, exact, lengths=(
               '    <FUNCTION NAME="ExactSolution"> <E VAR="u" VALUE="%s" /> </FUNCTION>' % exact,
               "  </CONDITIONS>", "</NEKTAR>"]
     return "\n".join(lines) + "\n"
+
+
+def with_orders(xml_text, orders, seed=0):
+    """The session xml_text with its elements spread over len(orders)
+    domain composites (seeded, every composite of every element type
+    non-empty where there are enough elements), composite k expanded with
+    orders[k] modes: a variable-order session as the reference's *_VarP
+    tests have them."""
+    import xml.etree.ElementTree as ET
+    root = ET.fromstring(xml_text)
+    geom = root.find("GEOMETRY")
+    comp = geom.find("COMPOSITE")
+    dom_ids = parse_id_list(geom.find("DOMAIN").text.strip()[2:-1])
+    rng = np.random.default_rng(seed)
+    new = {}
+    for c in list(comp):
+        if int(c.get("ID")) not in dom_ids:
+            continue
+        txt = c.text.strip()
+        letter, ids = txt[0], parse_id_list(txt[2:-1])
+        comp.remove(c)
+        perm = rng.permutation(len(ids))
+        for k in range(len(orders)):
+            part = sorted(ids[i] for i in perm[k::len(orders)])
+            if part:
+                new.setdefault(k, []).append("%s[%s]" % (letter, _seq(part)))
+    cids = []
+    for k, parts in sorted(new.items()):
+        cid = 100 + k
+        e = ET.SubElement(comp, "C", ID=str(cid))
+        e.text = " " + " ".join(parts) + " "
+        cids.append(cid)
+    geom.find("DOMAIN").text = " C[%s] " % ",".join(map(str, cids))
+    exps = root.find("EXPANSIONS")
+    for e in list(exps):
+        exps.remove(e)
+    for k, cid in zip(sorted(new), cids):
+        ET.SubElement(exps, "E", COMPOSITE="C[%d]" % cid, NUMMODES=str(orders[k]), FIELDS="u",
+                      TYPE="MODIFIED")
+    return ET.tostring(root, encoding="unicode")
 
 
 def write_box_session(shape, n, nummodes, lam, dirichlet, forcing, exact, shuffle_seed=None):

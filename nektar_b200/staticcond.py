@@ -401,6 +401,8 @@ class StaticCondSys:
                 p["S"] = R @ p["S"] @ R.T  # v_TransformedSchurCompl
         blocks = None
         if precon != "diagonal":
+            if (self.bsign == 0).any():
+                raise NotImplementedError("%s: meshes of variable order" % precon)
             blocks = entity_blocks(self.parts, self.bmap, self.bsign, self.ndir)
         self.nblocks = 0 if blocks is None else len(blocks)
         self.dense, self.W, self.V = [], [], []

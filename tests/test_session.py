@@ -132,6 +132,8 @@ UQ = "x*x + 2*y*z - z"  # in every P >= 2 space: the discrete solution is exact
 FQ = "2 - Lambda*(x*x + 2*y*z - z)"  # laplacian(u) - lambda u
 REF_PRISM = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Prism.xml"
 REF_TET = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Tet.xml"
+REF_PRISM_VARP = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Prism_VarP.xml"
+REF_TET_VARP = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Tet_VarP.xml"
 
 
 @pytest.mark.parametrize("shape", ["prism", "tet"])
@@ -180,13 +182,19 @@ def test_incompatible_triangle_orientation_is_rejected():
     (REF_PRISM, (0.000385246, 0.00539787), (1e-9, 1e-9)),
     # Helmholtz3D_CG_Tet.tst: L2 (tolerance 1e-8), Linf (1e-9)
     (REF_TET, (8.458e-05, 0.000862348), (1e-8, 1e-9)),
+    # Helmholtz3D_CG_Prism_VarP.tst (orders 4, 5, 6 by composite): tolerance 1e-9
+    (REF_PRISM_VARP, (0.000292496, 0.00539787), (1e-9, 1e-9)),
+    # Helmholtz3D_CG_Tet_VarP.tst (orders 3, 4, 5, 6): L2 (tolerance 1e-7), Linf (1e-6)
+    (REF_TET_VARP, (0.00416454, 0.0313733), (1e-7, 1e-6)),
 ])
 def test_reference_prism_tet_sessions_reproduce_their_records(path, record, tol):
     """The reference's own Prism / Tet regression sessions reproduce their
     recorded errors, including the reference's Dirichlet procedure on
     triangular faces (Radau -> GLL edge interpolation, boundary expansions
     grouped by type, face by face overwrites, copies to elements that only
-    touch the boundary)."""
+    touch the boundary) and, in the VarP sessions, variable order (edges and
+    faces with the modes of their lowest-order element, the others of sign 0,
+    Dirichlet faces projected at their element's order)."""
     _, linf, l2 = oracle_helm_solve(read_session(path))
     # the regression tester reads the demo's output, printed by cout with its
     # default six significant digits (Helmholtz3D.cpp: cout << vL2Error)
