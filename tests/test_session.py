@@ -223,3 +223,17 @@ def test_linear_solver_from_solver_info():
         linear_solver({"GlobalSysSoln": "IterativeFull", "Preconditioner": "Block"})
     with pytest.raises(ValueError):
         linear_solver({"Preconditioner": "FullLinearSpace"})
+
+
+def test_fld_variable_order_blocks(tmp_path):
+    """One ELEMENTS block per collection, each with its own order."""
+    from nektar_b200.fieldio import read_fld, write_fld
+    from nektar_b200.session import with_orders
+    m = SessionMesh(read_session(with_orders(write_box_session("tet", 2, 4, 1.0, U, F, U),
+                                             [3, 5], seed=2)))
+    coeffs = np.arange(m.nloc, dtype=np.float64)
+    write_fld(str(tmp_path / "v.fld"), m, {"u": coeffs})
+    blocks = read_fld(str(tmp_path / "v.fld"))
+    assert [b["NUMMODESPERDIR"] for b in blocks] == ["UNIORDER:3,3,3", "UNIORDER:5,5,5"]
+    assert sorted(i for b in blocks for i in b["ids"]) == list(range(48))
+    assert np.array_equal(np.concatenate([b["data"] for b in blocks]), coeffs)
