@@ -4,8 +4,10 @@ the reference's Helmholtz3D demo (library/Demos/MultiRegions/Helmholtz3D.cpp):
     forcing f at the quadrature points            (the "Forcing" function)
     b = -IProductWRTBase(f)                        (ContField::v_HelmSolve,
                                                     ContField.cpp:797-821)
+    b += Neumann / Robin boundary inner products     (ContField.cpp:822-855)
     x = Dirichlet values (boundary-constrained projection), zero elsewhere
-    solve (L + lambda M) x = b with the lifting     (GlobalLinSysIterativeFull)
+    solve (L + lambda M + Robin face mass) x = b with the lifting
+                                                   (GlobalLinSysIterativeFull)
     u = BwdTrans(x)
     L_inf, L_2, H_1 errors against "ExactSolution" (ExpList::Linf / L2 / H1)
 
@@ -108,16 +110,46 @@ def helm_solve(session, device=0, tol=1e-12, maxit=5000, check_interval=16, rais
         H = nb.Operator("helmholtz", c, device=device)
         H.set_factors(lam)
         Hs.append(H)
-    if solver == "full":
-        S = nb.GlobalLinSys(Hs, mesh.gmap, mesh.nglob, mesh.ndir, sign=mesh.sign, device=device)
-    else:
-        from .staticcond import StaticCondSys
-        S = StaticCondSys(Hs, mesh.gmap, mesh.nglob, mesh.ndir, sign=mesh.sign, device=device,
-                          precon=precon, lam=lam)
+    # Neumann / Robin: boundary inner products join the forcing, Robin face
+    # mass matrices the operator
+    rhs_w, robin = mesh.weak_terms()
+    b_loc = b_loc + rhs_w
     x0 = mesh.dirichlet_local()
+    nloc = mesh.nloc
+    if solver == "full":
+        # Robin blocks as extra per-face dense operators over the faces'
+        # global dofs (GlobalLinSysIterativeFull::v_DoMatrixMultiply adds
+        # AddRobinTraceContribution to the element operators)
+        ops, gms, sgs, x0s, bs = list(Hs), [mesh.gmap], [mesh.sign], [x0], [b_loc]
+        by_size = {}
+        for dofs, M, loc in robin:
+            by_size.setdefault(dofs.size, []).append((dofs, M, loc))
+        for grp in by_size.values():
+            ops.append(nb.DenseOperator(np.stack([M for _, M, _ in grp]), device=device))
+            gms.append(np.concatenate([d for d, _, _ in grp]))
+            sgs.append(np.ones(gms[-1].size))
+            x0s.append(np.concatenate([mesh.sign[lc] * x0[lc] for _, _, lc in grp]))
+            bs.append(np.zeros(gms[-1].size))
+        S = nb.GlobalLinSys(ops, np.concatenate(gms), mesh.nglob, mesh.ndir,
+                            sign=np.concatenate(sgs), device=device)
+        b_sys, x0_sys = np.concatenate(bs), np.concatenate(x0s)
+    else:
+        from .staticcond import StaticCondSys, element_matrices
+        K = [element_matrices(H) for H in Hs]
+        for dofs, M, loc in robin:  # Expansion3D::v_AddRobinMassMatrix
+            ci = int(np.searchsorted(mesh.offsets, loc[0], side="right")) - 1
+            nc = mesh.collections[ci].nc
+            el = int(loc[0] - mesh.offsets[ci]) // nc
+            li = loc - mesh.offsets[ci] - el * nc
+            sg = mesh.sign[loc]
+            K[ci][el][np.ix_(li, li)] += np.outer(sg, sg) * M
+        S = StaticCondSys(Hs, mesh.gmap, mesh.nglob, mesh.ndir, sign=mesh.sign, device=device,
+                          matrices=K, precon=precon, lam=lam)
+        b_sys, x0_sys = b_loc, x0
     t0 = time.perf_counter()
-    x, rep = S.solve(b_loc, x0, tol=tol, maxit=maxit, check_interval=check_interval,
+    x, rep = S.solve(b_sys, x0_sys, tol=tol, maxit=maxit, check_interval=check_interval,
                      raise_on_maxit=raise_on_maxit)
+    x = x[:nloc]
     ms = (time.perf_counter() - t0) * 1e3
     u = np.concatenate([nb.Operator("bwdtrans", c, device=device)(xc)
                         for c, xc in zip(cols, mesh.split(x))])

@@ -407,21 +407,24 @@ class SessionMesh:
     # ------------------------------------------------------------------ #
     def _dirichlet_faces(self):
         g, s = self.session.geometry, self.session
-        self._face_bc = {}
+        self._face_bc = {}    # Dirichlet faces
+        self._face_weak = {}  # Neumann and Robin faces (weak terms)
         for rid, comps in s.boundary_regions.items():
             conds = [bc for bc in s.boundary_conditions.get(rid, []) if bc.var == self.var]
             if not conds:
                 continue
             bc = conds[0]
-            if bc.kind != "D":
+            if bc.kind not in ("D", "N", "R"):
                 raise SessionError("boundary condition %r on region %d is not supported "
-                                   "(Dirichlet only)" % (bc.kind, rid))
+                                   % (bc.kind, rid))
+            if bc.kind == "R" and bc.primcoeff is None:
+                raise SessionError("Robin condition on region %d without PRIMCOEFF" % rid)
             for c in comps:
                 letter, ids = g.composites[c]
                 if letter not in ("F", "Q", "T"):
                     raise SessionError("boundary composite %d does not hold faces" % c)
                 for f in ids:
-                    self._face_bc[f] = bc
+                    (self._face_bc if bc.kind == "D" else self._face_weak)[f] = bc
 
     def _entity_orders(self):
         """Lowest order (modes) of the elements sharing each edge and face:
@@ -781,16 +784,100 @@ class SessionMesh:
         return out
 
     def _face_owners(self):
-        """Local coefficient range of the element that owns each boundary face."""
+        """Local coefficient range and order of the element that owns each
+        boundary face."""
         g = self.session.geometry
         out = {}
         for ci, col in enumerate(self.collections):
             base = int(self.offsets[ci])
             for el, eid in enumerate(col.elem_ids):
                 for f in g.elements[eid][1]:
-                    if f in self._face_bc:
+                    if f in self._face_bc or f in self._face_weak:
                         out[f] = (base + el * col.nc, base + (el + 1) * col.nc, col.nm)
         return out
+
+    # ------------------------------------------------------------------ #
+    def _quad_face_basis(self, f, nm):
+        """Quadrature of the quadrilateral boundary face f at its element's
+        order (nm modes, nm+1 GLL points per direction, the trace expansion's)
+        and the global basis functions living on it: (x [3, q, q], weights
+        with the surface Jacobian [q, q], global dofs, values [ndof, q, q]).
+        The functions are the global ones of the assembly: vertex modes,
+        edge modes along the edge's lower -> higher vertex id (its modes a
+        lower-order neighbour lacks left out), face modes in the face's
+        canonical frame (origin the lowest vertex, first axis towards its
+        lower-id neighbour)."""
+        g = self.session.geometry
+        A, zg, wg, _, _, _ = _tables_1d(nm)
+        cyc = self._face_cycle(f)
+        i0 = int(np.argmin(cyc))
+        O = cyc[i0]
+        nA, nB = sorted((cyc[(i0 + 1) % 4], cyc[(i0 - 1) % 4]))
+        AB = cyc[(i0 + 2) % 4]
+        P = lambda v: np.asarray(g.vertices[v], dtype=np.float64)  # noqa: E731
+        XO, XA, XB, XAB = P(O), P(nA), P(nB), P(AB)
+        za, zb = np.meshgrid(zg, zg, indexing="ij")
+        Na = [0.5 * (1 - za), 0.5 * (1 + za)]
+        Nb = [0.5 * (1 - zb), 0.5 * (1 + zb)]
+        x = (Na[0] * Nb[0])[..., None] * XO + (Na[1] * Nb[0])[..., None] * XA + \
+            (Na[0] * Nb[1])[..., None] * XB + (Na[1] * Nb[1])[..., None] * XAB
+        dxa = (0.5 * Nb[0])[..., None] * (XA - XO) + (0.5 * Nb[1])[..., None] * (XAB - XB)
+        dxb = (0.5 * Na[0])[..., None] * (XB - XO) + (0.5 * Na[1])[..., None] * (XAB - XA)
+        W = np.outer(wg, wg) * np.linalg.norm(np.cross(dxa, dxb), axis=-1)
+        dofs, F = [], []
+        for v, (i, j) in ((O, (0, 0)), (nA, (1, 0)), (nB, (0, 1)), (AB, (1, 1))):
+            dofs.append(self._base[("v", v)])
+            F.append(np.outer(A[i], A[j]))
+        for p, q, side, along in ((O, nA, 0, "a"), (O, nB, 0, "b"), (nA, AB, 1, "b"),
+                                  (nB, AB, 1, "a")):
+            key = ("e", min(p, q), max(p, q))
+            o, size = self._base[key], self._entities[key]
+            for k in range(2, min(nm, size + 2)):
+                sg = 1.0 if p < q else (-1.0) ** k
+                dofs.append(o + k - 2)
+                F.append(sg * (np.outer(A[k], A[side]) if along == "a"
+                               else np.outer(A[side], A[k])))
+        key = ("f",) + tuple(sorted(cyc))
+        o, lb = self._base[key], int(round(self._entities[key] ** 0.5))
+        for a in range(2, min(nm, lb + 2)):
+            for b in range(2, min(nm, lb + 2)):
+                dofs.append(o + (a - 2) * lb + (b - 2))
+                F.append(np.outer(A[a], A[b]))
+        return x.transpose(2, 0, 1), W, np.array(dofs, dtype=np.int64), np.array(F)
+
+    def weak_terms(self, time=0.0):
+        """The Neumann and Robin terms of the Helmholtz system
+        (ContField::v_HelmSolve, ContField.cpp:822-855: the boundary
+        expansions' inner products of the data added to the forcing;
+        Expansion3D::v_AddRobinMassMatrix / AddRobinTraceContribution,
+        Expansion3D.cpp:2045-: PRIMCOEFF-weighted face mass matrices added to
+        the operator, GlobalLinSysIterativeFull.cpp:133-150,213-231).
+        Returns (local right-hand side contribution [nloc], Robin blocks
+        [(global dofs, matrix, owner local indices)]), on quadrilateral
+        faces."""
+        g = self.session.geometry
+        rhs = np.zeros(self.nloc)
+        robin = []
+        if not self._face_weak:
+            return rhs, robin
+        owner = self._face_owners()
+        for f, bc in self._face_weak.items():
+            if g.faces[f][0] != "Q":
+                raise SessionError("Neumann / Robin conditions on triangular faces are not "
+                                   "supported")
+            lo, hi, nm = owner[f]
+            x, W, dofs, F = self._quad_face_basis(f, nm)
+            gl = self.gmap[lo:hi]
+            loc = np.empty(dofs.size, dtype=np.int64)
+            for i, d in enumerate(dofs):
+                hit = np.nonzero((gl == d) & (self.sign[lo:hi] != 0))[0]
+                loc[i] = lo + hit[0]
+            gv = bc.value.evaluate(x[0], x[1], x[2], time)
+            np.add.at(rhs, loc, self.sign[loc] * np.einsum("mij,ij->m", F, W * gv))
+            if bc.kind == "R":
+                al = np.broadcast_to(bc.primcoeff.evaluate(x[0], x[1], x[2], time), W.shape)
+                robin.append((dofs, np.einsum("mij,nij,ij->mn", F, F, W * al), loc))
+        return rhs, robin
 
     def _face_values(self, f, bc, time, nm):
         """{global dof: value} of the Dirichlet face f's boundary-constrained

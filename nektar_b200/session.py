@@ -422,6 +422,44 @@ def with_orders(xml_text, orders, seed=0):
     return ET.tostring(root, encoding="unicode")
 
 
+# Conditions of the reference's Helmholtz3D_Hex_AllBCs session on the box
+# writers' six sides (C[1] z=0, C[2] y=0, C[3] x=1, C[4] y=1, C[5] x=0,
+# C[6] z=1) for u = sin(PI/2 x) sin(PI/2 y) sin(PI/2 z): Dirichlet, Neumann
+# (the outward normal derivative) and Robin (du/dn + a u) data
+ALL_BCS = [
+    ([1, 5], "D", "sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)", None),
+    ([2], "N", "-sin(PI/2*x)*cos(PI/2*y)*sin(PI/2*z)*PI/2", None),
+    ([3], "R", "cos(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)*PI/2+2*sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)",
+     "2"),
+    ([4], "R", "sin(PI/2*x)*cos(PI/2*y)*sin(PI/2*z)*PI/2+3*sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)",
+     "3"),
+    ([6], "N", "sin(PI/2*x)*sin(PI/2*y)*cos(PI/2*z)*PI/2", None),
+]
+
+
+def with_conditions(xml_text, regions):
+    """The session xml_text with its boundary regions and conditions
+    replaced: regions is a list of (composite ids, kind 'D' / 'N' / 'R',
+    VALUE, PRIMCOEFF or None), one boundary region each."""
+    import xml.etree.ElementTree as ET
+    root = ET.fromstring(xml_text)
+    cond = root.find("CONDITIONS")
+    for tag in ("BOUNDARYREGIONS", "BOUNDARYCONDITIONS"):
+        old = cond.find(tag)
+        if old is not None:
+            cond.remove(old)
+    br = ET.SubElement(cond, "BOUNDARYREGIONS")
+    bc = ET.SubElement(cond, "BOUNDARYCONDITIONS")
+    for rid, (comps, kind, value, prim) in enumerate(regions):
+        b = ET.SubElement(br, "B", ID=str(rid))
+        b.text = " C[%s] " % _seq(sorted(comps))
+        r = ET.SubElement(bc, "REGION", REF=str(rid))
+        e = ET.SubElement(r, kind, VAR="u", VALUE=value)
+        if prim is not None:
+            e.set("PRIMCOEFF", prim)
+    return ET.tostring(root, encoding="unicode")
+
+
 def write_box_session(shape, n, nummodes, lam, dirichlet, forcing, exact, shuffle_seed=None):
     """XML text of a session on the unit cube cut into n^3 cells, each a
     hexahedron, two prisms (triangles in the x-z plane, extruded along y) or

@@ -32,13 +32,20 @@ def oracle_helm_solve(session, mesh=None):
         for e in range(ne):
             np.add.at(G, (gm[e][:, None], gm[e][None, :]), sg[e][:, None] * K[e] * sg[e][None, :])
         b_loc.append(-O.iproduct(c.shape, c.nm, c.nq, ne, To["b"], To["w"], c.jac, fc, True))
-    b_loc = np.concatenate(b_loc)
+    # Neumann / Robin: boundary inner products in the forcing, Robin face
+    # mass matrices in the operator
+    rhs_w, robin = m.weak_terms()
+    b_loc = np.concatenate(b_loc) + rhs_w
+    for dofs, M, _ in robin:
+        G[np.ix_(dofs, dofs)] += M
     # lifting with the local Dirichlet values element by element, as
     # GlobalLinSysIterativeFull::v_Solve does (GlobalLinSysIterativeFull.cpp:114-164)
     xdl = m.dirichlet_local()
     r_loc = b_loc - _apply_blocks(m, lam, xdl)
     b = np.zeros(m.nglob)
     np.add.at(b, m.gmap, m.sign * r_loc)
+    for dofs, M, loc in robin:
+        b[dofs] -= M @ (m.sign[loc] * xdl[loc])
     nd = m.ndir
     xg = np.concatenate([np.zeros(nd), np.linalg.solve(G[nd:, nd:], b[nd:])])
     xl = xdl + m.sign * xg[m.gmap]

@@ -101,3 +101,25 @@ def test_variable_order_session_matches_oracle(shape):
     rc = helm_solve(s, tol=1e-14, maxit=3000, raise_on_maxit=False,
                     solver_info={"GlobalSysSoln": "IterativeStaticCond"})
     assert rel_l2(rc.coeffs, xo) < 1e-10
+
+
+@pytest.mark.parametrize("info", [None, {"GlobalSysSoln": "IterativeStaticCond"},
+                                  {"GlobalSysSoln": "IterativeStaticCond",
+                                   "Preconditioner": "LowEnergyBlock"}])
+@pytest.mark.parametrize("orders", [None, [4, 6]])
+def test_neumann_robin_session_matches_oracle(info, orders):
+    """Dirichlet, Neumann and Robin sides (the reference's AllBCs
+    conditions) in rotated element frames: the Robin face mass matrices as
+    extra dense operators of the device CG (full solve) or folded into the
+    element matrices (condensed solves) give the oracle's solution."""
+    from nektar_b200.session import ALL_BCS, with_conditions, with_orders
+    txt = write_hex_box_session(3, 5, 1.0, U, F, U, shuffle_seed=4)
+    if orders:
+        if info and info.get("Preconditioner") == "LowEnergyBlock":
+            pytest.skip("LowEnergy takes one order")
+        txt = with_orders(txt, orders, seed=3)
+    s = read_session(with_conditions(txt, ALL_BCS))
+    r = helm_solve(s, tol=1e-14, maxit=3000, raise_on_maxit=False, solver_info=info)
+    xo, linf_o, l2_o = oracle_helm_solve(s, r.mesh)
+    assert rel_l2(r.coeffs, xo) < 1e-10
+    assert abs(r.l2 - l2_o) < 1e-9 * l2_o and abs(r.linf - linf_o) < 1e-9 * linf_o

@@ -103,9 +103,15 @@ def test_reader_rejects_what_the_path_does_not_take():
         read_session(txt.replace("</GEOMETRY>", '<CURVED><E ID="0" EDGEID="0" NUMPOINTS="3" '
                                  'TYPE="PolyEvenlySpaced"> 0 0 0 0.5 0 0 1 0 0 </E></CURVED>'
                                  "</GEOMETRY>"))
-    s = read_session(txt.replace('<D VAR="u"', '<N VAR="u"'))
+    s = read_session(txt.replace('<D VAR="u"', '<R VAR="u"'))  # Robin without PRIMCOEFF
     with pytest.raises(SessionError):
         SessionMesh(s)
+    # Neumann data on triangular faces (the weak terms cover quadrilaterals)
+    from nektar_b200.session import with_conditions
+    s = read_session(with_conditions(write_box_session("tet", 1, 4, 1.0, U, F, U),
+                                     [([1, 2, 3, 4, 5], "D", U, None), ([6], "N", "0", None)]))
+    with pytest.raises(SessionError):
+        SessionMesh(s).weak_terms()
 
 
 def test_fld_round_trip(tmp_path):
@@ -134,6 +140,7 @@ REF_PRISM = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Prism.
 REF_TET = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Tet.xml"
 REF_PRISM_VARP = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Prism_VarP.xml"
 REF_TET_VARP = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Tet_VarP.xml"
+REF_ALLBCS = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Hex_AllBCs_P6.xml"
 
 
 @pytest.mark.parametrize("shape", ["prism", "tet"])
@@ -186,15 +193,19 @@ def test_incompatible_triangle_orientation_is_rejected():
     (REF_PRISM_VARP, (0.000292496, 0.00539787), (1e-9, 1e-9)),
     # Helmholtz3D_CG_Tet_VarP.tst (orders 3, 4, 5, 6): L2 (tolerance 1e-7), Linf (1e-6)
     (REF_TET_VARP, (0.00416454, 0.0313733), (1e-7, 1e-6)),
+    # Helmholtz3D_CG_Hex_AllBCs.tst (Dirichlet, Neumann and Robin sides): tolerance 1e-12
+    (REF_ALLBCS, (0.000416575, 0.000871589), (1e-12, 1e-12)),
 ])
 def test_reference_prism_tet_sessions_reproduce_their_records(path, record, tol):
     """The reference's own Prism / Tet regression sessions reproduce their
     recorded errors, including the reference's Dirichlet procedure on
     triangular faces (Radau -> GLL edge interpolation, boundary expansions
     grouped by type, face by face overwrites, copies to elements that only
-    touch the boundary) and, in the VarP sessions, variable order (edges and
-    faces with the modes of their lowest-order element, the others of sign 0,
-    Dirichlet faces projected at their element's order)."""
+    touch the boundary), in the VarP sessions variable order (edges and faces
+    with the modes of their lowest-order element, the others of sign 0,
+    Dirichlet faces projected at their element's order), and in AllBCs the
+    Neumann and Robin terms (boundary inner products in the forcing,
+    PRIMCOEFF-weighted face mass matrices in the operator)."""
     _, linf, l2 = oracle_helm_solve(read_session(path))
     # the regression tester reads the demo's output, printed by cout with its
     # default six significant digits (Helmholtz3D.cpp: cout << vL2Error)
@@ -237,3 +248,35 @@ def test_fld_variable_order_blocks(tmp_path):
     assert [b["NUMMODESPERDIR"] for b in blocks] == ["UNIORDER:3,3,3", "UNIORDER:5,5,5"]
     assert sorted(i for b in blocks for i in b["ids"]) == list(range(48))
     assert np.array_equal(np.concatenate([b["data"] for b in blocks]), coeffs)
+
+
+def test_weak_terms_do_not_depend_on_element_frames():
+    """Neumann and Robin faces in rotated element frames (signs in the map):
+    the same discrete solution, so the same errors."""
+    from nektar_b200.session import ALL_BCS, with_conditions
+    errs = []
+    for seed in (None, 4, 7):
+        s = read_session(with_conditions(write_hex_box_session(2, 5, 1.0, U, F, U,
+                                                               shuffle_seed=seed), ALL_BCS))
+        _, linf, l2 = oracle_helm_solve(s)
+        errs.append((l2, linf))
+    for l2, linf in errs[1:]:
+        assert abs(l2 - errs[0][0]) < 1e-10 * errs[0][0] and abs(linf - errs[0][1]) < 1e-10
+
+
+def test_robin_blocks_are_face_mass_matrices():
+    """A Robin face's block is PRIMCOEFF times the face mass matrix of the
+    global functions on it: symmetric, positive definite, and the sum of the
+    vertex functions (the constant 1 on the face) integrates to the area."""
+    from nektar_b200.session import ALL_BCS, with_conditions
+    s = read_session(with_conditions(write_hex_box_session(2, 5, 1.0, U, F, U, shuffle_seed=4),
+                                     ALL_BCS))
+    m = SessionMesh(s)
+    _, robin = m.weak_terms()
+    assert robin
+    for dofs, M, loc in robin:
+        assert np.abs(M - M.T).max() < 1e-15 and np.linalg.eigvalsh(M)[0] > 0
+        one = np.zeros(dofs.size)
+        one[:4] = 1.0  # the four vertex functions come first
+        prim = 2.0 if M.sum() > 0 and abs(one @ M @ one - 2 * 0.25) < 1e-12 else 3.0
+        assert abs(one @ M @ one - prim * 0.25) < 1e-12  # faces of a 2^3 box: area 1/4
