@@ -118,16 +118,74 @@ def collapsed_to_standard(shape, e1, e2, e3):
     return 0.25 * (1 + e1) * (1 - e2) * (1 - e3) - 1, 0.5 * (1 + e2) * (1 - e3) - 1, e3
 
 
-def element_geometry(shape, X, z):
+def edge_bubble(shape, a, b, xi):
+    """The quadratic edge mode of local edge (a, b) of a shape (the modified
+    basis's mode 2 on that edge, zero on the other edges and faces not
+    holding it) and its gradient at standard points xi (n, 3): the product
+    of the edge's two end barycentrics (tet; prism edges in a triangle,
+    times the extrusion factor), or (1 - t^2)/4 along the edge times the
+    linear factors across it (hexahedra, prism edges along the extrusion)."""
+    V = STD_VERTS[shape]
+    n = xi.shape[0]
+    one = np.ones(n)
+    if shape == "hex":
+        d = int(np.nonzero(V[a] != V[b])[0][0])
+        fac, grad = [], []
+        for ax in range(3):
+            t = xi[:, ax]
+            if ax == d:
+                fac.append(0.25 * (1 - t * t))
+                grad.append(-0.5 * t)
+            else:
+                sg = V[a][ax]
+                fac.append(0.5 * (1 + sg * t))
+                grad.append(0.5 * sg * one)
+        phi = fac[0] * fac[1] * fac[2]
+        dphi = np.stack([grad[0] * fac[1] * fac[2], fac[0] * grad[1] * fac[2],
+                         fac[0] * fac[1] * grad[2]], axis=1)
+        return phi, dphi
+    x1, x2, x3 = xi[:, 0], xi[:, 1], xi[:, 2]
+    if shape == "tet":
+        lam = [-0.5 * (1 + x1 + x2 + x3), 0.5 * (1 + x1), 0.5 * (1 + x2), 0.5 * (1 + x3)]
+        dl = [np.array([-0.5, -0.5, -0.5]), np.array([0.5, 0, 0]), np.array([0, 0.5, 0]),
+              np.array([0, 0, 0.5])]
+        return lam[a] * lam[b], lam[a][:, None] * dl[b] + lam[b][:, None] * dl[a]
+    # prism: triangle (xi1, xi3) barycentrics, extrusion along xi2
+    lam = [-0.5 * (x1 + x3), 0.5 * (1 + x1), 0.5 * (1 + x3)]
+    dl = [np.array([-0.5, 0, -0.5]), np.array([0.5, 0, 0]), np.array([0, 0, 0.5])]
+    tri = {(-1, -1): 0, (1, -1): 1, (-1, 1): 2}
+    ta, tb = tri[(V[a][0], V[a][2])], tri[(V[b][0], V[b][2])]
+    if ta != tb:  # an edge of a triangle, at xi2 = +-1
+        sg = V[a][1]
+        h, dh = 0.5 * (1 + sg * x2), np.array([0, 0.5 * sg, 0])
+        phi = lam[ta] * lam[tb] * h
+        dphi = (lam[ta][:, None] * dl[tb] + lam[tb][:, None] * dl[ta]) * h[:, None] + \
+            (lam[ta] * lam[tb])[:, None] * dh
+        return phi, dphi
+    b2 = 0.25 * (1 - x2 * x2)
+    return lam[ta] * b2, dl[ta][None, :] * b2[:, None] + \
+        (lam[ta] * (-0.5 * x2))[:, None] * np.array([0, 1.0, 0])
+
+
+def element_geometry(shape, X, z, curves=None):
     """jac (nelmt*nt,), df (9, nelmt*nt), coordinates (3, nelmt*nt) of
-    straight-sided elements with vertex coordinates X (nelmt, nv, 3) at the
-    collapsed tensor points z = (z0, z1, z2) (point q = (k nq1 + j) nq0 + i)."""
+    elements with vertex coordinates X (nelmt, nv, 3) at the collapsed tensor
+    points z = (z0, z1, z2) (point q = (k nq1 + j) nq0 + i). curves: per
+    element a list of (local edge (a, b), mode-2 coefficient c (3,)) of its
+    quadratic curved edges, added to the vertex map as the reference's
+    geometry expansions add the edges' coefficients (Geometry3D::v_FillGeom;
+    the factors are the map's exact derivatives at the points)."""
     e1, e2, e3 = np.meshgrid(z[0], z[1], z[2], indexing="ij")  # [i, j, k]
     e = [a.transpose(2, 1, 0).reshape(-1) for a in (e1, e2, e3)]
     xi = np.stack(collapsed_to_standard(shape, *e), axis=1)
     N, dN = shape_functions(shape, xi)
     x = np.einsum("pc,ecd->edp", N, X)
     J = np.einsum("pcj,ecd->epdj", dN, X)  # J[e, p, d, j] = d x_d / d xi_j
+    for el, lst in enumerate(curves or []):
+        for (a, b), c in lst:
+            phi, dphi = edge_bubble(shape, a, b, xi)
+            x[el] += np.asarray(c)[:, None] * phi[None, :]
+            J[el] += np.asarray(c)[None, :, None] * dphi[:, None, :]
     det = np.linalg.det(J)
     if np.any(det <= 0):
         raise SessionError("element with a non-positive Jacobian")
@@ -359,8 +417,23 @@ class Collection:
         self.deformed = True
         self.lverts = np.array([local_vertices(geom, e) for e in self.elem_ids], dtype=np.int64)
         self.X = np.array([[geom.vertices[v] for v in row] for row in self.lverts])
+        curves = None
+        if geom.curved_edges:
+            eid = {tuple(sorted(vs)): i for i, vs in geom.edges.items()}
+            _, edges, _ = topology(shape, nm)
+            curves = []
+            for row in self.lverts:
+                lst = []
+                for a, b, _ in edges:
+                    ge = eid.get(tuple(sorted((int(row[a]), int(row[b])))))
+                    if ge in geom.curved_edges:
+                        p = geom.curved_edges[ge]
+                        lst.append(((a, b), 4.0 * (p[1] - 0.5 * (p[0] + p[2]))))
+                curves.append(lst)
+            self.deformed = True
+        self.curves = curves
         self.jac, self.df, self.xyz = element_geometry(
-            shape, self.X, tuple(np.asarray(z) for z in self.T["z"]))
+            shape, self.X, tuple(np.asarray(z) for z in self.T["z"]), curves)
 
     def quad_weights(self):
         """Integration weights jac * w0 w1 w2 at every quadrature point (the
@@ -631,15 +704,8 @@ class SessionMesh:
             nA, nB = nB, nA
         AB = cyc[(i0 + 2) % 4]
         P = lambda v: np.asarray(g.vertices[v], dtype=np.float64)  # noqa: E731
-        XO, XA, XB, XAB = P(O), P(nA), P(nB), P(AB)
         za, zb = np.meshgrid(z, z, indexing="ij")
-        Na = [0.5 * (1 - za), 0.5 * (1 + za)]
-        Nb = [0.5 * (1 - zb), 0.5 * (1 + zb)]
-        x = (Na[0] * Nb[0])[..., None] * XO + (Na[1] * Nb[0])[..., None] * XA + \
-            (Na[0] * Nb[1])[..., None] * XB + (Na[1] * Nb[1])[..., None] * XAB
-        dxa = (0.5 * Nb[0])[..., None] * (XA - XO) + (0.5 * Nb[1])[..., None] * (XAB - XB)
-        dxb = (0.5 * Na[0])[..., None] * (XB - XO) + (0.5 * Na[1])[..., None] * (XAB - XA)
-        J = np.linalg.norm(np.cross(dxa, dxb), axis=-1)
+        x, J = self._quad_map(O, nA, nB, AB, za, zb)
         fv = bc.value.evaluate(x[..., 0], x[..., 1], x[..., 2], time)
         ub = (vals[O] * np.outer(A[0], A[0]) + vals[nA] * np.outer(A[1], A[0])
               + vals[nB] * np.outer(A[0], A[1]) + vals[AB] * np.outer(A[1], A[1]))
@@ -691,6 +757,80 @@ class SessionMesh:
         M = np.einsum("mij,nij,ij->mn", F, F, W)
         o = self._base[key]
         out[o:o + len(modes)] = np.linalg.solve(M, rhs)
+
+    def _curve(self, a, b):
+        """Mode-2 coefficient (3,) of the edge between global vertices a and
+        b: 4 (midpoint - mean of the ends) for a quadratic curved edge
+        (SegGeom::v_FillGeom projects the curve on the edge's modes), zero
+        for a straight one. The same for either direction."""
+        g = self.session.geometry
+        if not g.curved_edges:
+            return np.zeros(3)
+        if not hasattr(self, "_edge_of"):
+            self._edge_of = {tuple(sorted(vs)): i for i, vs in g.edges.items()}
+        e = self._edge_of.get(tuple(sorted((a, b))))
+        if e not in g.curved_edges:
+            return np.zeros(3)
+        p = g.curved_edges[e]
+        return 4.0 * (p[1] - 0.5 * (p[0] + p[2]))
+
+    def _edge_points(self, a, b, s):
+        P = lambda v: np.asarray(self.session.geometry.vertices[v], dtype=np.float64)  # noqa: E731
+        return np.outer(0.5 * (1 - s), P(a)) + np.outer(0.5 * (1 + s), P(b)) + \
+            np.outer(0.25 * (1 - s * s), self._curve(a, b))
+
+    def _edge_speed(self, a, b, s):
+        P = lambda v: np.asarray(self.session.geometry.vertices[v], dtype=np.float64)  # noqa: E731
+        d = 0.5 * (P(b) - P(a))[None, :] - np.outer(0.5 * s, self._curve(a, b))
+        return np.linalg.norm(d, axis=1)
+
+    def _quad_map(self, O, nA, nB, AB, za, zb):
+        """Points and surface Jacobian of the quadrilateral face O, nA, AB, nB
+        (coordinates za along O -> nA, zb along O -> nB): the bilinear map
+        plus the quadratic curves of its edges."""
+        P = lambda v: np.asarray(self.session.geometry.vertices[v], dtype=np.float64)  # noqa: E731
+        XO, XA, XB, XAB = P(O), P(nA), P(nB), P(AB)
+        Na = [0.5 * (1 - za), 0.5 * (1 + za)]
+        Nb = [0.5 * (1 - zb), 0.5 * (1 + zb)]
+        x = (Na[0] * Nb[0])[..., None] * XO + (Na[1] * Nb[0])[..., None] * XA + \
+            (Na[0] * Nb[1])[..., None] * XB + (Na[1] * Nb[1])[..., None] * XAB
+        dxa = (0.5 * Nb[0])[..., None] * (XA - XO) + (0.5 * Nb[1])[..., None] * (XAB - XB)
+        dxb = (0.5 * Na[0])[..., None] * (XB - XO) + (0.5 * Na[1])[..., None] * (XAB - XA)
+        for p, q, t, u, along in ((O, nA, za, Nb[0], "a"), (nB, AB, za, Nb[1], "a"),
+                                  (O, nB, zb, Na[0], "b"), (nA, AB, zb, Na[1], "b")):
+            c = self._curve(p, q)
+            if not c.any():
+                continue
+            bub, dbub = 0.25 * (1 - t * t), -0.5 * t
+            du = -0.5 if u is Nb[0] or u is Na[0] else 0.5
+            x = x + (bub * u)[..., None] * c
+            if along == "a":
+                dxa = dxa + (dbub * u)[..., None] * c
+                dxb = dxb + (bub * du)[..., None] * c
+            else:
+                dxb = dxb + (dbub * u)[..., None] * c
+                dxa = dxa + (bub * du)[..., None] * c
+        return x, np.linalg.norm(np.cross(dxa, dxb), axis=-1)
+
+    def _tri_map(self, v0, v1, v2, xa, xb):
+        """Points and surface Jacobian (per unit d xa d xb) of the triangle
+        v0, v1, v2 at its standard coordinates: the linear map plus the
+        quadratic curves of its edges (products of the end barycentrics)."""
+        P = lambda v: np.asarray(self.session.geometry.vertices[v], dtype=np.float64)  # noqa: E731
+        lam = [-0.5 * (xa + xb), 0.5 * (1 + xa), 0.5 * (1 + xb)]
+        dl = [(-0.5, -0.5), (0.5, 0.0), (0.0, 0.5)]
+        V = [v0, v1, v2]
+        x = sum(lam[i][..., None] * P(V[i]) for i in range(3))
+        dxa = sum(dl[i][0] * P(V[i]) for i in range(3)) + 0 * x
+        dxb = sum(dl[i][1] * P(V[i]) for i in range(3)) + 0 * x
+        for i, j in ((0, 1), (1, 2), (0, 2)):
+            c = self._curve(V[i], V[j])
+            if not c.any():
+                continue
+            x = x + (lam[i] * lam[j])[..., None] * c
+            dxa = dxa + (dl[i][0] * lam[j] + dl[j][0] * lam[i])[..., None] * c
+            dxb = dxb + (dl[i][1] * lam[j] + dl[j][1] * lam[i])[..., None] * c
+        return x, np.linalg.norm(np.cross(dxa, dxb), axis=-1)
 
     def _face_cycle(self, f):
         """The global vertex ids of face f in cyclic order."""
@@ -773,8 +913,8 @@ class SessionMesh:
                     continue
                 for f in g.composites[c][1]:
                     kind = g.faces[f][0]
-                    regular = True
-                    if kind == "Q":  # a parallelogram has a constant Jacobian
+                    regular = not any(e in g.curved_edges for e in g.faces[f][1])
+                    if kind == "Q" and regular:  # a parallelogram has a constant Jacobian
                         cyc = [P(v) for v in self._face_cycle(f)]
                         regular = bool(np.allclose(cyc[0] + cyc[2], cyc[1] + cyc[3],
                                                    rtol=0, atol=1e-12))
@@ -815,15 +955,9 @@ class SessionMesh:
         nA, nB = sorted((cyc[(i0 + 1) % 4], cyc[(i0 - 1) % 4]))
         AB = cyc[(i0 + 2) % 4]
         P = lambda v: np.asarray(g.vertices[v], dtype=np.float64)  # noqa: E731
-        XO, XA, XB, XAB = P(O), P(nA), P(nB), P(AB)
         za, zb = np.meshgrid(zg, zg, indexing="ij")
-        Na = [0.5 * (1 - za), 0.5 * (1 + za)]
-        Nb = [0.5 * (1 - zb), 0.5 * (1 + zb)]
-        x = (Na[0] * Nb[0])[..., None] * XO + (Na[1] * Nb[0])[..., None] * XA + \
-            (Na[0] * Nb[1])[..., None] * XB + (Na[1] * Nb[1])[..., None] * XAB
-        dxa = (0.5 * Nb[0])[..., None] * (XA - XO) + (0.5 * Nb[1])[..., None] * (XAB - XB)
-        dxb = (0.5 * Na[0])[..., None] * (XB - XO) + (0.5 * Na[1])[..., None] * (XAB - XA)
-        W = np.outer(wg, wg) * np.linalg.norm(np.cross(dxa, dxb), axis=-1)
+        x, J = self._quad_map(O, nA, nB, AB, za, zb)
+        W = np.outer(wg, wg) * J
         dofs, F = [], []
         for v, (i, j) in ((O, (0, 0)), (nA, (1, 0)), (nB, (0, 1)), (AB, (1, 1))):
             dofs.append(self._base[("v", v)])
@@ -897,14 +1031,19 @@ class SessionMesh:
             nxt = E[(j + 1) % len(E)]
             fv.append(a if b in nxt else b)
         vals = {}
-        M1 = (A[2:] * wg) @ A[2:].T
 
-        def proj1d(data):
+        def proj1d(data, a=None, b=None):
+            """SegExp::FwdTransBndConstrained of edge data at the GLL points:
+            vertex values, then the L2 projection of the rest onto the
+            interior modes with the edge's Jacobian (|dx/ds|, not constant on
+            a curved edge)."""
             c = np.zeros(nm)
             c[0], c[1] = data[0], data[-1]
             if nb:
+                js = np.ones_like(zg) if a is None else self._edge_speed(a, b, zg)
+                wj = wg * js
                 rem = data - c[0] * A[0] - c[1] * A[1]
-                c[2:] = np.linalg.solve(M1, (A[2:] * wg) @ rem)
+                c[2:] = np.linalg.solve((A[2:] * wj) @ A[2:].T, (A[2:] * wj) @ rem)
             return c
 
         full = {}  # (a, b) -> the edge's coefficients along a -> b, all nm modes
@@ -925,8 +1064,8 @@ class SessionMesh:
                 vals[self._base[("v", v)]] = float(bcv(P(v)))
             for j in range(4):
                 a, b = fv[j], fv[(j + 1) % 4]
-                x = np.outer(0.5 * (1 - zg), P(a)) + np.outer(0.5 * (1 + zg), P(b))
-                put_edge(a, b, proj1d(bcv(x)))
+                x = self._edge_points(a, b, zg)
+                put_edge(a, b, proj1d(bcv(x), a, b))
             if nb:
                 out = np.zeros(self.ndir)
                 for gd, v in vals.items():
@@ -946,13 +1085,12 @@ class SessionMesh:
         X0, X1, X2 = P(v0), P(v1), P(v2)
         S, T = np.meshgrid(zg, zr, indexing="ij")
         xa = 0.5 * (1 + S) * (1 - T) - 1
-        x = (-0.5 * (xa + T))[..., None] * X0 + (0.5 * (1 + xa))[..., None] * X1 + \
-            (0.5 * (1 + T))[..., None] * X2
+        x, Jt = self._tri_map(v0, v1, v2, xa, T)
         data = bcv(x)  # [s, t]
         I = _interp_matrix(zr, zg)  # Gauss-Radau -> GLL
-        c0 = proj1d(data[:, 0])
-        c1 = proj1d(I @ data[-1, :])
-        c2 = proj1d(I @ data[0, :])
+        c0 = proj1d(data[:, 0], v0, v1)
+        c1 = proj1d(I @ data[-1, :], v1, v2)
+        c2 = proj1d(I @ data[0, :], v0, v2)
         vtab = {v0: c2[0], v1: c1[0], v2: c2[1]}  # edge 2 written last
         vtab[v1] = c1[0]
         for v, val in vtab.items():
@@ -974,8 +1112,7 @@ class SessionMesh:
                 ub = ub + c0[k] * np.outer(phi[k], Brow[(k, 0)]) \
                     + c2[k] * np.outer(phi[0], Brow[(0, k)]) + c1[k] * np.outer(phi[1], Brow[(1, k - 1)])
             F = np.stack([np.outer(phi[a], Brow[(a, b)]) for a, b in modes])
-            J = np.linalg.norm(np.cross(0.5 * (X1 - X0), 0.5 * (X2 - X0)))
-            W = np.outer(wg, wr) * J
+            W = np.outer(wg, wr) * Jt
             c = np.linalg.solve(np.einsum("mij,nij,ij->mn", F, F, W),
                                 np.einsum("mij,ij->m", F, W * (data - ub)))
             refl = v0 != corigin

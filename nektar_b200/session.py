@@ -17,7 +17,8 @@ Follows the reference readers section by section:
   ReadBoundaryRegions (:228-316), ReadBoundaryConditions (:318-).
 
 What the B200 path does not take is rejected with a clear message rather
-than read wrongly: CURVED sections, compressed (base64) geometry blocks,
+than read wrongly: curved faces and curves other than quadratic edges,
+compressed (base64) geometry blocks,
 per-direction orders (NUMMODES="4,6,8"), pyramids, and expansion types
 other than MODIFIED.
 """
@@ -48,6 +49,7 @@ class Geometry:
     elements: dict  # id -> (shape, [face ids])
     composites: dict  # id -> (letter, [ids])
     domain: list  # composite ids
+    curved_edges: dict = field(default_factory=dict)  # edge id -> (npts, 3) curve points
 
 
 @dataclass
@@ -109,8 +111,19 @@ def _read_geometry(root):
     if g is None:
         raise SessionError("no GEOMETRY section")
     dim, space = int(g.get("DIM", 3)), int(g.get("SPACE", 3))
-    if g.find("CURVED") is not None and len(list(g.find("CURVED"))):
-        raise SessionError("CURVED geometry is not supported by this reader")
+    curved = {}
+    cnode = g.find("CURVED")
+    for c in (list(cnode) if cnode is not None else []):
+        # MeshGraphIOXml::v_ReadCurves: edges with their points; quadratic
+        # curves (three points, the two vertices and the midpoint) only
+        if c.tag != "E":
+            raise SessionError("curved faces are not supported")
+        npts, ptype = int(c.get("NUMPOINTS")), c.get("TYPE")
+        if npts != 3 or ptype not in ("PolyEvenlySpaced", "GaussLobattoLegendre"):
+            raise SessionError("curved edge %s: %d %s points (quadratic curves only)"
+                               % (c.get("EDGEID"), npts, ptype))
+        vals = [float(v) for v in c.text.split()]
+        curved[int(c.get("EDGEID"))] = np.array(vals, dtype=np.float64).reshape(npts, 3)
     for sec in ("VERTEX", "EDGE", "FACE", "ELEMENT"):
         node = g.find(sec)
         if node is not None and node.get("COMPRESSED"):
@@ -165,7 +178,12 @@ def _read_geometry(root):
         composites[int(c.get("ID"))] = (refs[0][0], ids)
     dnode = g.find("DOMAIN")
     domain = [i for _, lst in parse_composite_refs(dnode.text) for i in lst]
-    return Geometry(dim, space, vertices, edges, faces, elements, composites, domain)
+    for e, pts in curved.items():
+        ends = {tuple(np.round(pts[0], 12)), tuple(np.round(pts[-1], 12))}
+        want = {tuple(np.round(np.asarray(vertices[v], dtype=np.float64), 12)) for v in edges[e]}
+        if ends != want:
+            raise SessionError("curved edge %d does not end at its vertices" % e)
+    return Geometry(dim, space, vertices, edges, faces, elements, composites, domain, curved)
 
 
 def _read_expansions(root):

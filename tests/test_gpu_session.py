@@ -123,3 +123,15 @@ def test_neumann_robin_session_matches_oracle(info, orders):
     xo, linf_o, l2_o = oracle_helm_solve(s, r.mesh)
     assert rel_l2(r.coeffs, xo) < 1e-10
     assert abs(r.l2 - l2_o) < 1e-9 * l2_o and abs(r.linf - linf_o) < 1e-9 * linf_o
+
+
+@pytest.mark.parametrize("shape", ["hex", "prism"])
+def test_curved_session_matches_oracle(shape):
+    """Quadratic curved edges (on the boundary and inside): the device solve
+    on the curved element maps matches the oracle's."""
+    from tests.test_session import _curve_session
+    s = _curve_session(shape)
+    r = helm_solve(s, tol=1e-14, maxit=3000, raise_on_maxit=False)
+    xo, linf_o, l2_o = oracle_helm_solve(s, r.mesh)
+    assert rel_l2(r.coeffs, xo) < 1e-10
+    assert abs(r.l2 - l2_o) < 1e-9 * l2_o

@@ -99,10 +99,13 @@ def test_reader_rejects_what_the_path_does_not_take():
     txt = write_hex_box_session(1, 4, 1.0, U, F, U)
     with pytest.raises(SessionError):
         read_session(txt.replace('NUMMODES="4"', 'NUMMODES="4,5,6"'))
-    with pytest.raises(SessionError):
-        read_session(txt.replace("</GEOMETRY>", '<CURVED><E ID="0" EDGEID="0" NUMPOINTS="3" '
-                                 'TYPE="PolyEvenlySpaced"> 0 0 0 0.5 0 0 1 0 0 </E></CURVED>'
-                                 "</GEOMETRY>"))
+    with pytest.raises(SessionError):  # a cubic curve
+        read_session(txt.replace("</GEOMETRY>", '<CURVED><E ID="0" EDGEID="0" NUMPOINTS="4" '
+                                 'TYPE="PolyEvenlySpaced"> 0 0 0 0.3 0 0 0.6 0 0 1 0 0 </E>'
+                                 "</CURVED></GEOMETRY>"))
+    with pytest.raises(SessionError):  # a curved face
+        read_session(txt.replace("</GEOMETRY>", '<CURVED><F ID="0" FACEID="0" NUMPOINTS="3" '
+                                 'TYPE="PolyEvenlySpaced"> 0 0 0 </F></CURVED></GEOMETRY>'))
     s = read_session(txt.replace('<D VAR="u"', '<R VAR="u"'))  # Robin without PRIMCOEFF
     with pytest.raises(SessionError):
         SessionMesh(s)
@@ -141,6 +144,7 @@ REF_TET = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Tet.xml"
 REF_PRISM_VARP = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Prism_VarP.xml"
 REF_TET_VARP = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Tet_VarP.xml"
 REF_ALLBCS = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Hex_AllBCs_P6.xml"
+REF_PRISM_DEF = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Prism_Deformed.xml"
 
 
 @pytest.mark.parametrize("shape", ["prism", "tet"])
@@ -195,6 +199,8 @@ def test_incompatible_triangle_orientation_is_rejected():
     (REF_TET_VARP, (0.00416454, 0.0313733), (1e-7, 1e-6)),
     # Helmholtz3D_CG_Hex_AllBCs.tst (Dirichlet, Neumann and Robin sides): tolerance 1e-12
     (REF_ALLBCS, (0.000416575, 0.000871589), (1e-12, 1e-12)),
+    # Helmholtz3D_CG_Prism_Deformed.tst (two quadratic curved edges): tolerance 1e-9
+    (REF_PRISM_DEF, (8.88011e-06, 7.59576e-05), (1e-9, 1e-9)),
 ])
 def test_reference_prism_tet_sessions_reproduce_their_records(path, record, tol):
     """The reference's own Prism / Tet regression sessions reproduce their
@@ -205,7 +211,10 @@ def test_reference_prism_tet_sessions_reproduce_their_records(path, record, tol)
     with the modes of their lowest-order element, the others of sign 0,
     Dirichlet faces projected at their element's order), and in AllBCs the
     Neumann and Robin terms (boundary inner products in the forcing,
-    PRIMCOEFF-weighted face mass matrices in the operator)."""
+    PRIMCOEFF-weighted face mass matrices in the operator), and in
+    Prism_Deformed quadratic curved edges (the elements' maps with the edges'
+    mode-2 coefficients, the boundary faces projected on their curved maps
+    and grouped as deformed)."""
     _, linf, l2 = oracle_helm_solve(read_session(path))
     # the regression tester reads the demo's output, printed by cout with its
     # default six significant digits (Helmholtz3D.cpp: cout << vL2Error)
@@ -280,3 +289,40 @@ def test_robin_blocks_are_face_mass_matrices():
         one[:4] = 1.0  # the four vertex functions come first
         prim = 2.0 if M.sum() > 0 and abs(one @ M @ one - 2 * 0.25) < 1e-12 else 3.0
         assert abs(one @ M @ one - prim * 0.25) < 1e-12  # faces of a 2^3 box: area 1/4
+
+
+def _curve_session(shape="hex", n=2, nm=5, seed=3, bulge=(0.0, 0.0, 0.08)):
+    """A box session with quadratic curves on the edges of the z = 1 face
+    along x and on one interior edge."""
+    s = read_session(write_box_session(shape, n, nm, 1.0, U, F, U, shuffle_seed=seed))
+    g = s.geometry
+    P = lambda v: np.asarray(g.vertices[v], dtype=np.float64)  # noqa: E731
+    for e, (a, b) in g.edges.items():
+        pa, pb = P(a), P(b)
+        top = pa[2] == 1.0 and pb[2] == 1.0 and pa[1] == pb[1] and pa[0] != pb[0]
+        inner = np.allclose(pa, [0.5, 0.5, 0.5]) and pb[2] == 0.5 and pb[1] == 0.5
+        if top or inner:
+            mid = 0.5 * (pa + pb) + np.asarray(bulge) * (1 if top else -0.5)
+            g.curved_edges[e] = np.array([pa, mid, pb])
+    return s
+
+
+@pytest.mark.parametrize("shape", ["hex", "prism"])
+def test_curved_edges_in_the_element_maps(shape):
+    """Elements holding a curved edge take the quadratic through its three
+    points: quadrature points on the edge lie on the curve, the map stays
+    invertible, and the volume changes by the bulge's swept volume."""
+    s = _curve_session(shape)
+    assert s.geometry.curved_edges
+    m = SessionMesh(s)
+    straight = SessionMesh(read_session(write_box_session(shape, 2, 5, 1.0, U, F, U,
+                                                          shuffle_seed=3)))
+    vol, vol0 = m.quad_weights().sum(), straight.quad_weights().sum()
+    assert all(c.jac.min() > 0 for c in m.collections)
+    # the top face bulges outwards by 0.08 (1 - s^2) across every element
+    # (s its local x coordinate): 0.08 * 2/3 of volume; the interior curve
+    # moves as much volume into one element as out of its neighbour
+    assert abs(vol - vol0 - 0.08 * 2.0 / 3.0) < 1e-12
+    for c in m.collections:  # points on a curved edge lie on its quadratic
+        if c.curves and any(c.curves):
+            assert c.deformed
