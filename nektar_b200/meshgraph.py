@@ -979,6 +979,46 @@ class SessionMesh:
                 F.append(np.outer(A[a], A[b]))
         return x.transpose(2, 0, 1), W, np.array(dofs, dtype=np.int64), np.array(F)
 
+    def _tri_face_basis(self, f, nm):
+        """_quad_face_basis for a triangular face: its canonical frame
+        (origin, end of the first axis, the apex its elements collapse
+        towards), the trace expansion's points (GLL nm+1 along the first
+        axis, Gauss-Radau (1, 0) nm towards the apex), and the global
+        functions on it: vertex modes (the apex mode the collapsed psi_01),
+        edge modes along each edge's lower -> higher vertex id, face modes
+        phi_a psi_ab in the canonical frame."""
+        g = self.session.geometry
+        A, zg, wg, Brow, zr, wr = _tables_1d(nm)
+        vs = sorted({v for e in g.faces[f][1] for v in g.edges[e]})
+        key = ("t",) + tuple(vs)
+        C, O = self._tri_frame[key]
+        E = [v for v in vs if v not in (C, O)][0]
+        S, T = np.meshgrid(zg, zr, indexing="ij")
+        xa = 0.5 * (1 + S) * (1 - T) - 1
+        x, Jt = self._tri_map(O, E, C, xa, T)
+        W = np.outer(wg, wr) * Jt
+        ones = np.ones_like(zg)
+        dofs = [self._base[("v", O)], self._base[("v", E)], self._base[("v", C)]]
+        F = [np.outer(A[0], Brow[(0, 0)]), np.outer(A[1], Brow[(1, 0)]),
+             np.outer(ones, Brow[(0, 1)])]
+        for p, q, fn in ((O, E, lambda k: np.outer(A[k], Brow[(k, 0)])),
+                         (O, C, lambda k: np.outer(A[0], Brow[(0, k)])),
+                         (E, C, lambda k: np.outer(A[1], Brow[(1, k - 1)]))):
+            ek = ("e", min(p, q), max(p, q))
+            o, size = self._base[ek], self._entities[ek]
+            for k in range(2, min(nm, size + 2)):
+                dofs.append(o + k - 2)
+                F.append((1.0 if p < q else (-1.0) ** k) * fn(k))
+        o = self._base[key]
+        lo = int(round(0.5 * (5 + (1 + 8 * self._entities[key]) ** 0.5)))  # the face's order
+        pos = 0
+        for a in range(2, lo):
+            for b in range(1, lo - a):
+                dofs.append(o + pos)
+                F.append(np.outer(A[a], Brow[(a, b)]))
+                pos += 1
+        return x.transpose(2, 0, 1), W, np.array(dofs, dtype=np.int64), np.array(F)
+
     def weak_terms(self, time=0.0):
         """The Neumann and Robin terms of the Helmholtz system
         (ContField::v_HelmSolve, ContField.cpp:822-855: the boundary
@@ -987,8 +1027,7 @@ class SessionMesh:
         Expansion3D.cpp:2045-: PRIMCOEFF-weighted face mass matrices added to
         the operator, GlobalLinSysIterativeFull.cpp:133-150,213-231).
         Returns (local right-hand side contribution [nloc], Robin blocks
-        [(global dofs, matrix, owner local indices)]), on quadrilateral
-        faces."""
+        [(global dofs, matrix, owner local indices)])."""
         g = self.session.geometry
         rhs = np.zeros(self.nloc)
         robin = []
@@ -996,11 +1035,11 @@ class SessionMesh:
             return rhs, robin
         owner = self._face_owners()
         for f, bc in self._face_weak.items():
-            if g.faces[f][0] != "Q":
-                raise SessionError("Neumann / Robin conditions on triangular faces are not "
-                                   "supported")
             lo, hi, nm = owner[f]
-            x, W, dofs, F = self._quad_face_basis(f, nm)
+            if g.faces[f][0] == "Q":
+                x, W, dofs, F = self._quad_face_basis(f, nm)
+            else:
+                x, W, dofs, F = self._tri_face_basis(f, nm)
             gl = self.gmap[lo:hi]
             loc = np.empty(dofs.size, dtype=np.int64)
             for i, d in enumerate(dofs):

@@ -106,14 +106,16 @@ def test_variable_order_session_matches_oracle(shape):
 @pytest.mark.parametrize("info", [None, {"GlobalSysSoln": "IterativeStaticCond"},
                                   {"GlobalSysSoln": "IterativeStaticCond",
                                    "Preconditioner": "LowEnergyBlock"}])
-@pytest.mark.parametrize("orders", [None, [4, 6]])
-def test_neumann_robin_session_matches_oracle(info, orders):
+@pytest.mark.parametrize("orders,shape", [(None, "hex"), ([4, 6], "hex"), (None, "prism"),
+                                          (None, "tet")])
+def test_neumann_robin_session_matches_oracle(info, orders, shape):
     """Dirichlet, Neumann and Robin sides (the reference's AllBCs
     conditions) in rotated element frames: the Robin face mass matrices as
     extra dense operators of the device CG (full solve) or folded into the
     element matrices (condensed solves) give the oracle's solution."""
     from nektar_b200.session import ALL_BCS, with_conditions, with_orders
-    txt = write_hex_box_session(3, 5, 1.0, U, F, U, shuffle_seed=4)
+    txt = (write_hex_box_session(3, 5, 1.0, U, F, U, shuffle_seed=4) if shape == "hex" else
+           write_box_session(shape, 2, 5, 1.0, U, F, U, shuffle_seed=4))
     if orders:
         if info and info.get("Preconditioner") == "LowEnergyBlock":
             pytest.skip("LowEnergy takes one order")

@@ -109,12 +109,12 @@ def test_reader_rejects_what_the_path_does_not_take():
     s = read_session(txt.replace('<D VAR="u"', '<R VAR="u"'))  # Robin without PRIMCOEFF
     with pytest.raises(SessionError):
         SessionMesh(s)
-    # Neumann data on triangular faces (the weak terms cover quadrilaterals)
+    # an unknown boundary condition kind
     from nektar_b200.session import with_conditions
-    s = read_session(with_conditions(write_box_session("tet", 1, 4, 1.0, U, F, U),
-                                     [([1, 2, 3, 4, 5], "D", U, None), ([6], "N", "0", None)]))
     with pytest.raises(SessionError):
-        SessionMesh(s).weak_terms()
+        SessionMesh(read_session(with_conditions(
+            write_box_session("tet", 1, 4, 1.0, U, F, U),
+            [([1, 2, 3, 4, 5], "D", U, None), ([6], "P", "0", None)])))
 
 
 def test_fld_round_trip(tmp_path):
@@ -326,3 +326,21 @@ def test_curved_edges_in_the_element_maps(shape):
     for c in m.collections:  # points on a curved edge lie on its quadratic
         if c.curves and any(c.curves):
             assert c.deformed
+
+
+@pytest.mark.parametrize("shape", ["prism", "tet", "hexprism"])
+def test_weak_terms_on_triangles_converge(shape):
+    """Neumann and Robin data on triangular faces (the prism and tet boxes'
+    y = 0 / y = 1 sides): frame-independent errors that fall spectrally with
+    the order, as a consistent discretisation's must."""
+    from nektar_b200.session import ALL_BCS, with_conditions
+    errs = {}
+    for nm in (4, 6, 8):
+        for seed in (None, 5):
+            s = read_session(with_conditions(write_box_session(shape, 2, nm, 1.0, U, F, U,
+                                                               shuffle_seed=seed), ALL_BCS))
+            m = SessionMesh(s)
+            assert any(g_kind == "T" for g_kind in (s.geometry.faces[f][0] for f in m._face_weak))
+            errs[(nm, seed)] = oracle_helm_solve(s, m)[2]
+        assert abs(errs[(nm, None)] - errs[(nm, 5)]) < 1e-9 * errs[(nm, None)]
+    assert errs[(6, None)] < 1e-2 * errs[(4, None)] and errs[(8, None)] < 1e-2 * errs[(6, None)]
