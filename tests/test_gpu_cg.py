@@ -129,3 +129,31 @@ def test_mixed_requires_fp32_operators():
     with pytest.raises(nb.NektarB200Error) as e:
         S.solve(b, mixed=True)
     assert e.value.code == nb.C.NKB_ERR_INVALID
+
+
+def test_sharded_solve_on_device_operators_matches_global_linsys():
+    """The sharded solve with one rank and the device Helmholtz operator as
+    its element operator gives the device CG's solution."""
+    from oracle import oracle as O
+    from nektar_b200.sharded import ShardedSystem, device_apply, partition
+    m = nb.BoxMesh("hex", 4, 6, 7, amp=0.05)
+    gmap, nglob, ndir = m.assembly()
+    nt, nc = m.nt, m.nc
+    T = dict(m.T)
+    T["w"] = m.T["ws"]
+
+    def factory(lo, hi):
+        op = nb.Operator("helmholtz", shape="hex", nm=6, nq=m.nq, nelmt=hi - lo, T=m.T,
+                         jac=m.jac[lo * nt:hi * nt],
+                         df=np.ascontiguousarray(m.df[:, lo * nt:hi * nt]), deformed=True)
+        op.set_factors(1.0)
+        return op
+
+    lo, hi = partition(m.nelmt, 1, 0)
+    diag = O.helmholtz_diag("hex", 6, m.nq, m.nelmt, T, m.jac, m.df, 1.0, True)
+    S = ShardedSystem(gmap, None, nc, ndir, lo, hi, device_apply(factory, lo, hi), diag)
+    b = np.random.default_rng(8).uniform(-1, 1, m.nelmt * nc)
+    x, it = S.solve(b, np.zeros_like(b), tol=1e-12)
+    op = factory(0, m.nelmt)
+    xg, rep = nb.GlobalLinSys([op], gmap, nglob, ndir).solve(b, tol=1e-12)
+    assert rel_l2(x, xg) < 1e-9
