@@ -161,6 +161,15 @@ int nkb_op_create_dense(int n, int nelmt, const double *mats, int device, nkb_op
 int nkb_op_create_dense_rect(int rows, int cols, int nelmt, const double *mats, int device,
                              nkb_op **op);
 
+/* Every element's matrix of an FP64 operator with as many outputs as inputs
+ * per element (Helmholtz, LinearADR, square dense blocks): K[e][i][j] is
+ * output i of element e for the unit input j, built on the device by nc
+ * applications (what GlobalLinSys::v_GetBlock, GlobalLinSys.cpp:341-345,
+ * asks the reference's element expansions for when it builds statically
+ * condensed matrices). K holds nelmt * nc * nc doubles; flags as
+ * nkb_op_apply. */
+int nkb_op_element_matrices(nkb_op *op, double *K, int flags, void *stream);
+
 /* Replaces Helmholtz_MatrixFree::UpdateFactors (Helmholtz.cpp:615-691):
  * lambda (eFactorLambda); diff_mode NKB_DIFF_CONST with diff =
  * (d00 d01 d11 d02 d12 d22) from eFactorCoeffD00..D22; NKB_DIFF_VAR fills the

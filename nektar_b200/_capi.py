@@ -110,6 +110,7 @@ SIGNATURES = {
     "nkb_sys_clone": (c_int, [c_void_p, P(c_void_p)]),
     "nkb_sys_set_lambda": (c_int, [c_void_p, c_double]),
     "nkb_sys_set_blocks": (c_int, [c_void_p, c_int, ip, ip, dp]),
+    "nkb_op_element_matrices": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "nkb_sys_footprint": (c_int, [c_void_p, P(c_size_t), P(c_size_t)]),
     "nkb_geom_nelmt": (c_long, [P(GeomRequest)]),
     "nkb_geom_fill": (c_int, [P(GeomRequest), dp, dp, dp]),

@@ -812,6 +812,73 @@ extern "C" int nkb_op_set_varcoeffs(nkb_op *op, const double *velx, const double
     return Repack(op);
 }
 
+// unit input for column j of every element's matrix
+__global__ void k_unit_col(long n, int nc, int j, double *__restrict__ x)
+{
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+        x[i] = (i % nc == j) ? 1.0 : 0.0;
+}
+
+// K[e][i][j] = y[e][i]
+__global__ void k_put_col(long n, int nc, int j, const double *__restrict__ y,
+                          double *__restrict__ K)
+{
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+        K[i * nc + j] = y[i];
+}
+
+extern "C" int nkb_op_element_matrices(nkb_op *op, double *K, int flags, void *stream)
+{
+    ClearError();
+    if (!op || !K)
+        return SetError(NKB_ERR_INVALID, "nkb_op_element_matrices: NULL argument");
+    long nin, nout;
+    nkb_op_sizes(op, &nin, &nout);
+    if (op->precision != NKB_FP64 || nin != nout || op->nelmt == 0 || nin % op->nelmt)
+        return SetError(NKB_ERR_INVALID,
+                        "nkb_op_element_matrices: needs an FP64 operator with as many outputs "
+                        "as inputs per element");
+    const int nc  = int(nin / op->nelmt);
+    const long n  = nin;
+    NKB_CUDA_TRY(cudaSetDevice(op->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double *x = nullptr, *y = nullptr, *dK = (flags & NKB_HOST_PTRS) ? nullptr : K;
+    auto release = [&]() {
+        cudaFree(x);
+        cudaFree(y);
+        if (flags & NKB_HOST_PTRS)
+            cudaFree(dK);
+    };
+    if (cudaMalloc(&x, n * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&y, n * sizeof(double)) != cudaSuccess ||
+        ((flags & NKB_HOST_PTRS) && cudaMalloc(&dK, size_t(n) * nc * sizeof(double)) != cudaSuccess))
+    {
+        release();
+        return SetError(NKB_ERR_NOMEM, "nkb_op_element_matrices: %ld x %d doubles", n, nc);
+    }
+    const int nb = int(std::min<long>((n + 255) / 256, 148L * 16));
+    for (int j = 0; j < nc; ++j)
+    {
+        k_unit_col<<<nb, 256, 0, s>>>(n, nc, j, x);
+        int rc = LaunchOp<double>(op, x, y, nullptr, nullptr, nullptr, nullptr, s);
+        if (rc)
+        {
+            release();
+            return rc;
+        }
+        k_put_col<<<nb, 256, 0, s>>>(n, nc, j, y, dK);
+    }
+    cudaError_t ce = cudaGetLastError();
+    if (ce == cudaSuccess && (flags & NKB_HOST_PTRS))
+        ce = cudaMemcpyAsync(K, dK, size_t(n) * nc * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess)
+        ce = cudaStreamSynchronize(s);
+    release();
+    if (ce != cudaSuccess)
+        return SetError(NKB_ERR_CUDA, "nkb_op_element_matrices: %s", cudaGetErrorString(ce));
+    return NKB_OK;
+}
+
 extern "C" int nkb_op_sizes(const nkb_op *op, long *in_size, long *out_size)
 {
     if (!op)

@@ -130,3 +130,20 @@ def test_set_blocks_rejects_bad_blocks():
     xb, _ = sys_.solve(b, tol=1e-12)
     xj, _ = nb.GlobalLinSys([op], gmap, nglob, ndir).solve(b, tol=1e-12)
     assert rel_l2(xb, xj) < 1e-9
+
+
+@pytest.mark.parametrize("shape", ["hex", "prism", "tet"])
+def test_element_matrices_on_device_match_unit_applications(shape):
+    """nkb_op_element_matrices equals the operator applied to unit vectors
+    one host call at a time, and is symmetric (a Helmholtz matrix)."""
+    from nektar_b200.staticcond import element_matrices
+    m = nb.BoxMesh(shape, 2, 5, 6, amp=0.05)
+    op = nb.Operator("helmholtz", m)
+    op.set_factors(0.7)
+    K = element_matrices(op)
+    nc, ne = m.nc, m.nelmt
+    for j in (0, nc // 2, nc - 1):
+        x = np.zeros(ne * nc)
+        x[j::nc] = 1.0
+        assert np.array_equal(K[:, :, j], op(x).reshape(ne, nc))
+    assert np.abs(K - K.transpose(0, 2, 1)).max() < 1e-13 * np.abs(K).max()
