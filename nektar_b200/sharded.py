@@ -61,11 +61,9 @@ class ShardedSystem:
             d = np.unique(gm[a:b])
             touch[d] += 1
             first[d] = np.minimum(first[d], r)
-        shared = np.nonzero(touch > 1)[0]
-        self.iface_pos = np.searchsorted(shared, self.dofs)
-        self.on_iface = (self.iface_pos < shared.size) & \
-            (shared[np.minimum(self.iface_pos, max(shared.size - 1, 0))] == self.dofs) \
-            if shared.size else np.zeros(self.dofs.size, dtype=bool)
+        shared = np.nonzero(touch > 1)[0]  # interface dofs, sorted
+        self.on_iface = np.isin(self.dofs, shared)
+        self.iface_pos = np.searchsorted(shared, self.dofs)  # slot in the exchange buffer
         self.niface = shared.size
         self.owned = (first[self.dofs] == rank) & self.free
         self.diag = self._assemble(np.asarray(diag_loc, np.float64), absolute=True)
