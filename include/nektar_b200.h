@@ -44,6 +44,8 @@ extern "C" {
 #define NKB_ERR_NOT_CONVERGED -5 /* CG reached maxit (reference: warning + return) */
 #define NKB_ERR_NONFINITE -6   /* NaN/Inf detected in a CG scalar */
 #define NKB_ERR_NO_DEVICE -7   /* no CUDA device visible */
+#define NKB_ERR_TIMEOUT -8     /* a bounded device wait gave up: the outputs of the elements
+                                  it guarded were not written (the context stays usable) */
 
 /* ---- enums (reference numbering) ---------------------------------------- */
 #define NKB_TET 5   /* LibUtilities::eTetrahedron */
@@ -213,7 +215,8 @@ int nkb_op_apply(nkb_op *op, const double *in, double *out0, double *out1, doubl
  * this instead: staging goes through one file-scope 32 MiB device array, so
  * the operator's input plus outputs must fit in 4 Mi doubles (larger ones
  * get NKB_ERR_INVALID). The first call on a device looks the array up
- * (cudaGetSymbolAddress); make it before capturing any stream. All calls
+ * (cudaGetSymbolAddress); make it before capturing any stream. The call
+ * makes the operator's device current and restores the caller's. All calls
  * share the array: calls that overlap on the GPU race and must be
  * serialised by the caller. FP64 operators; synchronous, like the
  * NKB_HOST_PTRS path it mirrors. */
@@ -243,12 +246,39 @@ int nkb_op_helmholtz_diag(nkb_op *op, double *diag, int flags, void *stream);
 /* Time in ms of the last nkb_op_apply's kernel on the device (CUDA events). */
 int nkb_op_last_kernel_ms(const nkb_op *op, float *ms);
 
+/* Status of the operator's device error word, read and cleared: NKB_OK, or
+ * NKB_ERR_TIMEOUT when a bounded wait inside one of its kernels gave up since
+ * the last check (the elements it guarded kept stale outputs). Call it once
+ * the operator's work has completed, e.g. after synchronising the stream of
+ * NKB_DEVICE_PTRS applies; host-pointer applies and CG solves check it
+ * themselves. The reference's kernels run on the host and have no such
+ * state; its ASSERTL0 on a failed apply is the nearest counterpart. */
+int nkb_op_check_error(nkb_op *op);
+
+/* Test hook: the number of polls after which a bounded wait inside the
+ * operator's kernels gives up (0: at once; negative: the default, 2^24). A
+ * wait that gives up records NKB_ERR_TIMEOUT and still waits (bounded) for
+ * its copy or MMA to complete before the kernel exits. Used by the tests to
+ * make the wait run out; no reference counterpart. */
+int nkb_op_set_wait_limit(nkb_op *op, int polls);
+
 /* Name of the device kernel the operator runs (the autotuned choice; gather =
  * 1: the one used when a system gathers its input through the map). For
  * reports; no reference counterpart. */
 const char *nkb_op_kernel(const nkb_op *op, int gather);
 
 void nkb_op_destroy(nkb_op *op);
+
+/* Self-test of the fifth-generation tensor-core building blocks the FP32 Hex
+ * Helmholtz kernel uses (no reference counterpart): D = A B for one 128-row
+ * tile, A (128 x 8*ksteps, row-major, host) written into the kernel's
+ * K-major operand form by its row writer (column_writer = 0) or its column
+ * writer (1) as TF32 high and low parts, B
+ * (8*ksteps x n, row-major, host) in its K-major table form, n in {16, 32,
+ * 64}; D (128 x n, host) read back from tensor memory. info[0]: the tensor
+ * memory address, info[1]: 1 when the MMA completion wait succeeded. */
+int nkb_tc_selftest(int column_writer, int n, int ksteps, const float *A, const float *B, float *D,
+                    unsigned *info);
 
 /* ---- batched application over many collections --------------------------
  * ExpList::GeneralMatrixOp (MultiRegions/ExpList.cpp:2666-2757) applies one

@@ -237,6 +237,17 @@ class Operator:
         check(lib().nkb_op_last_kernel_ms(self.h, ctypes.byref(ms)))
         return ms.value
 
+    def check_error(self):
+        """Raise if a bounded wait inside one of the operator's kernels gave
+        up since the last check (device-pointer applies; host applies and
+        solves check by themselves)."""
+        check(lib().nkb_op_check_error(self.h))
+
+    def set_wait_limit(self, polls):
+        """Test hook: polls after which the kernels' bounded waits give up
+        (0: at once; negative: the default)."""
+        check(lib().nkb_op_set_wait_limit(self.h, int(polls)))
+
     def helmholtz_diag(self):
         out = np.zeros(self.nelmt * ncoeffs(self.shape, self.nm))
         check(lib().nkb_op_helmholtz_diag(self.h, out.ctypes.data, HOST_PTRS, None))

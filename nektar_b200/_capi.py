@@ -23,6 +23,7 @@ NKB_ERR_NOMEM = -4
 NKB_ERR_NOT_CONVERGED = -5
 NKB_ERR_NONFINITE = -6
 NKB_ERR_NO_DEVICE = -7
+NKB_ERR_TIMEOUT = -8
 
 TET, PRISM, HEX = 5, 7, 8
 BWDTRANS, HELMHOLTZ, LINEAR_ADR, IPRODUCT, IPRODUCT_DERIV, PHYSDERIV = 0, 1, 2, 3, 4, 5
@@ -87,6 +88,9 @@ SIGNATURES = {
     "nkb_op_sizes": (c_int, [c_void_p, P(c_long), P(c_long)]),
     "nkb_op_helmholtz_diag": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "nkb_op_last_kernel_ms": (c_int, [c_void_p, P(c_float)]),
+    "nkb_op_check_error": (c_int, [c_void_p]),
+    "nkb_tc_selftest": (c_int, [c_int, c_int, c_int, fp, fp, fp, P(ctypes.c_uint)]),
+    "nkb_op_set_wait_limit": (c_int, [c_void_p, c_int]),
     "nkb_op_destroy": (None, [c_void_p]),
     "nkb_op_kernel": (c_char_p, [c_void_p, c_int]),
     "nkb_sys_create": (c_int, [P(SysDesc), P(c_void_p)]),

@@ -229,6 +229,9 @@ extern "C" int nkb_batch_apply(nkb_batch *B, const double *in, double *out, int 
         NKB_CUDA_TRY(cudaMemcpyAsync(out, dout, B->out_size * sizeof(double),
                                      cudaMemcpyDeviceToHost, run));
         NKB_CUDA_TRY(cudaStreamSynchronize(run));
+        for (nkb_op *op : B->ops)
+            if ((rc = CheckOpError(op)))
+                return rc;
     }
     else if (legacy)
     {

@@ -1643,6 +1643,13 @@ extern "C" int nkb_cg_end(nkb_sys *S, nkb_cg_report *rep)
         rep->kernel_launches = S->launches;
         rep->restarts        = v.restarts;
     }
+    // a bounded wait that gave up inside an operator kernel left some
+    // element outputs unwritten: the solve's result cannot be trusted
+    NKB_CUDA_TRY(cudaSetDevice(S->device));
+    for (const auto *ops : {&S->ops, &S->ops32})
+        for (nkb_op *op : *ops)
+            if (int rc = CheckOpError(op))
+                return rc;
     if (h.status == NKB_ERR_NONFINITE)
         return SetError(NKB_ERR_NONFINITE, "nkb_cg_solve: non-finite CG scalar at iteration %d", h.iter);
     if (h.status == NKB_ERR_NOT_CONVERGED || !h.done)

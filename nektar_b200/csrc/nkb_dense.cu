@@ -141,8 +141,8 @@ extern "C" int nkb_op_create_dense_rect(int rows, int cols, int nelmt, const dou
     if (cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&op->ev0) != cudaSuccess || cudaEventCreate(&op->ev1) != cudaSuccess)
         return fail(SetError(NKB_ERR_CUDA, "nkb_op_create_dense: stream/event creation failed"));
-    if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess ||
-        cudaMemset(op->d_err, 0, sizeof(int)) != cudaSuccess)
+    if (cudaMalloc(&op->d_err, 2 * sizeof(int)) != cudaSuccess ||
+        cudaMemset(op->d_err, 0, 2 * sizeof(int)) != cudaSuccess)
         return fail(SetError(NKB_ERR_CUDA, "nkb_op_create_dense: error word"));
     const size_t bytes = size_t(nelmt) * rows * cols * sizeof(double);
     if (bytes)

@@ -58,6 +58,99 @@ static bool ForceGeneric()
     return v && std::strcmp(v, "generic") == 0;
 }
 
+static bool SameTable(const std::vector<double> &a, const std::vector<double> &b);
+
+// TF32 high part of an FP32 value (round to nearest, ties away from zero,
+// as cvt.rna.tf32.f32)
+static float Tf32HiHost(float x)
+{
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u = (u + 0x1000u) & 0xFFFFE000u;
+    float h;
+    std::memcpy(&h, &u, 4);
+    return h;
+}
+
+// Tables of the tensor-core Hex kernel (nkb_hex_tc.cuh) for an FP32 Hex
+// Helmholtz operator with nq = nm + 1: per direction d, with B[p][i] the
+// basis at the points (Basis::GetBdata) and dB = D B its derivative
+// (Basis.cpp:493-495), the coefficient -> point table (K = mode p, rows
+// [B_hi | B_lo | dB_hi | dB_lo] over the points i, each padded to 8) and the
+// point -> coefficient table (K = point i, rows over the modes p). Directions
+// with equal tables share one copy. Built once per operator, in the order and
+// layout the kernel copies into shared memory.
+int BuildTcTables(nkb_op *op)
+{
+    const int nm = op->nm, nq = op->nq[0];
+    if (op->shape != NKB_HEX || op->optype != NKB_HELMHOLTZ || op->precision != NKB_FP32 ||
+        nm < kTcMinNm || nm > kTcMaxNm || nq != nm + 1 || op->nq[1] != nq || op->nq[2] != nq)
+        return NKB_OK;
+    auto pad8 = [](int v) { return (v + 7) / 8 * 8; };
+    const int KM = pad8(nm), KQ = pad8(nq), NQP = pad8(nq), NMN = pad8(nm);
+    const int TBROWS = 4 * NQP, TBTROWS = 4 * NMN;
+    const size_t tbn = size_t(TBROWS) * KM, tbtn = size_t(TBTROWS) * KQ;
+    std::vector<float> img;
+    int uniq[3] = {-1, -1, -1};
+    for (int d = 0; d < 3; ++d)
+    {
+        for (int e = 0; e < d && uniq[d] < 0; ++e)
+            if (SameTable(op->hB[d], op->hB[e]) && SameTable(op->hD[d], op->hD[e]))
+                uniq[d] = uniq[e];
+        if (uniq[d] >= 0)
+        {
+            op->tc_tb[d]  = op->tc_tb[uniq[d]];
+            op->tc_tbt[d] = op->tc_tbt[uniq[d]];
+            continue;
+        }
+        uniq[d] = d;
+        // B[p][i] and dB[p][i] = sum_m D[i][m] B[p][m] (host D column-major)
+        const std::vector<double> &hB = op->hB[d], &hD = op->hD[d];
+        std::vector<double> B(size_t(nm) * nq), dB(size_t(nm) * nq, 0.0);
+        for (int p = 0; p < nm; ++p)
+            for (int i = 0; i < nq; ++i)
+            {
+                B[p * nq + i] = hB[size_t(p) * nq + i];
+                double s      = 0.0;
+                for (int m = 0; m < nq; ++m)
+                    s += hD[size_t(m) * nq + i] * hB[size_t(p) * nq + m];
+                dB[p * nq + i] = s;
+            }
+        auto part = [&](int which, int p, int i) -> float {
+            const double v = (which < 2 ? B : dB)[p * nq + i];
+            const float hi = Tf32HiHost(float(v));
+            return (which & 1) ? float(v - double(hi)) : hi;
+        };
+        const size_t base = img.size();
+        img.resize(base + tbn + tbtn, 0.f);
+        for (int n = 0; n < TBROWS; ++n)
+            for (int k = 0; k < KM; ++k)
+            {
+                const int which = n / NQP, i = n % NQP, p = k;
+                if (i < nq && p < nm)
+                    img[base + tc::OffB(n, k, TBROWS) / 4] = part(which, p, i);
+            }
+        for (int n = 0; n < TBTROWS; ++n)
+            for (int k = 0; k < KQ; ++k)
+            {
+                const int which = n / NMN, p = n % NMN, i = k;
+                if (i < nq && p < nm)
+                    img[base + tbn + tc::OffB(n, k, TBTROWS) / 4] = part(which, p, i);
+            }
+        op->tc_tb[d]  = int(base * 4);
+        op->tc_tbt[d] = int((base + tbn) * 4);
+    }
+    img.resize((img.size() + 31) / 32 * 32, 0.f); // 128-byte multiple
+    cudaFree(op->tc_tab);
+    op->tc_tab = nullptr;
+    if (cudaMalloc(&op->tc_tab, img.size() * sizeof(float)) != cudaSuccess)
+        return SetError(NKB_ERR_NOMEM, "tensor-core Hex tables");
+    NKB_CUDA_TRY(cudaMemcpy(op->tc_tab, img.data(), img.size() * sizeof(float),
+                            cudaMemcpyHostToDevice));
+    op->tc_bytes = int(img.size() * sizeof(float));
+    return NKB_OK;
+}
+
 // kernel template and variants: nkb_hex_kernel.cuh, instantiated per precision
 // in nkb_hex_f64.cu and nkb_hex_f32.cu
 extern template int HexLaunchT<double>(const nkb_op *, const HexArgs<double> &, bool, cudaStream_t,
@@ -346,7 +439,8 @@ const char *KernelName(const nkb_op *op, bool gather)
         case 1: return "k_hex_helm (streamed geometry, 1 element per CTA)";
         case 2: return "k_hex_helm (streamed geometry, 2 elements per CTA)";
         case 3: return "k_hex_helm_mma (FP64 tensor cores)";
-        default: return "k_hex_helm_mma2 (FP64 tensor cores, two warps per element)";
+        case 4: return "k_hex_helm_mma2 (FP64 tensor cores, two warps per element)";
+        default: return "k_hex_helm_tc (tcgen05 TF32 high/low tensor cores, FP32 accumulate)";
     }
 }
 

@@ -26,7 +26,7 @@ template <typename T> struct HexArgs
     const T *B0, *B1, *B2, *D;
     T lambda;
     int nelmt;
-    int *err;
+    int *err;           // [0] error word, [1] first bound of bounded waits (0: kMaxPolls)
     const int *skip;    // optional: nonzero -> nothing to do (converged CG)
 };
 
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
     __syncthreads();
 
     // TMA geometry must have landed: bounded wait by every thread
-    if (GEO == kGeoTma && !MbarWaitBounded(bar, 0, a.err, 1))
+    if (GEO == kGeoTma && !MbarWaitBounded(bar, 0, a.err, 1, WaitPolls(a.err)))
         act = false;
 
     // gradient (i, j from shared memory, k from registers) and metric:
@@ -456,11 +456,20 @@ enum
 };
 
 // candidate (geometry staging, elements per CTA) of the tuned Hex kernel
+} // namespace nkb
+
+#include "nkb_hex_tc.cuh"
+
+namespace nkb
+{
+
 // 0: TMA-staged geometry; 1, 2: streamed geometry, 1 or 2 elements per CTA;
 // 3: FP64 tensor cores (DMMA, nq <= 8, FP64 arithmetic for both storage
 //    precisions; nkb_hex_mma.cuh); 4: the same with two warps per element
-//    (nkb_hex_mma2.cuh)
-constexpr int kNumHexVariants = 5;
+//    (nkb_hex_mma2.cuh); 5: fifth-generation tensor cores (tcgen05, TF32
+//    high/low operands, FP32 accumulation; FP32 operators, nm 2..9;
+//    nkb_hex_tc.cuh)
+constexpr int kNumHexVariants = 6;
 
 template <typename T, int NQ> constexpr int TmaEpb()
 {
@@ -539,11 +548,57 @@ template <typename TV, int NM>
 static int HexMma2Launch(const nkb_op *op, const HexArgs<TV> &a, bool gather, cudaStream_t s,
                          bool set_attr);
 
+template <int NM>
+static int HexTcLaunch(const nkb_op *op, const HexArgs<float> &a, bool gather, cudaStream_t s,
+                       bool set_attr)
+{
+    constexpr int NQ = NM + 1;
+    using Dm         = TcDims<NM, NQ>;
+    if (!op->tc_tab || op->optype != NKB_HELMHOLTZ)
+        return SetError(NKB_ERR_UNSUPPORTED, "tensor-core Hex kernel: FP32 Helmholtz only");
+    const size_t bytes = TcSmemBytes<NM, NQ>(op->tc_bytes);
+    if (bytes > 227 * 1024)
+        return SetError(NKB_ERR_UNSUPPORTED, "tensor-core Hex kernel needs %zu bytes of shared memory",
+                        bytes);
+    if (set_attr)
+    {
+        NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm_tc<NM, NQ, kModeLocal>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+        NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm_tc<NM, NQ, kModeGather>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+        return NKB_OK;
+    }
+    const long ntile = (long(op->nelmt) + Dm::EPT - 1) / Dm::EPT;
+    if (ntile == 0)
+        return NKB_OK;
+    TcTables tt;
+    tt.tab   = op->tc_tab;
+    tt.bytes = op->tc_bytes;
+    for (int d = 0; d < 3; ++d)
+    {
+        tt.tb[d]  = op->tc_tb[d];
+        tt.tbt[d] = op->tc_tbt[d];
+    }
+    if (gather)
+        k_hex_helm_tc<NM, NQ, kModeGather><<<unsigned(ntile), 128, bytes, s>>>(a, tt);
+    else
+        k_hex_helm_tc<NM, NQ, kModeLocal><<<unsigned(ntile), 128, bytes, s>>>(a, tt);
+    NKB_CUDA_TRY(cudaGetLastError());
+    return NKB_OK;
+}
+
 template <typename T, int NM>
 static int HexLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStream_t s, int variant,
                      bool set_attr)
 {
     constexpr int NQ = NM + 1;
+    if (variant == 5)
+    {
+        if constexpr (std::is_same<T, float>::value && NM >= kTcMinNm && NM <= kTcMaxNm)
+            return HexTcLaunch<NM>(op, a, gather, s, set_attr);
+        else
+            return SetError(NKB_ERR_UNSUPPORTED, "tensor-core Hex kernel: FP32 operators, nm 2..9");
+    }
     if (variant == 3)
         return HexMmaLaunch<T, NM>(op, a, gather, s, set_attr);
     if (variant == 4)

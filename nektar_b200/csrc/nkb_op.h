@@ -44,6 +44,12 @@ struct nkb_op
     int gen_threads = 0; // generic kernel: threads per CTA (0: default)
     void *kdata = nullptr;
     int *d_err  = nullptr; // device error word (bounded waits that gave up)
+    // tensor-core Hex kernel (FP32 Hex Helmholtz): B / dB tables split into
+    // TF32 high and low parts in the kernel's shared-memory layout
+    float *tc_tab = nullptr;
+    int tc_bytes  = 0;
+    int tc_tb[3]  = {0, 0, 0}, tc_tbt[3] = {0, 0, 0};
+    unsigned wait_polls = 1u << 24; // first bound of bounded waits (nkb_tma.cuh kMaxPolls)
 
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -78,6 +84,11 @@ int LaunchOp(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap
              const double *gsign, cudaStream_t s, const int *skip = nullptr,
              const double *lambda = nullptr);
 int ChooseKernel(nkb_op *op);
+// tables of the tensor-core Hex kernel (FP32 Hex Helmholtz ops, nm 2..9)
+int BuildTcTables(nkb_op *op);
+// reads and clears the operator's device error word (after its work has
+// completed): NKB_ERR_TIMEOUT when a bounded wait gave up, else NKB_OK
+int CheckOpError(nkb_op *op);
 // time the Hex variants once more with the local<-global gather a system
 // uses (xin: global vector, yl: local output) and keep the fastest for
 // gathered launches

@@ -683,8 +683,8 @@ extern "C" int nkb_op_create(const nkb_op_desc *desc, nkb_op **out)
     if (cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&op->ev0) != cudaSuccess || cudaEventCreate(&op->ev1) != cudaSuccess)
         return fail(SetError(NKB_ERR_CUDA, "nkb_op_create: stream/event creation failed"));
-    if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess ||
-        cudaMemset(op->d_err, 0, sizeof(int)) != cudaSuccess)
+    if (cudaMalloc(&op->d_err, 2 * sizeof(int)) != cudaSuccess ||
+        cudaMemset(op->d_err, 0, 2 * sizeof(int)) != cudaSuccess)
         return fail(SetError(NKB_ERR_CUDA, "nkb_op_create: error word"));
 
     // 1-D tables
@@ -729,6 +729,8 @@ extern "C" int nkb_op_create(const nkb_op_desc *desc, nkb_op **out)
         if ((rc = Repack(op)))
             return fail(rc);
     }
+    if ((rc = BuildTcTables(op)))
+        return fail(rc);
     if ((rc = ChooseKernel(op)))
         return fail(rc);
     *out = op;
@@ -876,7 +878,7 @@ extern "C" int nkb_op_element_matrices(nkb_op *op, double *K, int flags, void *s
     release();
     if (ce != cudaSuccess)
         return SetError(NKB_ERR_CUDA, "nkb_op_element_matrices: %s", cudaGetErrorString(ce));
-    return NKB_OK;
+    return CheckOpError(op);
 }
 
 extern "C" int nkb_op_sizes(const nkb_op *op, long *in_size, long *out_size)
@@ -899,6 +901,46 @@ extern "C" int nkb_op_sizes(const nkb_op *op, long *in_size, long *out_size)
         *in_size = in;
     if (out_size)
         *out_size = out;
+    return NKB_OK;
+}
+
+namespace nkb
+{
+int CheckOpError(nkb_op *op)
+{
+    if (!op || !op->d_err)
+        return NKB_OK;
+    int word = 0;
+    NKB_CUDA_TRY(cudaMemcpy(&word, op->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!word)
+        return NKB_OK;
+    NKB_CUDA_TRY(cudaMemset(op->d_err, 0, sizeof(int)));
+    return SetError(NKB_ERR_TIMEOUT,
+                    "operator kernel: a bounded wait for the geometry copy gave up (code %d); the "
+                    "outputs of the elements it guarded were not written",
+                    word);
+}
+} // namespace nkb
+
+extern "C" int nkb_op_check_error(nkb_op *op)
+{
+    ClearError();
+    if (!op)
+        return SetError(NKB_ERR_INVALID, "nkb_op_check_error: NULL op");
+    NKB_CUDA_TRY(cudaSetDevice(op->device));
+    return CheckOpError(op);
+}
+
+extern "C" int nkb_op_set_wait_limit(nkb_op *op, int polls)
+{
+    ClearError();
+    if (!op)
+        return SetError(NKB_ERR_INVALID, "nkb_op_set_wait_limit: NULL op");
+    if (polls >= (1 << 24))
+        return SetError(NKB_ERR_INVALID, "nkb_op_set_wait_limit: %d polls (at most 2^24 - 1)", polls);
+    NKB_CUDA_TRY(cudaSetDevice(op->device));
+    const int word = polls < 0 ? 0 : polls + 1;
+    NKB_CUDA_TRY(cudaMemcpy(op->d_err + 1, &word, sizeof(int), cudaMemcpyHostToDevice));
     return NKB_OK;
 }
 
@@ -951,7 +993,7 @@ extern "C" int nkb_op_apply(nkb_op *op, const double *in, double *out0, double *
             NKB_CUDA_TRY(cudaMemcpyAsync(outs[o], dout + o * nout, nout * sizeof(double),
                                          cudaMemcpyDeviceToHost, s));
         NKB_CUDA_TRY(cudaStreamSynchronize(s));
-        return NKB_OK;
+        return CheckOpError(op);
     }
     NKB_CUDA_TRY(cudaEventRecord(op->ev0, s));
     int rc = LaunchOp<double>(op, in, out0, out1, out2, nullptr, nullptr, s);
@@ -994,7 +1036,7 @@ extern "C" int nkb_op_apply3(nkb_op *op, const double *in0, const double *in1, c
         NKB_CUDA_TRY(cudaEventRecord(op->ev1, s));
         NKB_CUDA_TRY(cudaMemcpyAsync(out, dout, nout * sizeof(double), cudaMemcpyDeviceToHost, s));
         NKB_CUDA_TRY(cudaStreamSynchronize(s));
-        return NKB_OK;
+        return CheckOpError(op);
     }
     NKB_CUDA_TRY(cudaEventRecord(op->ev0, s));
     int rc = LaunchGeneric3<double>(op, in0, in1, in2, out, nullptr, nullptr, nullptr, nullptr, s);
@@ -1161,6 +1203,7 @@ extern "C" void nkb_op_destroy(nkb_op *op)
     cudaFree(op->geo32);
     cudaFree(op->scratch);
     cudaFree(op->d_err);
+    cudaFree(op->tc_tab);
     FreeKernelData(op);
     if (op->ev0)
         cudaEventDestroy(op->ev0);

@@ -62,6 +62,29 @@ int StaticScratch(int device, double **out)
 
 using namespace nkb;
 
+// the staged apply on the operator's device (current)
+static int ApplyStatic(nkb_op *op, const double *in, double *out0, double *out1, double *out2,
+                       long nin, long nout, int nouts, cudaStream_t s)
+{
+    double *scratch = nullptr;
+    int rc          = StaticScratch(op->device, &scratch);
+    if (rc)
+        return rc;
+    double *din  = scratch;
+    double *dout = scratch + nin;
+    NKB_CUDA_TRY(cudaMemcpyAsync(din, in, nin * sizeof(double), cudaMemcpyHostToDevice, s));
+    rc = LaunchOp<double>(op, din, dout, nouts > 1 ? dout + nout : nullptr,
+                          nouts > 2 ? dout + 2 * nout : nullptr, nullptr, nullptr, s);
+    if (rc)
+        return rc;
+    double *outs[3] = {out0, out1, out2};
+    for (int o = 0; o < nouts; ++o)
+        NKB_CUDA_TRY(cudaMemcpyAsync(outs[o], dout + o * nout, nout * sizeof(double),
+                                     cudaMemcpyDeviceToHost, s));
+    NKB_CUDA_TRY(cudaStreamSynchronize(s));
+    return CheckOpError(op);
+}
+
 extern "C" int nkb_op_apply_host_static(nkb_op *op, const double *in, double *out0, double *out1,
                                         double *out2, void *stream)
 {
@@ -74,30 +97,26 @@ extern "C" int nkb_op_apply_host_static(nkb_op *op, const double *in, double *ou
     if (nouts == 3 && (!out1 || !out2))
         return SetError(NKB_ERR_INVALID, "nkb_op_apply_host_static: PhysDeriv needs three outputs");
     long nin = 0, nout = 0;
-    nkb_op_sizes(op, &nin, &nout);
+    int rc = nkb_op_sizes(op, &nin, &nout);
+    if (rc)
+        return rc;
     const long need = nin + nouts * nout;
     if (need > NKB_STATIC_SCRATCH_DOUBLES)
         return SetError(NKB_ERR_INVALID,
                         "nkb_op_apply_host_static: operator needs %ld doubles of staging, the "
                         "static area holds %ld (32 MiB); use nkb_op_apply",
                         need, (long)NKB_STATIC_SCRATCH_DOUBLES);
+    // the operator's device is made current for the call; the caller's
+    // current device is restored on every return
+    int caller_dev = 0;
+    NKB_CUDA_TRY(cudaGetDevice(&caller_dev));
     NKB_CUDA_TRY(cudaSetDevice(op->device));
-    double *scratch = nullptr;
-    int rc          = StaticScratch(op->device, &scratch);
+    rc = ApplyStatic(op, in, out0, out1, out2, nin, nout, nouts, static_cast<cudaStream_t>(stream));
+    const cudaError_t ce = cudaSetDevice(caller_dev);
     if (rc)
         return rc;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    double *din    = scratch;
-    double *dout   = scratch + nin;
-    NKB_CUDA_TRY(cudaMemcpyAsync(din, in, nin * sizeof(double), cudaMemcpyHostToDevice, s));
-    rc = LaunchOp<double>(op, din, dout, nouts > 1 ? dout + nout : nullptr,
-                          nouts > 2 ? dout + 2 * nout : nullptr, nullptr, nullptr, s);
-    if (rc)
-        return rc;
-    double *outs[3] = {out0, out1, out2};
-    for (int o = 0; o < nouts; ++o)
-        NKB_CUDA_TRY(cudaMemcpyAsync(outs[o], dout + o * nout, nout * sizeof(double),
-                                     cudaMemcpyDeviceToHost, s));
-    NKB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (ce != cudaSuccess)
+        return SetError(NKB_ERR_CUDA, "nkb_op_apply_host_static: restoring device %d: %s",
+                        caller_dev, cudaGetErrorString(ce));
     return NKB_OK;
 }

@@ -69,11 +69,24 @@ __device__ __forceinline__ bool MbarTryWait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait for phase `parity` of bar. Returns true when the phase
-// completed; false (with *err set) when it did not within two bounds.
-__device__ __forceinline__ bool MbarWaitBounded(uint64_t *bar, uint32_t parity, int *err, int code)
+// first bound of a kernel's bounded waits: word [1] of its error buffer
+// holds bound + 1 when a test has set one (nkb_op_set_wait_limit; 1: give up
+// at once), 0 for the default kMaxPolls
+__device__ __forceinline__ unsigned WaitPolls(const int *err)
 {
-    for (unsigned n = 0; n < kMaxPolls; ++n)
+    const unsigned v = err ? static_cast<unsigned>(__ldg(err + 1)) : 0u;
+    return v ? v - 1u : kMaxPolls;
+}
+
+// Bounded wait for phase `parity` of bar. Returns true when the phase
+// completed within `polls` polls; otherwise *err is set and the wait goes on
+// for at most kMaxPolls more polls (so a copy still in flight lands before
+// the CTA can exit) and returns false. `polls` is kMaxPolls unless a test
+// lowers it (WaitPolls) to make the first bound run out.
+__device__ __forceinline__ bool MbarWaitBounded(uint64_t *bar, uint32_t parity, int *err, int code,
+                                                unsigned polls = kMaxPolls)
+{
+    for (unsigned n = 0; n < polls; ++n)
         if (MbarTryWait(bar, parity))
             return true;
     if (err)

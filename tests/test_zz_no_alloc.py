@@ -50,6 +50,26 @@ def test_static_apply_matches_allocating_apply(shape, optype, nm):
             assert rel_l2(g, r) < TOL64, (call, rel_l2(g, r))
 
 
+def test_static_apply_allocates_no_device_memory():
+    """On a freshly created operator whose staging would take about 32 MB, the
+    static apply leaves the device's free memory where it was (an allocating
+    apply would take it). A first call on another operator loads the library's
+    device code, so lazy module loading cannot count against the call."""
+    import torch
+    small = nb.Operator("helmholtz", nb.BoxMesh("hex", 2, 4, 5, amp=0.05))
+    _apply_static(small, np.ones(small.in_size))
+    m = nb.BoxMesh("hex", 18, 7, 8, amp=0.05)  # in + out = 4,000,752 doubles
+    op = nb.Operator("helmholtz", m)
+    x = np.random.default_rng(9).uniform(-1, 1, op.in_size)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    got = _apply_static(op, x)[0]
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free0 - free1 < (4 << 20), (free0, free1)
+    assert rel_l2(got, _apply_existing(op, x)[0]) < TOL64
+
+
 def test_static_apply_rejects_operators_beyond_the_limit():
     # 19^3 P=6 Hex Helmholtz: 2 x 6859 x 343 doubles > 4 Mi doubles
     m = nb.BoxMesh("hex", 19, 7, 8, amp=0.05)
