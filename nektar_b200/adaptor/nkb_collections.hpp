@@ -15,7 +15,8 @@
 // library's message, as NEKERROR / ASSERTL0 do in the reference
 // (LibUtilities/BasicUtils/ErrorUtil.hpp:57,210-235). Arrays are plain host
 // vectors here; in a Nektar++ build the same classes take Array<OneD, ...>
-// (see INTEGRATION.md).
+// (LibUtilities/BasicUtils/SharedArray.hpp) and hand their data pointers to
+// the C ABI the same way.
 #pragma once
 
 #include "../../include/nektar_b200.h"

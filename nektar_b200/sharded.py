@@ -17,9 +17,11 @@ device CG's.
 
 The element operator is passed in (apply(x_loc) -> y_loc over the rank's
 elements): the device Helmholtz operators on a GPU (`device_apply`), any
-restatement elsewhere. The collectives go through torch.distributed (NCCL
-between GPUs, gloo on the host); every rank takes the same collective steps
-in the same order, in the last iteration too.
+restatement elsewhere. The collectives go through torch.distributed: with a
+gloo group on host tensors; with an NCCL group the exchange buffers are
+copied to the rank's current CUDA device for the all-reduce and back (the
+vectors of this form stay on the host). Every rank takes the same collective
+steps in the same order, in the last iteration too.
 """
 import numpy as np
 
@@ -74,6 +76,10 @@ class ShardedSystem:
         if self.pg is None:
             return arr
         t = self.torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float64))
+        if self.pg.get_backend() == "nccl":  # NCCL reduces device tensors only
+            d = t.to("cuda:%d" % self.torch.cuda.current_device())
+            self.pg.all_reduce(d)
+            return d.cpu().numpy()
         self.pg.all_reduce(t)
         return t.numpy()
 

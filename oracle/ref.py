@@ -44,6 +44,33 @@ def best_isa():
     return "scalar"
 
 
+def physical_cpus():
+    """One logical CPU per physical core among those this process may run
+    on (sysfs topology; every allowed CPU when the topology is unreadable)."""
+    allowed = sorted(os.sched_getaffinity(0))
+    seen, out = set(), []
+    for c in allowed:
+        base = "/sys/devices/system/cpu/cpu%d/topology/" % c
+        try:
+            with open(base + "core_id") as f:
+                core = f.read().strip()
+            with open(base + "physical_package_id") as f:
+                pkg = f.read().strip()
+        except OSError:
+            return allowed
+        if (pkg, core) not in seen:
+            seen.add((pkg, core))
+            out.append(c)
+    return out
+
+
+def set_cpus(cpus):
+    """Pin the reference driver's worker thread t to cpus[t % len(cpus)]
+    (empty: no pinning)."""
+    arr = (ctypes.c_int * max(len(cpus), 1))(*cpus)
+    lib().nkref_set_cpus(len(cpus), arr)
+
+
 def available():
     return os.path.exists(os.path.join(REF_DIR, "libnkref_%s.so" % best_isa()))
 
@@ -86,6 +113,8 @@ def lib(isa=None):
     L.nkref_basis.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp]
     L.nkref_weight_factor.restype = ctypes.c_double
     L.nkref_weight_factor.argtypes = [ctypes.c_int]
+    L.nkref_set_cpus.restype = None
+    L.nkref_set_cpus.argtypes = [ctypes.c_int, ip]
     L.nkref_pcg_solve.restype = ctypes.c_int
     L.nkref_pcg_solve.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_long, ip, dp, ip,
                                   ctypes.POINTER(ctypes.c_long), vp, vp, dp, dp, dp,

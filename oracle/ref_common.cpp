@@ -25,10 +25,18 @@
 #include <thread>
 #include <vector>
 
+#include <pthread.h>
+#include <sched.h>
+
 #include <LibUtilities/Polylib/Polylib.h>
+
+extern "C" void nkref_pin_thread(int t);
 
 namespace
 {
+// host CPUs the worker threads are pinned to (worker t -> cpus[t % n]);
+// empty: no pinning
+std::vector<int> g_cpus;
 
 // Points types, numbered as LibUtilities::PointsType (PointsType.h:43-)
 enum
@@ -55,7 +63,10 @@ template <class F> void ParallelFor(long n, int nthreads, F &&f)
         {
             break;
         }
-        ts.emplace_back([&f, a, b, t] { f(a, b, t); });
+        ts.emplace_back([&f, a, b, t] {
+            nkref_pin_thread(t);
+            f(a, b, t);
+        });
     }
     for (auto &t : ts)
     {
@@ -67,6 +78,21 @@ template <class F> void ParallelFor(long n, int nthreads, F &&f)
 
 extern "C"
 {
+
+    // ---- worker-thread pinning (timed CPU baseline) ------------------------
+    void nkref_set_cpus(int n, const int *cpus)
+    {
+        g_cpus.assign(cpus, cpus + std::max(0, n));
+    }
+    void nkref_pin_thread(int t)
+    {
+        if (g_cpus.empty())
+            return;
+        cpu_set_t set;
+        CPU_ZERO(&set);
+        CPU_SET(g_cpus[size_t(t) % g_cpus.size()], &set);
+        pthread_setaffinity_np(pthread_self(), sizeof(set), &set);
+    }
 
     // ---- Polylib (reference code) -------------------------------------------
     void nkref_zwglj(double *z, double *w, int np, double alpha, double beta)

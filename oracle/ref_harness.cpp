@@ -67,6 +67,9 @@ template <class Dim, class T> struct Array
 };
 } // namespace Nektar
 
+// worker-thread pinning of the timed CPU baseline (ref_common.cpp)
+extern "C" void nkref_pin_thread(int t);
+
 #include <LibUtilities/BasicUtils/NekInline.hpp>
 #include <LibUtilities/BasicUtils/ShapeType.hpp>
 #include <LibUtilities/SimdLib/tinysimd.hpp>
@@ -801,9 +804,14 @@ extern "C"
         }
         std::vector<std::thread> ts;
         ts.reserve(o->chunks.size());
+        int ci = 0;
         for (auto &c : o->chunks)
         {
-            ts.emplace_back([o, &c, in, out0, out1, out2] { ApplyChunk(*o, c, in, out0, out1, out2); });
+            const int t = ci++;
+            ts.emplace_back([o, &c, in, out0, out1, out2, t] {
+                nkref_pin_thread(t);
+                ApplyChunk(*o, c, in, out0, out1, out2);
+            });
         }
         for (auto &t : ts)
         {

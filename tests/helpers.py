@@ -6,6 +6,14 @@ import sys
 import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+# the reference source tree (read-only; only CPU tests that read its session
+# files use it), as oracle/Makefile's REFDIR
+REFDIR = os.environ.get("REFDIR", "/root/reference")
+
+
+def ref_path(rel):
+    """A file of the reference tree by its path within the project."""
+    return os.path.join(REFDIR, rel)
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 

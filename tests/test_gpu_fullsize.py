@@ -1,0 +1,97 @@
+"""The full-size FP64 solves on the device against the reference CPU path's
+recorded runs of the same workloads (tests/golden/make_c2_reference.py: the
+reference's MatrixFreeOps kernels driven by the restated NekLinSysIterCG,
+PCG + Jacobi, lambda = 1, manufactured solution sin(pi x) sin(pi y) sin(pi z)
+on the curved box):
+
+* 32^3 hexes, P = 6, Q = 8 (the benchmark workload) and 24^3 hexes, P = 8,
+  Q = 10;
+* at a relative residual of 1e-10: the iteration count (within one), the
+  RMS error against the exact solution at the quadrature points (within
+  1e-3 relative) and the local solution at 10000 seeded positions;
+* at 1e-14 (the converged FP64 solution): the same digest.
+
+The digest bounds: two FP64 implementations that stop at the same residual
+criterion differ by far less than either differs from the converged
+solution (1.2e-8 relative at 1e-10 on 32^3, P = 6): 1e-9 at 1e-10 and 1e-11
+at 1e-14."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import nektar_b200 as nb
+from tests.helpers import ROOT
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+CASES = {"c2": (32, 7), "c3": (24, 9)}
+
+
+def _record(tag):
+    path = os.path.join(GOLDEN, "%s_reference_cg.json" % tag)
+    dpath = os.path.join(GOLDEN, "%s_reference_solution.npz" % tag)
+    if not (os.path.exists(path) and os.path.exists(dpath)):
+        pytest.skip("no recorded reference run for %s" % tag)
+    with open(path) as f:
+        rec = json.load(f)
+    with np.load(dpath) as z:
+        dig = {k: z[k] for k in z.files}
+    return rec, dig
+
+
+def _solve(n, nm, tols):
+    import torch
+    mesh = nb.BoxMesh("hex", n, nm, nm + 1, amp=0.05, coords=True)
+    gmap, nglob, ndir = mesh.assembly()
+    op = nb.Operator("helmholtz", mesh)
+    op.set_factors(1.0)
+    S = nb.GlobalLinSys([op], gmap, nglob, ndir)
+    x, y, z = mesh.xyz
+    u = np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z)
+    ipo = nb.Operator("iproduct", mesh)
+    b = ipo((3 * np.pi ** 2 + 1.0) * u)
+    ipo.close()
+    nloc = mesh.nelmt * mesh.nc
+    s = torch.cuda.Stream()
+    bd = torch.tensor(b, device="cuda")
+    out = {}
+    for tol in tols:
+        xd = torch.zeros(nloc, dtype=torch.float64, device="cuda")
+        rep = S.solve_device(bd.data_ptr(), xd.data_ptr(), tol=tol, maxit=20000, check_interval=32,
+                             stream=s.cuda_stream)
+        torch.cuda.synchronize()
+        out[tol] = (xd.cpu().numpy(), rep)
+    bwd = nb.Operator("bwdtrans", mesh)
+    rms = float(np.sqrt(np.mean((bwd(out[tols[0]][0]) - u) ** 2)))
+    for o in (bwd, op):
+        o.close()
+    S.close()
+    return out, rms
+
+
+@pytest.mark.parametrize("tag", sorted(CASES))
+def test_fullsize_solve_matches_reference_record(tag):
+    rec, dig = _record(tag)
+    n, nm = CASES[tag]
+    out, rms = _solve(n, nm, (1e-10, 1e-14))
+    x, rep = out[1e-10]
+    assert rep.converged and abs(rep.iterations - rec["iterations"]) <= 1, (rep.iterations,
+                                                                            rec["iterations"])
+    assert abs(rms - rec["rms_error_vs_exact"]) < 1e-3 * rec["rms_error_vs_exact"], rms
+    pos = dig["positions"]
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    assert rel(x[pos], dig["x"]) < 1e-9, rel(x[pos], dig["x"])
+    assert abs(np.linalg.norm(x) - float(dig["norm"])) < 1e-9 * float(dig["norm"])
+    xt, rept = out[1e-14]
+    assert abs(rept.iterations - rec["tight"]["iterations"]) <= 0.01 * rec["tight"]["iterations"]
+    assert rel(xt[pos], dig["x_tight"]) < 1e-11, rel(xt[pos], dig["x_tight"])
+    # the spread of the criterion itself, the same on both implementations
+    spread = float(np.linalg.norm(x - xt) / np.linalg.norm(xt))
+    assert abs(spread - rec["tight"]["rel_l2_of_tol_1e-10_solution"]) < \
+        0.05 * rec["tight"]["rel_l2_of_tol_1e-10_solution"], spread

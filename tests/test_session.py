@@ -15,12 +15,13 @@ from nektar_b200.expr import Expression, ExpressionError, evaluate_parameters
 from nektar_b200.meshgraph import SessionMesh
 from nektar_b200.session import SessionError, read_session, write_hex_box_session
 from oracle import oracle as O
+from tests.helpers import ref_path
 from tests.session_oracle import oracle_helm_solve
 
 U = "sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)"
 F = "-(Lambda + 3*PI*PI/4)*sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)"
 HEX_L2, HEX_LINF = 1.11818e-07, 5.66374e-07  # Helmholtz3D_CG_Hex.tst
-REF_HEX = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Hex_P6.xml"
+REF_HEX = ref_path("library/Demos/MultiRegions/Tests/Helmholtz3D_Hex_P6.xml")
 
 
 def test_expression_grammar():
@@ -139,12 +140,12 @@ from nektar_b200.session import write_box_session  # noqa: E402
 
 UQ = "x*x + 2*y*z - z"  # in every P >= 2 space: the discrete solution is exact
 FQ = "2 - Lambda*(x*x + 2*y*z - z)"  # laplacian(u) - lambda u
-REF_PRISM = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Prism.xml"
-REF_TET = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Tet.xml"
-REF_PRISM_VARP = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Prism_VarP.xml"
-REF_TET_VARP = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Tet_VarP.xml"
-REF_ALLBCS = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Hex_AllBCs_P6.xml"
-REF_PRISM_DEF = "/root/reference/library/Demos/MultiRegions/Tests/Helmholtz3D_Prism_Deformed.xml"
+REF_PRISM = ref_path("library/Demos/MultiRegions/Tests/Helmholtz3D_Prism.xml")
+REF_TET = ref_path("library/Demos/MultiRegions/Tests/Helmholtz3D_Tet.xml")
+REF_PRISM_VARP = ref_path("library/Demos/MultiRegions/Tests/Helmholtz3D_Prism_VarP.xml")
+REF_TET_VARP = ref_path("library/Demos/MultiRegions/Tests/Helmholtz3D_Tet_VarP.xml")
+REF_ALLBCS = ref_path("library/Demos/MultiRegions/Tests/Helmholtz3D_Hex_AllBCs_P6.xml")
+REF_PRISM_DEF = ref_path("library/Demos/MultiRegions/Tests/Helmholtz3D_Prism_Deformed.xml")
 
 
 @pytest.mark.parametrize("shape", ["prism", "tet"])
