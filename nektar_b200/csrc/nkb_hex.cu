@@ -52,6 +52,22 @@ int SmCount(int device)
     return counts[device];
 }
 
+int ResidentCtas(const void *fn, int threads, size_t smem)
+{
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess)
+        return 1;
+    const int warps    = (threads + 31) / 32;
+    const int regs     = ((fa.numRegs + 7) / 8) * 8;                // allocation granularity
+    const long by_regs = 65536L / (long(warps) * 32 * (regs > 0 ? regs : 1));
+    const long by_smem = long(227 * 1024) / long(smem + fa.sharedSizeBytes + 1024);
+    const long by_thr  = 2048L / (long(warps) * 32);
+    long n             = by_regs < by_smem ? by_regs : by_smem;
+    n                  = n < by_thr ? n : by_thr;
+    n                  = n < 32 ? n : 32;
+    return n < 1 ? 1 : int(n);
+}
+
 static bool ForceGeneric()
 {
     const char *v = std::getenv("NKB_KERNEL");
@@ -440,7 +456,8 @@ const char *KernelName(const nkb_op *op, bool gather)
         case 2: return "k_hex_helm (streamed geometry, 2 elements per CTA)";
         case 3: return "k_hex_helm_mma (FP64 tensor cores)";
         case 4: return "k_hex_helm_mma2 (FP64 tensor cores, two warps per element)";
-        default: return "k_hex_helm_tc (tcgen05 TF32 high/low tensor cores, FP32 accumulate)";
+        case 5: return "k_hex_helm_tc (tcgen05 TF32 high/low tensor cores, FP32 accumulate)";
+        default: return "k_hex_helm (persistent, double-buffered TMA geometry)";
     }
 }
 

@@ -15,6 +15,13 @@
 namespace nkb
 {
 
+int SmCount(int device); // multiprocessors of a device (nkb_hex.cu)
+// CTAs of a kernel that stay resident on one SM at `threads` threads and
+// `smem` bytes of dynamic shared memory, from its register and shared-memory
+// use (nkb_hex.cu)
+int ResidentCtas(const void *fn, int threads, size_t smem);
+
+
 template <typename T> struct HexArgs
 {
     const T *in;
@@ -42,7 +49,9 @@ enum
 enum
 {
     kGeoTma    = 0, // the element's whole geometry by one bulk TMA copy into shared memory
-    kGeoStream = 1  // coalesced loads into registers, one k-plane ahead
+    kGeoStream = 1, // coalesced loads into registers, one k-plane ahead
+    kGeoTma2   = 2  // persistent CTAs: the next element group's geometry copied into a
+                    // second buffer while the current group computes
 };
 
 __host__ __device__ constexpr int RoundUp(int a, int b)
@@ -70,8 +79,9 @@ template <int NQ> __host__ __device__ constexpr int HexRegion()
 
 template <typename T, int NM, int NQ, int GEO, int EPB> size_t HexSmem(long gstride)
 {
+    const size_t nbuf = GEO == kGeoTma ? 1 : (GEO == kGeoTma2 ? 2 : 0);
     return size_t(HexTabBytes<T, NM, NQ>()) +
-           size_t(EPB) * ((GEO == kGeoTma ? size_t(gstride) : 0) + 3 * HexRegion<NQ>()) * sizeof(T);
+           size_t(EPB) * (nbuf * size_t(gstride) + 3 * HexRegion<NQ>()) * sizeof(T);
 }
 
 // 1-D tables passed by value as a kernel parameter: entries read with
@@ -142,56 +152,46 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
     static_assert(RS % 2 == 0 && NMP % 2 == 0, "vector loads need even strides");
     static_assert(HexTabBytes<T, NM, NQ>() % 16 == 0, "work regions must start 16-byte aligned");
     static_assert(NM * NM * NMP <= RS && NM * NQ * NQ <= RS, "regions too small");
+    constexpr bool TMA = GEO == kGeoTma || GEO == kGeoTma2;
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
-    T *sB0        = reinterpret_cast<T *>(smem + 16);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem); // one per geometry buffer
+    T *sB0         = reinterpret_cast<T *>(smem + 16);
     T *sB1        = sB0 + NM * NQ;
     T *sB2        = sB1 + NM * NQ;
     T *sD         = sB2 + NM * NQ; // sD[i*NQP + m] = D(i, m) = l_m'(z_i)
     const long GS = a.gstride;
-    T *geo        = reinterpret_cast<T *>(smem + HexTabBytes<T, NM, NQ>());
-    T *us         = geo + (GEO == kGeoTma ? EPB * GS : 0); // GS is a multiple of 4
+    T *geob       = reinterpret_cast<T *>(smem + HexTabBytes<T, NM, NQ>());
+    T *us         = geob + (GEO == kGeoTma2 ? 2 : (GEO == kGeoTma ? 1 : 0)) * EPB * GS; // GS % 4 == 0
     T *v0s        = us + EPB * RS;
     T *v1s        = v0s + EPB * RS;
 
-    const int tid = threadIdx.x;
-    const long e0 = long(blockIdx.x) * EPB;
-    const int ne  = int(min(long(EPB), long(a.nelmt) - e0));
-    if (ne <= 0 || (a.skip && *a.skip))
+    const int tid       = threadIdx.x;
+    const long ngroups  = (long(a.nelmt) + EPB - 1) / EPB;
+    // the persistent variant walks groups blockIdx.x, + gridDim.x, ...; the
+    // others take one group each
+    const long gstep = GEO == kGeoTma2 ? long(gridDim.x) : ngroups;
+    if (long(blockIdx.x) >= ngroups || (a.skip && *a.skip))
         return;
-
-    if (GEO == kGeoTma && tid == 0)
+    auto group_bytes = [&](long grp) {
+        const long ng = min(long(EPB), long(a.nelmt) - grp * EPB);
+        return uint32_t(ng * GS * long(sizeof(T)));
+    };
+    if (TMA && tid == 0)
     {
-        MbarInit(bar, 1);
-        const uint32_t bytes = uint32_t(ne * GS * long(sizeof(T)));
-        MbarArriveExpectTx(bar, bytes);
-        BulkG2S(geo, a.geo + e0 * GS, bytes, bar);
-    }
-    if (GEO == kGeoStream && tid == 0)
-    {
-        // the CTA's whole geometry requested from DRAM at once (into L2); the
-        // per-plane loads below then hit L2
-        BulkPrefetchL2(a.geo + e0 * GS, uint32_t(ne * GS * long(sizeof(T))));
+        MbarInit(&bars[0], 1);
+        if (GEO == kGeoTma2)
+            MbarInit(&bars[1], 1);
+        const uint32_t bytes = group_bytes(blockIdx.x);
+        MbarArriveExpectTx(&bars[0], bytes);
+        BulkG2S(geob, a.geo + long(blockIdx.x) * EPB * GS, bytes, &bars[0]);
     }
 
     const int le   = tid / NQ2;
     const int ij   = tid - le * NQ2;
     const int i    = ij % NQ, j = ij / NQ;
-    bool act       = le < ne;
     const int lec  = le < EPB ? le : 0;
     const int eoff = lec * RS;
     T *xs = v0s + eoff, *As = v1s + eoff, *u_ = us + eoff, *v0 = v0s + eoff, *v1 = v1s + eoff;
-
-    // streamed geometry: plane 0 requested before any arithmetic
-    const T *Gg = a.geo + (e0 + lec) * GS;
-    T gc[NG];
-    if (GEO == kGeoStream && act)
-    {
-        const int q0 = j * NQ + i;
-#pragma unroll
-        for (int cc = 0; cc < NG; ++cc)
-            gc[cc] = __ldg(Gg + cc * NQ3 + q0);
-    }
 
     for (int t = tid; t < NM * NQ; t += blockDim.x)
     {
@@ -203,6 +203,40 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
     {
         const int r = t / NQ, cc = t - r * NQ;
         sD[r * NQP + cc] = c.D[r * NQ + cc];
+    }
+    int it = 0; // groups done by this CTA
+    for (long grp = blockIdx.x; grp < ngroups; grp += gstep, ++it)
+    {
+    const long e0  = grp * EPB;
+    const int ne   = int(min(long(EPB), long(a.nelmt) - e0));
+    bool act       = le < ne;
+    const int cur  = GEO == kGeoTma2 ? (it & 1) : 0;
+    T *geo         = geob + cur * EPB * GS;
+    if (GEO == kGeoTma2 && tid == 0 && grp + gstep < ngroups)
+    {
+        // the other buffer was last read by the previous group, which every
+        // thread has finished (the barrier ending that group)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const uint32_t bytes = group_bytes(grp + gstep);
+        MbarArriveExpectTx(&bars[cur ^ 1], bytes);
+        BulkG2S(geob + (cur ^ 1) * EPB * GS, a.geo + (grp + gstep) * EPB * GS, bytes,
+                &bars[cur ^ 1]);
+    }
+    if (GEO == kGeoStream && tid == 0)
+    {
+        // the CTA's whole geometry requested from DRAM at once (into L2); the
+        // per-plane loads below then hit L2
+        BulkPrefetchL2(a.geo + e0 * GS, uint32_t(ne * GS * long(sizeof(T))));
+    }
+    // streamed geometry: plane 0 requested before any arithmetic
+    const T *Gg = a.geo + (e0 + lec) * GS;
+    T gc[NG];
+    if (GEO == kGeoStream && act)
+    {
+        const int q0 = j * NQ + i;
+#pragma unroll
+        for (int cc = 0; cc < NG; ++cc)
+            gc[cc] = __ldg(Gg + cc * NQ3 + q0);
     }
     // coefficients into the v0 region, rows (r, q) padded to NMP (NM^2 NMP <= NQ3)
     for (int t = tid; t < ne * NC; t += blockDim.x)
@@ -282,8 +316,9 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
     }
     __syncthreads();
 
-    // TMA geometry must have landed: bounded wait by every thread
-    if (GEO == kGeoTma && !MbarWaitBounded(bar, 0, a.err, 1, WaitPolls(a.err)))
+    // TMA geometry must have landed: bounded wait by every thread (use
+    // it >> 1 of buffer cur)
+    if (TMA && !MbarWaitBounded(&bars[cur], uint32_t((it >> 1) & 1), a.err, 1, WaitPolls(a.err)))
         act = false;
 
     // gradient (i, j from shared memory, k from registers) and metric:
@@ -320,7 +355,7 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
             for (int m = 0; m < NQ; ++m)
                 g2 = fma(c.D[k * NQ + m], ur[m], g2);
             T W, G00, G11, G22, G01, G02, G12, A0 = 0, A1 = 0, A2 = 0;
-            if (GEO == kGeoTma)
+            if (TMA)
             {
                 W   = G[q];
                 G00 = G[NQ3 + q];
@@ -443,6 +478,8 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
             o[(r * NM + j) * NM + i] = DotRow<T, NQ>(v0 + (r * NM + j) * NQ, b0c, T(0));
         }
     }
+    __syncthreads(); // the work regions and this group's geometry buffer are free again
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -468,8 +505,21 @@ namespace nkb
 //    precisions; nkb_hex_mma.cuh); 4: the same with two warps per element
 //    (nkb_hex_mma2.cuh); 5: fifth-generation tensor cores (tcgen05, TF32
 //    high/low operands, FP32 accumulation; FP32 operators, nm 2..9;
-//    nkb_hex_tc.cuh)
-constexpr int kNumHexVariants = 6;
+//    nkb_hex_tc.cuh); 6: persistent CTAs with the geometry double-buffered
+//    (the next element group's bulk copy in flight while the current one
+//    computes)
+constexpr int kNumHexVariants = 7;
+
+// elements per CTA of the double-buffered variant: two geometry buffers and
+// three work regions per element in at most 72 KB (three CTAs per SM)
+template <typename T, int NQ> constexpr int Tma2Epb()
+{
+    constexpr int per = (2 * (7 * NQ * NQ * NQ + 4) + 3 * (NQ * NQ * NQ + 1)) * int(sizeof(T));
+    constexpr int e   = (72 * 1024) / per;
+    constexpr int lim = 512 / (NQ * NQ);
+    constexpr int v   = e < lim ? e : lim;
+    return v < 1 ? 1 : (v > 8 ? 8 : v);
+}
 
 template <typename T, int NQ> constexpr int TmaEpb()
 {
@@ -526,11 +576,21 @@ static int HexVariantLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, 
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
         return NKB_OK;
     }
-    const long nb = (long(op->nelmt) + EPB - 1) / EPB;
+    long nb = (long(op->nelmt) + EPB - 1) / EPB;
     if (nb == 0)
         return NKB_OK;
     const HexConst<T, NM, NQ> c = MakeHexConst<T, NM, NQ>(op);
     const unsigned th           = HexThreads<NQ, EPB>();
+    if (GEO == kGeoTma2)
+    {
+        // persistent grid: every CTA that stays resident walks its groups
+        const void *fn = mode == kModeGather
+                             ? (const void *)k_hex_helm<T, NM, NQ, GEO, EPB, kModeGather>
+                             : (mode == kModeAdv ? (const void *)k_hex_helm<T, NM, NQ, GEO, EPB, kModeAdv>
+                                                 : (const void *)k_hex_helm<T, NM, NQ, GEO, EPB, kModeLocal>);
+        const long resident = long(ResidentCtas(fn, int(th), bytes)) * SmCount(op->device);
+        nb                  = nb < resident ? nb : resident;
+    }
     if (mode == kModeGather)
         k_hex_helm<T, NM, NQ, GEO, EPB, kModeGather><<<unsigned(nb), th, bytes, s>>>(a, c);
     else if (mode == kModeAdv)
@@ -571,6 +631,11 @@ static int HexTcLaunch(const nkb_op *op, const HexArgs<float> &a, bool gather, c
     const long ntile = (long(op->nelmt) + Dm::EPT - 1) / Dm::EPT;
     if (ntile == 0)
         return NKB_OK;
+    // persistent grid: the CTAs per SM the launch bounds were built for
+    // (shared and tensor memory allow that many; ncu confirms the register
+    // limit), each walking its tiles
+    const long resident = long(Dm::MIN_CTAS) * SmCount(op->device);
+    const long nb       = ntile < resident ? ntile : resident;
     TcTables tt;
     tt.tab   = op->tc_tab;
     tt.bytes = op->tc_bytes;
@@ -580,9 +645,9 @@ static int HexTcLaunch(const nkb_op *op, const HexArgs<float> &a, bool gather, c
         tt.tbt[d] = op->tc_tbt[d];
     }
     if (gather)
-        k_hex_helm_tc<NM, NQ, kModeGather><<<unsigned(ntile), 128, bytes, s>>>(a, tt);
+        k_hex_helm_tc<NM, NQ, kModeGather><<<unsigned(nb), 128, bytes, s>>>(a, tt);
     else
-        k_hex_helm_tc<NM, NQ, kModeLocal><<<unsigned(ntile), 128, bytes, s>>>(a, tt);
+        k_hex_helm_tc<NM, NQ, kModeLocal><<<unsigned(nb), 128, bytes, s>>>(a, tt);
     NKB_CUDA_TRY(cudaGetLastError());
     return NKB_OK;
 }
@@ -607,6 +672,11 @@ static int HexLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStr
     {
         case 0:
             return HexVariantLaunch<T, NM, kGeoTma, TmaEpb<T, NQ>()>(op, a, gather, s, set_attr);
+        case 6:
+            if constexpr (NQ <= 9)
+                return HexVariantLaunch<T, NM, kGeoTma2, Tma2Epb<T, NQ>()>(op, a, gather, s, set_attr);
+            else
+                return SetError(NKB_ERR_UNSUPPORTED, "double-buffered Hex variant: nq <= 9");
         case 1:
             return HexVariantLaunch<T, NM, kGeoStream, 1>(op, a, gather, s, set_attr);
         default:

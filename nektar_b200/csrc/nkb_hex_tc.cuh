@@ -52,6 +52,11 @@ template <int NM, int NQ> struct TcDims
     static constexpr int TCOLS  = 8 * NQP <= 64 ? 64 : (8 * NQP <= 128 ? 128 : 256);
     static constexpr int TBROWS = 4 * NQP, TBTROWS = 4 * NMN;
     static constexpr int TB_BYTES = TBROWS * KM * 4, TBT_BYTES = TBTROWS * KQ * 4;
+    // CTAs per SM that shared memory (with the tables of one direction: Hex
+    // directions share their tables) and tensor memory (512 columns) allow;
+    // the launch bounds ask for that many
+    static constexpr int SMEM_CTAS = (227 * 1024) / (ABYTES + TB_BYTES + TBT_BYTES + 16);
+    static constexpr int MIN_CTAS  = SMEM_CTAS < 512 / TCOLS ? SMEM_CTAS : 512 / TCOLS;
     static_assert(RPE <= 128, "tensor-core Hex kernel: element rows exceed one 128-row tile");
     static_assert(NQP == 8 || NQP == 16, "tensor-core Hex kernel: nq up to 16");
 };
@@ -207,7 +212,8 @@ __device__ __forceinline__ void IssuePair(uint32_t a_hi, uint32_t cube, uint32_t
 } // namespace tcd
 
 template <int NM, int NQ, int MODE>
-__global__ void __launch_bounds__(128, 1) k_hex_helm_tc(HexArgs<float> a, TcTables tt)
+__global__ void __launch_bounds__(128, TcDims<NM, NQ>::MIN_CTAS)
+    k_hex_helm_tc(HexArgs<float> a, TcTables tt)
 {
     using Dm = TcDims<NM, NQ>;
     constexpr int NC = NM * NM * NM, NQ2 = NQ * NQ, NT = NQ2 * NQ;
@@ -221,14 +227,17 @@ __global__ void __launch_bounds__(128, 1) k_hex_helm_tc(HexArgs<float> a, TcTabl
     uint64_t *bar       = reinterpret_cast<uint64_t *>(abuf + Dm::ABYTES);
     uint32_t *slot      = reinterpret_cast<uint32_t *>(bar + 1);
 
-    // the element rows of this tile and their geometry, prefetched into L2
-    // while the first contractions run
-    if (t == 0)
-    {
-        const long e0 = long(blockIdx.x) * EPT;
-        const long ne = (a.nelmt - e0) < EPT ? (a.nelmt - e0) : EPT;
-        BulkPrefetchL2(a.geo + e0 * a.gstride, uint32_t(ne * a.gstride * sizeof(float)));
-    }
+    const long ntiles = (long(a.nelmt) + EPT - 1) / EPT;
+    // geometry of a tile into L2 (read at the metric step)
+    auto prefetch_geo = [&](long tile) {
+        if (t == 0 && tile < ntiles)
+        {
+            const long e0 = tile * EPT;
+            const long ne = (a.nelmt - e0) < EPT ? (a.nelmt - e0) : EPT;
+            BulkPrefetchL2(a.geo + e0 * a.gstride, uint32_t(ne * a.gstride * sizeof(float)));
+        }
+    };
+    prefetch_geo(blockIdx.x);
     for (int o = t * 16; o < tt.bytes; o += 128 * 16)
         *reinterpret_cast<float4 *>(sm + o) =
             __ldg(reinterpret_cast<const float4 *>(reinterpret_cast<const char *>(tt.tab) + o));
@@ -247,12 +256,10 @@ __global__ void __launch_bounds__(128, 1) k_hex_helm_tc(HexArgs<float> a, TcTabl
     const uint32_t sa   = tc::SmemU32(abuf);
     const uint32_t st   = tc::SmemU32(sm);
 
-    const int e     = t / RPE, rr = t % RPE;
-    const long elem = long(blockIdx.x) * EPT + e;
-    const bool ev   = e < EPT && elem < a.nelmt;
-    const int rowb  = e * RPE; // first row of this thread's element
-    bool ok         = true;
-    uint32_t phase  = 0;
+    const int e    = t / RPE, rr = t % RPE;
+    const int rowb = e * RPE; // first row of this thread's element in a tile
+    bool ok        = true;
+    uint32_t phase = 0;
     const unsigned polls = WaitPolls(a.err);
     auto cube_hi = [&](int c) { return abuf + 2 * c * CUBE; };
     auto cube_lo = [&](int c) { return abuf + (2 * c + 1) * CUBE; };
@@ -268,28 +275,40 @@ __global__ void __launch_bounds__(128, 1) k_hex_helm_tc(HexArgs<float> a, TcTabl
     };
     const uint32_t ccube = uint32_t(CUBE);
     auto ahi = [&](int c) { return sa + uint32_t(2 * c * CUBE); };
+    // this thread's coefficient row (r, q) of a tile's element: its nm values
+    const int xr = rr / MP, xq = rr % MP;
+    auto load_x = [&](long tile, float *x) {
+        const long el = tile * EPT + e;
+        if (!(tile < ntiles && e < EPT && el < a.nelmt && xr < NM && xq < NM))
+            return;
+        const long l0 = el * NC + (xr * NM + xq) * NM;
+#pragma unroll
+        for (int p = 0; p < NM; ++p)
+        {
+            if (MODE == kModeGather)
+            {
+                const int gi = a.gmap[l0 + p];
+                x[p]         = a.gsign ? float(a.gsign[l0 + p]) * a.in[gi] : a.in[gi];
+            }
+            else
+                x[p] = a.in[l0 + p];
+        }
+    };
+    float xcur[NM];
+#pragma unroll
+    for (int p = 0; p < NM; ++p)
+        xcur[p] = 0.f;
+    load_x(blockIdx.x, xcur);
+
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    {
+    const long elem = tile * EPT + e;
+    const bool ev   = e < EPT && elem < a.nelmt;
+    prefetch_geo(tile + gridDim.x);
 
     // ---- stage 1: contract p (rows (r, q), K-major) ----------------------
-    {
-        const int r = rr / MP, q = rr % MP;
-        if (ev && r < NM && q < NM)
-        {
-            float x[NM];
-            const long l0 = elem * NC + (r * NM + q) * NM;
-#pragma unroll
-            for (int p = 0; p < NM; ++p)
-            {
-                if (MODE == kModeGather)
-                {
-                    const int gi = a.gmap[l0 + p];
-                    x[p]         = a.gsign ? float(a.gsign[l0 + p]) * a.in[gi] : a.in[gi];
-                }
-                else
-                    x[p] = a.in[l0 + p];
-            }
-            tcd::WriteRowK<NM, Dm::KM>(cube_hi(0), cube_lo(0), t, x);
-        }
-    }
+    if (ev && xr < NM && xq < NM)
+        tcd::WriteRowK<NM, Dm::KM>(cube_hi(0), cube_lo(0), t, xcur);
     sync_issue();
     if (t == 0)
     {
@@ -387,6 +406,8 @@ __global__ void __launch_bounds__(128, 1) k_hex_helm_tc(HexArgs<float> a, TcTabl
             tcd::WriteRowK<NQ, Dm::KQ>(cube_hi(3), cube_lo(3), t, v0);
         }
     }
+    // the next tile's coefficients, in flight during the last three stages
+    load_x(tile + gridDim.x, xcur);
     sync_issue();
     if (t == 0)
     {
@@ -464,6 +485,8 @@ __global__ void __launch_bounds__(128, 1) k_hex_helm_tc(HexArgs<float> a, TcTabl
             for (int p = 0; p < NM; ++p)
                 o[p] = y[p];
         }
+    }
+
     }
 
     // every tensor-memory read and every MMA is complete here
