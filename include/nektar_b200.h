@@ -272,8 +272,9 @@ void nkb_op_destroy(nkb_op *op);
 /* Self-test of the fifth-generation tensor-core building blocks the FP32 Hex
  * Helmholtz kernel uses (no reference counterpart): D = A B for one 128-row
  * tile, A (128 x 8*ksteps, row-major, host) written into the kernel's
- * K-major operand form by its row writer (column_writer = 0) or its column
- * writer (1) as TF32 high and low parts, B
+ * K-major operand forms as TF32 high and low parts: by its row writer
+ * (column_writer = 0), its rotated column writer (1, dense layout) or its
+ * column writer for the padded layout (2), B
  * (8*ksteps x n, row-major, host) in its K-major table form, n in {16, 32,
  * 64}; D (128 x n, host) read back from tensor memory. info[0]: the tensor
  * memory address, info[1]: 1 when the MMA completion wait succeeded. */

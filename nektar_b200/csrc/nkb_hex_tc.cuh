@@ -32,6 +32,8 @@
 #include "nkb_tc.cuh"
 #include "nkb_tma.cuh"
 
+#include <type_traits>
+
 namespace nkb
 {
 
@@ -43,11 +45,17 @@ template <int NM, int NQ> struct TcDims
     static constexpr int KM = Pad8(NM), KQ = Pad8(NQ);
     static constexpr int KSM = KM / 8, KSQ = KQ / 8, KS = Max(KSM, KSQ);
     static constexpr int NQP = Pad8(NQ), NMN = Pad8(NM);
-    static constexpr int QP = Pad4(NQ), MP = Pad4(NM);
-    static constexpr int RPE = Pad4(Max(Max(NM * MP, NM * QP), Max(NQ * QP, NQ * MP)));
+    // nq <= 8: row strides of 8 and the padded operand layout, so a column
+    // store's offset is a compile-time constant from its row group; larger
+    // orders: strides of 4 (128 rows hold one element) and rotated stores
+    static constexpr bool FAST = NQ <= 8;
+    using AL                   = typename std::conditional<FAST, tc::ALayoutPad, tc::ALayoutStd>::type;
+    static constexpr int QP = FAST ? 8 : Pad4(NQ), MP = FAST ? 8 : Pad4(NM);
+    static constexpr int RPE0 = Max(Max(NM * MP, NM * QP), Max(NQ * QP, NQ * MP));
+    static constexpr int RPE  = FAST ? Pad8(RPE0) : Pad4(RPE0);
     static constexpr int EPT   = 128 / RPE;
-    static constexpr int NCUBE = 4;                      // operands of the widest stage
-    static constexpr int CUBE  = KS * int(tc::kOperandBytes); // bytes of one high or low part
+    static constexpr int NCUBE = 4;             // operands of the widest stage
+    static constexpr int CUBE  = KS * AL::STEP; // bytes of one high or low part
     static constexpr int ABYTES = 2 * NCUBE * CUBE;
     static constexpr int TCOLS  = 8 * NQP <= 64 ? 64 : (8 * NQP <= 128 ? 128 : 256);
     static constexpr int TBROWS = 4 * NQP, TBTROWS = 4 * NMN;
@@ -92,8 +100,8 @@ __device__ __forceinline__ void Split4(const float *v, float4 &hi, float4 &lo)
     lo.w = v[3] - hi.w;
 }
 
-// row m of a K-major operand pair: values v[0, len), zero up to kpad
-template <int LEN, int KPAD>
+// row m of a K-major operand pair (layout L): values v[0, LEN), zero up to KPAD
+template <class L, int LEN, int KPAD>
 __device__ __forceinline__ void WriteRowK(unsigned char *hi, unsigned char *lo, int m, const float *v)
 {
 #pragma unroll
@@ -105,47 +113,65 @@ __device__ __forceinline__ void WriteRowK(unsigned char *hi, unsigned char *lo, 
             w[u] = (4 * c + u < LEN) ? v[4 * c + u] : 0.f;
         float4 h, l;
         Split4(w, h, l);
-        const uint32_t o = tc::OffK(m, 4 * c);
+        const uint32_t o = L::Off(m, 4 * c);
         *reinterpret_cast<float4 *>(hi + o) = h;
         *reinterpret_cast<float4 *>(lo + o) = l;
     }
 }
 
 // rows m0 .. m0 + LEN - 1 of K column k of a K-major operand pair (a thread
-// that holds one K index of many rows): scalar stores, visited in the order
-// starting at row m0 + s (s < LEN) so that the threads of a warp, given
-// distinct s where they share k % 4, hit distinct shared-memory banks (the
-// bank of element (m, k) is (m % 8) * 4 + k % 4). The rotation of the value
-// array is done with compile-time indices (selects), keeping it in registers.
-template <int LEN>
+// that holds one K index of many rows): scalar stores.
+// ROT = false (m0 % 8 == 0, padded layout): offsets from the first store are
+// compile-time constants; the layout spreads a warp's stores over the banks.
+// ROT = true: the stores are visited in the order starting at row m0 + s
+// (s < LEN) so that the threads of a warp, given distinct s where they share
+// k % 4, hit distinct banks (the bank of element (m, k) is (m % 8) * 4 + k % 4
+// in the standard layout); the value array is rotated with compile-time
+// indices (selects), keeping it in registers.
+template <class L, int LEN, bool ROT>
 __device__ __forceinline__ void WriteColK(unsigned char *hi, unsigned char *lo, int m0, int k,
                                           const float *v, int s)
 {
-    float w[LEN];
-#pragma unroll
-    for (int j = 0; j < LEN; ++j)
-        w[j] = v[j];
-#pragma unroll
-    for (int bit = 1; bit < LEN; bit <<= 1)
+    if constexpr (!ROT)
     {
-        const bool on = (s & bit) != 0;
-        float r[LEN];
+        const uint32_t base = L::Off(m0, k);
 #pragma unroll
-        for (int j = 0; j < LEN; ++j)
-            r[j] = w[(j + bit) % LEN];
-#pragma unroll
-        for (int j = 0; j < LEN; ++j)
-            w[j] = on ? r[j] : w[j];
+        for (int c = 0; c < LEN; ++c)
+        {
+            const float h    = tc::Tf32Hi(v[c]);
+            const uint32_t o = base + uint32_t(c >> 3) * uint32_t(L::SBO) + uint32_t(c & 7) * 16u;
+            *reinterpret_cast<float *>(hi + o) = h;
+            *reinterpret_cast<float *>(lo + o) = v[c] - h;
+        }
     }
-#pragma unroll
-    for (int j = 0; j < LEN; ++j)
+    else
     {
-        int c = s + j;
-        c     = c >= LEN ? c - LEN : c;
-        const float h = tc::Tf32Hi(w[j]);
-        const uint32_t o = tc::OffK(m0 + c, k);
-        *reinterpret_cast<float *>(hi + o) = h;
-        *reinterpret_cast<float *>(lo + o) = w[j] - h;
+        float w[LEN];
+#pragma unroll
+        for (int j = 0; j < LEN; ++j)
+            w[j] = v[j];
+#pragma unroll
+        for (int bit = 1; bit < LEN; bit <<= 1)
+        {
+            const bool on = (s & bit) != 0;
+            float r[LEN];
+#pragma unroll
+            for (int j = 0; j < LEN; ++j)
+                r[j] = w[(j + bit) % LEN];
+#pragma unroll
+            for (int j = 0; j < LEN; ++j)
+                w[j] = on ? r[j] : w[j];
+        }
+#pragma unroll
+        for (int j = 0; j < LEN; ++j)
+        {
+            int c = s + j;
+            c     = c >= LEN ? c - LEN : c;
+            const float h = tc::Tf32Hi(w[j]);
+            const uint32_t o = L::Off(m0 + c, k);
+            *reinterpret_cast<float *>(hi + o) = h;
+            *reinterpret_cast<float *>(lo + o) = w[j] - h;
+        }
     }
 }
 
@@ -191,9 +217,10 @@ template <int NP> __device__ __forceinline__ void LdPair(uint32_t taddr, float *
     }
 }
 
-// MMAs of one K-major operand pair (high part at a_hi, low part a_hi + cube)
-// against rows [n0, n0 + n) of a B table of nrows rows at stab, over ks K
-// steps, into tensor-memory column tcol (acc: add to what is there)
+// MMAs of one K-major operand pair of layout L (high part at a_hi, low part
+// a_hi + cube) against rows [n0, n0 + n) of a B table of nrows rows at stab,
+// over ks K steps, into tensor-memory column tcol (acc: add to what is there)
+template <class L>
 __device__ __forceinline__ void IssuePair(uint32_t a_hi, uint32_t cube, uint32_t stab, int nrows,
                                           int n0, int n, int ks, uint32_t tcol, bool acc)
 {
@@ -201,10 +228,10 @@ __device__ __forceinline__ void IssuePair(uint32_t a_hi, uint32_t cube, uint32_t
     for (int s = 0; s < ks; ++s)
     {
         const uint64_t b = tc::DescKMajor(stab + uint32_t(s * nrows * 32 + (n0 >> 3) * 256));
-        const uint32_t ah = a_hi + uint32_t(s) * tc::kOperandBytes;
+        const uint32_t ah = a_hi + uint32_t(s) * uint32_t(L::STEP);
         const uint32_t al = ah + cube;
-        const uint64_t dh = tc::DescKMajor(ah);
-        const uint64_t dl = tc::DescKMajor(al);
+        const uint64_t dh = tc::Desc(ah, L::LBO, L::SBO);
+        const uint64_t dl = tc::Desc(al, L::LBO, L::SBO);
         tc::MmaTf32(tcol, dh, b, idesc, acc || s > 0);
         tc::MmaTf32(tcol, dl, b, idesc, true);
     }
@@ -219,6 +246,7 @@ __global__ void __launch_bounds__(128, TcDims<NM, NQ>::MIN_CTAS)
     constexpr int NC = NM * NM * NM, NQ2 = NQ * NQ, NT = NQ2 * NQ;
     constexpr int RPE = Dm::RPE, EPT = Dm::EPT, MP = Dm::MP, QP = Dm::QP;
     constexpr int NQP = Dm::NQP, NMN = Dm::NMN, CUBE = Dm::CUBE;
+    using AL          = typename Dm::AL;
     extern __shared__ __align__(1024) unsigned char sm[];
     if (a.skip && *a.skip)
         return;
@@ -308,12 +336,12 @@ __global__ void __launch_bounds__(128, TcDims<NM, NQ>::MIN_CTAS)
 
     // ---- stage 1: contract p (rows (r, q), K-major) ----------------------
     if (ev && xr < NM && xq < NM)
-        tcd::WriteRowK<NM, Dm::KM>(cube_hi(0), cube_lo(0), t, xcur);
+        tcd::WriteRowK<AL, NM, Dm::KM>(cube_hi(0), cube_lo(0), t, xcur);
     sync_issue();
     if (t == 0)
     {
         tc::FenceAfterSync();
-        tcd::IssuePair(ahi(0), ccube, st + tt.tb[0], Dm::TBROWS, 0, 4 * NQP, Dm::KSM, tmem,
+        tcd::IssuePair<AL>(ahi(0), ccube, st + tt.tb[0], Dm::TBROWS, 0, 4 * NQP, Dm::KSM, tmem,
                        false);
         tc::Commit(bar);
     }
@@ -328,17 +356,17 @@ __global__ void __launch_bounds__(128, TcDims<NM, NQ>::MIN_CTAS)
         if (ev && r < NM && q < NM)
         {
             const int sr = (rr >> 2) % NQ; // distinct where q % 4 is shared
-            tcd::WriteColK<NQ>(cube_hi(0), cube_lo(0), rowb + r * QP, q, T, sr);
-            tcd::WriteColK<NQ>(cube_hi(1), cube_lo(1), rowb + r * QP, q, Tp, sr);
+            tcd::WriteColK<AL, NQ, !Dm::FAST>(cube_hi(0), cube_lo(0), rowb + r * QP, q, T, sr);
+            tcd::WriteColK<AL, NQ, !Dm::FAST>(cube_hi(1), cube_lo(1), rowb + r * QP, q, Tp, sr);
         }
     }
     sync_issue();
     if (t == 0)
     {
         tc::FenceAfterSync();
-        tcd::IssuePair(ahi(0), ccube, st + tt.tb[1], Dm::TBROWS, 0, 4 * NQP, Dm::KSM, tmem,
+        tcd::IssuePair<AL>(ahi(0), ccube, st + tt.tb[1], Dm::TBROWS, 0, 4 * NQP, Dm::KSM, tmem,
                        false);
-        tcd::IssuePair(ahi(1), ccube, st + tt.tb[1], Dm::TBROWS, 0, 2 * NQP, Dm::KSM,
+        tcd::IssuePair<AL>(ahi(1), ccube, st + tt.tb[1], Dm::TBROWS, 0, 2 * NQP, Dm::KSM,
                        tmem + 4 * NQP, false);
         tc::Commit(bar);
     }
@@ -354,20 +382,20 @@ __global__ void __launch_bounds__(128, TcDims<NM, NQ>::MIN_CTAS)
         if (ev && r < NM && i < NQ)
         {
             const int sr = i % NQ; // distinct where r % 4 is shared
-            tcd::WriteColK<NQ>(cube_hi(0), cube_lo(0), rowb + i * QP, r, U, sr);
-            tcd::WriteColK<NQ>(cube_hi(1), cube_lo(1), rowb + i * QP, r, Up, sr);
-            tcd::WriteColK<NQ>(cube_hi(2), cube_lo(2), rowb + i * QP, r, V, sr);
+            tcd::WriteColK<AL, NQ, !Dm::FAST>(cube_hi(0), cube_lo(0), rowb + i * QP, r, U, sr);
+            tcd::WriteColK<AL, NQ, !Dm::FAST>(cube_hi(1), cube_lo(1), rowb + i * QP, r, Up, sr);
+            tcd::WriteColK<AL, NQ, !Dm::FAST>(cube_hi(2), cube_lo(2), rowb + i * QP, r, V, sr);
         }
     }
     sync_issue();
     if (t == 0)
     {
         tc::FenceAfterSync();
-        tcd::IssuePair(ahi(0), ccube, st + tt.tb[2], Dm::TBROWS, 0, 4 * NQP, Dm::KSM, tmem,
+        tcd::IssuePair<AL>(ahi(0), ccube, st + tt.tb[2], Dm::TBROWS, 0, 4 * NQP, Dm::KSM, tmem,
                        false);
-        tcd::IssuePair(ahi(1), ccube, st + tt.tb[2], Dm::TBROWS, 0, 2 * NQP, Dm::KSM,
+        tcd::IssuePair<AL>(ahi(1), ccube, st + tt.tb[2], Dm::TBROWS, 0, 2 * NQP, Dm::KSM,
                        tmem + 4 * NQP, false);
-        tcd::IssuePair(ahi(2), ccube, st + tt.tb[2], Dm::TBROWS, 0, 2 * NQP, Dm::KSM,
+        tcd::IssuePair<AL>(ahi(2), ccube, st + tt.tb[2], Dm::TBROWS, 0, 2 * NQP, Dm::KSM,
                        tmem + 6 * NQP, false);
         tc::Commit(bar);
     }
@@ -400,10 +428,10 @@ __global__ void __launch_bounds__(128, TcDims<NM, NQ>::MIN_CTAS)
                 v1[k] = fmaf(G12, g2[k], fmaf(G11, g1[k], G01 * g0[k]));
                 v2[k] = fmaf(G22, g2[k], fmaf(G12, g1[k], G02 * g0[k]));
             }
-            tcd::WriteRowK<NQ, Dm::KQ>(cube_hi(0), cube_lo(0), t, f);
-            tcd::WriteRowK<NQ, Dm::KQ>(cube_hi(1), cube_lo(1), t, v2);
-            tcd::WriteRowK<NQ, Dm::KQ>(cube_hi(2), cube_lo(2), t, v1);
-            tcd::WriteRowK<NQ, Dm::KQ>(cube_hi(3), cube_lo(3), t, v0);
+            tcd::WriteRowK<AL, NQ, Dm::KQ>(cube_hi(0), cube_lo(0), t, f);
+            tcd::WriteRowK<AL, NQ, Dm::KQ>(cube_hi(1), cube_lo(1), t, v2);
+            tcd::WriteRowK<AL, NQ, Dm::KQ>(cube_hi(2), cube_lo(2), t, v1);
+            tcd::WriteRowK<AL, NQ, Dm::KQ>(cube_hi(3), cube_lo(3), t, v0);
         }
     }
     // the next tile's coefficients, in flight during the last three stages
@@ -413,11 +441,11 @@ __global__ void __launch_bounds__(128, TcDims<NM, NQ>::MIN_CTAS)
     {
         tc::FenceAfterSync();
         const uint32_t tb = st + tt.tbt[2];
-        tcd::IssuePair(ahi(0), ccube, tb, Dm::TBTROWS, 0, 2 * NMN, Dm::KSQ, tmem, false);
-        tcd::IssuePair(ahi(1), ccube, tb, Dm::TBTROWS, 2 * NMN, 2 * NMN, Dm::KSQ, tmem, true);
-        tcd::IssuePair(ahi(2), ccube, tb, Dm::TBTROWS, 0, 2 * NMN, Dm::KSQ, tmem + 2 * NMN,
+        tcd::IssuePair<AL>(ahi(0), ccube, tb, Dm::TBTROWS, 0, 2 * NMN, Dm::KSQ, tmem, false);
+        tcd::IssuePair<AL>(ahi(1), ccube, tb, Dm::TBTROWS, 2 * NMN, 2 * NMN, Dm::KSQ, tmem, true);
+        tcd::IssuePair<AL>(ahi(2), ccube, tb, Dm::TBTROWS, 0, 2 * NMN, Dm::KSQ, tmem + 2 * NMN,
                        false);
-        tcd::IssuePair(ahi(3), ccube, tb, Dm::TBTROWS, 0, 2 * NMN, Dm::KSQ, tmem + 4 * NMN,
+        tcd::IssuePair<AL>(ahi(3), ccube, tb, Dm::TBTROWS, 0, 2 * NMN, Dm::KSQ, tmem + 4 * NMN,
                        false);
         tc::Commit(bar);
     }
@@ -433,9 +461,9 @@ __global__ void __launch_bounds__(128, TcDims<NM, NQ>::MIN_CTAS)
         if (ev && i < NQ && j < NQ)
         {
             const int sr = (rr >> 2) % NM; // distinct where j % 4 is shared
-            tcd::WriteColK<NM>(cube_hi(0), cube_lo(0), rowb + i * MP, j, X, sr);
-            tcd::WriteColK<NM>(cube_hi(1), cube_lo(1), rowb + i * MP, j, Y1, sr);
-            tcd::WriteColK<NM>(cube_hi(2), cube_lo(2), rowb + i * MP, j, Y0, sr);
+            tcd::WriteColK<AL, NM, !Dm::FAST>(cube_hi(0), cube_lo(0), rowb + i * MP, j, X, sr);
+            tcd::WriteColK<AL, NM, !Dm::FAST>(cube_hi(1), cube_lo(1), rowb + i * MP, j, Y1, sr);
+            tcd::WriteColK<AL, NM, !Dm::FAST>(cube_hi(2), cube_lo(2), rowb + i * MP, j, Y0, sr);
         }
     }
     sync_issue();
@@ -443,9 +471,9 @@ __global__ void __launch_bounds__(128, TcDims<NM, NQ>::MIN_CTAS)
     {
         tc::FenceAfterSync();
         const uint32_t tb = st + tt.tbt[1];
-        tcd::IssuePair(ahi(0), ccube, tb, Dm::TBTROWS, 0, 2 * NMN, Dm::KSQ, tmem, false);
-        tcd::IssuePair(ahi(1), ccube, tb, Dm::TBTROWS, 2 * NMN, 2 * NMN, Dm::KSQ, tmem, true);
-        tcd::IssuePair(ahi(2), ccube, tb, Dm::TBTROWS, 0, 2 * NMN, Dm::KSQ, tmem + 2 * NMN,
+        tcd::IssuePair<AL>(ahi(0), ccube, tb, Dm::TBTROWS, 0, 2 * NMN, Dm::KSQ, tmem, false);
+        tcd::IssuePair<AL>(ahi(1), ccube, tb, Dm::TBTROWS, 2 * NMN, 2 * NMN, Dm::KSQ, tmem, true);
+        tcd::IssuePair<AL>(ahi(2), ccube, tb, Dm::TBTROWS, 0, 2 * NMN, Dm::KSQ, tmem + 2 * NMN,
                        false);
         tc::Commit(bar);
     }
@@ -460,8 +488,8 @@ __global__ void __launch_bounds__(128, TcDims<NM, NQ>::MIN_CTAS)
         if (ev && i < NQ && r < NM)
         {
             const int sr = r % NM; // distinct where i % 4 is shared
-            tcd::WriteColK<NM>(cube_hi(0), cube_lo(0), rowb + r * MP, i, Z, sr);
-            tcd::WriteColK<NM>(cube_hi(1), cube_lo(1), rowb + r * MP, i, Z0, sr);
+            tcd::WriteColK<AL, NM, !Dm::FAST>(cube_hi(0), cube_lo(0), rowb + r * MP, i, Z, sr);
+            tcd::WriteColK<AL, NM, !Dm::FAST>(cube_hi(1), cube_lo(1), rowb + r * MP, i, Z0, sr);
         }
     }
     sync_issue();
@@ -469,8 +497,8 @@ __global__ void __launch_bounds__(128, TcDims<NM, NQ>::MIN_CTAS)
     {
         tc::FenceAfterSync();
         const uint32_t tb = st + tt.tbt[0];
-        tcd::IssuePair(ahi(0), ccube, tb, Dm::TBTROWS, 0, 2 * NMN, Dm::KSQ, tmem, false);
-        tcd::IssuePair(ahi(1), ccube, tb, Dm::TBTROWS, 2 * NMN, 2 * NMN, Dm::KSQ, tmem, true);
+        tcd::IssuePair<AL>(ahi(0), ccube, tb, Dm::TBTROWS, 0, 2 * NMN, Dm::KSQ, tmem, false);
+        tcd::IssuePair<AL>(ahi(1), ccube, tb, Dm::TBTROWS, 2 * NMN, 2 * NMN, Dm::KSQ, tmem, true);
         tc::Commit(bar);
     }
     wait_mma();

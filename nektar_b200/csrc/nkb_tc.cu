@@ -26,12 +26,14 @@ __global__ void __launch_bounds__(128, 1)
     k_tc_selftest(int colw, int n, int ks, const float *__restrict__ A, const float *__restrict__ B,
                   float *__restrict__ D, unsigned *info, int *err)
 {
-    __shared__ __align__(1024) unsigned char sa[2 * 2 * int(tc::kOperandBytes)];
+    __shared__ __align__(1024) unsigned char sa[2 * 2 * tc::ALayoutPad::STEP];
     __shared__ __align__(1024) unsigned char sb[kSelfMaxN * kSelfMaxK * 4];
     __shared__ uint64_t bar;
     __shared__ uint32_t slot;
     const int t = threadIdx.x, warp = t >> 5, K = 8 * ks;
-    unsigned char *hi = sa, *lo = sa + 2 * tc::kOperandBytes;
+    // high part: two K steps; low part after them (either layout fits)
+    const int step    = colw == 2 ? tc::ALayoutPad::STEP : tc::ALayoutStd::STEP;
+    unsigned char *hi = sa, *lo = sa + 2 * step;
     for (int o = t * 16; o < int(sizeof(sa)); o += 128 * 16)
         *reinterpret_cast<float4 *>(sa + o) = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int o = t * 16; o < int(sizeof(sb)); o += 128 * 16)
@@ -52,9 +54,9 @@ __global__ void __launch_bounds__(128, 1)
         for (int k = 0; k < kSelfMaxK; ++k)
             v[k] = k < K ? A[t * K + k] : 0.f;
         if (ks == 1)
-            tcd::WriteRowK<8, 8>(hi, lo, t, v);
+            tcd::WriteRowK<tc::ALayoutStd, 8, 8>(hi, lo, t, v);
         else
-            tcd::WriteRowK<16, 16>(hi, lo, t, v);
+            tcd::WriteRowK<tc::ALayoutStd, 16, 16>(hi, lo, t, v);
     }
     else if (t < K)
     {
@@ -63,7 +65,10 @@ __global__ void __launch_bounds__(128, 1)
             float v[8];
             for (int u = 0; u < 8; ++u)
                 v[u] = A[(m0 + u) * K + t];
-            tcd::WriteColK<8>(hi, lo, m0, t, v, t % 8);
+            if (colw == 1)
+                tcd::WriteColK<tc::ALayoutStd, 8, true>(hi, lo, m0, t, v, t % 8);
+            else
+                tcd::WriteColK<tc::ALayoutPad, 8, false>(hi, lo, m0, t, v, 0);
         }
     }
     if (t == 0)
@@ -78,8 +83,12 @@ __global__ void __launch_bounds__(128, 1)
     if (t == 0)
     {
         tc::FenceAfterSync();
-        tcd::IssuePair(tc::SmemU32(hi), 2 * tc::kOperandBytes, tc::SmemU32(sb), n, 0, n, ks, tmem,
-                       false);
+        if (colw == 2)
+            tcd::IssuePair<tc::ALayoutPad>(tc::SmemU32(hi), 2 * tc::ALayoutPad::STEP,
+                                           tc::SmemU32(sb), n, 0, n, ks, tmem, false);
+        else
+            tcd::IssuePair<tc::ALayoutStd>(tc::SmemU32(hi), 2 * tc::ALayoutStd::STEP,
+                                           tc::SmemU32(sb), n, 0, n, ks, tmem, false);
         tc::Commit(&bar);
     }
     const bool ok = MbarWaitBounded(&bar, 0, err, 3);
@@ -116,8 +125,9 @@ extern "C" int nkb_tc_selftest(int column_writer, int n, int ksteps, const float
 {
     ClearError();
     if (!A || !B || !D || !info || (ksteps != 1 && ksteps != 2) ||
-        (n != 16 && n != 32 && n != 64))
-        return SetError(NKB_ERR_INVALID, "nkb_tc_selftest: n in {16, 32, 64}, ksteps 1 or 2");
+        (n != 16 && n != 32 && n != 64) || column_writer < 0 || column_writer > 2)
+        return SetError(NKB_ERR_INVALID, "nkb_tc_selftest: n in {16, 32, 64}, ksteps 1 or 2, "
+                                         "column_writer 0..2");
     const int K  = 8 * ksteps;
     float *dA    = nullptr, *dB = nullptr, *dD = nullptr;
     unsigned *dI = nullptr;

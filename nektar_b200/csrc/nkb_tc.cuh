@@ -140,11 +140,31 @@ __device__ __forceinline__ float Tf32Hi(float a)
     return __uint_as_float(r);
 }
 
-// byte offsets of element (m, k) in an operand of 8-wide K steps
+// A K-major operand of 128 rows: 8-row groups SBO bytes apart, the two
+// 4-wide K chunks of a group LBO bytes apart (LBO >= 128, SBO >= LBO + 128),
+// one 8-wide K step STEP bytes. The standard packing (256, 128) is dense; the
+// padded one (272, 144) shifts consecutive row groups by 4 banks and the
+// second K chunk by 4 more, which makes the scalar column stores of a warp
+// (8 row groups, or 4 groups x 8 K values) hit distinct banks, for 1/16 more
+// shared memory.
+template <int SBO_, int LBO_> struct ALayout
+{
+    static constexpr int SBO = SBO_, LBO = LBO_, STEP = 16 * SBO_;
+    static_assert(LBO_ >= 128 && SBO_ >= LBO_ + 128 && SBO_ % 16 == 0 && LBO_ % 16 == 0,
+                  "K-major operand strides");
+    __host__ __device__ static constexpr uint32_t Off(int m, int k)
+    {
+        return uint32_t(k >> 3) * uint32_t(STEP) + uint32_t(m >> 3) * uint32_t(SBO) +
+               uint32_t((k & 7) >> 2) * uint32_t(LBO) + uint32_t(m & 7) * 16u + uint32_t(k & 3) * 4u;
+    }
+};
+using ALayoutStd = ALayout<256, 128>;
+using ALayoutPad = ALayout<272, 144>;
+
+// byte offsets of element (m, k) in a standard operand of 8-wide K steps
 __host__ __device__ constexpr uint32_t OffK(int m, int k)
 {
-    return uint32_t(k >> 3) * kOperandBytes + uint32_t(m >> 3) * 256u + uint32_t((k & 7) >> 2) * 128u +
-           uint32_t(m & 7) * 16u + uint32_t(k & 3) * 4u;
+    return ALayoutStd::Off(m, k);
 }
 
 // B operand (K-major, nrows rows padded to 8): element (n, k); one K step

@@ -45,11 +45,12 @@ def _tf32_trunc(a):
     return (np.asarray(a, dtype=np.float32).view(np.uint32) & np.uint32(0xFFFFE000)).view(np.float32)
 
 
-@pytest.mark.parametrize("colw", [0, 1])
+@pytest.mark.parametrize("colw", [0, 1, 2])
 @pytest.mark.parametrize("n,ks", [(16, 1), (32, 1), (64, 1), (16, 2), (32, 2)])
 def test_tc_building_blocks_compute_a_times_b(colw, n, ks):
-    """One 128-row tile through the kernel's operand writers (its row writer
-    or its bank-spread column writer, TF32 high/low parts, K-major), K-major
+    """One 128-row tile through the kernel's operand writers (its row writer,
+    its rotated column writer, its padded-layout column writer; TF32
+    high/low parts, K-major), K-major
     B table, MMA pair, commit and
     tensor-memory read-back: D = A B to FP32-class accuracy (B is read as
     TF32 by the hardware)."""
