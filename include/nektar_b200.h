@@ -163,6 +163,23 @@ int nkb_op_create_dense(int n, int nelmt, const double *mats, int device, nkb_op
 int nkb_op_create_dense_rect(int rows, int cols, int nelmt, const double *mats, int device,
                              nkb_op **op);
 
+/* Static condensation of per-element matrices on the device: the set-up of
+ * GlobalLinSysIterativeStaticCond (GlobalLinSysIterativeStaticCond.cpp:199,
+ * v_AssembleSchurComplement) and the per-element maps of
+ * GlobalLinSysStaticCond::v_Solve (GlobalLinSysStaticCond.cpp:98-227). K
+ * (device, nelmt x nc x nc, as nkb_op_element_matrices writes it) split by
+ * the host index lists bm (nb >= 1 boundary modes) and im (ni >= 0 interior
+ * modes, together a partition of the nc modes; im may be NULL when ni = 0);
+ * R (host, nb x nb row-major, or
+ * NULL for the identity) is the boundary transform (the low-energy basis).
+ * Outputs (device): S = R (Kbb - Kbi Kii^-1 Kib) R^T (nelmt x nb x nb),
+ * W (nelmt x nb x nc): W[:, bm] = R, W[:, im] = -R Kbi Kii^-1, and
+ * V (nelmt x nc x (nb + ni)): V[bm, :nb] = R^T, V[im, :nb] = -Kii^-1 Kib R^T,
+ * V[im, nb:] = Kii^-1. Kii is factored by Cholesky (NKB_ERR_INVALID if it
+ * is not positive definite). Synchronous on `stream`. */
+int nkb_condense(int nelmt, int nc, const double *K, int nb, const int *bm, int ni, const int *im,
+                 const double *R, double *S, double *W, double *V, int device, void *stream);
+
 /* Every element's matrix of an FP64 operator with as many outputs as inputs
  * per element (Helmholtz, LinearADR, square dense blocks): K[e][i][j] is
  * output i of element e for the unit input j, built on the device by nc
@@ -387,10 +404,33 @@ int nkb_sys_set_lambda(nkb_sys *sys, double lambda);
  * (indices counted from the first non-Dirichlet dof, 1..256 per block, no
  * dof in two blocks); binv holds the blocks' inverses one after another, each
  * n*n doubles column-major (for the symmetric blocks of an SPD system either
- * order). Dofs outside every block keep the Jacobi step. Host arrays, copied;
- * set once per system, before any clone; FP64 solves only. */
+ * order). Dofs outside every block keep the Jacobi step. bptr and bidx are
+ * host arrays, binv host or device memory (nkb_blocks_invert's output), all
+ * copied; set once per system, before any clone; FP64 solves only. */
 int nkb_sys_set_blocks(nkb_sys *sys, int nblk, const int *bptr, const int *bidx,
                        const double *binv);
+
+/* The entity blocks of the Block and LowEnergy preconditioners assembled on
+ * the device from condensed element matrices already there (nkb_condense's
+ * S; PreconditionerLowEnergy.cpp:568-760 gathers the same blocks on the
+ * host). Blocks as nkb_sys_set_blocks' bptr (n_b = bptr[b+1] - bptr[b]
+ * rows); A (device) holds the blocks one after another, n_b * n_b doubles
+ * row-major each. Contribution c of block b (cptr[b] <= c < cptr[b+1], host
+ * CSR) adds sign_i sign_j S[celm[c]][l_i][l_j] to A_b[i][j], l and sign the
+ * n_b entries of cloc / csgn (host) that follow the earlier contributions';
+ * S is nelmt x nbm x nbm (device). Contributions are added in their order
+ * (the result does not depend on the launch). One call per collection, then
+ * nkb_blocks_invert. Synchronous on `stream`. */
+int nkb_blocks_accumulate(int nblk, const int *bptr, int ncontrib, const int *cptr,
+                          const int *celm, const int *cloc, const signed char *csgn, int nelmt,
+                          int nbm, const double *S, double *A, int device, void *stream);
+
+/* Inverts every block of A (device, layout of nkb_blocks_accumulate) in
+ * place; on return each block is its inverse column-major, as
+ * nkb_sys_set_blocks takes it. Gauss-Jordan without pivoting: the blocks of
+ * an SPD system; NKB_ERR_INVALID if a pivot is not positive. Synchronous on
+ * `stream`. */
+int nkb_blocks_invert(int nblk, const int *bptr, double *A, int device, void *stream);
 
 /* Device bytes: shared by all clones (map, CSR, sign, split diagonal) and
  * owned by this instance (vectors, state, staging). Operators not included. */

@@ -331,6 +331,21 @@ class DenseOperator:
         self.h = h
         self.in_size, self.out_size = self.nelmt * cols, self.nelmt * rows
 
+    @classmethod
+    def from_device(cls, mats, device=0):
+        """The same from a (nelmt, rows, cols) FP64 device tensor (copied on
+        the device; the tensor may be freed afterwards)."""
+        self = object.__new__(cls)
+        self.nelmt, rows, cols = (int(v) for v in mats.shape)
+        self.n, self.rows, self.cols = cols, rows, cols
+        self.precision, self.optype = FP64, C.DENSE_BLOCK
+        h = ctypes.c_void_p()
+        check(lib().nkb_op_create_dense_rect(rows, cols, self.nelmt, ctypes.c_void_p(mats.data_ptr()),
+                                             device, ctypes.byref(h)))
+        self.h = h
+        self.in_size, self.out_size = self.nelmt * cols, self.nelmt * rows
+        return self
+
     def __call__(self, x):
         x = _f64(x)
         if x.size != self.in_size:
@@ -478,6 +493,17 @@ class GlobalLinSys:
         binv = np.concatenate([np.asarray(m, dtype=np.float64).T.ravel() for _, m in blocks])
         check(lib().nkb_sys_set_blocks(self.h, len(blocks), ptr.ctypes.data_as(C.ip),
                                        bidx.ctypes.data_as(C.ip), _dp(binv)))
+
+    def set_block_inverses(self, bptr, dofs, binv_ptr):
+        """Block-Jacobi preconditioner from inverses already in device memory
+        (nkb_blocks_invert's layout): bptr the block pointers, dofs the
+        blocks' global dofs (>= ndir) one block after another, binv_ptr the
+        device address of the inverses (copied)."""
+        bptr = np.ascontiguousarray(bptr, dtype=np.int32)
+        bidx = np.ascontiguousarray(np.asarray(dofs, dtype=np.int64) - self.ndir, dtype=np.int32)
+        check(lib().nkb_sys_set_blocks(self.h, bptr.size - 1, bptr.ctypes.data_as(C.ip),
+                                       bidx.ctypes.data_as(C.ip),
+                                       ctypes.cast(ctypes.c_void_p(binv_ptr), C.dp)))
 
     def footprint(self):
         """(shared bytes, instance bytes) of device memory held by the system."""

@@ -89,7 +89,12 @@ SIGNATURES = {
     "nkb_op_helmholtz_diag": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "nkb_op_last_kernel_ms": (c_int, [c_void_p, P(c_float)]),
     "nkb_op_check_error": (c_int, [c_void_p]),
+    "nkb_condense": (c_int, [c_int, c_int, c_void_p, c_int, ip, c_int, ip, dp, c_void_p, c_void_p,
+                             c_void_p, c_int, c_void_p]),
     "nkb_tc_selftest": (c_int, [c_int, c_int, c_int, fp, fp, fp, P(ctypes.c_uint)]),
+    "nkb_blocks_accumulate": (c_int, [c_int, ip, c_int, ip, ip, ip, P(ctypes.c_byte), c_int, c_int,
+                                      c_void_p, c_void_p, c_int, c_void_p]),
+    "nkb_blocks_invert": (c_int, [c_int, ip, c_void_p, c_int, c_void_p]),
     "nkb_op_set_wait_limit": (c_int, [c_void_p, c_int]),
     "nkb_op_destroy": (None, [c_void_p]),
     "nkb_op_kernel": (c_char_p, [c_void_p, c_int]),

@@ -1132,7 +1132,7 @@ extern "C" int nkb_sys_set_blocks(nkb_sys *S, int nblk, const int *bptr, const i
     if (cudaMemcpy(dp, bptr, (nblk + 1) * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(di, bidx, nidx * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(dof, boff.data(), nblk * sizeof(long), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(dm, binv, tot * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaMemcpy(dm, binv, tot * sizeof(double), cudaMemcpyDefault) != cudaSuccess)
     {
         release();
         return SetError(NKB_ERR_CUDA, "nkb_sys_set_blocks: upload");

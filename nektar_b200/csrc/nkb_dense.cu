@@ -149,7 +149,8 @@ extern "C" int nkb_op_create_dense_rect(int rows, int cols, int nelmt, const dou
     {
         if (cudaMalloc(&op->geo, bytes) != cudaSuccess)
             return fail(SetError(NKB_ERR_NOMEM, "nkb_op_create_dense: %zu bytes of blocks", bytes));
-        if (cudaMemcpy(op->geo, mats, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        // host or device blocks (unified addressing tells them apart)
+        if (cudaMemcpy(op->geo, mats, bytes, cudaMemcpyDefault) != cudaSuccess)
             return fail(SetError(NKB_ERR_CUDA, "nkb_op_create_dense: upload"));
     }
     *out = op;

@@ -26,6 +26,8 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--precon", default="diagonal,block,lowenergy")
     ap.add_argument("--shape", default="hex", choices=["hex", "prism", "tet"])
+    ap.add_argument("--setup", default="device", choices=["device", "host"],
+                    help="condensation on the device (nkb_condense) or in host numpy")
     ap.add_argument("--no-full", action="store_true",
                     help="condensed solves only (no full CG; for profiling them)")
     a = ap.parse_args()
@@ -48,6 +50,9 @@ def main():
         op.set_factors(1.0)
         ops.append(op)
     nloc = sum(o.in_size for o in ops)
+    import torch
+    torch.zeros(1, device="cuda")  # the process's CUDA start-up is not set-up time
+    torch.cuda.synchronize()
     b = np.random.default_rng(0).uniform(-1, 1, nloc)
     xf = rf = None
     if not a.no_full:
@@ -57,11 +62,13 @@ def main():
         xf, rf = full.solve(b, tol=a.tol)
         full_wall = time.perf_counter() - t0
     t0 = time.perf_counter()
-    K = [element_matrices(o) for o in ops]  # shared by the condensed systems
+    # host set-up: element matrices copied back once and shared by the
+    # condensed systems; device set-up: each system builds its own on the device
+    K = [element_matrices(o) for o in ops] if a.setup == "host" else None
     t_mats = time.perf_counter() - t0
     out = {
         "workload": "%d^3 %s, P=%d, CG to %g" % (a.n, what, a.p, a.tol),
-        "nglob": nglob, "element_matrices_s": t_mats,
+        "nglob": nglob, "setup": a.setup, "element_matrices_s": t_mats,
     }
     if rf is not None:
         out["full"] = {"precon": "diagonal", "iterations": rf.iterations,
@@ -69,7 +76,8 @@ def main():
                        "ms_per_iteration": rf.device_ms / max(rf.iterations, 1),
                        "solve_wall_s": full_wall}
     for pc in a.precon.split(","):
-        sc = StaticCondSys(ops, gmap, nglob, ndir, sign=sign, matrices=K, precon=pc)
+        sc = StaticCondSys(ops, gmap, nglob, ndir, sign=sign, matrices=K, precon=pc,
+                           setup=a.setup)
         sc.solve(b, tol=a.tol)
         t0 = time.perf_counter()
         xs, rs = sc.solve(b, tol=a.tol)
@@ -83,7 +91,8 @@ def main():
             "iterations": rs.iterations, "device_ms": rs.device_ms,
             "ms_per_iteration": rs.device_ms / max(rs.iterations, 1),
             "blocks": sc.nblocks, "boundary_dofs": sc.nglob_b,
-            "setup_s": sc.setup_s, "solve_wall_s": wall,
+            "setup_s": sc.setup_s, "setup_breakdown_s": sc.setup_breakdown,
+            "solve_wall_s": wall,
             "dense_kernel_ms": ms, "dense_kernel_GB_s": dense_bytes / ms / 1e6,
             "schur_bytes": dense_bytes,
             "rel_l2_difference": (None if xf is None else

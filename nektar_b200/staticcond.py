@@ -252,16 +252,20 @@ def lowenergy_transforms(shapes, nm, lam, device=0, reference=None):
     return {k: v for k, v in Rs.items() if k in shapes}
 
 
-def entity_blocks(parts, bmap, bsign, ndir):
-    """Assembled blocks of the condensed matrices (parts' "S") over the
-    interior modes of every mesh edge and face without Dirichlet dofs, as
-    PreconditionerBlock::BlockPreconditionerCG and the LowEnergy block step
-    gather them (PreconditionerLowEnergy.cpp:568-760): sign_i sign_j S_e[i, j]
-    summed over the elements sharing the entity, rows in global dof order.
-    Returns [(global dofs, inverse)], blocks of one dof left to Jacobi."""
+def entity_index(parts, bmap, bsign, ndir):
+    """The integer side of the entity blocks (PreconditionerBlock::
+    BlockPreconditionerCG and the LowEnergy block step gather them,
+    PreconditionerLowEnergy.cpp:568-760): every mesh edge and face with more
+    than one dof and no Dirichlet dof is one block, its rows its global dofs
+    in increasing order; blocks are numbered by size, then by first dof.
+    Returns (dofs, contributions): dofs[b] the global dofs of block b and,
+    per part, a list of (blocks, elements, rows, signs) arrays with one row
+    per contribution of an element to a block (rows: the element's boundary
+    rows in the block's row order; signs: the edge / face orientation
+    signs), one entry per block size."""
     groups = {}
     ob = 0
-    for p in parts:
+    for k, p in enumerate(parts):
         ne, nbm = p["ne"], p["bm"].size
         gb = bmap[ob:ob + ne * nbm].reshape(ne, nbm)
         sb = bsign[ob:ob + ne * nbm].reshape(ne, nbm)
@@ -272,33 +276,147 @@ def entity_blocks(parts, bmap, bsign, ndir):
             n = L.size
             if n < 2:
                 continue
-            order = np.argsort(gb[:, L], axis=1)
-            idx = L[order]
+            idx = L[np.argsort(gb[:, L], axis=1)]
             G = gb[er, idx]
-            sg = sb[er, idx]
             dirm = G < ndir
             if (dirm.any(axis=1) != dirm.all(axis=1)).any():
                 raise ValueError("an edge or face has Dirichlet and free dofs")
             keep = ~dirm[:, 0]
-            sub = p["S"][er[keep][:, :, None], idx[keep][:, :, None], idx[keep][:, None, :]]
-            sub = sub * (sg[keep][:, :, None] * sg[keep][:, None, :])
-            g = groups.setdefault(n, ([], [], []))
-            g[0].append(G[keep, 0])
-            g[1].append(G[keep])
-            g[2].append(sub)
-    blocks = []
+            groups.setdefault(n, []).append((k, er[keep, 0], G[keep], idx[keep],
+                                             sb[er, idx][keep].astype(np.int8)))
+    dofs = []
+    contrib = [[] for _ in parts]
     for n in sorted(groups):
-        keys = np.concatenate(groups[n][0])
-        G = np.concatenate(groups[n][1])
-        sub = np.concatenate(groups[n][2])
-        uk, first, inv = np.unique(keys, return_index=True, return_inverse=True)
+        G = np.concatenate([g[2] for g in groups[n]])
+        uk, first, inv = np.unique(G[:, 0], return_index=True, return_inverse=True)
         if (G != G[first][inv]).any():
             raise ValueError("entities with a shared first dof differ")
-        acc = np.zeros((uk.size, n, n))
-        np.add.at(acc, inv, sub)
-        for dofs, Minv in zip(G[first], np.linalg.inv(acc)):
-            blocks.append((dofs, Minv))
-    return blocks
+        base = len(dofs)
+        dofs.extend(G[first])
+        o = 0
+        for k, el, Gk, idx, sg in groups[n]:
+            contrib[k].append((base + inv[o:o + el.size], el, idx, sg))
+            o += el.size
+    return dofs, contrib
+
+
+def entity_blocks(parts, bmap, bsign, ndir):
+    """Assembled blocks of the condensed matrices (parts' "S", host) over the
+    blocks of entity_index: sign_i sign_j S_e[i, j] summed over the elements
+    sharing the entity. Returns [(global dofs, inverse)]; dofs outside every
+    block are left to Jacobi."""
+    dofs, contrib = entity_index(parts, bmap, bsign, ndir)
+    inv = [None] * len(dofs)
+    sizes = np.array([d.size for d in dofs])
+    for n in np.unique(sizes):
+        ids = np.flatnonzero(sizes == n)
+        acc = np.zeros((ids.size, n, n))
+        for p, entries in zip(parts, contrib):
+            for blk, el, idx, sg in entries:
+                if idx.shape[1] != n:
+                    continue
+                sub = p["S"][el[:, None, None], idx[:, :, None], idx[:, None, :]]
+                sgd = sg.astype(np.float64)
+                np.add.at(acc, blk - ids[0], sub * (sgd[:, :, None] * sgd[:, None, :]))
+        for b, Minv in zip(ids, np.linalg.inv(acc)):
+            inv[b] = Minv
+    return list(zip(dofs, inv))
+
+
+def _block_layout(dofs, device):
+    """bptr of entity_index's blocks and a zeroed device buffer for them
+    (n_b * n_b doubles each)."""
+    import torch
+    sizes = np.array([d.size for d in dofs], dtype=np.int64)
+    bptr = np.zeros(len(dofs) + 1, dtype=np.int32)
+    bptr[1:] = np.cumsum(sizes)
+    A = torch.zeros(int((sizes ** 2).sum()), dtype=torch.float64, device="cuda:%d" % device)
+    return bptr, A
+
+
+def contribution_arrays(entries, nblk):
+    """One part's contributions (entity_index) as nkb_blocks_accumulate takes
+    them: (cptr, celm, cloc, csgn), contributions grouped by block in a
+    stable order."""
+    blk = np.concatenate([e[0] for e in entries])
+    order = np.argsort(blk, kind="stable")  # contributions grouped by block
+    el = np.concatenate([e[1] for e in entries])[order].astype(np.int32)
+    # rows and signs of every contribution, padded to the widest block, put
+    # in that order and unpadded
+    nmax = max(e[2].shape[1] for e in entries)
+    rows = np.zeros((blk.size, nmax), dtype=np.int32)
+    sgns = np.zeros((blk.size, nmax), dtype=np.int8)
+    width = np.zeros(blk.size, dtype=np.int64)
+    o = 0
+    for b, _, idx, sg in entries:
+        rows[o:o + b.size, :idx.shape[1]] = idx
+        sgns[o:o + b.size, :idx.shape[1]] = sg
+        width[o:o + b.size] = idx.shape[1]
+        o += b.size
+    used = np.arange(nmax)[None, :] < width[order][:, None]
+    cloc = np.ascontiguousarray(rows[order][used])
+    csgn = np.ascontiguousarray(sgns[order][used])
+    cptr = np.searchsorted(blk[order], np.arange(nblk + 1)).astype(np.int32)
+    return cptr, el, cloc, csgn
+
+
+def _blocks_accumulate(bptr, A, p, S, entries, device):
+    """Adds one part's contributions (entity_index) from its condensed
+    matrices S (device tensor) to the blocks A (nkb_blocks_accumulate)."""
+    import ctypes
+
+    import nektar_b200 as nb
+    if not entries:
+        return
+    nblk = bptr.size - 1
+    cptr, el, cloc, csgn = contribution_arrays(entries, nblk)
+    ip = ctypes.POINTER(ctypes.c_int)
+    nb.check(nb.lib().nkb_blocks_accumulate(
+        nblk, bptr.ctypes.data_as(ip), int(el.size), cptr.ctypes.data_as(ip),
+        el.ctypes.data_as(ip), cloc.ctypes.data_as(ip),
+        csgn.ctypes.data_as(ctypes.POINTER(ctypes.c_byte)), p["ne"], p["bm"].size,
+        ctypes.c_void_p(S.data_ptr()), ctypes.c_void_p(A.data_ptr()), device, None))
+
+
+def _blocks_invert(bptr, A, device):
+    import ctypes
+
+    import nektar_b200 as nb
+    nb.check(nb.lib().nkb_blocks_invert(bptr.size - 1,
+                                        bptr.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                        ctypes.c_void_p(A.data_ptr()), device, None))
+
+
+def _condense_device(op, bm, im, R, device):
+    """(S, W, V) of an Operator's elements as device tensors: its element
+    matrices built on the device and condensed there (nkb_condense)."""
+    import ctypes
+
+    import torch
+
+    import nektar_b200 as nb
+    nc, ne = op.in_size // op.nelmt, op.nelmt
+    nbm, ni = len(bm), len(im)
+    dev = "cuda:%d" % device
+    K = torch.empty((ne, nc, nc), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    nb.check(nb.lib().nkb_op_element_matrices(op.h, ctypes.c_void_p(K.data_ptr()),
+                                              nb.DEVICE_PTRS, None))
+    S = torch.empty((ne, nbm, nbm), dtype=torch.float64, device=dev)
+    W = torch.empty((ne, nbm, nc), dtype=torch.float64, device=dev)
+    V = torch.empty((ne, nc, nbm + ni), dtype=torch.float64, device=dev)
+    bmi = np.ascontiguousarray(bm, dtype=np.int32)
+    imi = np.ascontiguousarray(im, dtype=np.int32)
+    Rc = None if R is None else np.ascontiguousarray(R, dtype=np.float64)
+    ip = ctypes.POINTER(ctypes.c_int)
+    nb.check(nb.lib().nkb_condense(ne, nc, ctypes.c_void_p(K.data_ptr()), nbm,
+                                   bmi.ctypes.data_as(ip), ni, imi.ctypes.data_as(ip),
+                                   None if Rc is None else Rc.ctypes.data_as(
+                                       ctypes.POINTER(ctypes.c_double)),
+                                   ctypes.c_void_p(S.data_ptr()), ctypes.c_void_p(W.data_ptr()),
+                                   ctypes.c_void_p(V.data_ptr()), device, None))
+    del K
+    return S, W, V
 
 
 def condense(K, bm, im):
@@ -337,23 +455,40 @@ def solve_maps(C, Kii_inv, Kib, bm, im, R=None):
 
 class StaticCondSys:
     """Statically condensed Helmholtz system over Helmholtz collection
-    operators (Operator) with the C0 map of the full local space. The set-up
-    (element matrices, condensation, low-energy transform, blocks) runs on the
-    host; a solve is three device steps: the right-hand side condensation
-    (per-element dense W), the CG on the condensed system, and the interior
-    back substitution (per-element dense V)."""
+    operators (Operator) with the C0 map of the full local space. A solve is
+    three device steps: the right-hand side condensation (per-element dense
+    W), the CG on the condensed system, and the interior back substitution
+    (per-element dense V).
+
+    The set-up (element matrices, condensation, the maps W and V) runs on the
+    device (setup="device": nkb_op_element_matrices into device memory, then
+    nkb_condense, the batched Cholesky condensation) or on the host
+    (setup="host": numpy, or when the element matrices are given); the
+    low-energy transform of a reference element and the block inverses of
+    the Block / LowEnergy preconditioners are built on the host."""
 
     def __init__(self, ops, gmap, nglob, ndir, sign=None, device=0, matrices=None,
-                 precon="diagonal", lam=None):
+                 precon="diagonal", lam=None, setup="device"):
         """precon: "diagonal", "block" or "lowenergy"; lam: the operators'
         Helmholtz lambda, which the low-energy reference element uses
         (default: the one last given to the operators' set_factors)."""
         import nektar_b200 as nb
         if precon not in ("diagonal", "block", "lowenergy"):
             raise ValueError("precon %r" % (precon,))
+        if setup not in ("device", "host"):
+            raise ValueError("setup %r" % (setup,))
         t0 = time.perf_counter()
         self.ops = list(ops)
         self.precon = precon
+        self.setup = "host" if matrices is not None else setup
+        # wall seconds of the set-up's phases
+        self.setup_breakdown = {}
+        tp = [t0]
+
+        def phase(name):
+            t = time.perf_counter()
+            self.setup_breakdown[name] = self.setup_breakdown.get(name, 0.0) + t - tp[0]
+            tp[0] = t
         self.parts = []
         gmap = np.asarray(gmap)
         sign = np.ones(gmap.size) if sign is None else np.asarray(sign, dtype=np.float64)
@@ -362,14 +497,12 @@ class StaticCondSys:
         for k, op in enumerate(self.ops):
             nc, ne = op.in_size // op.nelmt, op.nelmt
             bm, im = boundary_interior(op.shape, op.nm)
-            K = element_matrices(op) if matrices is None else matrices[k]
-            S, C, Kii_inv, Kib = condense(K, bm, im)
             gm = gmap[off:off + ne * nc].reshape(ne, nc)
             sg = sign[off:off + ne * nc].reshape(ne, nc)
             bglob.append(gm[:, bm].ravel())
             bsign.append(sg[:, bm].ravel())
-            self.parts.append(dict(nc=nc, ne=ne, bm=bm, im=im, S=S, C=C, Kii_inv=Kii_inv,
-                                   Kib=Kib, off=off, shape=op.shape, nm=op.nm, R=None))
+            self.parts.append(dict(nc=nc, ne=ne, bm=bm, im=im, off=off, shape=op.shape, nm=op.nm,
+                                   R=None))
             off += ne * nc
         self.nloc = off
         bglob = np.concatenate(bglob)
@@ -383,6 +516,7 @@ class StaticCondSys:
         self.bsign = np.concatenate(bsign)
         self.nglob_b, self.ndir = int(ids.size), int(ndir)
         self.nglob = int(nglob)
+        phase("maps")
         if precon == "lowenergy":
             if lam is None:
                 lam = getattr(self.ops[0], "lam", None)
@@ -396,26 +530,66 @@ class StaticCondSys:
             for p in self.parts:
                 R = Rs[p["shape"]]
                 p["R"], p["Rinv"] = R, np.linalg.inv(R)
-                p["S"] = R @ p["S"] @ R.T  # v_TransformedSchurCompl
-        blocks = None
-        if precon != "diagonal":
-            if (self.bsign == 0).any():
-                raise NotImplementedError("%s: meshes of variable order" % precon)
-            blocks = entity_blocks(self.parts, self.bmap, self.bsign, self.ndir)
-        self.nblocks = 0 if blocks is None else len(blocks)
+            phase("lowenergy_transform")
+        if precon != "diagonal" and (self.bsign == 0).any():
+            raise NotImplementedError("%s: meshes of variable order" % precon)
+        need_blocks = precon != "diagonal"
+        need_host_S = need_blocks and self.setup == "host"
+        if need_blocks and self.setup == "device":
+            dofs, contrib = entity_index(self.parts, self.bmap, self.bsign, self.ndir)
+            bptr, A = _block_layout(dofs, device)
+            phase("blocks")
         self.dense, self.W, self.V = [], [], []
-        for p in self.parts:
-            W, V = solve_maps(p.pop("C"), p.pop("Kii_inv"), p.pop("Kib"), p["bm"], p["im"],
-                              p["R"])
+        for k, (op, p) in enumerate(zip(self.ops, self.parts)):
+            if self.setup == "device":
+                S, W, V = _condense_device(op, p["bm"], p["im"], p["R"], device)
+                phase("condense")
+                if need_blocks:
+                    _blocks_accumulate(bptr, A, p, S, contrib[k], device)
+                    phase("blocks")
+                self.W.append(nb.DenseOperator.from_device(W, device=device))
+                self.V.append(nb.DenseOperator.from_device(V, device=device))
+                self.dense.append(nb.DenseOperator.from_device(S, device=device))
+                del S, W, V
+                phase("dense_operators")
+                continue
+            K = element_matrices(op) if matrices is None else matrices[k]
+            S, C, Kii_inv, Kib = condense(K, p["bm"], p["im"])
+            del K
+            if p["R"] is not None:
+                S = p["R"] @ S @ p["R"].T  # v_TransformedSchurCompl
+            W, V = solve_maps(C, Kii_inv, Kib, p["bm"], p["im"], p["R"])
+            del C, Kii_inv, Kib
             self.W.append(nb.DenseOperator(W, device=device))
             del W
             self.V.append(nb.DenseOperator(V, device=device))
             del V
-            self.dense.append(nb.DenseOperator(p.pop("S"), device=device))
+            if need_host_S:
+                p["S"] = S
+            self.dense.append(nb.DenseOperator(S, device=device))
+            del S
+            phase("condense")
+        blocks = None
+        if need_host_S:
+            blocks = entity_blocks(self.parts, self.bmap, self.bsign, self.ndir)
+            self.nblocks = len(blocks)
+        elif need_blocks:
+            if dofs:
+                _blocks_invert(bptr, A, device)
+            self.nblocks = len(dofs)
+        else:
+            self.nblocks = 0
+        for p in self.parts:
+            p.pop("S", None)
+        phase("blocks")
         self.sys = nb.GlobalLinSys(self.dense, self.bmap, self.nglob_b, self.ndir,
                                    sign=self.bsign, device=device)
         if blocks:
             self.sys.set_blocks(blocks)
+        elif need_blocks and self.nblocks:
+            self.sys.set_block_inverses(bptr, np.concatenate(dofs), A.data_ptr())
+            del A
+        phase("linsys")
         self.setup_s = time.perf_counter() - t0
 
     def _parts_of(self, v):

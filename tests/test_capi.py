@@ -76,3 +76,22 @@ def test_points_rejects_unknown_type():
     z = np.zeros(4)
     assert C.lib().nkb_points(1, 4, z.ctypes.data_as(C.dp), z.ctypes.data_as(C.dp),
                               None) == C.NKB_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("bm,im,msg", [
+    ([0, 1, 1], [2], b"bm is not part"),
+    ([0, 1], [1, 2], b"im is not part"),
+    ([0, 4], [1, 2], b"bm is not part"),
+    ([0, 1], [2, 3], b"bad arguments"),  # nb + ni != nc
+])
+def test_condense_rejects_index_lists_that_do_not_partition_the_modes(bm, im, msg):
+    """The boundary / interior split is checked on the host before any
+    device work (a dummy K pointer is never dereferenced)."""
+    ip = ctypes.POINTER(ctypes.c_int)
+    b = np.asarray(bm, dtype=np.int32)
+    i = np.asarray(im, dtype=np.int32)
+    dummy = ctypes.c_void_p(16)
+    nc = len(bm) + len(im) - (msg == b"bad arguments")
+    rc = C.lib().nkb_condense(4, nc, dummy, len(bm), b.ctypes.data_as(ip), len(im),
+                              i.ctypes.data_as(ip), None, dummy, dummy, dummy, 0, None)
+    assert rc == C.NKB_ERR_INVALID and msg in C.lib().nkb_last_error()

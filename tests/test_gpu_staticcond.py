@@ -147,3 +147,60 @@ def test_element_matrices_on_device_match_unit_applications(shape):
         x[j::nc] = 1.0
         assert np.array_equal(K[:, :, j], op(x).reshape(ne, nc))
     assert np.abs(K - K.transpose(0, 2, 1)).max() < 1e-13 * np.abs(K).max()
+
+
+@pytest.mark.parametrize("shape,n,nm", [("hex", 3, 5), ("hex", 2, 7), ("prism", 2, 5),
+                                        ("tet", 2, 4), ("hexprism", 2, 5)])
+@pytest.mark.parametrize("precon", ["diagonal", "block", "lowenergy"])
+def test_device_setup_matches_host_setup(shape, n, nm, precon):
+    """The device set-up (element matrices kept on the device, nkb_condense:
+    batched Cholesky, Schur complements and the W / V maps, the low-energy
+    transform folded in; the Block / LowEnergy entity blocks accumulated
+    and inverted there, nkb_blocks_accumulate / nkb_blocks_invert) gives the
+    host set-up's condensed operators, preconditioned iterations and
+    solutions."""
+    from nektar_b200.meshgraph import SessionMesh
+    from nektar_b200.session import read_session, write_box_session
+    U = "sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)"
+    F = "-(Lambda + 3*PI*PI/4)*sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)"
+    s = read_session(write_box_session(shape, n, nm - 1, 1.0, U, F, U, shuffle_seed=5))
+    mesh = SessionMesh(s)
+    ops = []
+    for c in mesh.collections:
+        H = nb.Operator("helmholtz", c)
+        H.set_factors(1.0)
+        ops.append(H)
+    b = np.random.default_rng(nm).uniform(-1, 1, mesh.nloc)
+    x0 = mesh.dirichlet_local()
+    kw = dict(sign=mesh.sign, precon=precon, lam=1.0)
+    host = StaticCondSys(ops, mesh.gmap, mesh.nglob, mesh.ndir, setup="host", **kw)
+    dev = StaticCondSys(ops, mesh.gmap, mesh.nglob, mesh.ndir, setup="device", **kw)
+    rng = np.random.default_rng(1)
+    for group in ("dense", "W", "V"):
+        for dh, dd in zip(getattr(host, group), getattr(dev, group)):
+            x = rng.uniform(-1, 1, dh.in_size)
+            assert rel_l2(dd(x), dh(x)) < 1e-11, group
+    xh, rh = host.solve(b, x0, tol=1e-12)
+    xd, rd = dev.solve(b, x0, tol=1e-12)
+    assert rd.converged and rel_l2(xd, xh) < 1e-10
+    assert abs(rd.iterations - rh.iterations) <= 2
+
+
+def test_device_condensation_rejects_an_indefinite_interior_block():
+    import ctypes
+    ne, nc = 2, 4
+    K = -np.tile(np.eye(nc), (ne, 1, 1))  # negative definite
+    import torch
+    Kd = torch.tensor(K, device="cuda")
+    S = torch.empty((ne, 2, 2), dtype=torch.float64, device="cuda")
+    W = torch.empty((ne, 2, 4), dtype=torch.float64, device="cuda")
+    V = torch.empty((ne, 4, 4), dtype=torch.float64, device="cuda")
+    bm = np.array([0, 3], dtype=np.int32)
+    im = np.array([1, 2], dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    rc = nb.lib().nkb_condense(ne, nc, ctypes.c_void_p(Kd.data_ptr()), 2, bm.ctypes.data_as(ip), 2,
+                               im.ctypes.data_as(ip), None, ctypes.c_void_p(S.data_ptr()),
+                               ctypes.c_void_p(W.data_ptr()), ctypes.c_void_p(V.data_ptr()), 0,
+                               None)
+    assert rc == nb.C.NKB_ERR_INVALID
+    assert b"positive definite" in nb.lib().nkb_last_error()

@@ -405,3 +405,59 @@ def test_prism_lowenergy_is_conforming_and_preconditions(shape):
         ev = np.linalg.eigvalsh(L.T @ A @ L)
         kappa[name] = ev[-1] / ev[0]
     assert kappa["lowenergy"] < 0.5 * kappa["jacobi"]
+
+
+def _gauss_jordan_colmajor(M):
+    """The in-place Gauss-Jordan inversion of nkb_blocks_invert (no pivoting,
+    normalised pivot row, column k stashed before the update), then the
+    transpose it ends with."""
+    M = M.copy()
+    n = M.shape[0]
+    for k in range(n):
+        pinv = 1.0 / M[k, k]
+        col = M[:, k].copy()
+        row = M[k, :] * pinv
+        row[k] = pinv
+        upd = M.copy()
+        upd[:, k] = 0.0
+        M = upd - np.outer(col, row)
+        M[k, :] = row
+    return M.T
+
+
+@pytest.mark.parametrize("case", ["hex", "prism", "hexprism"])
+def test_device_block_inputs_reproduce_entity_blocks(case):
+    """What the device builds the Block / LowEnergy blocks from: the
+    contribution arrays (blocks, elements, rows in block order, signs),
+    summed in their order as nkb_blocks_accumulate does, and inverted as
+    nkb_blocks_invert does, give entity_blocks' inverses, in the column-major
+    layout that nkb_sys_set_blocks takes."""
+    from nektar_b200.staticcond import contribution_arrays, entity_blocks, entity_index
+    if case == "hex":
+        d = _rotated_hex_condensed(nm=6, n=3)
+        parts = [dict(S=d["S"], ne=d["ne"], bm=d["bm"], shape="hex", nm=d["nm"])]
+        bmap, bsign, nd = d["bmap"], d["bsign"], d["ndir"]
+    else:
+        parts, bmap, bsign, _, nd = _session_parts(case, 5, 2, 1.3, 6)
+    dofs, contrib = entity_index(parts, bmap, bsign, nd)
+    ref = entity_blocks(parts, bmap, bsign, nd)
+    assert len(ref) == len(dofs) > 0
+    sizes = np.array([x.size for x in dofs])
+    A = [np.zeros((n, n)) for n in sizes]
+    for p, entries in zip(parts, contrib):
+        if not entries:
+            continue
+        cptr, celm, cloc, csgn = contribution_arrays(entries, len(dofs))
+        assert cptr[0] == 0 and cptr[-1] == celm.size and (np.diff(cptr) >= 0).all()
+        off = 0
+        for b in range(len(dofs)):
+            n = sizes[b]
+            for c in range(cptr[b], cptr[b + 1]):
+                l, sg = cloc[off:off + n], csgn[off:off + n].astype(np.float64)
+                A[b] += np.outer(sg, sg) * p["S"][celm[c]][np.ix_(l, l)]
+                off += n
+        assert off == cloc.size
+    for (rd, rinv), dd, a in zip(ref, dofs, A):
+        assert np.array_equal(rd, dd)
+        inv_cm = _gauss_jordan_colmajor(a)
+        assert np.allclose(inv_cm.T, rinv, rtol=1e-10, atol=1e-13 * np.abs(rinv).max())
