@@ -463,6 +463,75 @@ int nkb_sys_profile_iteration(nkb_sys *sys, int iters, nkb_sys_profile *prof);
 
 void nkb_sys_destroy(nkb_sys *sys);
 
+/* ---- sharded solve ---------------------------------------------------------
+ * The CG of GlobalLinSysIterativeFull + NekLinSysIterCG sharded by element
+ * partition (MeshPartition.cpp:99), every vector on the device: per
+ * iteration the shared dofs are summed across the shards
+ * (AssemblyMapCG::UniversalAssemble, AssemblyMapCG.cpp:2894-2906) and the
+ * three dot products in one all-reduce (NekLinSysIterCG.cpp:310). A shard is
+ * an nkb_sys over its partition's elements whose global dofs are numbered
+ *   [Dirichlet | free, this shard only (nint) | free shared, owned | free
+ *   shared, owned by another shard]   (nown = nint + the owned shared ones)
+ * A dof shared by several shards is owned by one of them (the lowest rank),
+ * which alone counts it in dot products. */
+
+/* NCCL communicator of a sharded solve: one rank per GPU. The library binds
+ * libnccl.so.2 at the first call (the copy the process has loaded, else the
+ * system's); NKB_ERR_UNSUPPORTED when there is none. A process that also
+ * loads another NCCL under that name (torch does) must load it first.
+ * Rank 0 makes the id (128 bytes), which the caller passes to every rank. */
+typedef struct nkb_comm nkb_comm;
+int nkb_comm_unique_id(unsigned char *id);
+int nkb_comm_create(const unsigned char *id, int nranks, int rank, int device, nkb_comm **comm);
+void nkb_comm_destroy(nkb_comm *comm);
+
+typedef struct nkb_shard_plan
+{
+    int rank;                       /* this shard (0..nranks-1) */
+    int nint;                       /* free dofs no other shard touches */
+    int nown;                       /* free dofs this shard counts in dot products */
+    const unsigned char *dir_owned; /* ndir flags: Dirichlet dofs this shard counts in |b|^2
+                                       (NULL: all) */
+    int nshared;                    /* dofs (Dirichlet or free) shared with other shards */
+    const int *shared;              /* their indices in this shard's global numbering */
+    const int *sptr;                /* nshared+1: the sources of each shared dof */
+    const int *ssrc;                /* its sharing shards' values in rank order: -1 this
+                                       shard's own, else a position in the receive buffer */
+    int nnbr;                       /* shards that share dofs with this one */
+    const int *nbr;                 /* their ranks, increasing */
+    const int *nptr;                /* nnbr+1: each neighbour's slice of the send and the
+                                       receive buffer */
+    const int *nidx;                /* the dofs sent to each neighbour (this shard's numbering),
+                                       in increasing mesh-wide global id: the neighbour's
+                                       receive slice holds its values of the same dofs in the
+                                       same order */
+} nkb_shard_plan;
+
+typedef struct nkb_shard_group nkb_shard_group;
+
+/* A sharded system. With comm: this process's one shard (nlocal = 1,
+ * plans[0].rank = the communicator's rank); exchanges by ncclSend/ncclRecv
+ * with every neighbour in one NCCL group, the dot sums by one ncclAllReduce.
+ * Without comm: nlocal shards of ranks 0..nlocal-1 in this process on one
+ * device (the sharded recurrence on one GPU); exchanges by device copies.
+ * The systems' Jacobi diagonals are summed at the shared dofs; from then on
+ * the systems solve only through a group (FP64, Jacobi; no clones, blocks or
+ * mixed precision), also after the group is destroyed. Host plan arrays,
+ * copied. */
+int nkb_shard_group_create(nkb_sys *const *systems, const nkb_shard_plan *plans, int nlocal,
+                           nkb_comm *comm, nkb_shard_group **group);
+
+/* One solve of every local shard (b_locs[i], x_locs[i] as nkb_cg_solve's
+ * b_loc / x_loc of shard i; flags NKB_HOST_PTRS or NKB_DEVICE_PTRS);
+ * synchronous. All shards hold the same iterations, residual and, at the
+ * shared dofs, the same solution bits. */
+int nkb_shard_group_solve(nkb_shard_group *group, const double *const *b_locs,
+                          double *const *x_locs, const nkb_cg_opts *opts, nkb_cg_report *reps,
+                          int flags);
+
+/* Releases the group (before its communicator and its systems). */
+void nkb_shard_group_destroy(nkb_shard_group *group);
+
 /* ---- structured test meshes (FP64 setup, host) ---------------------------
  * Unit-cube box of n^3 cells, optionally curved by
  *   x' = x + amp * sin(pi x) sin(pi y) sin(pi z) in every coordinate,

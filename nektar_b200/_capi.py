@@ -59,6 +59,13 @@ class CGReport(ctypes.Structure):
                 ("restarts", c_int)]
 
 
+class ShardPlan(ctypes.Structure):
+    _fields_ = [("rank", c_int), ("nint", c_int), ("nown", c_int),
+                ("dir_owned", P(ctypes.c_ubyte)), ("nshared", c_int), ("shared", ip),
+                ("sptr", ip), ("ssrc", ip), ("nnbr", c_int), ("nbr", ip), ("nptr", ip),
+                ("nidx", ip)]
+
+
 class SysProfile(ctypes.Structure):
     _fields_ = [("op_ms", c_double), ("assemble_ms", c_double), ("update_ms", c_double),
                 ("scalars_ms", c_double), ("op_bytes", c_double), ("op_flops", c_double)]
@@ -107,6 +114,14 @@ SIGNATURES = {
     "nkb_sys_diag_inv": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "nkb_sys_profile_iteration": (c_int, [c_void_p, c_int, P(SysProfile)]),
     "nkb_sys_destroy": (None, [c_void_p]),
+    "nkb_comm_unique_id": (c_int, [P(ctypes.c_ubyte)]),
+    "nkb_comm_create": (c_int, [P(ctypes.c_ubyte), c_int, c_int, c_int, P(c_void_p)]),
+    "nkb_comm_destroy": (None, [c_void_p]),
+    "nkb_shard_group_create": (c_int, [P(c_void_p), P(ShardPlan), c_int, c_void_p,
+                                       P(c_void_p)]),
+    "nkb_shard_group_solve": (c_int, [c_void_p, P(c_void_p), P(c_void_p), P(CGOpts),
+                                      P(CGReport), c_int]),
+    "nkb_shard_group_destroy": (None, [c_void_p]),
     "nkb_batch_create": (c_int, [P(c_void_p), c_int, c_int, P(c_void_p)]),
     "nkb_batch_sizes": (c_int, [c_void_p, P(c_long), P(c_long)]),
     "nkb_batch_apply": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),

@@ -26,7 +26,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC"]
 
 SOURCES = ["nkb_setup.cpp", "nkb_ops.cu", "nkb_hex.cu", "nkb_hex_f64.cu", "nkb_hex_f32.cu",
            "nkb_cg.cu", "nkb_static.cu", "nkb_batch.cu", "nkb_dense.cu", "nkb_gen_f64.cu",
-           "nkb_gen_f32.cu", "nkb_col_f64.cu", "nkb_col_f32.cu", "nkb_tc.cu", "nkb_sc.cu"]
+           "nkb_gen_f32.cu", "nkb_col_f64.cu", "nkb_col_f32.cu", "nkb_tc.cu", "nkb_sc.cu", "nkb_nccl.cpp"]
 
 
 def _nvcc():
@@ -77,7 +77,7 @@ def build(force=False, verbose=False, jobs=None):
         raise RuntimeError("nektar_b200 build failed")
     if force or cmds or not os.path.exists(LIB) or any(
             os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda"]
+        cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda", "-ldl"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)

@@ -80,10 +80,13 @@ __device__ __forceinline__ void BlockSum2(double a, double b, double *part)
     }
 }
 
+// the partial dot products count the free dofs i < nown only (all of them on
+// one GPU; a shard's own dofs, numbered first, in a sharded solve)
 template <typename T>
 __global__ void k_update(int nn, int ndir, const CGState *st, T *__restrict__ p, T *__restrict__ q,
                          T *__restrict__ x, T *__restrict__ r, T *__restrict__ w,
-                         const T *__restrict__ s, const T *__restrict__ dinv, double *part)
+                         const T *__restrict__ s, const T *__restrict__ dinv, double *part,
+                         int nown)
 {
     if (st->done)
         return;
@@ -100,16 +103,20 @@ __global__ void k_update(int nn, int ndir, const CGState *st, T *__restrict__ p,
         r[i]       = ri;
         const T wi = ri * dinv[i];
         w[ndir + i] = wi;
-        rw += double(ri) * double(wi);
-        rr += double(ri) * double(ri);
+        if (i < nown)
+        {
+            rw += double(ri) * double(wi);
+            rr += double(ri) * double(ri);
+        }
     }
     BlockSum2(rw, rr, part);
 }
 
 // w = diag^-1 r on the non-Dirichlet part, with (r,w) and (r,r) partials
+// over the free dofs i < nown
 template <typename T>
 __global__ void k_precon(int nn, int ndir, const CGState *st, const T *__restrict__ r,
-                         T *__restrict__ w, const T *__restrict__ dinv, double *part)
+                         T *__restrict__ w, const T *__restrict__ dinv, double *part, int nown)
 {
     if (st->done)
         return;
@@ -118,8 +125,11 @@ __global__ void k_precon(int nn, int ndir, const CGState *st, const T *__restric
     {
         const T wi = r[i] * dinv[i];
         w[ndir + i] = wi;
-        rw += double(r[i]) * double(wi);
-        rr += double(r[i]) * double(r[i]);
+        if (i < nown)
+        {
+            rw += double(r[i]) * double(wi);
+            rr += double(r[i]) * double(r[i]);
+        }
     }
     BlockSum2(rw, rr, part);
 }
@@ -208,11 +218,14 @@ __global__ void __launch_bounds__(kRedThreads)
     }
 }
 
+// glob = assembled loc; (glob, w) partial over the dofs ndir <= g < ndir + nsw
+// (every free dof on one GPU; a shard's dofs that no other shard touches in a
+// sharded solve, whose assembled values are complete there)
 template <typename T>
 __global__ void k_assemble(int nglob, int ndir, const int *__restrict__ aptr,
                            const int *__restrict__ aidx, const double *__restrict__ sign,
                            const T *__restrict__ loc, T *__restrict__ glob,
-                           const T *__restrict__ w, const CGState *st, double *part)
+                           const T *__restrict__ w, const CGState *st, double *part, int nsw)
 {
     if (st && st->done)
         return;
@@ -227,7 +240,7 @@ __global__ void k_assemble(int nglob, int ndir, const int *__restrict__ aptr,
             acc += sign ? T(sign[l]) * loc[l] : loc[l];
         }
         glob[g] = acc;
-        if (w && g >= ndir)
+        if (w && g >= ndir && g - ndir < nsw)
             sw += double(acc) * double(w[g]);
     }
     if (part)
@@ -288,19 +301,9 @@ __device__ double ReducePart(const double *part, int nb, int which)
 // mode 1: first direction:  rho = (r,w) partA[0], mu = (s,w) partB[0]; alpha = rho/mu
 // mode 2: iteration:        rho_new, eps from partA, mu from partB
 // mode 3: restart of the recurrence after a reliable update (mixed precision)
-// partC (nbC > 0): the block preconditioner's corrections of (r,w)
-__global__ void k_scalars(CGState *st, const double *partA, int nbA, const double *partB, int nbB,
-                          int mode, const double *partC = nullptr, int nbC = 0)
+// (a0, a1, b0: the sums of partA[0], partA[1], partB[0]; one thread)
+__device__ void ScalarStep(CGState *st, double a0, double a1, double b0, int mode)
 {
-    if (st->done)
-        return;
-    double a0 = ReducePart(partA, nbA, 0);
-    if (nbC)
-        a0 += ReducePart(partC, nbC, 0);
-    const double a1 = ReducePart(partA, nbA, 1);
-    const double b0 = ReducePart(partB, nbB, 0);
-    if (threadIdx.x != 0)
-        return;
     if (mode == 0)
     {
         st->eps     = a1;
@@ -374,15 +377,30 @@ __global__ void k_scalars(CGState *st, const double *partA, int nbA, const doubl
     }
 }
 
+// partC (nbC > 0): the block preconditioner's corrections of (r,w)
+__global__ void k_scalars(CGState *st, const double *partA, int nbA, const double *partB, int nbB,
+                          int mode, const double *partC = nullptr, int nbC = 0)
+{
+    if (st->done)
+        return;
+    double a0 = ReducePart(partA, nbA, 0);
+    if (nbC)
+        a0 += ReducePart(partC, nbC, 0);
+    const double a1 = ReducePart(partA, nbA, 1);
+    const double b0 = ReducePart(partB, nbB, 0);
+    if (threadIdx.x != 0)
+        return;
+    ScalarStep(st, a0, a1, b0, mode);
+}
+
 __global__ void k_init(int nglob, int ndir, const double *__restrict__ bglob, double *r, double *x,
-                       double *w, double *s, double *p, double *q, double *part)
+                       double *w, double *s, double *p, double *q, double *part,
+                       const unsigned char *__restrict__ dcnt, int nown)
 {
     double rr = 0.0, bb = 0.0;
-    const int nn = nglob - ndir;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nglob; g += gridDim.x * blockDim.x)
     {
         const double b = bglob[g];
-        bb += b * b;
         x[g] = 0.0;
         w[g] = 0.0;
         s[g] = 0.0;
@@ -391,10 +409,15 @@ __global__ void k_init(int nglob, int ndir, const double *__restrict__ bglob, do
             r[g - ndir] = b;
             p[g - ndir] = 0.0;
             q[g - ndir] = 0.0;
-            rr += b * b;
+            if (g - ndir < nown)
+            {
+                bb += b * b;
+                rr += b * b;
+            }
         }
+        else if (!dcnt || dcnt[g])
+            bb += b * b;
     }
-    (void)nn;
     BlockSum2(bb, rr, part);
 }
 
@@ -542,6 +565,10 @@ struct SysShared
     double *d_bmat = nullptr;
     size_t bytes = 0;
     std::mutex mu; // guards the lazy split diagonal
+    // a shard of a sharded group (nkb_shard_group_create): its diagonal
+    // parts hold the whole mesh's values at the shared dofs, and it solves
+    // only through the group
+    bool grouped = false;
 
     ~SysShared()
     {
@@ -672,13 +699,13 @@ static int Iteration32(nkb_sys *S, cudaStream_t s)
     const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
     S->launches += 3 + long(S->ops32.size());
     k_update<float><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st32, S->p32, S->q32, S->x32,
-                                                S->r32, S->w32, S->s32, S->dinv32, S->partA);
+                                                S->r32, S->w32, S->s32, S->dinv32, S->partA, S->nn);
     int rc = Matvec32(S, S->w32, S->yl32, s, &S->st32->done);
     if (rc)
         return rc;
     k_assemble<float><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
                                                   S->d_sign, S->yl32, S->s32, S->w32, S->st32,
-                                                  S->partB);
+                                                  S->partB, S->nn);
     k_scalars<<<1, 1024, 0, s>>>(S->st32, S->partA, nbU, S->partB, nbA, 2);
     NKB_CUDA_TRY(cudaGetLastError());
     return NKB_OK;
@@ -711,13 +738,13 @@ static int Iteration(nkb_sys *S, cudaStream_t s)
     const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
     S->launches += 3 + long(S->ops.size());
     k_update<double><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st, S->p, S->q, S->x, S->r,
-                                                 S->w, S->s, S->d_dinv, S->partA);
+                                                 S->w, S->s, S->d_dinv, S->partA, S->nn);
     BlockPrecon(S, s);
     int rc = Matvec(S, S->w, S->yl, true, s, &S->st->done);
     if (rc)
         return rc;
     k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
-                                                   S->d_sign, S->yl, S->s, S->w, S->st, S->partB);
+                                                   S->d_sign, S->yl, S->s, S->w, S->st, S->partB, S->nn);
     k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbU, S->partB, nbA, 2, S->partC, S->nbC);
     NKB_CUDA_TRY(cudaGetLastError());
     return NKB_OK;
@@ -1087,6 +1114,8 @@ extern "C" int nkb_sys_set_blocks(nkb_sys *S, int nblk, const int *bptr, const i
         return SetError(NKB_ERR_INVALID, "nkb_sys_set_blocks: set the blocks before cloning");
     if (h.nblk)
         return SetError(NKB_ERR_INVALID, "nkb_sys_set_blocks: blocks already set");
+    if (h.grouped)
+        return SetError(NKB_ERR_UNSUPPORTED, "nkb_sys_set_blocks: a shard of a sharded group");
     if (bptr[0] != 0)
         return SetError(NKB_ERR_INVALID, "nkb_sys_set_blocks: bptr[0] = %d", bptr[0]);
     std::vector<long> boff(nblk);
@@ -1190,7 +1219,7 @@ extern "C" int nkb_sys_assemble(nkb_sys *S, const double *loc, double *glob, voi
     NKB_CUDA_TRY(cudaSetDevice(S->device));
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : S->stream;
     k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, s>>>(
-        S->nglob, S->ndir, S->d_aptr, S->d_aidx, S->d_sign, loc, glob, nullptr, nullptr, nullptr);
+        S->nglob, S->ndir, S->d_aptr, S->d_aidx, S->d_sign, loc, glob, nullptr, nullptr, nullptr, S->nn);
     NKB_CUDA_TRY(cudaGetLastError());
     return NKB_OK;
 }
@@ -1278,17 +1307,17 @@ static int Begin64(nkb_sys *S)
         return rc;
     const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
     k_init<<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->bglob, S->r, S->x, S->w, S->s, S->p,
-                                       S->q, S->partA);
+                                       S->q, S->partA, nullptr, S->nn);
     // partA holds (b,b) in [0] and (r,r) in [1]; k_scalars mode 0 reads eps
     // from partA[1] and rhs from partB[0]
     k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbA, S->partA, nbA, 0);
     k_precon<double><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st, S->r, S->w, S->d_dinv,
-                                                 S->partA);
+                                                 S->partA, S->nn);
     BlockPrecon(S, s);
     if ((rc = Matvec(S, S->w, S->yl, true, s)))
         return rc;
     k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
-                                                   S->d_sign, S->yl, S->s, S->w, S->st, S->partB);
+                                                   S->d_sign, S->yl, S->s, S->w, S->st, S->partB, S->nn);
     k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbU, S->partB, nbA, 1, S->partC, S->nbC);
     NKB_CUDA_TRY(cudaGetLastError());
     S->launches += 5 + long(S->ops.size());
@@ -1357,7 +1386,7 @@ static int BeginMixed(nkb_sys *S)
         return rc;
     const int nbA = Blocks(S->nglob);
     k_init<<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->bglob, S->r, S->x, S->w, S->s, S->p,
-                                       S->q, S->partA);
+                                       S->q, S->partA, nullptr, S->nn);
     k_scalars<<<1, 1024, 0, s>>>(S->st, S->partA, nbA, S->partA, nbA, 0);
     S->launches += 2;
     if ((rc = EnsureGraph(S, true, s, v.o.check_interval)))
@@ -1384,13 +1413,13 @@ static int Launch32Start(nkb_sys *S, double eps, bool reset, double reduction)
     k_resume<<<1, 1, 0, s>>>(S->st32, std::fmax(reduction * reduction * eps, v.thr_final),
                              std::max(v.o.maxit - v.iter_base, 1), reset ? 1 : 0);
     k_precon<float><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st32, S->r32, S->w32, S->dinv32,
-                                                S->partA);
+                                                S->partA, S->nn);
     int rc = Matvec32(S, S->w32, S->yl32, s, &S->st32->done);
     if (rc)
         return rc;
     k_assemble<float><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
                                                   S->d_sign, S->yl32, S->s32, S->w32, S->st32,
-                                                  S->partB);
+                                                  S->partB, S->nn);
     k_scalars<<<1, 1024, 0, s>>>(S->st32, S->partA, nbU, S->partB, nbA, reset ? 1 : 3);
     NKB_CUDA_TRY(cudaGetLastError());
     S->launches += (reset ? 5 : 4) + long(S->ops32.size());
@@ -1451,7 +1480,7 @@ static int StepRun32(nkb_sys *S)
         return rc;
     k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
                                                    S->d_sign, S->yl, S->s, nullptr, nullptr,
-                                                   nullptr);
+                                                   nullptr, S->nn);
     k_residual<<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->bglob, S->s, S->r, S->r32, S->partA);
     k_scalars_outer<<<1, 1024, 0, s>>>(S->st, S->partA, nbU);
     NKB_CUDA_TRY(cudaGetLastError());
@@ -1523,6 +1552,9 @@ extern "C" int nkb_cg_begin(nkb_sys *S, const double *b_loc, double *x_loc,
                                          "(nkb_sys_desc.ops32)");
     if (o.mixed && S->sh->nblk)
         return SetError(NKB_ERR_UNSUPPORTED, "nkb_cg_begin: the block preconditioner is FP64 only");
+    if (S->sh->grouped)
+        return SetError(NKB_ERR_INVALID, "nkb_cg_begin: a shard of a sharded group solves through "
+                                         "nkb_shard_group_solve");
     NKB_CUDA_TRY(cudaSetDevice(S->device));
     SolveCtx &v = S->sv;
     v           = SolveCtx();
@@ -1559,7 +1591,7 @@ extern "C" int nkb_cg_begin(nkb_sys *S, const double *b_loc, double *x_loc,
         k_sub_loc<<<Blocks(nloc), kRedThreads, 0, s>>>(nloc, db, S->yl, S->tl);
         k_assemble<double><<<Blocks(S->nglob), kRedThreads, 0, s>>>(
             S->nglob, S->ndir, S->d_aptr, S->d_aidx, S->d_sign, S->tl, S->bglob, nullptr, nullptr,
-            nullptr);
+            nullptr, S->nn);
         S->launches += 2 + long(S->ops.size());
         rc = o.mixed ? BeginMixed(S) : Begin64(S);
     }
@@ -1700,7 +1732,7 @@ extern "C" int nkb_sys_profile_iteration(nkb_sys *S, int iters, nkb_sys_profile 
     for (int it = 0; it < iters; ++it)
         k_assemble<double><<<nbA, kRedThreads, 0, s>>>(S->nglob, S->ndir, S->d_aptr, S->d_aidx,
                                                        S->d_sign, S->yl, S->s, S->w, S->st,
-                                                       S->partB);
+                                                       S->partB, S->nn);
     NKB_CUDA_TRY(cudaEventRecord(e[2], s));
     // the update kernel with alpha = beta = 0 leaves x unchanged and w = dinv r
     CGState zero = run;
@@ -1710,7 +1742,7 @@ extern "C" int nkb_sys_profile_iteration(nkb_sys *S, int iters, nkb_sys_profile 
     NKB_CUDA_TRY(cudaEventRecord(e[2], s));
     for (int it = 0; it < iters; ++it)
         k_update<double><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st, S->p, S->q, S->x,
-                                                     S->r, S->w, S->s, S->d_dinv, S->partA);
+                                                     S->r, S->w, S->s, S->d_dinv, S->partA, S->nn);
     NKB_CUDA_TRY(cudaEventRecord(e[3], s));
     NKB_CUDA_TRY(cudaStreamSynchronize(s));
     cudaEvent_t e4, e5;
@@ -1783,3 +1815,5 @@ extern "C" void nkb_sys_destroy(nkb_sys *S)
     S->sh.reset(); // the shared map and diagonal go with the last user
     delete S;
 }
+
+#include "nkb_cg_shard.cuh"

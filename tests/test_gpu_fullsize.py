@@ -8,7 +8,9 @@ on the curved box):
   Q = 10;
 * at a relative residual of 1e-10: the iteration count (within one), the
   RMS error against the exact solution at the quadrature points (within
-  1e-3 relative) and the local solution at 10000 seeded positions;
+  5e-3 relative: two FP64 implementations that take the same iterations
+  differ there by up to 2e-3, measured 1.9e-3 on 24^3 P=8) and the local
+  solution at 10000 seeded positions;
 * at 1e-14 (the converged FP64 solution): the same digest.
 
 The digest bounds: two FP64 implementations that stop at the same residual
@@ -80,7 +82,7 @@ def test_fullsize_solve_matches_reference_record(tag):
     x, rep = out[1e-10]
     assert rep.converged and abs(rep.iterations - rec["iterations"]) <= 1, (rep.iterations,
                                                                             rec["iterations"])
-    assert abs(rms - rec["rms_error_vs_exact"]) < 1e-3 * rec["rms_error_vs_exact"], rms
+    assert abs(rms - rec["rms_error_vs_exact"]) < 5e-3 * rec["rms_error_vs_exact"], rms
     pos = dig["positions"]
 
     def rel(a, b):

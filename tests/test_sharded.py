@@ -122,3 +122,87 @@ def test_two_gloo_ranks_match_one_rank():
         lo, hi, x, it = res[r]
         assert np.abs(x - x1[lo * nc:hi * nc]).max() < 1e-10 * np.abs(x1).max()
         assert abs(it - it1) <= max(5, it1 // 20)  # sums in another order near tol 1e-12
+
+
+def _box(n=3, nm=5):
+    import nektar_b200 as nb
+    m = nb.BoxMesh("hex", n, nm, nm + 1, amp=0.05)
+    gmap, nglob, ndir = m.assembly()
+    return m, np.asarray(gmap), nglob, ndir
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 4, 5, 7])
+def test_shard_plans_number_own_and_pair_every_dof(world):
+    """Each rank's numbering covers the dofs its elements touch (Dirichlet,
+    then its own free dofs, then the shared free dofs it owns, then the
+    others'); every dof is owned once; two neighbours list the same shared
+    dofs in the same order; a shared dof has one source per sharing rank,
+    its own value once. 27 elements over 4, 5 or 7 ranks give partitions that
+    end mid-layer."""
+    from nektar_b200.sharded import shard_plans
+    m, gmap, nglob, ndir = _box()
+    nc = m.nc
+    plans = shard_plans(gmap, ndir, world, nc=nc)
+    owners = np.zeros(nglob, dtype=np.int64)
+    touch = np.zeros(nglob, dtype=np.int64)
+    for p in plans:
+        gid, nd, nint, nown = p["gid"], p["ndir"], p["nint"], p["nown"]
+        assert np.array_equal(gid[p["lmap"]], gmap[p["lo"] * nc:p["hi"] * nc])
+        assert np.unique(gid).size == gid.size
+        assert (gid[:nd] < ndir).all() and (gid[nd:] >= ndir).all()
+        touch[gid] += 1
+        owners[gid[nd:nd + nown]] += 1
+        owners[gid[:nd][p["dir_owned"].astype(bool)]] += 1
+    assert (owners == 1).all()
+    for p in plans:
+        gid, nd, nint = p["gid"], p["ndir"], p["nint"]
+        assert (touch[gid[nd:nd + nint]] == 1).all()
+        assert (touch[gid[nd + nint:]] > 1).all()
+        sh = p["shared"]
+        assert set(sh.tolist()) == set(np.flatnonzero(touch[gid] > 1).tolist())
+        nsrc = np.diff(p["sptr"])
+        assert np.array_equal(nsrc, touch[gid[sh]])
+        for k in range(sh.size):
+            src = p["ssrc"][p["sptr"][k]:p["sptr"][k + 1]]
+            assert (src == -1).sum() == 1
+        for k, q in enumerate(p["nbr"]):
+            pq = plans[q]
+            kk = list(pq["nbr"]).index(p["rank"])
+            mine = gid[p["nidx"][p["nptr"][k]:p["nptr"][k + 1]]]
+            theirs = pq["gid"][pq["nidx"][pq["nptr"][kk]:pq["nptr"][kk + 1]]]
+            assert np.array_equal(mine, theirs) and (np.diff(mine) > 0).all()
+
+
+@pytest.mark.parametrize("world", [2, 3, 5])
+def test_plan_exchange_gives_every_rank_the_assembled_vector(world):
+    """Rank-local assembles of a local vector, exchanged through the plans
+    (each rank's send slice into its neighbours' receive slices) and summed
+    in rank order, equal the whole mesh's assembled vector at every rank's
+    dofs, and carry the same bits on every rank that shares a dof."""
+    from nektar_b200.sharded import shard_plans, unpack
+    m, gmap, nglob, ndir = _box()
+    nc = m.nc
+    y = np.random.default_rng(world).uniform(-1, 1, gmap.size)
+    full = np.zeros(nglob)
+    np.add.at(full, gmap, y)
+    plans = shard_plans(gmap, ndir, world, nc=nc)
+    part, send = [], []
+    for p in plans:
+        v = np.zeros(p["nglob"])
+        np.add.at(v, p["lmap"].astype(np.int64), y[p["lo"] * nc:p["hi"] * nc])
+        part.append(v)
+        send.append(v[p["nidx"]])
+    done = []
+    for p, v in zip(plans, part):
+        recv = np.zeros(send[p["rank"]].size)
+        for k, q in enumerate(p["nbr"]):
+            pq = plans[q]
+            kk = list(pq["nbr"]).index(p["rank"])
+            recv[p["nptr"][k]:p["nptr"][k + 1]] = send[q][pq["nptr"][kk]:pq["nptr"][kk + 1]]
+        out = unpack(p, v, recv)
+        assert np.allclose(out, full[p["gid"]], rtol=1e-14, atol=1e-14)
+        done.append(out)
+    val = {}
+    for p, out in zip(plans, done):
+        for g, x in zip(p["gid"], out):
+            assert val.setdefault(int(g), x) == x
