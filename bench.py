@@ -55,6 +55,9 @@ def parse():
                     help="only the headline solve (no parity, mixed, P=8, operator and "
                          "mixed-element keys)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="hex32_p6")
+    ap.add_argument("--shard", action="store_true",
+                    help="one solve sharded over the N GPUs by element partition (strong "
+                         "scaling; NCCL exchange of the shared dofs) instead of N replicas")
     args = ap.parse_args()
     global N_CELLS, NM, WORKLOAD
     N_CELLS, NM, WORKLOAD = WORKLOADS[args.workload]
@@ -622,11 +625,92 @@ def run_b200(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def run_shard(args, rank, world, local):
+    """The headline solve sharded over the N GPUs: rank r holds elements
+    partition(nelmt, N, r) and its dofs; per iteration the shared dofs go to
+    the neighbour ranks by NCCL send/recv and the three dot sums through one
+    NCCL all-reduce, inside the CUDA graph of the iterations (strong scaling:
+    the whole job is one solve). Each step is one solve through the public
+    call with host buffers (right-hand side in, solution out); `value` is
+    timed by the device events around the solve (after the copy in, before
+    the copy out), `e2e` by the wall clock around the call, both the maximum
+    over ranks."""
+    import time
+
+    import torch
+    import nektar_b200 as nb
+
+    from nektar_b200 import replicas
+    from nektar_b200.sharded import DeviceShardGroup, close_comm, make_comm, shard_plans
+    torch.cuda.set_device(local)
+    pg = replicas.init(world, local, "nccl")
+    mesh = nb.BoxMesh("hex", N_CELLS, NM, NM + 1, amp=AMP, coords=True)
+    gmap, nglob, ndir = mesh.assembly()
+    nc, nt = mesh.nc, mesh.nt
+    p = shard_plans(np.asarray(gmap), ndir, world, nc=nc)[rank]
+    lo, hi = p["lo"], p["hi"]
+    op = nb.Operator("helmholtz", shape="hex", nm=NM, nq=mesh.nq, nelmt=hi - lo, T=mesh.T,
+                     jac=mesh.jac[lo * nt:hi * nt],
+                     df=np.ascontiguousarray(mesh.df[:, lo * nt:hi * nt]), deformed=True,
+                     device=local)
+    op.set_factors(LAM)
+    ipo = nb.Operator("iproduct", shape="hex", nm=NM, nq=mesh.nq, nelmt=hi - lo, T=mesh.T,
+                      jac=mesh.jac[lo * nt:hi * nt], deformed=True, device=local)
+    x, y, z = (c[lo * nt:hi * nt] for c in mesh.xyz)
+    b = ipo((3 * np.pi ** 2 + LAM) * np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z))
+    ipo.close()
+    mesh.xyz = mesh.jac = mesh.df = None
+    os.environ.setdefault("NCCL_DEBUG", "WARN")  # stdout carries the one JSON line
+    comm = make_comm(pg, local)
+    G = DeviceShardGroup([p], [[op]], comm=comm, device=local)
+    b_pin = torch.tensor(b).pin_memory().numpy()
+    for _ in range(max(args.warmup, 3)):
+        G.solve([b_pin], tol=TOL, maxit=20000, check_interval=K_CHECK)
+    dev_ms, wall, its = 0.0, 0.0, 0
+    with ClockSampler(local) as clocks:
+        replicas.barrier(pg)
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            _, reps = G.solve([b_pin], tol=TOL, maxit=20000, check_interval=K_CHECK)
+            wall += time.perf_counter() - t0
+            dev_ms += reps[0].device_ms
+            its = reps[0].iterations
+        replicas.barrier(pg)
+    ms_max = replicas.max_over_ranks(dev_ms, pg, f"cuda:{local}")
+    wall_max = replicas.max_over_ranks(wall, pg, f"cuda:{local}")
+    nloc_r = (hi - lo) * nc
+    G.close()
+    close_comm(comm)
+    op.close()
+    line = {
+        "metric": METRIC, "value": 1e3 * args.steps / ms_max, "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (manufactured solution, zero Dirichlet data)",
+        "config": dict(workload_config(mesh.nelmt, mesh.nelmt * nc, nglob, ndir, world),
+                       parallelism="shard%d" % world),
+        "iterations": its,
+        "shard": {"elements_per_rank_max": int(-(-mesh.nelmt // world)),
+                  "shared_dofs_rank0": int(p["shared"].size),
+                  "neighbours_rank0": [int(q) for q in p["nbr"]]},
+        "e2e": {"value": args.steps / wall_max, "unit": "solves/s",
+                "h2d_bytes_per_step": 2 * nloc_r * 8, "d2h_bytes_per_step": nloc_r * 8},
+        "clocks": clocks.summary(),
+        "gpu_launches": int(reps[0].kernel_launches) * args.steps,
+    }
+    replicas.finish(pg)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.shard:
+        run_shard(args, rank, world, local)
     else:
         run_b200(args, rank, world, local)
 
