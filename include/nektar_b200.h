@@ -131,7 +131,8 @@ typedef struct nkb_op_desc
     /* host arrays, reference layouts (see top of file); NULL where the
      * operator does not need them: BwdTrans needs bdata; IProduct bdata, w, jac;
      * PhysDeriv z, D, df; Helmholtz, LinearADR and IProductWRTDerivBase
-     * bdata, w, z, D, jac, df. */
+     * bdata, w, z, D, jac, df. jac and df may also be device memory (copied
+     * device to device). */
     const double *bdata[3];
     const double *w[3];
     const double *z[3];
@@ -558,6 +559,14 @@ long nkb_geom_nelmt(const nkb_geom_request *req);
  * NULL, the physical coordinates of every quadrature point (3 rows of
  * nelmt*nqtot). */
 int nkb_geom_fill(const nkb_geom_request *req, double *jac, double *df, double *xyz);
+
+/* The same into device memory (jac, df, xyz device pointers; req and its
+ * arrays on the host), computed on the device: one thread per element and
+ * point, the host fill's arithmetic with the device's sin / cos (the last
+ * bit may differ). At most 32 points per direction. Synchronous on
+ * `stream`. */
+int nkb_geom_fill_device(const nkb_geom_request *req, double *jac, double *df, double *xyz,
+                         int device, void *stream);
 
 /* C0 assembly map for a hex box of n^3 elements with nm modes per direction
  * (Modified_A): boundary (Dirichlet) coefficients numbered first, as

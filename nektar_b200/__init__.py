@@ -101,7 +101,11 @@ class BoxMesh:
     optionally curved by x' = x + amp sin(pi x) sin(pi y) sin(pi z), with
     analytic geometric factors at the quadrature points (Collections layout)."""
 
-    def __init__(self, shape, n, nm, nq0, amp=0.0, deformed=None, cells=None, coords=False):
+    def __init__(self, shape, n, nm, nq0, amp=0.0, deformed=None, cells=None, coords=False,
+                 geom_device=None):
+        """geom_device: a CUDA device index to compute jac / df (and xyz) on
+        that device (torch tensors, nkb_geom_fill_device) instead of the host
+        (numpy arrays, nkb_geom_fill)."""
         self.shape, self.n, self.nm, self.amp = shape, n, nm, amp
         self.deformed = bool(amp != 0.0) if deformed is None else bool(deformed)
         self.T, self.nq = shape_tables(shape, nm, nq0)
@@ -118,6 +122,17 @@ class BoxMesh:
         req.deformed = int(self.deformed)
         self.nelmt = int(lib().nkb_geom_nelmt(ctypes.byref(req)))
         ncol = self.nelmt * self.nt if self.deformed else self.nelmt
+        if geom_device is not None:
+            import torch
+            dev = "cuda:%d" % geom_device
+            self.jac = torch.empty(ncol, dtype=torch.float64, device=dev)
+            self.df = torch.empty((9, ncol), dtype=torch.float64, device=dev)
+            self.xyz = (torch.empty((3, self.nelmt * self.nt), dtype=torch.float64, device=dev)
+                        if coords else None)
+            check(lib().nkb_geom_fill_device(
+                ctypes.byref(req), self.jac.data_ptr(), self.df.data_ptr(),
+                None if self.xyz is None else self.xyz.data_ptr(), geom_device, None))
+            return
         self.jac = np.zeros(ncol)
         self.df = np.zeros((9, ncol))
         self.xyz = np.zeros((3, self.nelmt * self.nt)) if coords else None
@@ -159,14 +174,23 @@ class Operator:
             return (C.dp * 3)(*[_dp(a) for a in arrs])
 
         d.bdata, d.w, d.z, d.D = arr3("b"), arr3("w"), arr3("z"), arr3("D")
+
+        def geom(a):
+            # a CUDA tensor (FP64, contiguous) stays on the device: its
+            # address is passed and the library copies device to device
+            if hasattr(a, "is_cuda") and a.is_cuda:
+                if str(a.dtype) != "torch.float64" or not a.is_contiguous():
+                    raise ValueError("device geometry must be contiguous FP64")
+                self._keep.append(a)
+                return ctypes.cast(ctypes.c_void_p(a.data_ptr()), C.dp)
+            a = _f64(a)
+            self._keep.append(a)
+            return _dp(a)
+
         if jac is not None:
-            jac = _f64(jac)
-            self._keep.append(jac)
-            d.jac = _dp(jac)
+            d.jac = geom(jac)
         if df is not None:
-            df = _f64(df)
-            self._keep.append(df)
-            d.df = _dp(df)
+            d.df = geom(df)
         d.precision, d.device = self.precision, device
         h = ctypes.c_void_p()
         check(lib().nkb_op_create(ctypes.byref(d), ctypes.byref(h)))

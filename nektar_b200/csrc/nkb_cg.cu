@@ -1161,7 +1161,8 @@ extern "C" int nkb_sys_set_blocks(nkb_sys *S, int nblk, const int *bptr, const i
     if (cudaMemcpy(dp, bptr, (nblk + 1) * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(di, bidx, nidx * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(dof, boff.data(), nblk * sizeof(long), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(dm, binv, tot * sizeof(double), cudaMemcpyDefault) != cudaSuccess)
+        cudaMemcpy(dm, binv, tot * sizeof(double), cudaMemcpyDefault) != cudaSuccess ||
+        cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess) // binv may be device memory
     {
         release();
         return SetError(NKB_ERR_CUDA, "nkb_sys_set_blocks: upload");

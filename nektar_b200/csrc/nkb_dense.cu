@@ -150,7 +150,10 @@ extern "C" int nkb_op_create_dense_rect(int rows, int cols, int nelmt, const dou
         if (cudaMalloc(&op->geo, bytes) != cudaSuccess)
             return fail(SetError(NKB_ERR_NOMEM, "nkb_op_create_dense: %zu bytes of blocks", bytes));
         // host or device blocks (unified addressing tells them apart)
-        if (cudaMemcpy(op->geo, mats, bytes, cudaMemcpyDefault) != cudaSuccess)
+        // a copy from device memory does not wait for itself: finished here,
+        // so the caller may free the source on return
+        if (cudaMemcpy(op->geo, mats, bytes, cudaMemcpyDefault) != cudaSuccess ||
+            cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess)
             return fail(SetError(NKB_ERR_CUDA, "nkb_op_create_dense: upload"));
     }
     *out = op;

@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace nkb
@@ -554,13 +555,26 @@ static int Repack(nkb_op *op)
     return NKB_OK;
 }
 
+// a device copy of n doubles given in host or device memory (FP64: copied as
+// they are; FP32: converted on the host)
 template <typename T> static int Upload(T **dst, const double *src, size_t n)
 {
-    std::vector<T> tmp(n);
-    for (size_t i = 0; i < n; ++i)
-        tmp[i] = T(src[i]);
     NKB_CUDA_TRY(cudaMalloc(dst, n * sizeof(T)));
-    NKB_CUDA_TRY(cudaMemcpy(*dst, tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+    if constexpr (std::is_same_v<T, double>)
+    {
+        // a copy from device memory does not wait for itself: finish it
+        // before the pack (on the operator's own stream) reads it and the
+        // caller frees the source
+        NKB_CUDA_TRY(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyDefault));
+        NKB_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
+    }
+    else
+    {
+        std::vector<T> tmp(n);
+        for (size_t i = 0; i < n; ++i)
+            tmp[i] = T(src[i]);
+        NKB_CUDA_TRY(cudaMemcpy(*dst, tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+    }
     return NKB_OK;
 }
 

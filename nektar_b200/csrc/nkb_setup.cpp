@@ -11,10 +11,12 @@
 // (GeomFactors.cpp:248-477): jac = |det dx/dxi|, df[k*3+j] = d xi_j / d x_k,
 // evaluated from the analytic Jacobian of the curved map.
 #include "nkb_internal.h"
+#include "nkb_geom.h"
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 namespace nkb
@@ -229,133 +231,7 @@ extern "C" int nkb_basis(int btype, int nm, int np, const double *z, const doubl
 // ---------------------------------------------------------------------------
 // Structured test meshes
 // ---------------------------------------------------------------------------
-namespace
-{
-
-struct Affine
-{
-    double x0[3];
-    double M[3][3]; // x = x0 + M (xi + 1)/2, M[k][i] = d x_k / d ((xi_i+1)/2)
-};
-
-int ElementsPerCell(int shape)
-{
-    return shape == NKB_HEX ? 1 : (shape == NKB_PRISM ? 2 : 6);
-}
-
-double Det3(const double A[3][3])
-{
-    return A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
-           A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
-           A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
-}
-
-// Affine map of sub-element s of cell (cx, cy, cz), h = 1/n.
-Affine CellMap(int shape, int n, int cell, int s)
-{
-    const double h = 1.0 / n;
-    int cx = cell % n, cy = (cell / n) % n, cz = cell / (n * n);
-    double o[3] = {cx * h, cy * h, cz * h};
-    Affine A;
-    std::memset(&A, 0, sizeof(A));
-    if (shape == NKB_HEX)
-    {
-        for (int k = 0; k < 3; ++k)
-        {
-            A.x0[k]    = o[k];
-            A.M[k][k]  = h;
-        }
-    }
-    else if (shape == NKB_PRISM)
-    {
-        // standard prism: triangle {xi0 + xi2 <= 0} in (xi0, xi2), extruded in xi1
-        if (s == 0)
-        {
-            for (int k = 0; k < 3; ++k)
-            {
-                A.x0[k]   = o[k];
-                A.M[k][k] = h;
-            }
-        }
-        else
-        {
-            // the other half x_l + z_l >= 1: x_l = 1 - a, z_l = 1 - c
-            A.x0[0]   = o[0] + h;
-            A.x0[1]   = o[1];
-            A.x0[2]   = o[2] + h;
-            A.M[0][0] = -h;
-            A.M[1][1] = h;
-            A.M[2][2] = -h;
-        }
-    }
-    else
-    {
-        // Kuhn split: tet s visits 0 -> e_a -> e_a + e_b -> (1,1,1)
-        static const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2},
-                                       {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
-        double v[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {1, 1, 1}};
-        v[1][perm[s][0]] = 1;
-        v[2][perm[s][0]] = 1;
-        v[2][perm[s][1]] = 1;
-        double M[3][3];
-        for (int k = 0; k < 3; ++k)
-            for (int i = 0; i < 3; ++i)
-                M[k][i] = h * (v[i + 1][k] - v[0][k]);
-        if (Det3(M) < 0)
-            for (int k = 0; k < 3; ++k)
-                std::swap(M[k][0], M[k][1]);
-        for (int k = 0; k < 3; ++k)
-        {
-            A.x0[k] = o[k];
-            for (int i = 0; i < 3; ++i)
-                A.M[k][i] = M[k][i];
-        }
-    }
-    return A;
-}
-
-// standard coordinates xi of a quadrature point given in the collapsed
-// coordinates eta of the shape (Nektar's collapsed systems).
-void Uncollapse(int shape, const double eta[3], double xi[3])
-{
-    if (shape == NKB_HEX)
-    {
-        xi[0] = eta[0];
-        xi[1] = eta[1];
-        xi[2] = eta[2];
-    }
-    else if (shape == NKB_PRISM)
-    {
-        xi[2] = eta[2];
-        xi[1] = eta[1];
-        xi[0] = 0.5 * (1.0 + eta[0]) * (1.0 - eta[2]) - 1.0;
-    }
-    else
-    {
-        xi[2] = eta[2];
-        xi[1] = 0.5 * (1.0 + eta[1]) * (1.0 - eta[2]) - 1.0;
-        xi[0] = 0.5 * (1.0 + eta[0]) * (-xi[1] - xi[2]) - 1.0;
-    }
-}
-
-// x' = x + amp S(x) (every coordinate), S = sin(pi x) sin(pi y) sin(pi z)
-void CurvedMap(double amp, const double x[3], double xp[3], double Jm[3][3])
-{
-    const double sx = std::sin(M_PI * x[0]), sy = std::sin(M_PI * x[1]),
-                 sz = std::sin(M_PI * x[2]);
-    const double cx = std::cos(M_PI * x[0]), cy = std::cos(M_PI * x[1]),
-                 cz = std::cos(M_PI * x[2]);
-    const double S     = sx * sy * sz;
-    const double dS[3] = {M_PI * cx * sy * sz, M_PI * sx * cy * sz, M_PI * sx * sy * cz};
-    for (int k = 0; k < 3; ++k)
-    {
-        xp[k] = x[k] + amp * S;
-        for (int l = 0; l < 3; ++l)
-            Jm[k][l] = (k == l ? 1.0 : 0.0) + amp * dS[l];
-    }
-}
-
-} // namespace
+using namespace nkb::geom;
 
 extern "C" long nkb_geom_nelmt(const nkb_geom_request *req)
 {
@@ -383,7 +259,9 @@ extern "C" int nkb_geom_fill(const nkb_geom_request *req, double *jac, double *d
             return SetError(NKB_ERR_INVALID, "nkb_geom_fill: missing points for dir %d", d);
     const long ncol = req->deformed ? nelmt * nt : nelmt;
 
-    for (long c = 0; c < ncells; ++c)
+    // cells split over host threads: every element writes its own columns
+    auto fill_cells = [&](long c0, long c1) {
+    for (long c = c0; c < c1; ++c)
     {
         int cell = req->cells ? req->cells[c] : int(c);
         for (int s = 0; s < epc; ++s)
@@ -397,38 +275,10 @@ extern "C" int nkb_geom_fill(const nkb_geom_request *req, double *jac, double *d
                 double eta[3] = {req->z[0][i], req->z[1][j], req->z[2][k]};
                 if (!req->deformed)
                     eta[0] = eta[1] = eta[2] = -0.5; // any interior point: affine
-                double xi[3], x[3], xp[3], Jc[3][3], J[3][3];
-                Uncollapse(req->shape, eta, xi);
-                for (int a = 0; a < 3; ++a)
-                {
-                    x[a] = A.x0[a];
-                    for (int b = 0; b < 3; ++b)
-                        x[a] += A.M[a][b] * 0.5 * (xi[b] + 1.0);
-                }
-                CurvedMap(req->amp, x, xp, Jc);
-                // J[k][i] = d x'_k / d xi_i = sum_l Jc[k][l] M[l][i] / 2
-                for (int a = 0; a < 3; ++a)
-                    for (int b = 0; b < 3; ++b)
-                    {
-                        double v = 0.0;
-                        for (int l = 0; l < 3; ++l)
-                            v += Jc[a][l] * A.M[l][b];
-                        J[a][b] = 0.5 * v;
-                    }
-                double det = Det3(J);
-                // inverse: Ji[i][k] = d xi_i / d x_k
-                double Ji[3][3];
-                Ji[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
-                Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
-                Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
-                Ji[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / det;
-                Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
-                Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
-                Ji[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
-                Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
-                Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+                double xp[3], Ji[3][3], jv;
+                AtPoint(req->shape, req->amp, A, eta, jv, Ji, xp);
                 long col  = req->deformed ? e * nt + q : e;
-                jac[col]  = std::fabs(det);
+                jac[col]  = jv;
                 for (int kk = 0; kk < 3; ++kk)
                     for (int jj = 0; jj < 3; ++jj)
                         df[(kk * 3 + jj) * ncol + col] = Ji[jj][kk];
@@ -458,6 +308,20 @@ extern "C" int nkb_geom_fill(const nkb_geom_request *req, double *jac, double *d
             }
         }
     }
+    };
+    const long work     = ncells * epc * (req->deformed ? nt : 1);
+    const int nthreads  = int(std::max<long>(1, std::min<long>({long(std::thread::hardware_concurrency()),
+                                                              32L, work / 65536 + 1, ncells})));
+    if (nthreads == 1)
+        fill_cells(0, ncells);
+    else
+    {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nthreads; ++t)
+            pool.emplace_back(fill_cells, ncells * t / nthreads, ncells * (t + 1) / nthreads);
+        for (std::thread &th : pool)
+            th.join();
+    }
     return NKB_OK;
 }
 
@@ -484,35 +348,46 @@ extern "C" int nkb_hex_box_assembly(int n, int nm, int *map, int *nglob, int *nd
             return long(c + 1) * (nm - 1);
         return long(c) * (nm - 1) + (p - 1);
     };
-    auto onb = [&](long d) { return d == 0 || d == N1 - 1; };
-    std::vector<int> num(N3, -1);
-    int cnt = 0;
-    for (int pass = 0; pass < 2; ++pass)
-        for (long d = 0; d < N3; ++d)
+    // Boundary dofs first, then interior ones, each set in lexicographic
+    // (c, b, a) order; both ranks have closed forms: a boundary plane (c = 0
+    // or N1-1) holds N1^2 boundary dofs, an interior plane 4 N1 - 4 (its first
+    // and last rows whole, two of every other row).
+    const long M1 = N1 - 2, ndirc = N3 - M1 * M1 * M1;
+    auto onb = [&](long x) { return x == 0 || x == N1 - 1; };
+    auto rank = [&](long a, long b, long c) -> long {
+        if (!(onb(a) || onb(b) || onb(c)))
+            return ndirc + ((c - 1) * M1 + (b - 1)) * M1 + (a - 1);
+        const long before = c == 0 ? 0 : N1 * N1 + (c - 1) * (4 * N1 - 4);
+        if (onb(c))
+            return before + b * N1 + a;
+        const long row = b == 0 ? 0 : N1 + (b - 1) * 2;
+        if (onb(b))
+            return before + row + a;
+        return before + row + (a == 0 ? 0 : 1);
+    };
+    const long nelmt = long(n) * n * n, nc = long(nm) * nm * nm;
+    const int nthreads = int(std::max<long>(
+        1, std::min<long>({long(std::thread::hardware_concurrency()), 32L, nelmt * nc / 262144 + 1})));
+    auto fill = [&](long e0, long e1) {
+        for (long e = e0; e < e1; ++e)
         {
-            long a = d % N1, b = (d / N1) % N1, c = d / (N1 * N1);
-            bool bnd = onb(a) || onb(b) || onb(c);
-            if ((pass == 0) == bnd)
-                num[d] = cnt++;
+            int cx = int(e % n), cy = int((e / n) % n), cz = int(e / (long(n) * n));
+            for (int r = 0; r < nm; ++r)
+                for (int q = 0; q < nm; ++q)
+                    for (int p = 0; p < nm; ++p)
+                        map[e * nc + (long(r) * nm + q) * nm + p] =
+                            int(rank(dof1(cx, p), dof1(cy, q), dof1(cz, r)));
         }
-    long ndirc = 0;
-    for (long d = 0; d < N3; ++d)
+    };
+    if (nthreads == 1)
+        fill(0, nelmt);
+    else
     {
-        long a = d % N1, b = (d / N1) % N1, c = d / (N1 * N1);
-        if (onb(a) || onb(b) || onb(c))
-            ++ndirc;
-    }
-    const long nc = long(nm) * nm * nm;
-    for (long e = 0; e < long(n) * n * n; ++e)
-    {
-        int cx = int(e % n), cy = int((e / n) % n), cz = int(e / (long(n) * n));
-        for (int r = 0; r < nm; ++r)
-            for (int q = 0; q < nm; ++q)
-                for (int p = 0; p < nm; ++p)
-                {
-                    long d = dof1(cx, p) + N1 * (dof1(cy, q) + N1 * dof1(cz, r));
-                    map[e * nc + (long(r) * nm + q) * nm + p] = num[d];
-                }
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nthreads; ++t)
+            pool.emplace_back(fill, nelmt * t / nthreads, nelmt * (t + 1) / nthreads);
+        for (std::thread &th : pool)
+            th.join();
     }
     *nglob = int(N3);
     *ndir  = int(ndirc);

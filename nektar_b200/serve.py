@@ -331,13 +331,19 @@ class CudaContext:
         n, P = key
         nm = P + 1
         self.key, self.device, self.check_interval = key, device, check_interval
-        self.mesh = nb.BoxMesh("hex", n, nm, nm + 1, amp=0.05)
-        gmap, nglob, ndir = self.mesh.assembly()
-        self.op = nb.Operator("helmholtz", self.mesh, device=device)
-        self.op32 = nb.Operator("helmholtz", self.mesh, device=device, precision="fp32")
+        # the geometric factors are computed on the device and copied there
+        # into both operators
+        m = nb.BoxMesh("hex", n, nm, nm + 1, amp=0.05, geom_device=device)
+        self.mesh = m
+        gmap, nglob, ndir = m.assembly()
+        jac, df = m.jac, m.df
+        m.jac = m.df = None
+        kw = dict(shape="hex", nm=nm, nq=m.nq, nelmt=m.nelmt, T=m.T, jac=jac, df=df,
+                  deformed=m.deformed, device=device)
+        self.op = nb.Operator("helmholtz", **kw)
+        self.op32 = nb.Operator("helmholtz", precision="fp32", **kw)
+        del jac, df, kw
         self.sys = nb.GlobalLinSys([self.op], gmap, nglob, ndir, device=device, ops32=[self.op32])
-        # the operators hold their own device copies: drop the host geometry
-        self.mesh.jac = self.mesh.df = None
         shared, inst = self.sys.footprint()
         self.bytes = (_op_bytes(self.mesh.nelmt, nm, nm + 1, False)
                       + _op_bytes(self.mesh.nelmt, nm, nm + 1, True) + shared + inst)

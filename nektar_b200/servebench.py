@@ -27,6 +27,9 @@ def main():
     ap.add_argument("--budget-frac", type=float, default=0.8,
                     help="admission budget as a fraction of the free device memory")
     ap.add_argument("--prewarm", action="store_true")
+    ap.add_argument("--detail", default=None,
+                    help="write one JSON line per request (mesh, order, lambda, tolerance, "
+                         "precision, iterations, convergence, times) to this file")
     a = ap.parse_args()
     import torch
 
@@ -57,6 +60,16 @@ def main():
                        "max": max(r.iterations for r in res)},
     })
     sch.close()
+    if a.detail:
+        by_id = {r.rid: r for r in reqs}
+        with open(a.detail, "w") as f:
+            for r in sorted(res, key=lambda r: r.rid):
+                q = by_id[r.rid]
+                f.write(json.dumps({"rid": r.rid, "n": q.n, "P": q.P, "lam": q.lam, "tol": q.tol,
+                                    "mixed": q.mixed, "iterations": r.iterations,
+                                    "converged": r.converged, "rel_residual": r.rel_residual,
+                                    "device_ms": r.device_ms, "latency_s": r.latency,
+                                    "new_context": r.new_context}) + "\n")
     print(json.dumps(s), flush=True)
 
 

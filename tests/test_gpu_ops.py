@@ -364,3 +364,23 @@ def test_hex_kernel_variants_are_repeatable(monkeypatch, variant):
     y0 = op(x)
     bad = sum(not np.array_equal(op(x), y0) for _ in range(150))
     assert bad == 0
+
+
+@pytest.mark.parametrize("shape,n,nm,amp,coords", [("hex", 4, 7, 0.05, True), ("prism", 3, 5, 0.05, False),
+                                                   ("tet", 3, 4, 0.0, True), ("hex", 3, 5, 0.0, False)])
+def test_device_geometry_matches_host_geometry(shape, n, nm, amp, coords):
+    """nkb_geom_fill_device: the host fill's arithmetic on the device (its
+    sin / cos may round the last bit differently), curved and affine, with
+    and without the point coordinates; an operator built from the device
+    factors applies as the host-built one does."""
+    mh = nb.BoxMesh(shape, n, nm, nm + 1, amp=amp, coords=coords)
+    md = nb.BoxMesh(shape, n, nm, nm + 1, amp=amp, coords=coords, geom_device=0)
+    for a, b in ((mh.jac, md.jac), (mh.df, md.df)) + (((mh.xyz, md.xyz),) if coords else ()):
+        b = b.cpu().numpy()
+        assert np.abs(a - b).max() <= 1e-14 * max(1.0, np.abs(a).max())
+    x = np.random.default_rng(nm).uniform(-1, 1, mh.nelmt * mh.nc)
+    oh = nb.Operator("helmholtz", mh)
+    od = nb.Operator("helmholtz", md)
+    for o in (oh, od):
+        o.set_factors(1.3)
+    assert rel_l2(od(x), oh(x)) < 1e-13
