@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -240,6 +241,9 @@ template <typename T> static int AutotuneHex(nkb_op *op, int *best)
             break;
         float ms = 0.f;
         cudaEventElapsedTime(&ms, op->ev0, op->ev1);
+        if (std::getenv("NKB_TUNE_VERBOSE"))
+            std::fprintf(stderr, "hex tune nm=%d nelmt=%d fp%d variant %d: %.4f ms per launch\n",
+                         op->nm, op->nelmt, op->precision == NKB_FP64 ? 64 : 32, v, ms / 3);
         if (ms < best_ms)
         {
             best_ms = ms;

@@ -131,8 +131,11 @@ __device__ __forceinline__ T DotRow(const T *__restrict__ row, const T (&c)[N], 
 template <typename T, int NQ, int GEO, int EPB> __host__ __device__ constexpr int HexMinBlocks()
 {
     // resident CTAs per SM the register allocation must allow: a register
-    // budget per thread of 160 (nq <= 8), 168 (nq <= 10) or 255
-    constexpr int regs = NQ <= 8 ? 160 : (NQ <= 10 ? 168 : 255);
+    // budget per thread of 160 (nq <= 8), 168 (nq <= 10) or 255; the streamed
+    // variants up to nq = 10 (no shared-memory geometry buffer, so registers
+    // set the occupancy) take 128
+    constexpr int regs = GEO == kGeoStream && NQ <= 10 ? 128
+                                                      : (NQ <= 8 ? 160 : (NQ <= 10 ? 168 : 255));
     constexpr int b    = 65536 / (HexThreads<NQ, EPB>() * regs);
     return b < 1 ? 1 : b;
 }
