@@ -461,7 +461,8 @@ const char *KernelName(const nkb_op *op, bool gather)
         case 3: return "k_hex_helm_mma (FP64 tensor cores)";
         case 4: return "k_hex_helm_mma2 (FP64 tensor cores, two warps per element)";
         case 5: return "k_hex_helm_tc (tcgen05 TF32 high/low tensor cores, FP32 accumulate)";
-        default: return "k_hex_helm (persistent, double-buffered TMA geometry)";
+        case 6: return "k_hex_helm (persistent, double-buffered TMA geometry)";
+        default: return "k_hex_helm (TMA-staged geometry, small groups)";
     }
 }
 

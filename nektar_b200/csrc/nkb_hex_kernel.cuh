@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <type_traits>
@@ -50,8 +51,10 @@ enum
 {
     kGeoTma    = 0, // the element's whole geometry by one bulk TMA copy into shared memory
     kGeoStream = 1, // coalesced loads into registers, one k-plane ahead
-    kGeoTma2   = 2  // persistent CTAs: the next element group's geometry copied into a
+    kGeoTma2   = 2, // persistent CTAs: the next element group's geometry copied into a
                     // second buffer while the current group computes
+    kGeoTmaS   = 3  // as kGeoTma, with element groups of at most 48 KB and 128 registers
+                    // per thread (more CTAs per SM)
 };
 
 __host__ __device__ constexpr int RoundUp(int a, int b)
@@ -79,7 +82,7 @@ template <int NQ> __host__ __device__ constexpr int HexRegion()
 
 template <typename T, int NM, int NQ, int GEO, int EPB> size_t HexSmem(long gstride)
 {
-    const size_t nbuf = GEO == kGeoTma ? 1 : (GEO == kGeoTma2 ? 2 : 0);
+    const size_t nbuf = (GEO == kGeoTma || GEO == kGeoTmaS) ? 1 : (GEO == kGeoTma2 ? 2 : 0);
     return size_t(HexTabBytes<T, NM, NQ>()) +
            size_t(EPB) * (nbuf * size_t(gstride) + 3 * HexRegion<NQ>()) * sizeof(T);
 }
@@ -134,8 +137,9 @@ template <typename T, int NQ, int GEO, int EPB> __host__ __device__ constexpr in
     // budget per thread of 160 (nq <= 8), 168 (nq <= 10) or 255; the streamed
     // variants up to nq = 10 (no shared-memory geometry buffer, so registers
     // set the occupancy) take 128
-    constexpr int regs = GEO == kGeoStream && NQ <= 10 ? 128
-                                                      : (NQ <= 8 ? 160 : (NQ <= 10 ? 168 : 255));
+    constexpr int regs = (GEO == kGeoStream && NQ <= 10) || GEO == kGeoTmaS
+                             ? 128
+                             : (NQ <= 8 ? 160 : (NQ <= 10 ? 168 : 255));
     constexpr int b    = 65536 / (HexThreads<NQ, EPB>() * regs);
     return b < 1 ? 1 : b;
 }
@@ -155,7 +159,7 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
     static_assert(RS % 2 == 0 && NMP % 2 == 0, "vector loads need even strides");
     static_assert(HexTabBytes<T, NM, NQ>() % 16 == 0, "work regions must start 16-byte aligned");
     static_assert(NM * NM * NMP <= RS && NM * NQ * NQ <= RS, "regions too small");
-    constexpr bool TMA = GEO == kGeoTma || GEO == kGeoTma2;
+    constexpr bool TMA = GEO == kGeoTma || GEO == kGeoTma2 || GEO == kGeoTmaS;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem); // one per geometry buffer
     T *sB0         = reinterpret_cast<T *>(smem + 16);
@@ -164,7 +168,7 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
     T *sD         = sB2 + NM * NQ; // sD[i*NQP + m] = D(i, m) = l_m'(z_i)
     const long GS = a.gstride;
     T *geob       = reinterpret_cast<T *>(smem + HexTabBytes<T, NM, NQ>());
-    T *us         = geob + (GEO == kGeoTma2 ? 2 : (GEO == kGeoTma ? 1 : 0)) * EPB * GS; // GS % 4 == 0
+    T *us         = geob + (GEO == kGeoTma2 ? 2 : (TMA ? 1 : 0)) * EPB * GS; // GS % 4 == 0
     T *v0s        = us + EPB * RS;
     T *v1s        = v0s + EPB * RS;
 
@@ -510,8 +514,9 @@ namespace nkb
 //    high/low operands, FP32 accumulation; FP32 operators, nm 2..9;
 //    nkb_hex_tc.cuh); 6: persistent CTAs with the geometry double-buffered
 //    (the next element group's bulk copy in flight while the current one
-//    computes)
-constexpr int kNumHexVariants = 7;
+//    computes); 7: TMA-staged geometry in element groups of at most 48 KB,
+//    128 registers per thread (more, smaller CTAs per SM than variant 0)
+constexpr int kNumHexVariants = 8;
 
 // elements per CTA of the double-buffered variant: two geometry buffers and
 // three work regions per element in at most 72 KB (three CTAs per SM)
@@ -528,6 +533,17 @@ template <typename T, int NQ> constexpr int TmaEpb()
 {
     constexpr int per = (10 * NQ * NQ * NQ + 4) * int(sizeof(T));
     constexpr int e   = (90 * 1024) / per;
+    constexpr int lim = 512 / (NQ * NQ);
+    constexpr int v   = e < lim ? e : lim;
+    return v < 1 ? 1 : (v > 8 ? 8 : v);
+}
+
+// elements per CTA of variant 7: groups of at most 48 KB (one element when a
+// single element needs more)
+template <typename T, int NQ> constexpr int TmaSmallEpb()
+{
+    constexpr int per = (10 * NQ * NQ * NQ + 4) * int(sizeof(T));
+    constexpr int e   = (48 * 1024) / per;
     constexpr int lim = 512 / (NQ * NQ);
     constexpr int v   = e < lim ? e : lim;
     return v < 1 ? 1 : (v > 8 ? 8 : v);
@@ -571,12 +587,22 @@ static int HexVariantLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, 
         return SetError(NKB_ERR_UNSUPPORTED, "LinearADR has no gathered Hex kernel");
     if (set_attr)
     {
+        // the limit of each mode's kernel covers every operator that may
+        // launch it: Helmholtz packs 7 geometry values per point, LinearADR
+        // 10 (another operator's set-up must not lower it under this one's)
+        const long nt = long(NQ) * NQ * NQ;
+        const size_t hb = HexSmem<T, NM, NQ, GEO, EPB>((7 * nt + 3) & ~3L);
+        const size_t ab = HexSmem<T, NM, NQ, GEO, EPB>((10 * nt + 3) & ~3L);
         NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm<T, NM, NQ, GEO, EPB, kModeLocal>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(std::max(hb, bytes))));
         NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm<T, NM, NQ, GEO, EPB, kModeGather>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
-        NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm<T, NM, NQ, GEO, EPB, kModeAdv>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(std::max(hb, bytes))));
+        if (ab <= 227 * 1024)
+            NKB_CUDA_TRY(cudaFuncSetAttribute(k_hex_helm<T, NM, NQ, GEO, EPB, kModeAdv>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              int(std::max(ab, bytes))));
         return NKB_OK;
     }
     long nb = (long(op->nelmt) + EPB - 1) / EPB;
@@ -682,6 +708,9 @@ static int HexLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStr
                 return SetError(NKB_ERR_UNSUPPORTED, "double-buffered Hex variant: nq <= 9");
         case 1:
             return HexVariantLaunch<T, NM, kGeoStream, 1>(op, a, gather, s, set_attr);
+        case 7:
+            return HexVariantLaunch<T, NM, kGeoTmaS, TmaSmallEpb<T, NQ>()>(op, a, gather, s,
+                                                                           set_attr);
         default:
             return HexVariantLaunch<T, NM, kGeoStream, 2>(op, a, gather, s, set_attr);
     }
