@@ -245,25 +245,41 @@ __global__ void __launch_bounds__(HexThreads<NQ, EPB>(), (HexMinBlocks<T, NQ, GE
         for (int cc = 0; cc < NG; ++cc)
             gc[cc] = __ldg(Gg + cc * NQ3 + q0);
     }
-    // coefficients into the v0 region, rows (r, q) padded to NMP (NM^2 NMP <= NQ3)
-    for (int t = tid; t < ne * NC; t += blockDim.x)
+    // coefficients into the v0 region, rows (r, q) padded to NMP (NM^2 NMP <= NQ3):
+    // every map entry of the thread first, then every value, then the stores,
+    // so the loads of one thread are in flight together
     {
-        const int lt  = t / NC;
-        const int m   = t - lt * NC;
-        const long gi = (e0 + lt) * NC + m;
-        T v;
-        if (GATHER)
+        constexpr int TH  = HexThreads<NQ, EPB>();
+        constexpr int PER = (EPB * NC + TH - 1) / TH;
+        const int nall    = ne * NC;
+        // gathered: the global index; local: the offset in the group
+        const T *in0 = GATHER ? a.in : a.in + e0 * NC;
+        int src[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u)
         {
-            v = a.in[a.gmap[gi]];
-            if (a.gsign)
-                v *= T(a.gsign[gi]);
+            const int t = tid + u * TH;
+            src[u]      = t < nall ? (GATHER ? a.gmap[e0 * NC + t] : t) : -1;
         }
-        else
+        T val[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u)
+            val[u] = src[u] >= 0 ? in0[src[u]] : T(0);
+#pragma unroll
+        for (int u = 0; u < PER; ++u)
         {
-            v = a.in[gi];
+            const int t = tid + u * TH;
+            if (t < nall)
+            {
+                T v = val[u];
+                if (GATHER && a.gsign)
+                    v *= T(a.gsign[e0 * NC + t]);
+                const int lt = t / NC;
+                const int m  = t - lt * NC;
+                const int rq = m / NM;
+                v0s[lt * RS + rq * NMP + (m - rq * NM)] = v;
+            }
         }
-        const int rq = m / NM;
-        v0s[lt * RS + rq * NMP + (m - rq * NM)] = v;
     }
     __syncthreads();
 
