@@ -83,21 +83,30 @@ __global__ void __launch_bounds__(ColDims<SHAPE, NM>::THREADS) k_col_helm(GenArg
         D1[l] = ColLd(a.t.D1 + l);
     for (int l = tid; l < Q2 * Q2; l += blockDim.x)
         D2[l] = ColLd(a.t.D2 + l);
-    for (int m = tid; m < NC; m += blockDim.x)
+    // the element's coefficients: every map entry of the thread, then every
+    // value, then the stores, so a thread's loads are in flight together
     {
-        const long gi = e * NC + m;
-        T v;
-        if (GATHER)
+        constexpr int TH  = C::THREADS;
+        constexpr int PER = (NC + TH - 1) / TH;
+        const T *in0      = GATHER ? a.in : a.in + e * NC;
+        int src[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u)
         {
-            v = a.in[a.gmap[gi]];
-            if (a.gsign)
-                v *= T(a.gsign[gi]);
+            const int m = tid + u * TH;
+            src[u]      = m < NC ? (GATHER ? a.gmap[e * NC + m] : m) : -1;
         }
-        else
+        T val[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u)
+            val[u] = src[u] >= 0 ? in0[src[u]] : T(0);
+#pragma unroll
+        for (int u = 0; u < PER; ++u)
         {
-            v = a.in[gi];
+            const int m = tid + u * TH;
+            if (m < NC)
+                x[m] = (GATHER && a.gsign) ? val[u] * T(a.gsign[e * NC + m]) : val[u];
         }
-        x[m] = v;
     }
     __syncthreads();
 
