@@ -229,19 +229,51 @@ __global__ void k_assemble(int nglob, int ndir, const int *__restrict__ aptr,
 {
     if (st && st->done)
         return;
-    double sw = 0.0;
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nglob; g += gridDim.x * blockDim.x)
+    // a thread's dofs g0, g0 + stride, ... are taken four at a time with their
+    // entries walked in lockstep, so the index and value loads of four dofs
+    // are in flight together; every dof still sums its entries in CSR order
+    // and the thread visits its dofs in the same order
+    constexpr int U = 4;
+    const int stride = gridDim.x * blockDim.x;
+    double sw        = 0.0;
+    for (int g0 = blockIdx.x * blockDim.x + threadIdx.x; g0 < nglob; g0 += U * stride)
     {
-        T acc = 0;
-        const int k1 = aptr[g + 1];
-        for (int k = aptr[g]; k < k1; ++k)
+        int k0[U], k1[U];
+        int kmax = 0;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
         {
-            const int l = aidx[k];
-            acc += sign ? T(sign[l]) * loc[l] : loc[l];
+            const int g = g0 + u * stride;
+            k0[u]       = g < nglob ? aptr[g] : 0;
+            k1[u]       = g < nglob ? aptr[g + 1] : 0;
+            kmax        = max(kmax, k1[u] - k0[u]);
         }
-        glob[g] = acc;
-        if (w && g >= ndir && g - ndir < nsw)
-            sw += double(acc) * double(w[g]);
+        T acc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            acc[u] = 0;
+        for (int j = 0; j < kmax; ++j)
+        {
+            int l[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                l[u] = k0[u] + j < k1[u] ? aidx[k0[u] + j] : -1;
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (l[u] >= 0)
+                    acc[u] += sign ? T(sign[l[u]]) * loc[l[u]] : loc[l[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int g = g0 + u * stride;
+            if (g < nglob)
+            {
+                glob[g] = acc[u];
+                if (w && g >= ndir && g - ndir < nsw)
+                    sw += double(acc[u]) * double(w[g]);
+            }
+        }
     }
     if (part)
         BlockSum2(sw, 0.0, part);
