@@ -835,12 +835,13 @@ __global__ void k_unit_col(long n, int nc, int j, double *__restrict__ x)
         x[i] = (i % nc == j) ? 1.0 : 0.0;
 }
 
-// K[e][i][j] = y[e][i]
-__global__ void k_put_col(long n, int nc, int j, const double *__restrict__ y,
+// K[e][i][j] = y[e][i], K rows of `stride` doubles (nc, or the width of a
+// column group)
+__global__ void k_put_col(long n, int stride, int j, const double *__restrict__ y,
                           double *__restrict__ K)
 {
     for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
-        K[i * nc + j] = y[i];
+        K[i * stride + j] = y[i];
 }
 
 extern "C" int nkb_op_element_matrices(nkb_op *op, double *K, int flags, void *stream)
@@ -857,36 +858,48 @@ extern "C" int nkb_op_element_matrices(nkb_op *op, double *K, int flags, void *s
     const int nc  = int(nin / op->nelmt);
     const long n  = nin;
     NKB_CUDA_TRY(cudaSetDevice(op->device));
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    double *x = nullptr, *y = nullptr, *dK = (flags & NKB_HOST_PTRS) ? nullptr : K;
+    cudaStream_t s   = static_cast<cudaStream_t>(stream);
+    const bool host  = (flags & NKB_HOST_PTRS) != 0;
+    // host K: built a group of columns at a time in a device buffer of at
+    // most 1 GiB, each group copied into the strided host rows by one 2-D copy
+    const int width  = host ? int(std::max<long>(1, std::min<long>(nc, (1L << 30) / (n * 8)))) : nc;
+    double *x = nullptr, *y = nullptr, *dK = host ? nullptr : K;
     auto release = [&]() {
         cudaFree(x);
         cudaFree(y);
-        if (flags & NKB_HOST_PTRS)
+        if (host)
             cudaFree(dK);
     };
     if (cudaMalloc(&x, n * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&y, n * sizeof(double)) != cudaSuccess ||
-        ((flags & NKB_HOST_PTRS) && cudaMalloc(&dK, size_t(n) * nc * sizeof(double)) != cudaSuccess))
+        (host && cudaMalloc(&dK, size_t(n) * width * sizeof(double)) != cudaSuccess))
     {
         release();
-        return SetError(NKB_ERR_NOMEM, "nkb_op_element_matrices: %ld x %d doubles", n, nc);
+        return SetError(NKB_ERR_NOMEM, "nkb_op_element_matrices: %ld x %d doubles", n, width);
     }
-    const int nb = int(std::min<long>((n + 255) / 256, 148L * 16));
-    for (int j = 0; j < nc; ++j)
+    const int nb   = int(std::min<long>((n + 255) / 256, 148L * 16));
+    cudaError_t ce = cudaSuccess;
+    for (int j0 = 0; j0 < nc && ce == cudaSuccess; j0 += width)
     {
-        k_unit_col<<<nb, 256, 0, s>>>(n, nc, j, x);
-        int rc = LaunchOp<double>(op, x, y, nullptr, nullptr, nullptr, nullptr, s);
-        if (rc)
+        const int w = std::min(width, nc - j0);
+        for (int j = j0; j < j0 + w; ++j)
         {
-            release();
-            return rc;
+            k_unit_col<<<nb, 256, 0, s>>>(n, nc, j, x);
+            int rc = LaunchOp<double>(op, x, y, nullptr, nullptr, nullptr, nullptr, s);
+            if (rc)
+            {
+                cudaStreamSynchronize(s);
+                release();
+                return rc;
+            }
+            k_put_col<<<nb, 256, 0, s>>>(n, host ? width : nc, host ? j - j0 : j, y, dK);
         }
-        k_put_col<<<nb, 256, 0, s>>>(n, nc, j, y, dK);
+        ce = cudaGetLastError();
+        if (ce == cudaSuccess && host)
+            ce = cudaMemcpy2DAsync(K + j0, size_t(nc) * sizeof(double), dK,
+                                   size_t(width) * sizeof(double), size_t(w) * sizeof(double),
+                                   size_t(n), cudaMemcpyDeviceToHost, s);
     }
-    cudaError_t ce = cudaGetLastError();
-    if (ce == cudaSuccess && (flags & NKB_HOST_PTRS))
-        ce = cudaMemcpyAsync(K, dK, size_t(n) * nc * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (ce == cudaSuccess)
         ce = cudaStreamSynchronize(s);
     release();
