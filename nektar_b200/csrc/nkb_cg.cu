@@ -81,12 +81,14 @@ __device__ __forceinline__ void BlockSum2(double a, double b, double *part)
 }
 
 // the partial dot products count the free dofs i < nown only (all of them on
-// one GPU; a shard's own dofs, numbered first, in a sharded solve)
+// one GPU; a shard's own dofs, numbered first, in a sharded solve). wjac: the
+// previous w is the Jacobi step of the previous r (no block step has changed
+// it), so it is recomputed as r dinv, the same product, instead of read.
 template <typename T>
 __global__ void k_update(int nn, int ndir, const CGState *st, T *__restrict__ p, T *__restrict__ q,
                          T *__restrict__ x, T *__restrict__ r, T *__restrict__ w,
                          const T *__restrict__ s, const T *__restrict__ dinv, double *part,
-                         int nown)
+                         int nown, int wjac)
 {
     if (st->done)
         return;
@@ -94,14 +96,16 @@ __global__ void k_update(int nn, int ndir, const CGState *st, T *__restrict__ p,
     double rw = 0.0, rr = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x)
     {
-        const T pi = fma(beta, p[i], w[ndir + i]);
-        const T qi = fma(beta, q[i], s[ndir + i]);
+        const T rold = r[i], dv = dinv[i];
+        const T wold = wjac ? rold * dv : w[ndir + i];
+        const T pi   = fma(beta, p[i], wold);
+        const T qi   = fma(beta, q[i], s[ndir + i]);
         p[i]       = pi;
         q[i]       = qi;
         x[ndir + i] = fma(alpha, pi, x[ndir + i]);
-        const T ri = fma(-alpha, qi, r[i]);
+        const T ri = fma(-alpha, qi, rold);
         r[i]       = ri;
-        const T wi = ri * dinv[i];
+        const T wi = ri * dv;
         w[ndir + i] = wi;
         if (i < nown)
         {
@@ -731,7 +735,7 @@ static int Iteration32(nkb_sys *S, cudaStream_t s)
     const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
     S->launches += 3 + long(S->ops32.size());
     k_update<float><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st32, S->p32, S->q32, S->x32,
-                                                S->r32, S->w32, S->s32, S->dinv32, S->partA, S->nn);
+                                                S->r32, S->w32, S->s32, S->dinv32, S->partA, S->nn, 0);
     int rc = Matvec32(S, S->w32, S->yl32, s, &S->st32->done);
     if (rc)
         return rc;
@@ -770,7 +774,7 @@ static int Iteration(nkb_sys *S, cudaStream_t s)
     const int nbU = Blocks(S->nn), nbA = Blocks(S->nglob);
     S->launches += 3 + long(S->ops.size());
     k_update<double><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st, S->p, S->q, S->x, S->r,
-                                                 S->w, S->s, S->d_dinv, S->partA, S->nn);
+                                                 S->w, S->s, S->d_dinv, S->partA, S->nn, S->sh->nblk ? 0 : 1);
     BlockPrecon(S, s);
     int rc = Matvec(S, S->w, S->yl, true, s, &S->st->done);
     if (rc)
@@ -1775,7 +1779,7 @@ extern "C" int nkb_sys_profile_iteration(nkb_sys *S, int iters, nkb_sys_profile 
     NKB_CUDA_TRY(cudaEventRecord(e[2], s));
     for (int it = 0; it < iters; ++it)
         k_update<double><<<nbU, kRedThreads, 0, s>>>(S->nn, S->ndir, S->st, S->p, S->q, S->x,
-                                                     S->r, S->w, S->s, S->d_dinv, S->partA, S->nn);
+                                                     S->r, S->w, S->s, S->d_dinv, S->partA, S->nn, S->sh->nblk ? 0 : 1);
     NKB_CUDA_TRY(cudaEventRecord(e[3], s));
     NKB_CUDA_TRY(cudaStreamSynchronize(s));
     cudaEvent_t e4, e5;

@@ -288,7 +288,7 @@ static int GroupIteration(nkb_shard_group *G)
         nkb_sys *S = d.S;
         k_update<double><<<Blocks(S->nn), kRedThreads, 0, s>>>(S->nn, S->ndir, S->st, S->p, S->q,
                                                                S->x, S->r, S->w, S->s, S->d_dinv,
-                                                               S->partA, d.nown);
+                                                               S->partA, d.nown, 1);
         int rc = Matvec(S, S->w, S->yl, true, s, &S->st->done);
         if (rc)
             return rc;
