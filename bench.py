@@ -436,9 +436,31 @@ def digest_check(rec, xl, x_conv):
             "positions": int(pos.size)}
 
 
-def operator_roofline(nb, torch, dev, n, p, precision, hbm, iters=20):
+def compute_peaks(nb, dev):
+    """The device's FP64 FMA, FP64 tensor-core MMA and FP32 FMA rates in
+    TFLOP/s, measured in place (nkb_peak_probe); None where unmeasurable."""
+    import ctypes
+    out = {}
+    for kind, key in ((0, "fp64_fma_tflops"), (1, "fp64_mma_tflops"), (2, "fp32_fma_tflops")):
+        v = ctypes.c_double(0.0)
+        rc = nb.lib().nkb_peak_probe(kind, dev, ctypes.byref(v))
+        out[key] = v.value if rc == 0 else None
+    return out
+
+
+def hex_flops(nm, nq):
+    """Algorithmic FLOPs of one Hex Helmholtz element (sum factorisation:
+    BwdTrans and one inner product, the collocation gradient and its
+    transpose, the metric and the mass term)."""
+    return (4 * (nq * nm ** 3 + nq ** 2 * nm ** 2 + nq ** 3 * nm) + 12 * nq ** 4
+            + 18 * nq ** 3)
+
+
+def operator_roofline(nb, torch, dev, n, p, precision, hbm, iters=20, peaks=None):
     """Element Helmholtz apply on an n^3 curved box at order p (local
-    vectors, autotuned kernel): ms, GB/s of the algorithmic bytes, fraction."""
+    vectors, autotuned kernel): ms, GB/s of the algorithmic bytes, fraction;
+    with peaks, TFLOP/s of the algorithmic FLOPs and their fraction of the
+    precision's measured rate (FP64: the higher of FMA and tensor-core MMA)."""
     nm = p + 1
     m = nb.BoxMesh("hex", n, nm, nm + 1, amp=AMP)
     op = nb.Operator("helmholtz", m, device=dev, precision=precision)
@@ -461,6 +483,14 @@ def operator_roofline(nb, torch, dev, n, p, precision, hbm, iters=20):
     out = {"mesh": "%d^3" % n, "P": p, "precision": precision, "kernel": op.kernel(), "ms": ms,
            "gb_s": byts / ms / 1e6, "frac": byts / ms / 1e6 / hbm,
            "algorithmic_bytes": byts}
+    flops = m.nelmt * hex_flops(nm, nm + 1)
+    out["algorithmic_flops"] = flops
+    out["tflops"] = flops / (ms * 1e-3) / 1e12
+    if peaks:
+        pk = (max(v for v in (peaks.get("fp64_fma_tflops"), peaks.get("fp64_mma_tflops")) if v)
+              if precision == "fp64" else peaks.get("fp32_fma_tflops"))
+        if pk:
+            out["compute_frac"] = out["tflops"] / pk
     op.close()
     return out
 
@@ -495,6 +525,7 @@ def run_b200(args, rank, world, local):
         except Exception as exc:  # the baseline must never sink the GPU number
             cpu_base = {"value": None, "unavailable": repr(exc)[:200]}
 
+    peaks_c = compute_peaks(nb, dev)
     P = Problem(nb, torch, N_CELLS, NM, dev)
     nloc, nglob, ndir = P.nloc, P.nglob, P.ndir
     b_pin = torch.tensor(P.b_host).pin_memory()
@@ -555,6 +586,10 @@ def run_b200(args, rank, world, local):
                                                       "scalars_ms")},
                 "iteration": {"ms": it_ms, "algorithmic_bytes": it_bytes,
                               "frac": it_bytes / (it_ms * 1e-3) / 1e9 / hbm}}
+    fp64_peak = max([v for v in (peaks_c.get("fp64_fma_tflops"), peaks_c.get("fp64_mma_tflops"))
+                     if v] or [0.0])
+    if fp64_peak:
+        roofline["compute_frac"] = roofline["fp64_tflops"] / fp64_peak
 
     extras = {}
     rec = reference_iterations()
@@ -595,7 +630,7 @@ def run_b200(args, rank, world, local):
         del x3, x3c
         c3.close()
         # ---- element operators alone at P = 4, 6, 8 (FP64 and FP32) ------------
-        extras["operators"] = [operator_roofline(nb, torch, dev, n, p, prec, hbm)
+        extras["operators"] = [operator_roofline(nb, torch, dev, n, p, prec, hbm, peaks=peaks_c)
                                for n, p in ((32, 4), (32, 6), (24, 8))
                                for prec in ("fp64", "fp32")]
         # ---- mixed-element batched apply (110000 hexes, prisms and tets) -------
@@ -616,7 +651,7 @@ def run_b200(args, rank, world, local):
         "helmholtz_gdof_s": nloc / (prof["op_ms"] * 1e-3) / 1e9,
         "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": 2 * nloc * 8,
                 "d2h_bytes_per_step": nloc * 8},
-        "roofline": roofline, "cpu_baseline": cpu_base,
+        "roofline": roofline, "compute_peaks": peaks_c, "cpu_baseline": cpu_base,
         "clocks": clocks.summary(), "gpu_launches": int(sum(r.kernel_launches for r in reps)),
     }
     line.update(extras)

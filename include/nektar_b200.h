@@ -552,6 +552,13 @@ typedef struct nkb_geom_request
     int deformed;       /* 1: per-point factors, 0: one value per element */
 } nkb_geom_request;
 
+/* Arithmetic rate of the device measured in place, in TFLOP/s: kind 0 FP64
+ * fused multiply-add on the CUDA cores, 1 FP64 tensor-core MMA (m8n8k4),
+ * 2 FP32 fused multiply-add (independent chains per thread, the best of five
+ * timed launches after three warm-up ones). The compute denominators of the
+ * operators' rooflines; no counterpart in the reference. */
+int nkb_peak_probe(int kind, int device, double *tflops);
+
 /* Number of elements the request produces. */
 long nkb_geom_nelmt(const nkb_geom_request *req);
 

@@ -138,6 +138,7 @@ SIGNATURES = {
     "nkb_sys_footprint": (c_int, [c_void_p, P(c_size_t), P(c_size_t)]),
     "nkb_geom_nelmt": (c_long, [P(GeomRequest)]),
     "nkb_geom_fill": (c_int, [P(GeomRequest), dp, dp, dp]),
+    "nkb_peak_probe": (c_int, [c_int, c_int, dp]),
     "nkb_geom_fill_device": (c_int, [P(GeomRequest), c_void_p, c_void_p, c_void_p, c_int,
                                      c_void_p]),
     "nkb_hex_box_assembly": (c_int, [c_int, c_int, ip, ip, ip]),

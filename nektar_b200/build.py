@@ -27,7 +27,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC"]
 SOURCES = ["nkb_setup.cpp", "nkb_ops.cu", "nkb_hex.cu", "nkb_hex_f64.cu", "nkb_hex_f32.cu",
            "nkb_cg.cu", "nkb_static.cu", "nkb_batch.cu", "nkb_dense.cu", "nkb_gen_f64.cu",
            "nkb_gen_f32.cu", "nkb_col_f64.cu", "nkb_col_f32.cu", "nkb_tc.cu", "nkb_sc.cu", "nkb_nccl.cpp",
-           "nkb_geom.cu"]
+           "nkb_geom.cu", "nkb_peak.cu"]
 
 
 def _nvcc():

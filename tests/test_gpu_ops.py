@@ -384,3 +384,20 @@ def test_device_geometry_matches_host_geometry(shape, n, nm, amp, coords):
     for o in (oh, od):
         o.set_factors(1.3)
     assert rel_l2(od(x), oh(x)) < 1e-13
+
+
+def test_peak_probe_rates_are_plausible():
+    """nkb_peak_probe: the device's FP64 FMA, FP64 tensor-core MMA and FP32
+    FMA rates (TFLOP/s) lie within the bounds a B200-class part can reach,
+    FP32 above FP64; an unknown kind is rejected."""
+    import ctypes
+    rates = []
+    for kind in (0, 1, 2):
+        v = ctypes.c_double(0.0)
+        nb.check(nb.lib().nkb_peak_probe(kind, 0, ctypes.byref(v)))
+        rates.append(v.value)
+    fma64, mma64, fma32 = rates
+    assert 5.0 < fma64 < 100.0 and 5.0 < mma64 < 150.0 and 20.0 < fma32 < 250.0, rates
+    assert fma32 > fma64, rates
+    v = ctypes.c_double(0.0)
+    assert nb.lib().nkb_peak_probe(3, 0, ctypes.byref(v)) == nb.C.NKB_ERR_INVALID
