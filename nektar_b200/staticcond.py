@@ -36,7 +36,11 @@ classes for GlobalLinSysIterativeStaticCond):
                step of "block" built from S~, and the solution is mapped back
                with R^T (v_DoTransformCoeffsFromLowEnergy). Hexahedra,
                tetrahedra and prisms (the prism's transform assembled from the
-               hexahedron's and the tetrahedron's), one order.
+               hexahedron's and the tetrahedron's). On meshes of variable
+               order the transforms are built at the highest order and cut
+               down to each element's modes (ExtractLocMat), and the modes a
+               lower-order neighbour lacks are masked out of S, the
+               right-hand side and the solution (CreateVariablePMask).
 """
 import time
 
@@ -194,6 +198,68 @@ def _maps(shape, nm):
     return bm.size, V, E, F
 
 
+def boundary_keys(shape, nm):
+    """Identity of each boundary mode (in boundary_interior's order) that
+    does not depend on the order: ("v", vertex), ("e", edge, k) for the
+    edge's polynomial index k, ("f", face, a, b) for the face's indices."""
+    bm, _ = boundary_interior(shape, nm)
+    verts, edges, faces = topology(shape, nm)
+    key = {m: ("v", v) for v, m in enumerate(verts)}
+    for e, (_, _, lst) in enumerate(edges):
+        key.update({m: ("e", e, k) for m, k in lst})
+    for f, (_, _, lst) in enumerate(faces):
+        key.update({m: ("f", f, a, b) for m, a, b in lst})
+    return [key[int(m)] for m in bm]
+
+
+def transform_of_order(shape, nm, nmax, Rmax):
+    """The transform of an element of order nm cut from the one built at the
+    mesh's highest order nmax (PreconditionerLowEnergy::ExtractLocMat,
+    PreconditionerLowEnergy.cpp:2317-2405): unit diagonal and the
+    vertex-edge, vertex-face and edge-face entries of Rmax between the modes
+    with the same vertex, edge or face and polynomial indices. Rmax has no
+    other off-diagonal entries, so this is the submatrix of Rmax on the
+    element's modes."""
+    if nm == nmax:
+        return Rmax
+    pos = {k: i for i, k in enumerate(boundary_keys(shape, nmax))}
+    sel = np.array([pos[k] for k in boundary_keys(shape, nm)], dtype=np.int64)
+    return Rmax[np.ix_(sel, sel)].copy()
+
+
+def lowenergy_part_transforms(parts, bsign, lam, device=0, reference=None):
+    """Sets each part's "R" (its shape's transform at its order), "Rinv" and
+    "mask" ((ne, nb) booleans, False on the local boundary modes of sign 0
+    that a lower-order neighbour lacks; None when there are none) from the
+    transforms of the mesh's highest order (SetupBlockTransformationMatrix
+    and CreateVariablePMask, PreconditionerLowEnergy.cpp:940-1045,
+    1255-1275)."""
+    nmax = max(p["nm"] for p in parts)
+    Rs = lowenergy_transforms({p["shape"] for p in parts}, nmax, lam, device, reference)
+    ob = 0
+    for p in parts:
+        nbm = p["bm"].size
+        R = transform_of_order(p["shape"], p["nm"], nmax, Rs[p["shape"]])
+        mask = bsign[ob:ob + p["ne"] * nbm].reshape(p["ne"], nbm) != 0
+        ob += p["ne"] * nbm
+        p["R"], p["Rinv"] = R, np.linalg.inv(R)
+        p["mask"] = None if mask.all() else mask
+
+
+def element_transforms(p, rows=None):
+    """The transform applied to a part's elements (all, or those of rows):
+    R with the columns of the masked modes zeroed, R M_e, so that
+    S~ = R M S M R^T (v_TransformedSchurCompl), b~ = R M b
+    (v_DoTransformBasisToLowEnergy) and x = M R^T x~
+    (v_DoTransformCoeffsFromLowEnergy); one (nb, nb) matrix without a mask,
+    else one per element."""
+    R, mask = p["R"], p.get("mask")
+    if R is None or mask is None:
+        return R
+    m = mask if rows is None else mask[rows]
+    return R[None, :, :] * m[:, None, :]
+
+
 def lowenergy_transforms(shapes, nm, lam, device=0, reference=None):
     """R per shape for a mesh with the given shapes at nm modes, as
     SetUpReferenceElements (PreconditionerLowEnergy.cpp:1662-1876) sets them
@@ -271,19 +337,27 @@ def entity_index(parts, bmap, bsign, ndir):
         sb = bsign[ob:ob + ne * nbm].reshape(ne, nbm)
         ob += ne * nbm
         _, E, F, _, _ = _entities(p["shape"], p["nm"], p["bm"])
-        er = np.arange(ne)[:, None]
         for L in E + F:
-            n = L.size
-            if n < 2:
+            if L.size < 2:
                 continue
-            idx = L[np.argsort(gb[:, L], axis=1)]
-            G = gb[er, idx]
-            dirm = G < ndir
-            if (dirm.any(axis=1) != dirm.all(axis=1)).any():
-                raise ValueError("an edge or face has Dirichlet and free dofs")
-            keep = ~dirm[:, 0]
-            groups.setdefault(n, []).append((k, er[keep, 0], G[keep], idx[keep],
-                                             sb[er, idx][keep].astype(np.int8)))
+            # on meshes of variable order only the modes of nonzero sign (those
+            # of the entity's lowest-order element) form the block
+            act = sb[:, L] != 0
+            cnt = act.sum(axis=1)
+            for n in np.unique(cnt):
+                if n < 2:
+                    continue
+                el = np.flatnonzero(cnt == n)
+                er = el[:, None]
+                Ln = L[np.argsort(~act[el], axis=1, kind="stable")[:, :n]]
+                idx = np.take_along_axis(Ln, np.argsort(gb[er, Ln], axis=1), axis=1)
+                G = gb[er, idx]
+                dirm = G < ndir
+                if (dirm.any(axis=1) != dirm.all(axis=1)).any():
+                    raise ValueError("an edge or face has Dirichlet and free dofs")
+                keep = ~dirm[:, 0]
+                groups.setdefault(int(n), []).append((k, el[keep], G[keep], idx[keep],
+                                                      sb[er, idx][keep].astype(np.int8)))
     dofs = []
     contrib = [[] for _ in parts]
     for n in sorted(groups):
@@ -387,14 +461,26 @@ def _blocks_invert(bptr, A, device):
                                         ctypes.c_void_p(A.data_ptr()), device, None))
 
 
-def _condense_device(op, bm, im, R, device):
+def _mask_groups(p):
+    """[(element rows or None for all, transform)]: the part's elements
+    grouped by their variable-order mask, one transform per group."""
+    if p.get("mask") is None:
+        return [(None, p["R"])]
+    pats, inv = np.unique(p["mask"], axis=0, return_inverse=True)
+    inv = inv.reshape(-1)
+    return [(np.flatnonzero(inv == g), p["R"] * pat[None, :]) for g, pat in enumerate(pats)]
+
+
+def _condense_device(op, p, device):
     """(S, W, V) of an Operator's elements as device tensors: its element
-    matrices built on the device and condensed there (nkb_condense)."""
+    matrices built on the device and condensed there (nkb_condense), one
+    call per group of elements that share a transform."""
     import ctypes
 
     import torch
 
     import nektar_b200 as nb
+    bm, im = p["bm"], p["im"]
     nc, ne = op.in_size // op.nelmt, op.nelmt
     nbm, ni = len(bm), len(im)
     dev = "cuda:%d" % device
@@ -407,14 +493,28 @@ def _condense_device(op, bm, im, R, device):
     V = torch.empty((ne, nc, nbm + ni), dtype=torch.float64, device=dev)
     bmi = np.ascontiguousarray(bm, dtype=np.int32)
     imi = np.ascontiguousarray(im, dtype=np.int32)
-    Rc = None if R is None else np.ascontiguousarray(R, dtype=np.float64)
     ip = ctypes.POINTER(ctypes.c_int)
-    nb.check(nb.lib().nkb_condense(ne, nc, ctypes.c_void_p(K.data_ptr()), nbm,
-                                   bmi.ctypes.data_as(ip), ni, imi.ctypes.data_as(ip),
-                                   None if Rc is None else Rc.ctypes.data_as(
-                                       ctypes.POINTER(ctypes.c_double)),
-                                   ctypes.c_void_p(S.data_ptr()), ctypes.c_void_p(W.data_ptr()),
-                                   ctypes.c_void_p(V.data_ptr()), device, None))
+    for rows, R in _mask_groups(p):
+        if rows is None:
+            Kg, Sg, Wg, Vg = K, S, W, V
+        else:
+            ri = torch.as_tensor(rows, device=dev)
+            Kg = K.index_select(0, ri)
+            Sg, Wg, Vg = (torch.empty((rows.size,) + t.shape[1:], dtype=torch.float64, device=dev)
+                          for t in (S, W, V))
+        Rc = None if R is None else np.ascontiguousarray(R, dtype=np.float64)
+        nb.check(nb.lib().nkb_condense(int(Kg.shape[0]), nc, ctypes.c_void_p(Kg.data_ptr()), nbm,
+                                       bmi.ctypes.data_as(ip), ni, imi.ctypes.data_as(ip),
+                                       None if Rc is None else Rc.ctypes.data_as(
+                                           ctypes.POINTER(ctypes.c_double)),
+                                       ctypes.c_void_p(Sg.data_ptr()),
+                                       ctypes.c_void_p(Wg.data_ptr()),
+                                       ctypes.c_void_p(Vg.data_ptr()), device, None))
+        if rows is not None:
+            torch.cuda.synchronize(dev)
+            S[ri], W[ri], V[ri] = Sg, Wg, Vg
+            del Kg, Sg, Wg, Vg
+    torch.cuda.synchronize(dev)
     del K
     return S, W, V
 
@@ -438,19 +538,53 @@ def solve_maps(C, Kii_inv, Kib, bm, im, R=None):
                           x_i = Kii^-1 b_i - Kii^-1 Kib R^T x~
                                                         from [x~_e, b_i,e]
 
-    with R the low-energy transform (identity if None); V's rows are in the
-    element's local mode order."""
+    with R the low-energy transform (identity if None; one for all elements
+    or one per element); V's rows are in the element's local mode order."""
     ne, nbm, ni = C.shape
     nc = nbm + ni
     R = np.eye(nbm) if R is None else R
+    RT = np.swapaxes(R, -1, -2)
     W = np.zeros((ne, nbm, nc))
     W[:, :, bm] = R
     W[:, :, im] = -(R @ C)
     V = np.zeros((ne, nc, nbm + ni))
-    V[:, bm, :nbm] = R.T
-    V[:, im, :nbm] = -(Kii_inv @ (Kib @ R.T))
+    V[:, bm, :nbm] = RT
+    V[:, im, :nbm] = -(Kii_inv @ (Kib @ RT))
     V[:, im, nbm:] = Kii_inv
     return W, V
+
+
+def condensed_parts(collections):
+    """One dict per collection (shape, nm, number of elements) with its
+    boundary / interior mode split and its offset in the local space."""
+    parts, off = [], 0
+    for shape, nm, ne in collections:
+        nc = ncoeffs(shape, nm)
+        bm, im = boundary_interior(shape, nm)
+        parts.append(dict(nc=nc, ne=ne, bm=bm, im=im, off=off, shape=shape, nm=nm, R=None,
+                          mask=None))
+        off += ne * nc
+    return parts
+
+
+def boundary_map(parts, gmap, sign, nglob, ndir):
+    """(bmap, bsign, number of boundary dofs): the local boundary modes' map
+    to the boundary dofs, renumbered in their original order (the Dirichlet
+    dofs first, as they were), and their signs."""
+    gmap = np.asarray(gmap)
+    sign = np.ones(gmap.size) if sign is None else np.asarray(sign, dtype=np.float64)
+    bglob, bsign = [], []
+    for p in parts:
+        ne, nc, off = p["ne"], p["nc"], p["off"]
+        bglob.append(gmap[off:off + ne * nc].reshape(ne, nc)[:, p["bm"]].ravel())
+        bsign.append(sign[off:off + ne * nc].reshape(ne, nc)[:, p["bm"]].ravel())
+    bglob = np.concatenate(bglob)
+    ids = np.unique(bglob)
+    if ndir and (ids[:ndir] != np.arange(ndir)).any():
+        raise ValueError("Dirichlet dofs must be boundary dofs numbered first")
+    renum = np.full(nglob, -1, dtype=np.int64)
+    renum[ids] = np.arange(ids.size)
+    return renum[bglob].astype(np.int32), np.concatenate(bsign), int(ids.size)
 
 
 class StaticCondSys:
@@ -489,50 +623,18 @@ class StaticCondSys:
             t = time.perf_counter()
             self.setup_breakdown[name] = self.setup_breakdown.get(name, 0.0) + t - tp[0]
             tp[0] = t
-        self.parts = []
-        gmap = np.asarray(gmap)
-        sign = np.ones(gmap.size) if sign is None else np.asarray(sign, dtype=np.float64)
-        off = 0
-        bglob, bsign = [], []
-        for k, op in enumerate(self.ops):
-            nc, ne = op.in_size // op.nelmt, op.nelmt
-            bm, im = boundary_interior(op.shape, op.nm)
-            gm = gmap[off:off + ne * nc].reshape(ne, nc)
-            sg = sign[off:off + ne * nc].reshape(ne, nc)
-            bglob.append(gm[:, bm].ravel())
-            bsign.append(sg[:, bm].ravel())
-            self.parts.append(dict(nc=nc, ne=ne, bm=bm, im=im, off=off, shape=op.shape, nm=op.nm,
-                                   R=None))
-            off += ne * nc
-        self.nloc = off
-        bglob = np.concatenate(bglob)
-        # boundary dofs renumbered in their original order (Dirichlet first kept)
-        ids = np.unique(bglob)
-        if ndir and (ids[:ndir] != np.arange(ndir)).any():
-            raise ValueError("Dirichlet dofs must be boundary dofs numbered first")
-        renum = np.full(nglob, -1, dtype=np.int64)
-        renum[ids] = np.arange(ids.size)
-        self.bmap = renum[bglob].astype(np.int32)
-        self.bsign = np.concatenate(bsign)
-        self.nglob_b, self.ndir = int(ids.size), int(ndir)
-        self.nglob = int(nglob)
+        self.parts = condensed_parts([(op.shape, op.nm, op.nelmt) for op in self.ops])
+        self.nloc = sum(p["ne"] * p["nc"] for p in self.parts)
+        self.bmap, self.bsign, self.nglob_b = boundary_map(self.parts, gmap, sign, nglob, ndir)
+        self.ndir, self.nglob = int(ndir), int(nglob)
         phase("maps")
         if precon == "lowenergy":
             if lam is None:
                 lam = getattr(self.ops[0], "lam", None)
             if lam is None:
                 raise ValueError("lowenergy needs the Helmholtz lambda")
-            nms = {p["nm"] for p in self.parts}
-            if len(nms) != 1:
-                raise NotImplementedError("lowenergy: collections of one order only")
-            Rs = lowenergy_transforms({p["shape"] for p in self.parts}, nms.pop(), float(lam),
-                                      device)
-            for p in self.parts:
-                R = Rs[p["shape"]]
-                p["R"], p["Rinv"] = R, np.linalg.inv(R)
+            lowenergy_part_transforms(self.parts, self.bsign, float(lam), device)
             phase("lowenergy_transform")
-        if precon != "diagonal" and (self.bsign == 0).any():
-            raise NotImplementedError("%s: meshes of variable order" % precon)
         need_blocks = precon != "diagonal"
         need_host_S = need_blocks and self.setup == "host"
         if need_blocks and self.setup == "device":
@@ -542,7 +644,7 @@ class StaticCondSys:
         self.dense, self.W, self.V = [], [], []
         for k, (op, p) in enumerate(zip(self.ops, self.parts)):
             if self.setup == "device":
-                S, W, V = _condense_device(op, p["bm"], p["im"], p["R"], device)
+                S, W, V = _condense_device(op, p, device)
                 phase("condense")
                 if need_blocks:
                     _blocks_accumulate(bptr, A, p, S, contrib[k], device)
@@ -556,9 +658,10 @@ class StaticCondSys:
             K = element_matrices(op) if matrices is None else matrices[k]
             S, C, Kii_inv, Kib = condense(K, p["bm"], p["im"])
             del K
-            if p["R"] is not None:
-                S = p["R"] @ S @ p["R"].T  # v_TransformedSchurCompl
-            W, V = solve_maps(C, Kii_inv, Kib, p["bm"], p["im"], p["R"])
+            Re = element_transforms(p)
+            if Re is not None:
+                S = Re @ S @ np.swapaxes(Re, -1, -2)  # v_TransformedSchurCompl
+            W, V = solve_maps(C, Kii_inv, Kib, p["bm"], p["im"], Re)
             del C, Kii_inv, Kib
             self.W.append(nb.DenseOperator(W, device=device))
             del W

@@ -9,16 +9,14 @@ import numpy as np
 from oracle import oracle as O
 
 
-def oracle_helm_solve(session, mesh=None):
-    """(local coefficients, L_inf, L_2) of the session's Helmholtz solve."""
-    from nektar_b200.meshgraph import SessionMesh
-    m = mesh or SessionMesh(session)
+def oracle_system(session, m):
+    """(element matrices per collection, local right-hand side, Robin
+    blocks) of the session's Helmholtz problem from the oracle's element
+    operators."""
     lam = session.parameters["Lambda"]
-    G = np.zeros((m.nglob, m.nglob))
     f = session.function("Forcing").evaluate(*m.xyz)
-    b_loc, us = [], []
-    for c, gmc, sgc, fc in zip(m.collections, m.split(m.gmap), m.split(m.sign),
-                               m.split(f, "phys")):
+    Ks, b_loc = [], []
+    for c, fc in zip(m.collections, m.split(f, "phys")):
         To = dict(c.T)
         To["w"] = c.T["ws"]
         nc, ne = c.nc, c.nelmt
@@ -28,14 +26,36 @@ def oracle_helm_solve(session, mesh=None):
             x[j::nc] = 1.0
             K[:, :, j] = O.helmholtz(c.shape, c.nm, c.nq, ne, To, c.jac, c.df, x, lam,
                                      True).reshape(ne, nc)
-        gm, sg = gmc.reshape(ne, nc), sgc.reshape(ne, nc)
-        for e in range(ne):
-            np.add.at(G, (gm[e][:, None], gm[e][None, :]), sg[e][:, None] * K[e] * sg[e][None, :])
+        Ks.append(K)
         b_loc.append(-O.iproduct(c.shape, c.nm, c.nq, ne, To["b"], To["w"], c.jac, fc, True))
     # Neumann / Robin: boundary inner products in the forcing, Robin face
     # mass matrices in the operator
     rhs_w, robin = m.weak_terms()
-    b_loc = np.concatenate(b_loc) + rhs_w
+    return Ks, np.concatenate(b_loc) + rhs_w, robin
+
+
+def oracle_errors(session, m, x_loc):
+    """(L_inf, L_2) of local coefficients against the session's exact
+    solution (the oracle's backward transform, the mesh's quadrature)."""
+    us = [O.bwdtrans(c.shape, c.nm, c.nq, c.nelmt, c.T["b"], xc)
+          for c, xc in zip(m.collections, m.split(x_loc))]
+    u = np.concatenate(us)
+    ue = session.function("ExactSolution").evaluate(*m.xyz)
+    W = m.quad_weights()
+    return float(np.max(np.abs(u - ue))), float(np.sqrt(np.sum(W * (u - ue) ** 2)))
+
+
+def oracle_helm_solve(session, mesh=None):
+    """(local coefficients, L_inf, L_2) of the session's Helmholtz solve."""
+    from nektar_b200.meshgraph import SessionMesh
+    m = mesh or SessionMesh(session)
+    lam = session.parameters["Lambda"]
+    Ks, b_loc, robin = oracle_system(session, m)
+    G = np.zeros((m.nglob, m.nglob))
+    for c, K, gmc, sgc in zip(m.collections, Ks, m.split(m.gmap), m.split(m.sign)):
+        gm, sg = gmc.reshape(c.nelmt, c.nc), sgc.reshape(c.nelmt, c.nc)
+        for e in range(c.nelmt):
+            np.add.at(G, (gm[e][:, None], gm[e][None, :]), sg[e][:, None] * K[e] * sg[e][None, :])
     for dofs, M, _ in robin:
         G[np.ix_(dofs, dofs)] += M
     # lifting with the local Dirichlet values element by element, as
@@ -49,12 +69,7 @@ def oracle_helm_solve(session, mesh=None):
     nd = m.ndir
     xg = np.concatenate([np.zeros(nd), np.linalg.solve(G[nd:, nd:], b[nd:])])
     xl = xdl + m.sign * xg[m.gmap]
-    for c, xc in zip(m.collections, m.split(xl)):
-        us.append(O.bwdtrans(c.shape, c.nm, c.nq, c.nelmt, c.T["b"], xc))
-    u = np.concatenate(us)
-    ue = session.function("ExactSolution").evaluate(*m.xyz)
-    W = m.quad_weights()
-    return xl, float(np.max(np.abs(u - ue))), float(np.sqrt(np.sum(W * (u - ue) ** 2)))
+    return (xl,) + oracle_errors(session, m, xl)
 
 
 def _apply_blocks(m, lam, x_loc):

@@ -171,7 +171,8 @@ def test_host_element_matrices_built_in_column_groups():
 
 
 @pytest.mark.parametrize("shape,n,nm", [("hex", 3, 5), ("hex", 2, 7), ("prism", 2, 5),
-                                        ("tet", 2, 4), ("hexprism", 2, 5)])
+                                        ("tet", 2, 4), ("hexprism", 2, 5), ("tet", 2, [3, 5, 4]),
+                                        ("hexprism", 2, [5, 4])])
 @pytest.mark.parametrize("precon", ["diagonal", "block", "lowenergy"])
 def test_device_setup_matches_host_setup(shape, n, nm, precon):
     """The device set-up (element matrices kept on the device, nkb_condense:
@@ -179,13 +180,20 @@ def test_device_setup_matches_host_setup(shape, n, nm, precon):
     transform folded in; the Block / LowEnergy entity blocks accumulated
     and inverted there, nkb_blocks_accumulate / nkb_blocks_invert) gives the
     host set-up's condensed operators, preconditioned iterations and
-    solutions."""
+    solutions; on meshes of variable order (nm a list of orders) the device
+    condenses each group of elements that share a variable-order mask with
+    its own masked transform."""
     from nektar_b200.meshgraph import SessionMesh
-    from nektar_b200.session import read_session, write_box_session
+    from nektar_b200.session import read_session, with_orders, write_box_session
     U = "sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)"
     F = "-(Lambda + 3*PI*PI/4)*sin(PI/2*x)*sin(PI/2*y)*sin(PI/2*z)"
-    s = read_session(write_box_session(shape, n, nm - 1, 1.0, U, F, U, shuffle_seed=5))
+    orders = nm if isinstance(nm, list) else None
+    nm = max(orders) if orders else nm
+    txt = write_box_session(shape, n, nm - 1, 1.0, U, F, U, shuffle_seed=5)
+    s = read_session(with_orders(txt, orders, seed=2) if orders else txt)
     mesh = SessionMesh(s)
+    if orders:
+        assert (mesh.sign == 0).any()
     ops = []
     for c in mesh.collections:
         H = nb.Operator("helmholtz", c)
