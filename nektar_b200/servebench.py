@@ -50,7 +50,7 @@ def main():
     wall = time.perf_counter() - t0
     s = summarize(res, reqs)
     s.update({
-        "metric": "Helmholtz solve requests served per second (Poisson %.0f req/s)" % a.rate,
+        "metric": "Helmholtz solve requests served per second (Poisson %g req/s)" % a.rate,
         "mode": "prewarmed contexts" if a.prewarm else "contexts built on demand",
         "prewarm_setup_s": setup_s, "wall_s": wall, "budget_bytes": budget,
         "peak_bytes": sch.peak, "max_active": a.max_active,
