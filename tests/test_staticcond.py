@@ -629,3 +629,26 @@ def test_reference_tet_varp_lowenergy_session_reproduces_its_record():
     linf, l2 = oracle_errors(s, d["m"], x)
     printed = lambda v: float("%g" % v)  # noqa: E731  (the demo prints six digits)
     assert abs(printed(l2) - 0.00416454) < 1e-7 and abs(printed(linf) - 0.0313733) < 1e-6
+
+
+def test_mask_groups_cover_every_element_once_with_its_own_transform():
+    """The device set-up condenses each group of elements that share a
+    variable-order mask with one transform: the groups partition the
+    elements, and each group's transform is every member's R M_e."""
+    from nektar_b200.session import read_session, with_orders, write_box_session
+    from nektar_b200.staticcond import _mask_groups, element_transforms
+    s = read_session(with_orders(write_box_session("tet", 2, 5, 1.0, "x", "0", "x",
+                                                   shuffle_seed=3), [3, 5, 4], seed=1))
+    d = _lowenergy_condensed(s, 1.0)
+    masked = [p for p in d["parts"] if p["mask"] is not None]
+    assert masked
+    for p in d["parts"]:
+        groups = _mask_groups(p)
+        if p["mask"] is None:
+            assert len(groups) == 1 and groups[0][0] is None and groups[0][1] is p["R"]
+            continue
+        rows = np.concatenate([r for r, _ in groups])
+        assert np.array_equal(np.sort(rows), np.arange(p["ne"]))
+        Re = element_transforms(p)
+        for r, R in groups:
+            assert np.array_equal(Re[r], np.broadcast_to(R, (r.size,) + R.shape))
