@@ -479,6 +479,7 @@ const char *KernelName(const nkb_op *op, bool gather)
         case 4: return "k_hex_helm_mma2 (FP64 tensor cores, two warps per element)";
         case 5: return "k_hex_helm_tc (tcgen05 TF32 high/low tensor cores, FP32 accumulate)";
         case 6: return "k_hex_helm (persistent, double-buffered TMA geometry)";
+        case 8: return "k_hex_helm (TMA-staged geometry, groups up to 72 KB)";
         default: return "k_hex_helm (TMA-staged geometry, small groups)";
     }
 }

@@ -531,8 +531,11 @@ namespace nkb
 //    nkb_hex_tc.cuh); 6: persistent CTAs with the geometry double-buffered
 //    (the next element group's bulk copy in flight while the current one
 //    computes); 7: TMA-staged geometry in element groups of at most 48 KB,
-//    128 registers per thread (more, smaller CTAs per SM than variant 0)
-constexpr int kNumHexVariants = 8;
+//    128 registers per thread (more, smaller CTAs per SM than variant 0);
+//    8: the same in groups of at most 72 KB (offered where that holds more
+//    elements than variant 7's groups: at nq = 6, four elements of 36
+//    threads fill 144 of 160 lanes where two fill 72 of 96)
+constexpr int kNumHexVariants = 9;
 
 // elements per CTA of the double-buffered variant: two geometry buffers and
 // three work regions per element in at most 72 KB (three CTAs per SM)
@@ -556,10 +559,10 @@ template <typename T, int NQ> constexpr int TmaEpb()
 
 // elements per CTA of variant 7: groups of at most 48 KB (one element when a
 // single element needs more)
-template <typename T, int NQ> constexpr int TmaSmallEpb()
+template <typename T, int NQ, int KB = 48> constexpr int TmaSmallEpb()
 {
     constexpr int per = (10 * NQ * NQ * NQ + 4) * int(sizeof(T));
-    constexpr int e   = (48 * 1024) / per;
+    constexpr int e   = (KB * 1024) / per;
     constexpr int lim = 512 / (NQ * NQ);
     constexpr int v   = e < lim ? e : lim;
     return v < 1 ? 1 : (v > 8 ? 8 : v);
@@ -727,6 +730,13 @@ static int HexLaunch(const nkb_op *op, const HexArgs<T> &a, bool gather, cudaStr
         case 7:
             return HexVariantLaunch<T, NM, kGeoTmaS, TmaSmallEpb<T, NQ>()>(op, a, gather, s,
                                                                            set_attr);
+        case 8:
+            if constexpr (TmaSmallEpb<T, NQ, 72>() > TmaSmallEpb<T, NQ>())
+                return HexVariantLaunch<T, NM, kGeoTmaS, TmaSmallEpb<T, NQ, 72>()>(op, a, gather,
+                                                                                   s, set_attr);
+            else
+                return SetError(NKB_ERR_UNSUPPORTED,
+                                "Hex variant 8: no larger group than variant 7 at nq=%d", NQ);
         default:
             return HexVariantLaunch<T, NM, kGeoStream, 2>(op, a, gather, s, set_attr);
     }

@@ -131,7 +131,7 @@ def test_device_pointer_path_matches_host_path():
 
 
 @pytest.mark.parametrize("n,nm", [(1, 5), (3, 7), (2, 9), (1, 11), (5, 2)])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 6, 7])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 6, 7, 8])
 def test_tuned_and_generic_hex_helmholtz_agree(monkeypatch, n, nm, variant):
     """Every variant of the tuned Hex kernel (nkb_hex.cu: TMA-staged or
     streamed geometry, 1-2 elements per CTA, FP64 tensor cores for nq <= 8)
@@ -149,7 +149,7 @@ def test_tuned_and_generic_hex_helmholtz_agree(monkeypatch, n, nm, variant):
 
 
 @pytest.mark.parametrize("n,nm", [(1, 5), (3, 7), (2, 9), (1, 11), (5, 2)])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 6, 7])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 6, 7, 8])
 def test_hex_kernel_variants_linear_adr_match_oracle(monkeypatch, n, nm, variant):
     """LinearADR through every variant of the tuned Hex kernel (its advection
     mode) against the oracle; a variant without room for the three extra
@@ -350,7 +350,7 @@ def test_fp32_linear_adr_matches_oracle(shape):
     assert rel_l2(yd.double().cpu().numpy(), yo) < TOL32
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 6, 7])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 6, 7, 8])
 def test_hex_kernel_variants_are_repeatable(monkeypatch, variant):
     """Repeated applications of every Hex variant to one input give the same
     bits: a race between the warps of an element (a shared-memory store
