@@ -33,7 +33,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Helmholtz CG solves/s (FP64, PCG+Jacobi, rel. residual 1e-10)"
 AMP, LAM, TOL = 0.05, 1.0, 1e-10
-MIXED_INNER_TOL = 0.1
+# FP32-residual reduction between the mixed solve's FP64 reliable updates. Measured at
+# equal accuracy (1e-10 of the converged FP64 solution) against FP64: 24^3 P=8 1.24x,
+# 1.26x, 1.38x, 1.24x and 32^3 P=6 1.548x, 1.552x, 1.541x, 1.486x at 0.05, 0.1, 0.25,
+# 0.5 (at 0.25 the P=8 solve restarts its FP32 recurrence once instead of twice)
+MIXED_INNER_TOL = 0.25
 # the default is the 32^3, P=6 solve; 24^3 at P=8 is the higher-order
 # companion (same map, same criterion)
 WORKLOADS = {
