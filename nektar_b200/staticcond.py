@@ -246,9 +246,9 @@ def lowenergy_part_transforms(parts, bsign, lam, device=0, reference=None):
         p["mask"] = None if mask.all() else mask
 
 
-def element_transforms(p, rows=None):
-    """The transform applied to a part's elements (all, or those of rows):
-    R with the columns of the masked modes zeroed, R M_e, so that
+def element_transforms(p):
+    """The transform applied to a part's elements: R with the columns of the
+    masked modes zeroed, R M_e, so that
     S~ = R M S M R^T (v_TransformedSchurCompl), b~ = R M b
     (v_DoTransformBasisToLowEnergy) and x = M R^T x~
     (v_DoTransformCoeffsFromLowEnergy); one (nb, nb) matrix without a mask,
@@ -256,8 +256,7 @@ def element_transforms(p, rows=None):
     R, mask = p["R"], p.get("mask")
     if R is None or mask is None:
         return R
-    m = mask if rows is None else mask[rows]
-    return R[None, :, :] * m[:, None, :]
+    return R[None, :, :] * mask[:, None, :]
 
 
 def lowenergy_transforms(shapes, nm, lam, device=0, reference=None):
