@@ -106,6 +106,9 @@ struct CollectionData
 {
     ShapeType shape;
     int nm;
+    // modes per direction as the expansions report them (GetBasisNumModes(0..2));
+    // zeros mean nm in every direction
+    std::array<int, 3> nmodes{};
     std::array<int, 3> nq, ptype;
     int nelmt;
     bool deformed;
@@ -193,6 +196,17 @@ class B200OpHandle
 public:
     B200OpHandle(const CollectionData &d, int optype)
     {
+        // the descriptor carries one order for all directions; a collection of
+        // per-direction orders (which the reference's MatrixFree operators take
+        // through their run-time-sized path) stays with the reference's own
+        // implementation
+        for (int i = 0; i < 3; ++i)
+            if (d.nmodes[i] != 0 && d.nmodes[i] != d.nm)
+                throw NekError(NKB_ERR_UNSUPPORTED,
+                               "eB200 operators take one order in all directions (modes " +
+                                   std::to_string(d.nmodes[0]) + "," +
+                                   std::to_string(d.nmodes[1]) + "," +
+                                   std::to_string(d.nmodes[2]) + ")");
         nkb_op_desc desc{};
         desc.shape    = d.shape;
         desc.optype   = optype;

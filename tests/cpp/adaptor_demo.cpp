@@ -49,9 +49,23 @@ int main()
     int nglob = 0, ndir = 0;
     Check(nkb_hex_box_assembly(n, nm, map.data(), &nglob, &ndir));
 
+    // a collection of per-direction orders is refused before any device work
+    int aniso = 0;
     try
     {
         RegisterB200Operators();
+        CollectionData da = d;
+        da.nmodes         = {nm, nm + 1, nm};
+        FactorMap fa;
+        GetOperatorFactory().CreateInstance(OperatorKey(eHexahedron, eHelmholtz, eB200, false),
+                                            da, fa);
+    }
+    catch (const NekError &e)
+    {
+        aniso = e.Code();
+    }
+    try
+    {
         FactorMap f;
         f.lambda = 1.5;
         auto op  = GetOperatorFactory().CreateInstance(OperatorKey(eHexahedron, eHelmholtz, eB200,
@@ -113,13 +127,14 @@ int main()
         std::printf("{\"helmholtz_norm2\": %.17g, \"iproduct_deriv_norm2\": %.17g, "
                     "\"linear_adr_norm2\": %.17g, "
                     "\"dir_call_threw\": %d, \"cg_iterations\": %d, "
-                    "\"cg_rel_residual\": %.6g, \"nelmt\": %d}\n",
-                    ny, ng, na, int(threw), r.iterations, r.rel_residual, d.nelmt);
+                    "\"cg_rel_residual\": %.6g, \"nelmt\": %d, \"per_direction_orders\": %d}\n",
+                    ny, ng, na, int(threw), r.iterations, r.rel_residual, d.nelmt, aniso);
         return 0;
     }
     catch (const NekError &e)
     {
-        std::printf("{\"nekerror\": %d, \"what\": \"%s\"}\n", e.Code(), e.what());
+        std::printf("{\"nekerror\": %d, \"what\": \"%s\", \"per_direction_orders\": %d}\n",
+                    e.Code(), e.what(), aniso);
         return 3;
     }
 }

@@ -30,6 +30,8 @@ def test_adaptor_compiles_and_reports_errors_as_nekerror(tmp_path):
         assert p.returncode == 0, p.stdout + p.stderr
     else:
         assert p.returncode == 3 and out["nekerror"] in (-7, -3), out
+    # per-direction orders: refused with NKB_ERR_UNSUPPORTED before any device work
+    assert out["per_direction_orders"] == -2, out
 
 
 @pytest.mark.gpu
