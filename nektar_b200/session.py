@@ -186,23 +186,76 @@ def _read_geometry(root):
     return Geometry(dim, space, vertices, edges, faces, elements, composites, domain, curved)
 
 
-def _read_expansions(root):
+# the bases and points TYPE="MODIFIED" gives each shape at nm modes
+# (SpatialDomains/MeshGraph.cpp:1709-1750): basis types, point types and point
+# counts (nm + 1 GLL points, nm Gauss-Radau points in collapsed directions)
+_MODIFIED = {
+    "H": (("Modified_A",) * 3, ("GaussLobattoLegendre",) * 3, (1, 1, 1)),
+    "R": (("Modified_A", "Modified_A", "Modified_B"),
+          ("GaussLobattoLegendre", "GaussLobattoLegendre", "GaussRadauMAlpha1Beta0"), (1, 1, 0)),
+    "A": (("Modified_A", "Modified_B", "Modified_C"),
+          ("GaussLobattoLegendre", "GaussRadauMAlpha1Beta0", "GaussRadauMAlpha2Beta0"),
+          (1, 0, 0)),
+}
+
+
+def _explicit_order(e, letters):
+    """The order of an explicit expansion (BASISTYPE, NUMMODES, POINTSTYPE,
+    NUMPOINTS per direction) when it is the one TYPE="MODIFIED" gives the
+    composite's shapes at one order in all directions; SessionError naming
+    what differs otherwise."""
+    def parts(key):
+        v = e.get(key)
+        if v is None:
+            raise SessionError("explicit expansion without %s" % key)
+        return [x.strip() for x in v.split(",")]
+    nms = [int(x) for x in parts("NUMMODES")]
+    nqs = [int(x) for x in parts("NUMPOINTS")]
+    if len(set(nms)) != 1:
+        raise SessionError("per-direction orders NUMMODES=%s are not supported" %
+                           ",".join(map(str, nms)))
+    nm = nms[0]
+    bts, pts = parts("BASISTYPE"), parts("POINTSTYPE")
+    for letter in letters:
+        if letter not in _MODIFIED:
+            raise SessionError("no expansion for element type %r" % letter)
+        want_b, want_p, extra = _MODIFIED[letter]
+        want_q = [nm + x for x in extra]
+        if len(bts) == 1:
+            bts = bts * 3
+        if len(pts) == 1:
+            pts = pts * 3
+        if len(nqs) == 1:
+            nqs = nqs * 3
+        if (tuple(bts), tuple(pts), list(nqs)) != (want_b, want_p, want_q):
+            raise SessionError("explicit expansion %s / %s / %s is not the standard modified "
+                               "expansion of its elements (%s / %s / %s)" % (
+                                   ",".join(bts), ",".join(pts), ",".join(map(str, nqs)),
+                                   ",".join(want_b), ",".join(want_p), ",".join(map(str, want_q))))
+    return nm
+
+
+def _read_expansions(root, composites):
     node = root.find("EXPANSIONS")
     if node is None:
         raise SessionError("no EXPANSIONS section")
     nummodes, etype = {}, None
     for e in node.findall("E"):
+        refs = parse_composite_refs(e.get("COMPOSITE"))
         t = e.get("TYPE")
         if t is None:
-            raise SessionError("only TYPE-based expansions are supported")
-        if t.upper() != "MODIFIED":
-            raise SessionError("expansion type %r is not supported (MODIFIED only)" % t)
-        nm = e.get("NUMMODES").replace(" ", "")
-        if "," in nm:
-            raise SessionError("per-direction orders NUMMODES=%r are not supported" % nm)
-        for _, ids in parse_composite_refs(e.get("COMPOSITE")):
+            letters = {composites[c][0] for _, ids in refs for c in ids if c in composites}
+            nm = _explicit_order(e, letters)
+        else:
+            if t.upper() != "MODIFIED":
+                raise SessionError("expansion type %r is not supported (MODIFIED only)" % t)
+            nmt = e.get("NUMMODES").replace(" ", "")
+            if "," in nmt:
+                raise SessionError("per-direction orders NUMMODES=%r are not supported" % nmt)
+            nm = int(nmt)
+        for _, ids in refs:
             for c in ids:
-                nummodes[c] = int(nm)
+                nummodes[c] = nm
         etype = "MODIFIED"
     return nummodes, etype
 
@@ -258,7 +311,7 @@ def read_session(path_or_text):
     if root.tag != "NEKTAR":
         raise SessionError("root element is %r, not NEKTAR" % root.tag)
     geom = _read_geometry(root)
-    nummodes, etype = _read_expansions(root)
+    nummodes, etype = _read_expansions(root, geom.composites)
     params, solver_info, variables, regions, bcs_raw, funcs_raw = _read_conditions(root)
     bcs = {}
     for rid, lst in bcs_raw.items():

@@ -345,3 +345,51 @@ def test_weak_terms_on_triangles_converge(shape):
             errs[(nm, seed)] = oracle_helm_solve(s, m)[2]
         assert abs(errs[(nm, None)] - errs[(nm, 5)]) < 1e-9 * errs[(nm, None)]
     assert errs[(6, None)] < 1e-2 * errs[(4, None)] and errs[(8, None)] < 1e-2 * errs[(6, None)]
+
+
+def _explicit_expansions(txt, override=None):
+    """The session text with every TYPE="MODIFIED" expansion written out as
+    the bases and points it stands for (override: attributes to replace)."""
+    import xml.etree.ElementTree as ET
+    root = ET.fromstring(txt)
+    comps = {int(c.get("ID")): c.text.strip()[0] for c in root.find("GEOMETRY").find("COMPOSITE")}
+    std = {"H": ("Modified_A,Modified_A,Modified_A",
+                 "GaussLobattoLegendre,GaussLobattoLegendre,GaussLobattoLegendre", (1, 1, 1)),
+           "R": ("Modified_A,Modified_A,Modified_B",
+                 "GaussLobattoLegendre,GaussLobattoLegendre,GaussRadauMAlpha1Beta0", (1, 1, 0)),
+           "A": ("Modified_A,Modified_B,Modified_C",
+                 "GaussLobattoLegendre,GaussRadauMAlpha1Beta0,GaussRadauMAlpha2Beta0", (1, 0, 0))}
+    for e in root.find("EXPANSIONS").findall("E"):
+        nm = int(e.get("NUMMODES"))
+        letter = comps[int(e.get("COMPOSITE").strip()[2:-1].split(",")[0].split("-")[0])]
+        b, p, extra = std[letter]
+        del e.attrib["TYPE"]
+        e.set("BASISTYPE", b)
+        e.set("POINTSTYPE", p)
+        e.set("NUMMODES", ",".join([str(nm)] * 3))
+        e.set("NUMPOINTS", ",".join(str(nm + x) for x in extra))
+        for k, v in (override or {}).items():
+            e.set(k, v)
+    return ET.tostring(root, encoding="unicode")
+
+
+@pytest.mark.parametrize("shape", ["hex", "prism", "tet"])
+def test_explicit_expansions_read_as_their_type(shape):
+    """An expansion written out as bases and points (BASISTYPE, NUMMODES,
+    POINTSTYPE, NUMPOINTS) that is the standard modified expansion reads as
+    TYPE="MODIFIED" does: the same mesh and the same solution; per-direction
+    orders (the reference's Hex_Heterogeneous session) and other point sets
+    are refused by name."""
+    txt = write_box_session(shape, 2, 4, 1.0, U, F, U, shuffle_seed=2)
+    s0, s1 = read_session(txt), read_session(_explicit_expansions(txt))
+    m0, m1 = SessionMesh(s0), SessionMesh(s1)
+    assert [(c.shape, c.nm, c.nq) for c in m0.collections] == \
+        [(c.shape, c.nm, c.nq) for c in m1.collections]
+    assert np.array_equal(m0.gmap, m1.gmap) and np.array_equal(m0.sign, m1.sign)
+    x0, _, _ = oracle_helm_solve(s0)
+    x1, _, _ = oracle_helm_solve(s1)
+    assert np.array_equal(x0, x1)
+    with pytest.raises(SessionError, match="per-direction orders"):
+        read_session(_explicit_expansions(txt, {"NUMMODES": "4,5,6"}))
+    with pytest.raises(SessionError, match="not the standard modified expansion"):
+        read_session(_explicit_expansions(txt, {"NUMPOINTS": "7,7,7"}))
