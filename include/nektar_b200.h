@@ -123,7 +123,11 @@ typedef struct nkb_op_desc
     int shape;    /* NKB_HEX / NKB_PRISM / NKB_TET */
     int optype;   /* NKB_BWDTRANS / NKB_HELMHOLTZ / NKB_LINEAR_ADR / NKB_IPRODUCT /
                      NKB_IPRODUCT_DERIV / NKB_PHYSDERIV */
-    int nm;       /* modes per direction (equal in all directions) */
+    int nm;       /* modes per direction, equal in all directions (bdata[i] holds
+                     nm x nq[i] values); collections of per-direction orders, which the
+                     reference's MatrixFree operators take through their run-time-sized
+                     path (MatrixFreeOps/Helmholtz.h:374-384), are not representable and
+                     stay on the reference's own implementation types */
     int nq[3];    /* points per direction (Tet: nq0, nq0-1, nq0-1; Prism: nq0, nq0, nq0-1) */
     int ptype[3]; /* points type per direction */
     int nelmt;    /* elements in the collection */
