@@ -167,14 +167,71 @@ def edge_bubble(shape, a, b, xi):
         (lam[ta] * (-0.5 * x2))[:, None] * np.array([0, 1.0, 0])
 
 
-def element_geometry(shape, X, z, curves=None):
+def face_bubble_coeff(pts):
+    """The (2, 2) mode coefficient (3,) of a quadrilateral face's quadratic
+    curve, its 3 x 3 points in tensor order (QuadGeom::v_FillGeom projects
+    the interpolant of the points on the face's modes; the biquadratic's
+    (2, 2) coefficient is 16 (centre - mean of the midpoints x 2 + mean of
+    the corners), the same for every orientation and either point order)."""
+    p = np.asarray(pts, dtype=np.float64)
+    return 16.0 * (p[4] - 0.5 * (p[1] + p[3] + p[5] + p[7]) + 0.25 * (p[0] + p[2] + p[6] + p[8]))
+
+
+def face_bubble(shape, lf, xi):
+    """The (2, 2) mode of local quadrilateral face lf of a hexahedron or
+    prism and its gradient at standard points xi (n, 3): the two in-face
+    quadratic bubbles (1 - t^2)/4 times the linear factor across the face
+    (hexahedra); for a prism the product of the face's two triangle
+    barycentrics (its (2, *) collapsed modes) times (1 - xi2^2)/4. On the
+    face it is the face's own (2, 2) mode, so the coefficient of the face
+    carries over unchanged (HexGeom / PrismGeom::v_FillGeom)."""
+    V = STD_VERTS[shape]
+    _, _, faces = topology(shape, 3)
+    kind, frame, _ = faces[lf]
+    if kind != "Q":
+        raise ValueError("face %d of a %s is a triangle" % (lf, shape))
+    n = xi.shape[0]
+    one = np.ones(n)
+    if shape == "hex":
+        o, a, c = (V[v] for v in frame)
+        ax = int(np.nonzero((o == a) & (o == c))[0][0])
+        fac, grad = [], []
+        for d in range(3):
+            t = xi[:, d]
+            if d == ax:
+                fac.append(0.5 * (1 + o[d] * t))
+                grad.append(0.5 * o[d] * one)
+            else:
+                fac.append(0.25 * (1 - t * t))
+                grad.append(-0.5 * t)
+        phi = fac[0] * fac[1] * fac[2]
+        dphi = np.stack([grad[0] * fac[1] * fac[2], fac[0] * grad[1] * fac[2],
+                         fac[0] * fac[1] * grad[2]], axis=1)
+        return phi, dphi
+    if shape != "prism":
+        raise ValueError("no quadrilateral faces on a %s" % shape)
+    x1, x2, x3 = xi[:, 0], xi[:, 1], xi[:, 2]
+    lam = [-0.5 * (x1 + x3), 0.5 * (1 + x1), 0.5 * (1 + x3)]
+    dl = [np.array([-0.5, 0, -0.5]), np.array([0.5, 0, 0]), np.array([0, 0, 0.5])]
+    tri = {(-1, -1): 0, (1, -1): 1, (-1, 1): 2}
+    ta, tb = sorted({tri[(V[v][0], V[v][2])] for v in frame})
+    b2, db2 = 0.25 * (1 - x2 * x2), -0.5 * x2
+    phi = lam[ta] * lam[tb] * b2
+    dphi = (lam[ta][:, None] * dl[tb] + lam[tb][:, None] * dl[ta]) * b2[:, None] + \
+        (lam[ta] * lam[tb] * db2)[:, None] * np.array([0, 1.0, 0])
+    return phi, dphi
+
+
+def element_geometry(shape, X, z, curves=None, faces=None):
     """jac (nelmt*nt,), df (9, nelmt*nt), coordinates (3, nelmt*nt) of
     elements with vertex coordinates X (nelmt, nv, 3) at the collapsed tensor
     points z = (z0, z1, z2) (point q = (k nq1 + j) nq0 + i). curves: per
     element a list of (local edge (a, b), mode-2 coefficient c (3,)) of its
-    quadratic curved edges, added to the vertex map as the reference's
-    geometry expansions add the edges' coefficients (Geometry3D::v_FillGeom;
-    the factors are the map's exact derivatives at the points)."""
+    quadratic curved edges; faces: per element a list of (local face,
+    (2, 2) coefficient (3,)) of its curved quadrilateral faces; both added to
+    the vertex map as the reference's geometry expansions add the edges' and
+    faces' coefficients (Geometry3D::v_FillGeom; the factors are the map's
+    exact derivatives at the points)."""
     e1, e2, e3 = np.meshgrid(z[0], z[1], z[2], indexing="ij")  # [i, j, k]
     e = [a.transpose(2, 1, 0).reshape(-1) for a in (e1, e2, e3)]
     xi = np.stack(collapsed_to_standard(shape, *e), axis=1)
@@ -184,6 +241,11 @@ def element_geometry(shape, X, z, curves=None):
     for el, lst in enumerate(curves or []):
         for (a, b), c in lst:
             phi, dphi = edge_bubble(shape, a, b, xi)
+            x[el] += np.asarray(c)[:, None] * phi[None, :]
+            J[el] += np.asarray(c)[None, :, None] * dphi[:, None, :]
+    for el, lst in enumerate(faces or []):
+        for lf, c in lst:
+            phi, dphi = face_bubble(shape, lf, xi)
             x[el] += np.asarray(c)[:, None] * phi[None, :]
             J[el] += np.asarray(c)[None, :, None] * dphi[:, None, :]
     det = np.linalg.det(J)
@@ -432,8 +494,16 @@ class Collection:
                 curves.append(lst)
             self.deformed = True
         self.curves = curves
+        fcurves = None
+        if geom.curved_faces:
+            fcurves = []
+            for e in self.elem_ids:
+                fcurves.append([(lf, face_bubble_coeff(geom.curved_faces[f]))
+                                for lf, f in enumerate(geom.elements[e][1])
+                                if f in geom.curved_faces and geom.faces[f][0] == "Q"])
+        self.face_curves = fcurves
         self.jac, self.df, self.xyz = element_geometry(
-            shape, self.X, tuple(np.asarray(z) for z in self.T["z"]), curves)
+            shape, self.X, tuple(np.asarray(z) for z in self.T["z"]), curves, fcurves)
 
     def quad_weights(self):
         """Integration weights jac * w0 w1 w2 at every quadrature point (the
@@ -784,10 +854,24 @@ class SessionMesh:
         d = 0.5 * (P(b) - P(a))[None, :] - np.outer(0.5 * s, self._curve(a, b))
         return np.linalg.norm(d, axis=1)
 
+    def _face_curve(self, vs):
+        """(2, 2) coefficient (3,) of the quadrilateral face with global
+        vertices vs if it is curved, else zero."""
+        g = self.session.geometry
+        if not g.curved_faces:
+            return np.zeros(3)
+        if not hasattr(self, "_face_of"):
+            self._face_of = {frozenset(v for e in es for v in g.edges[e]): f
+                             for f, (kind, es) in g.faces.items() if kind == "Q"}
+        f = self._face_of.get(frozenset(vs))
+        if f not in g.curved_faces:
+            return np.zeros(3)
+        return face_bubble_coeff(g.curved_faces[f])
+
     def _quad_map(self, O, nA, nB, AB, za, zb):
         """Points and surface Jacobian of the quadrilateral face O, nA, AB, nB
         (coordinates za along O -> nA, zb along O -> nB): the bilinear map
-        plus the quadratic curves of its edges."""
+        plus the quadratic curves of its edges and of the face itself."""
         P = lambda v: np.asarray(self.session.geometry.vertices[v], dtype=np.float64)  # noqa: E731
         XO, XA, XB, XAB = P(O), P(nA), P(nB), P(AB)
         Na = [0.5 * (1 - za), 0.5 * (1 + za)]
@@ -810,6 +894,12 @@ class SessionMesh:
             else:
                 dxb = dxb + (dbub * u)[..., None] * c
                 dxa = dxa + (bub * du)[..., None] * c
+        cf = self._face_curve((O, nA, nB, AB))
+        if cf.any():
+            ba, bb = 0.25 * (1 - za * za), 0.25 * (1 - zb * zb)
+            x = x + (ba * bb)[..., None] * cf
+            dxa = dxa + (-0.5 * za * bb)[..., None] * cf
+            dxb = dxb + (ba * -0.5 * zb)[..., None] * cf
         return x, np.linalg.norm(np.cross(dxa, dxb), axis=-1)
 
     def _tri_map(self, v0, v1, v2, xa, xb):
@@ -913,7 +1003,8 @@ class SessionMesh:
                     continue
                 for f in g.composites[c][1]:
                     kind = g.faces[f][0]
-                    regular = not any(e in g.curved_edges for e in g.faces[f][1])
+                    regular = not any(e in g.curved_edges for e in g.faces[f][1]) and \
+                        f not in g.curved_faces
                     if kind == "Q" and regular:  # a parallelogram has a constant Jacobian
                         cyc = [P(v) for v in self._face_cycle(f)]
                         regular = bool(np.allclose(cyc[0] + cyc[2], cyc[1] + cyc[3],

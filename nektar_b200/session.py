@@ -17,8 +17,8 @@ Follows the reference readers section by section:
   ReadBoundaryRegions (:228-316), ReadBoundaryConditions (:318-).
 
 What the B200 path does not take is rejected with a clear message rather
-than read wrongly: curved faces and curves other than quadratic edges,
-compressed (base64) geometry blocks,
+than read wrongly: curves beyond quadratic order (edges of more than 3
+points, faces of more than 3 x 3 or 6), compressed (base64) geometry blocks,
 per-direction orders (NUMMODES="4,6,8"), pyramids, and expansion types
 other than MODIFIED.
 """
@@ -50,6 +50,7 @@ class Geometry:
     composites: dict  # id -> (letter, [ids])
     domain: list  # composite ids
     curved_edges: dict = field(default_factory=dict)  # edge id -> (npts, 3) curve points
+    curved_faces: dict = field(default_factory=dict)  # face id -> (npts, 3) face points
 
 
 @dataclass
@@ -111,19 +112,26 @@ def _read_geometry(root):
     if g is None:
         raise SessionError("no GEOMETRY section")
     dim, space = int(g.get("DIM", 3)), int(g.get("SPACE", 3))
-    curved = {}
+    curved, curved_faces = {}, {}
     cnode = g.find("CURVED")
     for c in (list(cnode) if cnode is not None else []):
-        # MeshGraphIOXml::v_ReadCurves: edges with their points; quadratic
-        # curves (three points, the two vertices and the midpoint) only
-        if c.tag != "E":
-            raise SessionError("curved faces are not supported")
+        # MeshGraphIOXml::v_ReadCurves: edges and faces with their points;
+        # quadratic curves only (an edge's two vertices and midpoint; a
+        # quadrilateral's 3 x 3 points, a triangle's 6)
         npts, ptype = int(c.get("NUMPOINTS")), c.get("TYPE")
+        vals = np.array([float(v) for v in c.text.split()], dtype=np.float64)
+        if c.tag == "F":
+            if npts not in (6, 9) or ptype not in ("PolyEvenlySpaced", "GaussLobattoLegendre"):
+                raise SessionError("curved face %s: %d %s points (quadratic curves only)"
+                                   % (c.get("FACEID"), npts, ptype))
+            curved_faces[int(c.get("FACEID"))] = vals.reshape(npts, 3)
+            continue
+        if c.tag != "E":
+            raise SessionError("curved %s records are not supported" % c.tag)
         if npts != 3 or ptype not in ("PolyEvenlySpaced", "GaussLobattoLegendre"):
             raise SessionError("curved edge %s: %d %s points (quadratic curves only)"
                                % (c.get("EDGEID"), npts, ptype))
-        vals = [float(v) for v in c.text.split()]
-        curved[int(c.get("EDGEID"))] = np.array(vals, dtype=np.float64).reshape(npts, 3)
+        curved[int(c.get("EDGEID"))] = vals.reshape(npts, 3)
     for sec in ("VERTEX", "EDGE", "FACE", "ELEMENT"):
         node = g.find(sec)
         if node is not None and node.get("COMPRESSED"):
@@ -183,7 +191,22 @@ def _read_geometry(root):
         want = {tuple(np.round(np.asarray(vertices[v], dtype=np.float64), 12)) for v in edges[e]}
         if ends != want:
             raise SessionError("curved edge %d does not end at its vertices" % e)
-    return Geometry(dim, space, vertices, edges, faces, elements, composites, domain, curved)
+    for f, pts in curved_faces.items():
+        if f not in faces:
+            raise SessionError("curved face %d is no face of the mesh" % f)
+        kind, fe = faces[f]
+        if (kind == "Q") != (len(pts) == 9):
+            raise SessionError("curved face %d: %d points for a %s" % (
+                f, len(pts), "quadrilateral" if kind == "Q" else "triangle"))
+        want = {tuple(np.round(np.asarray(vertices[v], dtype=np.float64), 12))
+                for e in fe for v in edges[e]}
+        # a quadrilateral's points in tensor order: corners 0, 2, 6, 8
+        got = {tuple(np.round(pts[i], 12)) for i in ((0, 2, 6, 8) if kind == "Q" else
+                                                       range(len(pts)))}
+        if not want <= got or (kind == "Q" and got != want):
+            raise SessionError("curved face %d does not have its vertices as corners" % f)
+    return Geometry(dim, space, vertices, edges, faces, elements, composites, domain, curved,
+                    curved_faces)
 
 
 # the bases and points TYPE="MODIFIED" gives each shape at nm modes

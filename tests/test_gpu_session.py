@@ -144,3 +144,22 @@ def test_curved_session_matches_oracle(shape):
     xo, linf_o, l2_o = oracle_helm_solve(s, r.mesh)
     assert rel_l2(r.coeffs, xo) < 1e-10
     assert abs(r.l2 - l2_o) < 1e-9 * l2_o
+
+
+@pytest.mark.parametrize("shape", ["hex", "prism"])
+def test_curved_face_session_matches_oracle(shape):
+    """Quadratic curved faces (a bulged top surface and a bulged interior
+    plane): the device solve on those element maps, full and condensed,
+    matches the oracle's."""
+    from nektar_b200.session import write_box_session
+    from tests.test_session import _bulged_top
+    base = write_box_session(shape, 2, 5, 1.0, U, F, U, shuffle_seed=2)
+    s = read_session(_bulged_top(_bulged_top(base, 0.8), 0.5, z0=0.5))
+    assert s.geometry.curved_faces
+    r = helm_solve(s, tol=1e-14, maxit=3000, raise_on_maxit=False)
+    xo, linf_o, l2_o = oracle_helm_solve(s, r.mesh)
+    assert rel_l2(r.coeffs, xo) < 1e-10
+    assert abs(r.l2 - l2_o) < 1e-9 * l2_o
+    rc = helm_solve(s, tol=1e-14, maxit=3000, raise_on_maxit=False,
+                    solver_info={"GlobalSysSoln": "IterativeStaticCond"})
+    assert rel_l2(rc.coeffs, xo) < 1e-10

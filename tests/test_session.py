@@ -393,3 +393,103 @@ def test_explicit_expansions_read_as_their_type(shape):
         read_session(_explicit_expansions(txt, {"NUMMODES": "4,5,6"}))
     with pytest.raises(SessionError, match="not the standard modified expansion"):
         read_session(_explicit_expansions(txt, {"NUMPOINTS": "7,7,7"}))
+
+
+def _bulged_top(txt, amp, with_faces=True, z0=1.0):
+    """The box session with its plane z = z0 moved to
+    z = z0 + amp x (1 - x) y (1 - y): the plane's vertices moved, its edges
+    given their quadratic curves and (with_faces) its quadrilaterals their
+    3 x 3 points in the CURVED section (MeshGraphIOXml's E and F records)."""
+    import xml.etree.ElementTree as ET
+    g = read_session(txt).geometry
+    bump = lambda x, y: z0 + amp * x * (1 - x) * y * (1 - y)  # noqa: E731
+    top = {v for v, p in g.vertices.items() if abs(p[2] - z0) < 1e-12}
+    P = {v: np.array([p[0], p[1], bump(p[0], p[1]) if v in top else p[2]])
+         for v, p in g.vertices.items()}
+    root = ET.fromstring(txt)
+    geo = root.find("GEOMETRY")
+    for v in geo.find("VERTEX"):
+        vid = int(v.get("ID"))
+        v.text = "%.17g %.17g %.17g" % tuple(P[vid])
+    cur = geo.find("CURVED")
+    if cur is None:
+        cur = ET.SubElement(geo, "CURVED")
+
+    def on_top(x, y):
+        return np.array([x, y, bump(x, y)])
+    k = len(cur)
+    for e, (a, b) in sorted(g.edges.items()):
+        if a in top and b in top:
+            m = 0.5 * (P[a] + P[b])
+            pts = [P[a], on_top(m[0], m[1]), P[b]]
+            c = ET.SubElement(cur, "E", ID=str(k), EDGEID=str(e), NUMPOINTS="3",
+                              TYPE="PolyEvenlySpaced")
+            c.text = " ".join("%.17g" % x for p in pts for x in p)
+            k += 1
+    if with_faces:
+        for f, (kind, es) in sorted(g.faces.items()):
+            vs = {v for e in es for v in g.edges[e]}
+            if kind != "Q" or not vs <= top:
+                continue
+            # the face's vertex cycle v0 v1 v2 v3 and its points in tensor order
+            cyc = [g.edges[es[0]][0], g.edges[es[0]][1]]
+            while len(cyc) < 4:
+                cyc.append(next(w for e in es for w in g.edges[e]
+                                if cyc[-1] in g.edges[e] and w not in cyc))
+            v0, v1, v3 = P[cyc[0]], P[cyc[1]], P[cyc[3]]
+            pts = []
+            for t in (0.0, 0.5, 1.0):
+                for sv in (0.0, 0.5, 1.0):
+                    xy = v0[:2] + sv * (v1[:2] - v0[:2]) + t * (v3[:2] - v0[:2])
+                    pts.append(on_top(*xy))
+            c = ET.SubElement(cur, "F", ID=str(k), FACEID=str(f), NUMPOINTS="9",
+                              TYPE="PolyEvenlySpaced")
+            c.text = " ".join("%.17g" % x for p in pts for x in p)
+            k += 1
+    return ET.tostring(root, encoding="unicode")
+
+
+@pytest.mark.parametrize("shape", ["hex", "prism"])
+def test_curved_faces_bend_the_element_maps(shape):
+    """Quadratic curved faces (CURVED F records of 3 x 3 points): the (2, 2)
+    mode of each curved quadrilateral joins the element maps of both its
+    elements and the boundary-face maps, so a top surface bulged by a
+    biquadratic is reproduced exactly (the domain's volume 1 + amp/36; a
+    linear solution, Dirichlet data projected on the curved faces, solved
+    to rounding), where curved edges alone miss the bulge."""
+    amp = 0.8
+    ul, fl = "x + 2*y + 3*z", "-Lambda*(x + 2*y + 3*z)"
+    base = write_box_session(shape, 2, 4, 1.0, ul, fl, ul, shuffle_seed=1)
+    s = read_session(_bulged_top(base, amp))
+    assert s.geometry.curved_faces
+    m = SessionMesh(s)
+    assert abs(m.quad_weights().sum() - (1.0 + amp / 36.0)) < 1e-13
+    _, linf, l2 = oracle_helm_solve(s, m)
+    assert linf < 1e-11 and l2 < 1e-12, (linf, l2)
+    me = SessionMesh(read_session(_bulged_top(base, amp, with_faces=False)))
+    assert abs(me.quad_weights().sum() - (1.0 + amp / 36.0)) > 1e-4
+    # a curved interior plane: both elements of every curved face take its
+    # mode, so the maps still meet (the volume stays 1, the linear solution
+    # stays exact)
+    si = read_session(_bulged_top(base, 0.6 * amp, z0=0.5))
+    mi = SessionMesh(si)
+    assert abs(mi.quad_weights().sum() - 1.0) < 1e-13
+    _, linf, l2 = oracle_helm_solve(si, mi)
+    assert linf < 1e-11 and l2 < 1e-12, (linf, l2)
+
+
+def test_curved_face_records_are_checked():
+    """A curved face must have its vertices as corners; curves beyond
+    quadratic order are refused by name."""
+    base = write_box_session("hex", 1, 3, 1.0, U, F, U)
+    txt = _bulged_top(base, 0.5)
+    bad = txt.replace('NUMPOINTS="9"', 'NUMPOINTS="16"', 1)
+    with pytest.raises(SessionError, match="quadratic curves only"):
+        read_session(bad)
+    import re
+    m = re.search(r'(<F ID="\d+" FACEID="\d+" NUMPOINTS="9" TYPE="PolyEvenlySpaced">)([^<]*)', txt)
+    vals = m.group(2).split()
+    vals[0] = str(float(vals[0]) + 0.25)
+    moved = txt.replace(m.group(0), m.group(1) + " ".join(vals))
+    with pytest.raises(SessionError, match="vertices as corners"):
+        read_session(moved)
