@@ -217,6 +217,11 @@ static float TunedMs(int variant, float ms)
 
 template <typename T> static int AutotuneHex(nkb_op *op, int *best)
 {
+    if (op->nelmt == 0)
+    {
+        *best = 1; // nothing to time: the streamed variant exists at every order
+        return NKB_OK;
+    }
     const auto key = std::make_tuple(op->optype, op->precision, op->nm, op->nelmt);
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -488,6 +493,8 @@ template <typename T>
 int LaunchOp(const nkb_op *op, const T *in, T *o0, T *o1, T *o2, const int *gmap,
              const double *gsign, cudaStream_t s, const int *skip, const double *lambda)
 {
+    if (op->nelmt == 0)
+        return NKB_OK; // an empty collection: nothing to launch (a zero-CTA grid is invalid)
     if (op->optype == NKB_DENSE_BLOCK)
     {
         if (!std::is_same<T, double>::value)

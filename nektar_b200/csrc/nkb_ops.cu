@@ -823,7 +823,8 @@ extern "C" int nkb_op_set_varcoeffs(nkb_op *op, const double *velx, const double
     // LinearAdvectionDiffusionReaction.cpp:662-672: scaled by -1/lambda at
     // the time of the update
     const int nb = int(std::min<size_t>((3 * fld + 255) / 256, 148 * 16));
-    k_scale<<<nb, 256, 0, op->stream>>>(op->dvel, 3 * fld, -1 / op->factor_lambda);
+    if (nb > 0) // an empty collection has nothing to scale
+        k_scale<<<nb, 256, 0, op->stream>>>(op->dvel, 3 * fld, -1 / op->factor_lambda);
     NKB_CUDA_TRY(cudaGetLastError());
     return Repack(op);
 }

@@ -157,3 +157,24 @@ def test_sharded_solve_on_device_operators_matches_global_linsys():
     op = factory(0, m.nelmt)
     xg, rep = nb.GlobalLinSys([op], gmap, nglob, ndir).solve(b, tol=1e-12)
     assert rel_l2(x, xg) < 1e-9
+
+
+def test_all_dirichlet_system_returns_the_dirichlet_values():
+    """A system whose every dof is Dirichlet (one linear hexahedron: no
+    interior modes) has nothing to solve (GlobalLinSysStaticCond /
+    IterativeFull return at once when nGlobDofs - nDirBndDofs == 0): the
+    solve returns the local Dirichlet values after zero iterations."""
+    m = nb.BoxMesh("hex", 1, 2, 3, amp=0.05)
+    gmap, nglob, ndir = m.assembly()
+    assert nglob == ndir
+    op = nb.Operator("helmholtz", m)
+    op.set_factors(1.0)
+    S = nb.GlobalLinSys([op], gmap, nglob, ndir)
+    rng = np.random.default_rng(4)
+    xd = rng.uniform(-1, 1, nglob)
+    x0 = xd[np.asarray(gmap)]
+    x, rep = S.solve(rng.uniform(-1, 1, m.nelmt * m.nc), x0, tol=1e-12)
+    S.close()
+    op.close()
+    assert rep.converged and rep.iterations == 0
+    assert np.array_equal(x, x0)

@@ -401,3 +401,15 @@ def test_peak_probe_rates_are_plausible():
     assert fma32 > fma64, rates
     v = ctypes.c_double(0.0)
     assert nb.lib().nkb_peak_probe(3, 0, ctypes.byref(v)) == nb.C.NKB_ERR_INVALID
+
+
+@pytest.mark.parametrize("shape,nm", [("hex", 4), ("hex", 7), ("prism", 5), ("tet", 6)])
+def test_empty_collection_applies_as_a_no_op(shape, nm):
+    """An operator over no elements (a rank or batch slot left without
+    elements) is created and applied without launching anything."""
+    m = nb.BoxMesh(shape, 1, nm, nm + 1, amp=0.05)
+    op = nb.Operator("helmholtz", shape=shape, nm=nm, nq=m.nq, nelmt=0, T=m.T,
+                     jac=m.jac[:0], df=np.ascontiguousarray(m.df[:, :0]), deformed=True)
+    op.set_factors(1.0)
+    assert op.in_size == 0 and op(np.zeros(0)).size == 0
+    op.close()
