@@ -3,7 +3,8 @@ MatrixFreeOps kernels and Polylib, compiled in place into oracle/_ref by
 `make -C oracle ref` (this needs the reference source tree, so it runs where
 the reference is mounted; the fixtures are committed and travel instead).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py           # the fixtures that are missing
+    python tests/golden/make_golden.py --force   # all of them
 
 Every case stores its seeded inputs, the reference-generated 1-D tables and
 the reference kernels' outputs. Inputs follow the pattern of the reference's
@@ -108,14 +109,25 @@ def make_case(shape, nm, nq0, deformed, seed, ne=3):
 
 CASES = [(s, nm, nm + 1, dfm) for s in ("hex", "prism", "tet") for nm in (2, 3, 5)
          for dfm in (False, True)]
+# the benchmark orders: Hex P=6 (nm 7, Q=8) and P=8 (nm 9, Q=10), Prism and Tet at
+# nm 7; two elements each, to keep the fixtures small
+CASES += [(s, nm, nm + 1, dfm) for s, nm in (("hex", 7), ("hex", 9), ("prism", 7), ("tet", 7))
+          for dfm in (False, True)]
 
 
-def main():
+def main(force=False):
+    """Writes the fixtures that are missing (all with force=True)."""
     for shape, nm, nq0, deformed in CASES:
         name = "%s_nm%d_nq%d_%s.npz" % (shape, nm, nq0, "deformed" if deformed else "regular")
-        arrays = make_case(shape, nm, nq0, deformed, seed=1000 * nm + nq0 + int(deformed))
-        np.savez_compressed(os.path.join(HERE, name), **arrays)
+        path = os.path.join(HERE, name)
+        if os.path.exists(path) and not force:
+            continue
+        arrays = make_case(shape, nm, nq0, deformed, seed=1000 * nm + nq0 + int(deformed),
+                           ne=3 if nm <= 5 else 2)
+        np.savez_compressed(path, **arrays)
         print("wrote", name)
+    if os.path.exists(os.path.join(HERE, "polylib_basis.npz")) and not force:
+        return
     # quadrature / basis known answers from the reference Polylib
     pts = {}
     for pt in (ref.GLL, ref.RADAU_A1, ref.RADAU_A2):
@@ -135,4 +147,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(force="--force" in sys.argv[1:])
