@@ -493,3 +493,46 @@ def test_curved_face_records_are_checked():
     moved = txt.replace(m.group(0), m.group(1) + " ".join(vals))
     with pytest.raises(SessionError, match="vertices as corners"):
         read_session(moved)
+
+
+@pytest.mark.parametrize("shape", ["hex", "prism"])
+def test_face_bubbles_are_the_faces_own_modes(shape):
+    """Each quadrilateral face's bubble (meshgraph.face_bubble) is
+    (1 - s^2)(1 - t^2)/16 on its own face, zero on every other face, and its
+    gradient is the derivative of the function."""
+    from nektar_b200.meshgraph import STD_VERTS, face_bubble, topology
+    V = STD_VERTS[shape]
+    _, _, faces = topology(shape, 3)
+    rng = np.random.default_rng(9)
+    st = rng.uniform(-1, 1, (40, 2))
+    for lf, (kind, frame, _) in enumerate(faces):
+        if kind != "Q":
+            continue
+        o, a, c = (np.asarray(V[v], dtype=np.float64) for v in frame)
+        # points of the face: o + (1+s)/2 (a - o) + (1+t)/2 (c - o)
+        pts = o + np.outer(0.5 * (1 + st[:, 0]), a - o) + np.outer(0.5 * (1 + st[:, 1]), c - o)
+        phi, _ = face_bubble(shape, lf, pts)
+        want = 0.25 * (1 - st[:, 0] ** 2) * 0.25 * (1 - st[:, 1] ** 2)
+        assert np.abs(phi - want).max() < 1e-14
+        for lg, (kg, fg, _) in enumerate(faces):
+            if lg == lf:
+                continue
+            og, ag, cg = (np.asarray(V[v], dtype=np.float64) for v in fg)
+            if kg == "Q":
+                q = og + np.outer(0.5 * (1 + st[:, 0]), ag - og) + \
+                    np.outer(0.5 * (1 + st[:, 1]), cg - og)
+            else:  # a triangle: barycentric points
+                u = 0.5 * (1 + st)
+                u = np.where((u.sum(axis=1) > 1)[:, None], 1 - u, u)
+                q = og + np.outer(u[:, 0], ag - og) + np.outer(u[:, 1], cg - og)
+            assert np.abs(face_bubble(shape, lf, q)[0]).max() < 1e-14
+        x = rng.uniform(-0.9, 0.9, (30, 3))
+        if shape == "prism":
+            x[:, 2] = np.minimum(x[:, 2], -x[:, 0])  # inside: xi1 + xi3 <= 0
+        _, g = face_bubble(shape, lf, x)
+        h = 1e-6
+        for d in range(3):
+            e = np.zeros(3)
+            e[d] = h
+            fd = (face_bubble(shape, lf, x + e)[0] - face_bubble(shape, lf, x - e)[0]) / (2 * h)
+            assert np.abs(fd - g[:, d]).max() < 1e-8
