@@ -67,6 +67,13 @@ def errors(mesh, u, exact, device=0):
 SOLVERS = {"IterativeFull": "full", "DirectFull": "full", "XxtFull": "full", "PETScFull": "full",
            "IterativeStaticCond": "staticcond", "DirectStaticCond": "staticcond",
            "XxtStaticCond": "staticcond", "PETScStaticCond": "staticcond"}
+# the multi-level variants condense the boundary system again over patches
+# (GlobalLinSysStaticCond::v_Solve's next-level branch,
+# GlobalLinSysStaticCond.cpp:190-205): the same discrete system, solved here
+# by the one-level condensed CG (their regression records equal the one-level
+# sessions', e.g. Helmholtz3D_CG_Hex_AllBCs_iter_ml.tst and _AllBCs.tst)
+SOLVERS.update({k + "MultiLevelStaticCond": "staticcond"
+                for k in ("Iterative", "Direct", "Xxt", "PETSc")})
 PRECONS = {"Diagonal": "diagonal", "Block": "block", "LowEnergyBlock": "lowenergy"}
 
 

@@ -61,12 +61,16 @@ def test_device_solve_reproduces_polynomial_solution(shape):
     assert r.linf < 1e-10 and r.l2 < 1e-11
 
 
-@pytest.mark.parametrize("precon", ["Diagonal", "Block", "LowEnergyBlock"])
-def test_static_condensation_solvers_reproduce_reference_record(precon):
-    """-I GlobalSysSoln=IterativeStaticCond -I Preconditioner=...: the
-    condensed solves give the Hex record's errors as the full solve does."""
+@pytest.mark.parametrize("soln,precon", [("IterativeStaticCond", "Diagonal"),
+                                         ("IterativeStaticCond", "Block"),
+                                         ("IterativeStaticCond", "LowEnergyBlock"),
+                                         ("IterativeMultiLevelStaticCond", "Diagonal")])
+def test_static_condensation_solvers_reproduce_reference_record(soln, precon):
+    """-I GlobalSysSoln=IterativeStaticCond (or IterativeMultiLevelStaticCond,
+    the *_iter_ml.tst setting) -I Preconditioner=...: the condensed solves
+    give the Hex record's errors as the full solve does."""
     s = read_session(write_hex_box_session(2, 6, 1.0, U, F, U, shuffle_seed=4))
-    info = {"GlobalSysSoln": "IterativeStaticCond", "Preconditioner": precon}
+    info = {"GlobalSysSoln": soln, "Preconditioner": precon}
     r = helm_solve(s, tol=1e-14, maxit=2000, raise_on_maxit=False, solver_info=info)
     assert (r.solver, r.precon) == ("staticcond", {"Diagonal": "diagonal", "Block": "block",
                                                    "LowEnergyBlock": "lowenergy"}[precon])

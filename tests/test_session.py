@@ -240,6 +240,11 @@ def test_linear_solver_from_solver_info():
     assert linear_solver({"GlobalSysSoln": "IterativeStaticCond",
                           "Preconditioner": "LowEnergyBlock"}) == ("staticcond", "lowenergy")
     assert linear_solver({"GlobalSysSoln": "DirectStaticCond"}) == ("staticcond", "diagonal")
+    # the reference's *_iter_ml.tst settings: multi-level condensation of the
+    # same system, with the one-level records
+    for k in ("Iterative", "Direct", "Xxt", "PETSc"):
+        assert linear_solver({"GlobalSysSoln": k + "MultiLevelStaticCond"}) == \
+            ("staticcond", "diagonal")
     with pytest.raises(ValueError):
         linear_solver({"GlobalSysSoln": "IterativeFull", "Preconditioner": "Block"})
     with pytest.raises(ValueError):
