@@ -113,6 +113,9 @@ CASES = [(s, nm, nm + 1, dfm) for s in ("hex", "prism", "tet") for nm in (2, 3, 
 # nm 7; two elements each, to keep the fixtures small
 CASES += [(s, nm, nm + 1, dfm) for s, nm in (("hex", 7), ("hex", 9), ("prism", 7), ("tet", 7))
           for dfm in (False, True)]
+# over-integration as the reference's *_OverInt Collections tests set it up
+# (TestHexCollection.cpp:4423-4470: 4 modes, 8 quadrature points per direction)
+CASES += [(s, 4, 8, dfm) for s in ("hex", "prism", "tet") for dfm in (False, True)]
 
 
 def main(force=False):
