@@ -652,3 +652,29 @@ def test_mask_groups_cover_every_element_once_with_its_own_transform():
         Re = element_transforms(p)
         for r, R in groups:
             assert np.array_equal(Re[r], np.broadcast_to(R, (r.size,) + R.shape))
+
+
+_REF_PRISM = ref_path("library/Demos/MultiRegions/Tests/Helmholtz3D_Prism.xml")
+
+
+@pytest.mark.skipif(not os.path.exists(_REF_PRISM), reason="reference tree not mounted")
+def test_reference_prism_lowenergy_session_reproduces_its_record():
+    """Helmholtz3D_CG_Prism_VarP_iterLE.tst (-I GlobalSysSoln=IterativeStaticCond
+    -I Preconditioner=LowEnergyBlock on the Prism session): the prism
+    transform assembled from the cube's and the tetrahedron's entries
+    (ReSetPrismMaxRMat) keeps the basis conforming on the reference's own
+    mesh, so the condensed low-energy solve gives the recorded L2 0.000385246
+    and Linf 0.00539787 (tolerance 1e-9)."""
+    from nektar_b200.meshgraph import SessionMesh
+    from nektar_b200.session import read_session
+    from tests.session_oracle import oracle_errors, oracle_system
+    s = read_session(_REF_PRISM)
+    lam = float(s.parameters["Lambda"])
+    Ks, b_loc, robin = oracle_system(s, SessionMesh(s))
+    assert not robin
+    d = _lowenergy_condensed(s, lam, Ks)
+    assert {p["shape"] for p in d["parts"]} == {"prism"}
+    x, _, _ = _lowenergy_solve(d, b_loc, d["m"].dirichlet_local())
+    linf, l2 = oracle_errors(s, d["m"], x)
+    printed = lambda v: float("%g" % v)  # noqa: E731  (the demo prints six digits)
+    assert abs(printed(l2) - 0.000385246) < 1e-9 and abs(printed(linf) - 0.00539787) < 1e-9
